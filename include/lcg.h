@@ -1,0 +1,254 @@
+/*
+ * lcg.h — C ABI of the B200 light-curve engine.
+ *
+ * This is the drop-in boundary for lcurve_re's model-evaluation hot path.
+ * Every entry point takes plain pointers and sizes; no C++ or torch types
+ * cross it. The reference interface each one replaces is cited beside it
+ * (paths are relative to the lcurve_re source tree).
+ *
+ *   lcg_light_curve        <- Lcurve::light_curve_comp
+ *                             (src/lcurve_base/lcurve.h:669-674,
+ *                              src/lcurve_base/light_curve_comp.cpp:119-599)
+ *   lcg_light_curve_batch  <- many light_curve_comp calls at once (the
+ *                             MCMC / Levenberg-Marquardt callers,
+ *                             new_scripts/mcmc_solver.cpp:1062-1070,
+ *                             new_scripts/levmarq_solver.cpp:789-886)
+ *   lcg_star_grid          <- Lcurve::set_star_grid + set_star_continuum
+ *                             (src/lcurve_base/lcurve.h:528,550)
+ *   lcg_sum_star_multi     <- Lcurve::flat_sum_star1_multi / _star2_multi
+ *                             (src/lcurve_base/lcurve.h:299-307) and the
+ *                             reference CUDA hooks cuda_sum_star{1,2}_multi
+ *                             (src/lcurve_base/comp_light_cuda.h:13-20)
+ *
+ * Errors: every call returns an lcg_status. The reference throws C++
+ * exceptions instead (Lcurve::Lcurve_Error, Roche::Roche_Error); a C++ shim
+ * rethrows Lcurve_Error(lcg_last_error(ctx)) for any status != LCG_OK.
+ * There is no CPU fallback: a missing device or a CUDA failure is an error.
+ *
+ * Threading: a context owns one CUDA stream and its device buffers. A
+ * context is used by one host thread at a time (the reference keeps its
+ * caches thread_local, light_curve_comp.cpp:161).
+ */
+#ifndef LCG_H
+#define LCG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LCG_ABI_VERSION 1
+
+typedef enum lcg_status {
+    LCG_OK = 0,
+    LCG_E_INVALID = 1,      /* bad argument (null pointer, n < 1, q <= 0 ...) */
+    LCG_E_LOBE = 2,         /* a star overfills its Roche lobe (Lcurve_Error) */
+    LCG_E_ROCHE = 3,        /* radius / eclipse solve failed (Roche_Error)    */
+    LCG_E_NOCONVERGE = 4,   /* an iteration cap was reached                   */
+    LCG_E_UNSUPPORTED = 5,  /* disc, bright spot or iscale models             */
+    LCG_E_CUDA = 6,         /* CUDA runtime failure or no device              */
+    LCG_E_NOMEM = 7,        /* device or host allocation failed               */
+    LCG_E_CAPACITY = 8      /* a size exceeds a fixed capacity                */
+} lcg_status;
+
+/* Limb-darkening law, Lcurve::LDC::LDCtype (src/lcurve_base/lcurve.h:204). */
+enum { LCG_LIMB_POLY = 0, LCG_LIMB_CLARET = 1 };
+
+/* Which star, Roche::STAR (src/lroche_base/roche.h:13). */
+enum { LCG_STAR1 = 0, LCG_STAR2 = 1 };
+
+/* Arithmetic of the per-face flux sum.
+ *   LCG_PREC_FP64  : every element in FP64, faces summed in 1024-face blocks
+ *                    in ascending order and the blocks merged in order, the
+ *                    same arithmetic sequence as comp_light_flat.cpp:241-372.
+ *   LCG_PREC_MIXED : element geometry and intensity in FP32, eclipse masks
+ *                    in 32-bit fixed-point phase, FP32 partial sums of at
+ *                    most LCG_MIXED_FOLD faces folded into FP64.
+ * The grid, eclipse and continuum stages are FP64 in both modes. */
+enum { LCG_PREC_FP64 = 0, LCG_PREC_MIXED = 1 };
+#define LCG_MIXED_FOLD 64
+
+/* Flags of lcg_light_curve, the bool arguments of light_curve_comp. */
+enum {
+    LCG_FLAG_SCALE = 1,        /* scale: fit the single scale factor (re_scale) */
+    LCG_FLAG_RDATA = 2,        /* rdata: real data, compute chi**2             */
+    LCG_FLAG_INFO = 4,         /* info: print face counts to stderr            */
+    LCG_FLAG_DIAGNOSTICS = 8,  /* diagnostics: wdwarf, logg1/2, rv1/2          */
+    LCG_FLAG_NO_CACHE = 16     /* rebuild grids even if the geometry is equal
+                                  (LCURVE_NO_GRID_CACHE, light_curve_comp.cpp:162) */
+};
+
+/* Indices into the scalars[] output of lcg_light_curve: the scalar
+ * out-parameters of light_curve_comp, in signature order. */
+enum {
+    LCG_OUT_WDWARF = 0, LCG_OUT_CHISQ = 1, LCG_OUT_WNOK = 2,
+    LCG_OUT_LOGG1 = 3, LCG_OUT_LOGG2 = 4, LCG_OUT_RV1 = 5, LCG_OUT_RV2 = 6,
+    LCG_NOUT = 7
+};
+
+/* Every Model field that the hot path reads (src/lcurve_base/lcurve.h:340-396),
+ * as plain values. Pparam values are given by value; "defined" flags only
+ * matter for the optional star spots (set_star_continuum.cpp:58-65). */
+typedef struct lcg_model {
+    double q, iangle, r1, r2, cphi3, cphi4, spin1, spin2;
+    double t1, t2;
+    double ldc1[4], ldc2[4];
+    double velocity_scale, beam_factor1, beam_factor2;
+    double t0, period, pdot, deltat;
+    double gravity_dark1, gravity_dark2;
+    double absorb, slope, quad, cube, third;
+    /* star spots 11,12,13,21,22: {long, lat, fwhm, tcen}; a spot is on when
+       all four of its Pparams are defined */
+    double stsp[5][4];
+    int32_t stsp_defined[5];
+    /* uniform equatorial spot: long1, long2, lathw, taper, temp */
+    double uesp[5];
+    int32_t uesp_defined;
+    /* computational parameters */
+    double delta_phase;
+    int32_t nlat1f, nlat2f, nlat1c, nlat2c;
+    int32_t npole, nlatfill, nlngfill;
+    double lfudge, llo, lhi, phase1, phase2, wavelength;
+    int32_t roche1, roche2, eclipse1, eclipse2, glens1, use_radii;
+    double tperiod;
+    int32_t gdark_bolom1, gdark_bolom2;
+    double mucrit1, mucrit2;
+    int32_t limb1, limb2;
+    int32_t mirror, add_disc, opaque, add_spot, iscale;
+    int32_t pad_;
+} lcg_model;
+
+/* One light-curve point, byte-compatible with Lcurve::Datum
+ * (src/lcurve_base/lcurve.h:427-445): a Data vector's storage can be passed
+ * as-is. */
+typedef struct lcg_datum {
+    double time, expose, flux, ferr, weight;
+    int32_t ndiv;
+    int32_t pad_;
+} lcg_datum;
+
+typedef struct lcg_options {
+    int32_t device;        /* CUDA device ordinal                          */
+    int32_t precision;     /* LCG_PREC_FP64 or LCG_PREC_MIXED              */
+    int32_t verbose;       /* print per-stage timings at destroy when > 0  */
+    int32_t reserved[5];
+} lcg_options;
+
+typedef struct lcg_ctx lcg_ctx;
+
+/* ---- context ----------------------------------------------------------- */
+
+/* Fills *opt with defaults: device 0, mixed precision. */
+void lcg_default_options(lcg_options *opt);
+
+/* Creates a context on opt->device. Fails with LCG_E_CUDA when there is no
+ * usable sm_100 device. */
+lcg_status lcg_create(lcg_ctx **ctx, const lcg_options *opt);
+
+void lcg_destroy(lcg_ctx *ctx);
+
+/* Message of the last failing call on ctx ("" if none). Valid until the next
+ * call on ctx. A NULL ctx returns the message of the last failed create. */
+const char *lcg_last_error(const lcg_ctx *ctx);
+
+int32_t lcg_abi_version(void);
+
+/* The context's cudaStream_t, so callers can order their own work and
+ * events against the engine. */
+void *lcg_stream(lcg_ctx *ctx);
+
+/* ---- the hot path ------------------------------------------------------ */
+
+/* One light curve for one model: Lcurve::light_curve_comp.
+ *   data[n]      the points (time, expose, flux, ferr, weight, ndiv)
+ *   flags        LCG_FLAG_*
+ *   sfac[5]      in: sfac[0] is the scale when LCG_FLAG_SCALE is clear;
+ *                out: all five set to the fitted scale when it is set
+ *   calc[n]      out: the model light curve
+ *   scalars[7]   out: wdwarf, chisq, wnok, logg1, logg2, rv1, rv2
+ * Grids are rebuilt only when a geometry parameter changed since the last
+ * call on this context, and the continuum only when a brightness parameter
+ * changed (the exact-reuse cache of light_curve_comp.cpp:34-117). */
+lcg_status lcg_light_curve(lcg_ctx *ctx, const lcg_model *model,
+                           const lcg_datum *data, int32_t n, int32_t flags,
+                           double *sfac, double *calc, double *scalars);
+
+/* nmodels light curves over the same data points, one per model.
+ *   calc[nmodels*n], chisq[nmodels], wnok[nmodels], sfac[nmodels*5] out;
+ *   status[nmodels] out: the per-model status (a failed model does not fail
+ *   the batch; its calc row is zero). sfac is read when SCALE is clear.
+ * Returns LCG_OK unless the batch as a whole could not run. */
+lcg_status lcg_light_curve_batch(lcg_ctx *ctx, const lcg_model *models,
+                                 int32_t nmodels, const lcg_datum *data,
+                                 int32_t n, int32_t flags, double *sfac,
+                                 double *calc, double *chisq, double *wnok,
+                                 int32_t *status);
+
+/* ---- stage-level seams, for parity tests and integrations -------------- */
+
+/* Number of faces of one star grid (Lcurve::numface, numface.cpp:14-52, and
+ * the infill band of set_star_grid.cpp:113-159). */
+lcg_status lcg_star_face_count(lcg_ctx *ctx, const lcg_model *model,
+                               int32_t star, int32_t fine, int32_t *nface);
+
+/* Builds one star grid with its continuum, in the reference's face order
+ * (set_star_grid.cpp:49-523 then set_star_continuum.cpp:26-297). Outputs are
+ * host arrays of length nface (posn, dirn: 3*nface, x,y,z interleaved).
+ * ecl_in/ecl_out hold the ingress/egress phase of faces with neclipse = 1. */
+lcg_status lcg_star_grid(lcg_ctx *ctx, const lcg_model *model, int32_t star,
+                         int32_t fine, int32_t nface, double *posn,
+                         double *dirn, float *area, float *gravity,
+                         float *flux, int32_t *neclipse, double *ecl_in,
+                         double *ecl_out);
+
+/* The blocked multi-phase flux sweep over one flattened grid: out[k] is the
+ * unweighted flux sum for phase entry k (flat_sum_star{1,2}_multi).
+ *   grid: n faces in FlatGrid order, [0,n0) never eclipsed, [n0,n) one
+ *         eclipse range (in1/out1 indexed i-n0). Faces with two or more
+ *         ranges do not occur for stars without a disc.
+ *   ldc[4], ltype, mucrit: limb darkening; beam, spin, vfac, xcofm: Doppler
+ *   beaming (comp_light_flat.cpp:109-168); glens1/rlens1: lensing (star 2).
+ * Host arrays in and out. */
+lcg_status lcg_sum_star_multi(lcg_ctx *ctx, int32_t star, int64_t n,
+                              int64_t n0, const double *dx, const double *dy,
+                              const double *dz, const double *px,
+                              const double *py, const double *pz,
+                              const double *flux, const double *in1,
+                              const double *out1, int32_t nent,
+                              const double *ex, const double *ey,
+                              const double *ez, const double *phin,
+                              const double *ldc, int32_t ltype, double mucrit,
+                              double beam, double spin, double vfac,
+                              double xcofm, int32_t glens1, double rlens1,
+                              double *out);
+
+/* ---- measurement ------------------------------------------------------- */
+
+/* Stage timings recorded with CUDA events on the context's stream when
+ * profiling is on: device milliseconds summed since the last reset, and the
+ * number of launches, per stage. */
+enum {
+    LCG_STAGE_GRID = 0, LCG_STAGE_ECLIPSE = 1, LCG_STAGE_CONTINUUM = 2,
+    LCG_STAGE_FLATTEN = 3, LCG_STAGE_PHASES = 4, LCG_STAGE_FLUX = 5,
+    LCG_STAGE_REDUCE = 6, LCG_NSTAGE = 7
+};
+void lcg_set_profiling(lcg_ctx *ctx, int32_t on);
+void lcg_stage_times(lcg_ctx *ctx, double *ms, int64_t *launches,
+                     int32_t reset);
+
+/* Elements (face x sub-phase pairs) summed by the flux stage since the last
+ * reset: the algorithmic unit of the flux roofline. */
+int64_t lcg_flux_elements(lcg_ctx *ctx, int32_t reset);
+
+/* Measures the device's FP32 FMA throughput in TFLOP/s (2 FLOP per FMA)
+ * with a register-resident FFMA chain kernel; the denominator of the flux
+ * roofline. */
+lcg_status lcg_measure_fp32_peak(lcg_ctx *ctx, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LCG_H */

@@ -1,0 +1,146 @@
+// engine.h — kernel parameter blocks and launchers shared by the host engine
+// (engine.cpp) and the kernel files (geometry.cu, flux.cu, flux64.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "roche.cuh"
+
+namespace lcg {
+
+// One latitude ring of a star grid (set_star_grid.cpp:280-320), computed on
+// the host with the reference's libm so ring sizes match exactly.
+struct RingRec {
+    double sint, cost, phi1, span, latspan;  // span = phi2 - phi1, latspan = thi - tlo
+    int32_t nphi, nl, off, hoff;             // hoff: first half-face of the ring
+};
+
+// Point-order star grid on the device (the reference's vector<Point>).
+struct GridDev {
+    double *px, *py, *pz, *nx, *ny, *nz;
+    float *area, *grav, *flux;
+    uint8_t *necl;
+    double *ein, *eout;
+    int64_t n;
+};
+
+struct GridParams {
+    int32_t star, roche, npole, nrings;
+    int64_t nhalf;  // total half-faces (sum over rings of (nphi+1)/2)
+    double q, spin, rref, pref, acc, gref, rad_sphere;
+};
+
+// Eclipse of one star's faces by its companion (set_star_grid.cpp:372-386).
+struct EclParams {
+    int32_t comp_star;   // the eclipsing star
+    int32_t comp_roche;  // Roche-distorted eclipser (else a sphere of radius comp_r)
+    double q, comp_spin, comp_rref, comp_pref, comp_r, cosi, sini, delta;
+};
+
+// Continuum of one star (set_star_continuum.cpp:26-297).
+struct ContParams {
+    int32_t star, mirror, nspot, uesp_on;
+    double t_own, t_other;    // t1/t2 of this star and of the other (model values)
+    double absorb, gdcbol, wavelength, rcomp, efac;
+    double spot_dir[3][3], spot_fwhm[3], spot_tcen[3];
+    double uesp_dir[3], uesp_longhw, uesp_lathw, uesp_taper, uesp_temp;
+};
+
+// One light-curve point, the byte layout of lcg_datum / Lcurve::Datum.
+struct DatumRec {
+    double time, expose, flux, ferr, weight;
+    int32_t ndiv, pad_;
+};
+
+// Device status word: the first failure wins.
+struct DevStatus {
+    int32_t code;
+    int32_t face;
+};
+
+// Flattened grid for the flux sweep (FlatGrid, comp_light_flat.cpp:26-65).
+// Faces [0,n0) are never eclipsed, [n0,n) have one eclipse range. The
+// mixed-precision view packs (nx,ny,nz,flux) as float4 and the eclipse range
+// as 32-bit fixed-point phase (start, width+1); the FP64 view keeps the
+// reference's doubles. Arrays are padded with zero faces to npad.
+struct FlatDev {
+    int64_t n, npad;
+    int64_t *n0;  // device scalar, written by the partition
+    float4 *geo;  // mixed
+    uint2 *ecl;
+    float4 *pos;  // (px,py,pz,0): beaming and lensing only
+    double *dx, *dy, *dz, *px, *py, *pz, *flux, *in1, *out1;  // FP64
+};
+
+// Sub-exposure phase entries of all data points (light_curve_comp.cpp:416-455).
+struct PhaseDev {
+    double *ex, *ey, *ez, *phin, *w1, *w2;
+    float4 *ef;     // (ex, ey, ez, phin as 32-bit fixed point bits)
+    uint8_t *type;  // Ginterp::type
+    int64_t nent;
+};
+
+struct PhaseParams {
+    double t0, period, pdot, deltat, slope, quad, cube, middle, range, cosi, sini;
+    Ginterp gi;
+};
+
+// Limb darkening and beaming/lensing constants of one flux sweep.
+struct FluxConsts {
+    double c[4], base, mucrit;
+    int32_t ltype, beam_on, glens;
+    double beam, spin, vfac, xcofm, rlens1;
+};
+
+struct ScatterParams {
+    int32_t copy1, copy2;
+    int64_t nchunk1f, nchunk1c, nchunk2f, nchunk2c;  // partial rows per sweep
+    int64_t ldp;                                     // row stride of partials
+    double third;
+};
+
+// ---- launchers (geometry.cu) ------------------------------------------------
+void launch_grid(const GridParams &p, const RingRec *rings, GridDev g, DevStatus *st,
+                 cudaStream_t s);
+void launch_eclipse(const EclParams &p, int32_t eclipse_on, GridDev g, int32_t *queue,
+                    int32_t *counters, DevStatus *st, int nsm, cudaStream_t s);
+void launch_continuum(const ContParams &p, GridDev g, cudaStream_t s);
+void launch_flatten(GridDev g, FlatDev f, int32_t *blockcnt, int mixed, int need_pos,
+                    DevStatus *st, cudaStream_t s);
+void launch_phases(const PhaseParams &p, const DatumRec *data, const int64_t *off, int32_t n,
+                   PhaseDev ph, cudaStream_t s);
+void launch_scatter(const ScatterParams &p, const double *part1f, const double *part1c,
+                    const double *part2f, const double *part2c, const PhaseDev &ph,
+                    const DatumRec *data, const int64_t *off, int32_t n, double *calc,
+                    cudaStream_t s);
+// finalize: scale / chi**2 (re_scale.cpp:16-42, light_curve_comp.cpp:557-585).
+// out[0] = chisq, out[1] = wnok, out[2] = 1 when they were computed.
+void launch_finalize(int32_t flags, const DatumRec *data, int32_t n, double *calc,
+                     double *scratch, double *sfac_io, double *out, cudaStream_t s);
+// flux-weighted gravity / volume-averaged radius sums (comp_gravity.cpp,
+// comp_radius.cpp): out[0..3] = sum f*g, sum f, sum solid angle, sum volume
+void launch_diagnostics(int star, GridDev g, double *out, cudaStream_t s);
+
+void launch_pack_flat(FlatDev f, int64_t n0, int need_pos, cudaStream_t s);
+void launch_pack_phases(PhaseDev ph, cudaStream_t s);
+
+// ---- launchers (flux.cu, flux64.cu) -----------------------------------------
+struct FluxPlan {
+    int ppt;        // phase entries per thread
+    int threads;    // threads per CTA
+    int64_t chunk;  // faces per CTA
+    int64_t nchunk;
+    int64_t ntile;  // phase tiles
+};
+FluxPlan plan_flux(int mixed, int64_t nface, int64_t nent, int nsm);
+void launch_flux(int mixed, int star, const FluxConsts &k, const FlatDev &f,
+                 const PhaseDev &ph, const FluxPlan &plan, double *part, int64_t ldp,
+                 DevStatus *st, cudaStream_t s);
+// FP32 FMA throughput probe: fills *gflop with the FLOPs it executed.
+void launch_fma_probe(float *sink, int blocks, int iters, double *gflop, cudaStream_t s);
+void launch_flux64(int star, const FluxConsts &k, const FlatDev &f, const PhaseDev &ph,
+                   const FluxPlan &plan, double *part, int64_t ldp, DevStatus *st,
+                   cudaStream_t s);
+
+}  // namespace lcg

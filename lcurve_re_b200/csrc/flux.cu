@@ -1,0 +1,294 @@
+// flux.cu — mixed-precision multi-phase flux sweep (the hot loop).
+//
+// Computes, for every sub-exposure phase entry k and every face i of one
+// flattened star grid, the element flux of comp_light_flat.cpp:80-168
+//   mu = e_k . n_i;  I(mu) Claret or polynomial;  v = mu * flux_i * I(mu)
+// masked by mu > max(mucrit, 0) and by the face's eclipse range, and sums it
+// over faces (sum_star{1,2}_multi_t, comp_light_flat.cpp:241-372).
+//
+// Layout and schedule:
+//  * grid (phase tiles, face chunks). A CTA stages its face chunk
+//    (float4 n/flux records, uint2 fixed-point eclipse ranges) into shared
+//    memory with one bulk TMA copy per array, completed on an mbarrier.
+//  * each thread keeps PPT phase entries in registers and walks the staged
+//    faces; all lanes read the same face record (shared-memory broadcast).
+//  * element math in FP32; sums over at most 64 faces in FP32, folded into
+//    FP64 accumulators; one FP64 partial per (chunk, entry) is written and
+//    merged in chunk order by k_scatter (deterministic, no atomics).
+//  * eclipse test in 32-bit fixed-point phase: (phase - ingress) mod 2^32 <
+//    width + 1, exact except within 2^-32 of a boundary.
+#include "engine.h"
+#include "tma.cuh"
+
+namespace lcg {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kFold = 64;  // LCG_MIXED_FOLD
+
+__device__ __forceinline__ float sqrt_approx(float x) {
+    float r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+template <int LT>
+__device__ __forceinline__ float intensity(float mu, float c1, float c2, float c3, float c4,
+                                           float base) {
+    if constexpr (LT == 1) {
+        const float s = sqrt_approx(mu);  // NaN for mu < 0: masked by the caller
+        return fmaf(s, fmaf(s, fmaf(s, fmaf(s, c4, c3), c2), c1), base);
+    } else {
+        const float om = 1.f - mu;
+        return fmaf(-om, fmaf(om, fmaf(om, fmaf(om, c4, c3), c2), c1), 1.f);
+    }
+}
+
+// lensing magnification of star 2 by star 1 (comp_light_flat.cpp:138-149),
+// in FP64: the difference pd - ph cancels near the lens.
+__device__ __forceinline__ float magnification(float4 s, float ex, float ey, float ez,
+                                               double rlens1) {
+    const double d = -((double)s.x * ex + (double)s.y * ey + (double)s.z * ez);
+    if (!(d > 0.0)) return 1.f;
+    const double qx = s.x + d * ex, qy = s.y + d * ey, qz = s.z + d * ez;
+    const double p = sqrt(qx * qx + qy * qy + qz * qz);
+    const double ph = 0.5 * p, rd = rlens1 * d;
+    const double pd = (ph * ph > 25.0 * rd) ? p + rd / p : ph + sqrt(ph * ph + rd);
+    return (float)(pd * pd / (pd - ph) / ph / 4.0);
+}
+
+struct FaceConsts {
+    float c1, c2, c3, c4, base, cut, mucrit, vfac, spin, xcofm, beam;
+    double rlens1;
+};
+
+// Sums faces [lo, hi) of the staged chunk (first face c0) into acc, in FP32
+// runs of kFold faces folded into FP64.
+template <int PPT, int LT, bool BEAM, bool GLENS, int STAR, bool ECL>
+__device__ __forceinline__ void sweep(const float4 *sgeo, const uint2 *secl, const float4 *spos,
+                                      int64_t c0, int64_t lo, int64_t hi, const float *ex,
+                                      const float *ey, const float *ez, const uint32_t *pf,
+                                      const FaceConsts &k, double *acc) {
+    constexpr bool need_pos = BEAM || GLENS;
+    for (int64_t b = lo; b < hi; b += kFold) {
+        const int cnt = (int)((b + kFold < hi) ? kFold : hi - b);
+        const float4 *gp = sgeo + (b - c0);
+        const uint2 *ep = secl + (b - c0);
+        const float4 *pp4 = spos + (b - c0);
+        float s[PPT];
+#pragma unroll
+        for (int j = 0; j < PPT; j++) s[j] = 0.f;
+#pragma unroll 4
+        for (int i = 0; i < cnt; i++) {
+            const float4 g = gp[i];
+            uint2 ec = make_uint2(0u, 0u);
+            if constexpr (ECL) ec = ep[i];
+            float4 pp = make_float4(0.f, 0.f, 0.f, 0.f);
+            float vx = 0.f, vy = 0.f, vn = 0.f;
+            if constexpr (need_pos) pp = pp4[i];
+            if constexpr (BEAM) {
+                vx = -k.vfac * k.spin * pp.y;
+                vy = STAR == 0 ? k.vfac * (k.spin * pp.x - k.xcofm)
+                               : k.vfac * (k.spin * (pp.x - 1.f) + 1.f - k.xcofm);
+                vn = g.x * vx + g.y * vy;
+            }
+#pragma unroll
+            for (int j = 0; j < PPT; j++) {
+                const float mu = fmaf(ez[j], g.z, fmaf(ey[j], g.y, ex[j] * g.x));
+                // without beaming I(mu) = 0 for mu <= 0, so mu > max(mucrit, 0);
+                // with beaming the intensity is taken at mu' and only mu > mucrit
+                bool vis = BEAM ? mu > k.mucrit : mu > k.cut;
+                if constexpr (ECL) vis = vis && ((pf[j] - ec.x) >= ec.y);
+                float v;
+                if constexpr (BEAM) {
+                    const float vr = -(ex[j] * vx + ey[j] * vy);
+                    const float mud = mu - mu * vr - vn;
+                    vis = vis && (mud > 0.f);
+                    v = mu * (1.f - k.beam * vr) * intensity<LT>(mud, k.c1, k.c2, k.c3, k.c4, k.base);
+                } else {
+                    v = mu * intensity<LT>(mu, k.c1, k.c2, k.c3, k.c4, k.base);
+                }
+                if constexpr (GLENS) v *= magnification(pp, ex[j], ey[j], ez[j], k.rlens1);
+                s[j] = vis ? fmaf(v, g.w, s[j]) : s[j];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < PPT; j++) acc[j] += (double)s[j];
+    }
+}
+
+template <int PPT, int LT, bool BEAM, bool GLENS, int STAR>
+__global__ void __launch_bounds__(kThreads)
+    k_flux_mixed(FluxConsts k, FlatDev f, PhaseDev ph, int64_t chunk, double *part,
+                 int64_t ldp, DevStatus *st) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ uint64_t bar;
+    const int tid = threadIdx.x;
+    const int64_t c0 = (int64_t)blockIdx.y * chunk;
+    const int64_t n = f.n, n0 = *f.n0;
+    const int64_t cend = (c0 + chunk < n) ? c0 + chunk : n;
+    const bool need_ecl = cend > n0;
+    constexpr bool need_pos = BEAM || GLENS;
+    float4 *sgeo = reinterpret_cast<float4 *>(smem);
+    uint2 *secl = reinterpret_cast<uint2 *>(smem + chunk * 16);
+    float4 *spos = reinterpret_cast<float4 *>(smem + chunk * 24);
+
+    if (tid == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    if (tid == 0) {
+        uint32_t bytes = (uint32_t)(chunk * 16) + (need_ecl ? (uint32_t)(chunk * 8) : 0u) +
+                         (need_pos ? (uint32_t)(chunk * 16) : 0u);
+        mbar_arrive_expect_tx(&bar, bytes);
+        bulk_g2s(sgeo, f.geo + c0, (uint32_t)(chunk * 16), &bar);
+        if (need_ecl) bulk_g2s(secl, f.ecl + c0, (uint32_t)(chunk * 8), &bar);
+        if (need_pos) bulk_g2s(spos, f.pos + c0, (uint32_t)(chunk * 16), &bar);
+    }
+
+    // phase entries of this thread, loaded while the faces stream in
+    float ex[PPT], ey[PPT], ez[PPT];
+    uint32_t pf[PPT];
+    const int64_t ebase = (int64_t)blockIdx.x * kThreads * PPT + tid;
+#pragma unroll
+    for (int j = 0; j < PPT; j++) {
+        const int64_t e = ebase + (int64_t)j * kThreads;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (e < ph.nent) v = ph.ef[e];
+        ex[j] = v.x;
+        ey[j] = v.y;
+        ez[j] = v.z;
+        pf[j] = __float_as_uint(v.w);
+    }
+    const float c1 = (float)k.c[0], c2 = (float)k.c[1], c3 = (float)k.c[2], c4 = (float)k.c[3];
+    const float base = (float)k.base;
+    const float cut = (float)(k.mucrit > 0. ? k.mucrit : 0.);
+    const float vfac = (float)k.vfac, spin = (float)k.spin, xcofm = (float)k.xcofm;
+    const float beam = (float)k.beam;
+
+    if (!mbar_wait_bounded(&bar, 0)) {
+        if (tid == 0) {
+            if (atomicCAS(&st->code, 0, 6) == 0) st->face = (int32_t)c0;
+        }
+        mbar_wait_bounded(&bar, 0);  // let the copy land before the CTA exits
+        return;
+    }
+
+    double acc[PPT];
+#pragma unroll
+    for (int j = 0; j < PPT; j++) acc[j] = 0.0;
+    const FaceConsts fc{c1, c2, c3, c4, base, cut, (float)k.mucrit, vfac, spin, xcofm, beam,
+                        k.rlens1};
+    // plain faces [c0, min(n0,cend)), then one-range faces [max(n0,c0), cend)
+    sweep<PPT, LT, BEAM, GLENS, STAR, false>(sgeo, secl, spos, c0, c0, n0 < cend ? n0 : cend,
+                                            ex, ey, ez, pf, fc, acc);
+    sweep<PPT, LT, BEAM, GLENS, STAR, true>(sgeo, secl, spos, c0, n0 > c0 ? n0 : c0, cend, ex,
+                                           ey, ez, pf, fc, acc);
+#pragma unroll
+    for (int j = 0; j < PPT; j++) {
+        const int64_t e = ebase + (int64_t)j * kThreads;
+        if (e < ph.nent) part[(int64_t)blockIdx.y * ldp + e] = acc[j];
+    }
+}
+
+template <int PPT, int LT, bool BEAM, bool GLENS, int STAR>
+void launch_t(const FluxConsts &k, const FlatDev &f, const PhaseDev &ph, const FluxPlan &plan,
+              double *part, int64_t ldp, DevStatus *st, cudaStream_t s) {
+    const size_t smem = (size_t)plan.chunk * ((BEAM || GLENS) ? 40 : 24);
+    auto kern = k_flux_mixed<PPT, LT, BEAM, GLENS, STAR>;
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 40 * 4096);
+        attr_set = true;
+    }
+    dim3 grid((unsigned)plan.ntile, (unsigned)plan.nchunk);
+    kern<<<grid, kThreads, smem, s>>>(k, f, ph, plan.chunk, part, ldp, st);
+}
+
+template <int PPT, int LT>
+void launch_ppt_lt(int star, const FluxConsts &k, const FlatDev &f, const PhaseDev &ph,
+                   const FluxPlan &plan, double *part, int64_t ldp, DevStatus *st,
+                   cudaStream_t s) {
+    const bool beam = k.beam_on != 0, glens = (star == 1) && k.glens;
+    if (star == 0) {
+        if (beam) launch_t<PPT, LT, true, false, 0>(k, f, ph, plan, part, ldp, st, s);
+        else launch_t<PPT, LT, false, false, 0>(k, f, ph, plan, part, ldp, st, s);
+    } else if (glens) {
+        if (beam) launch_t<PPT, LT, true, true, 1>(k, f, ph, plan, part, ldp, st, s);
+        else launch_t<PPT, LT, false, true, 1>(k, f, ph, plan, part, ldp, st, s);
+    } else {
+        if (beam) launch_t<PPT, LT, true, false, 1>(k, f, ph, plan, part, ldp, st, s);
+        else launch_t<PPT, LT, false, false, 1>(k, f, ph, plan, part, ldp, st, s);
+    }
+}
+
+template <int PPT>
+void launch_ppt(int star, const FluxConsts &k, const FlatDev &f, const PhaseDev &ph,
+                const FluxPlan &plan, double *part, int64_t ldp, DevStatus *st,
+                cudaStream_t s) {
+    if (k.ltype == 1) launch_ppt_lt<PPT, 1>(star, k, f, ph, plan, part, ldp, st, s);
+    else launch_ppt_lt<PPT, 0>(star, k, f, ph, plan, part, ldp, st, s);
+}
+
+// 8 independent FFMA chains per thread keep the FP32 pipes full.
+__global__ void __launch_bounds__(256) k_fma_probe(float *sink, int iters) {
+    float a0 = threadIdx.x * 1e-3f, a1 = a0 + 1.f, a2 = a0 + 2.f, a3 = a0 + 3.f;
+    float a4 = a0 + 4.f, a5 = a0 + 5.f, a6 = a0 + 6.f, a7 = a0 + 7.f;
+    const float m = 0.999999f, c = 1e-6f;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+            a0 = fmaf(a0, m, c); a1 = fmaf(a1, m, c); a2 = fmaf(a2, m, c); a3 = fmaf(a3, m, c);
+            a4 = fmaf(a4, m, c); a5 = fmaf(a5, m, c); a6 = fmaf(a6, m, c); a7 = fmaf(a7, m, c);
+        }
+    }
+    const float r = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+    if (r == 12345.f) sink[0] = r;  // keeps the chains live
+}
+
+}  // namespace
+
+void launch_fma_probe(float *sink, int blocks, int iters, double *gflop, cudaStream_t s) {
+    k_fma_probe<<<blocks, 256, 0, s>>>(sink, iters);
+    *gflop = 2.0 * 8 * 16 * (double)iters * 256.0 * blocks * 1e-9;
+}
+
+FluxPlan plan_flux(int mixed, int64_t nface, int64_t nent, int nsm) {
+    FluxPlan p;
+    if (mixed) {
+        p.threads = kThreads;
+        p.ppt = nent >= 16384 ? 8 : (nent >= 2048 ? 4 : 1);
+        p.ntile = (nent + (int64_t)kThreads * p.ppt - 1) / ((int64_t)kThreads * p.ppt);
+        if (p.ntile < 1) p.ntile = 1;
+        // enough CTAs to fill the SMs a few times over; chunk a power of two
+        // in [64, 4096] so that chunks tile the 4096-padded face arrays
+        const int64_t want = ((int64_t)nsm * 4 + p.ntile - 1) / p.ntile;
+        int64_t chunk = 4096;
+        while (chunk > 64 && (nface + chunk - 1) / chunk < want) chunk >>= 1;
+        p.chunk = chunk;
+    } else {
+        p.threads = 128;
+        p.ppt = nent >= 8192 ? 4 : (nent >= 1024 ? 2 : 1);
+        p.ntile = (nent + (int64_t)p.threads * p.ppt - 1) / ((int64_t)p.threads * p.ppt);
+        if (p.ntile < 1) p.ntile = 1;
+        p.chunk = 1024;  // FACE_BLOCK of comp_light_flat.cpp:239
+    }
+    p.nchunk = nface > 0 ? (nface + p.chunk - 1) / p.chunk : 0;
+    return p;
+}
+
+void launch_flux(int mixed, int star, const FluxConsts &k, const FlatDev &f,
+                 const PhaseDev &ph, const FluxPlan &plan, double *part, int64_t ldp,
+                 DevStatus *st, cudaStream_t s) {
+    if (plan.nchunk == 0 || ph.nent == 0) return;
+    if (!mixed) {
+        launch_flux64(star, k, f, ph, plan, part, ldp, st, s);
+        return;
+    }
+    switch (plan.ppt) {
+    case 8: launch_ppt<8>(star, k, f, ph, plan, part, ldp, st, s); break;
+    case 4: launch_ppt<4>(star, k, f, ph, plan, part, ldp, st, s); break;
+    default: launch_ppt<1>(star, k, f, ph, plan, part, ldp, st, s); break;
+    }
+}
+
+}  // namespace lcg

@@ -1,0 +1,212 @@
+// flux64.cu — FP64 multi-phase flux sweep with the reference's arithmetic.
+//
+// Same sums as sum_star{1,2}_multi_t (comp_light_flat.cpp:241-372): faces in
+// blocks of 1024 (FACE_BLOCK, :239) in FlatGrid order; per block and phase
+// entry, element values of s1_elem / s2_elem (:109-168) are added in
+// ascending face order; k_scatter then adds the block partials in block
+// order. Compiled with --fmad=false, every operation rounds as in the
+// reference, so given the same FlatGrid and phases the result is
+// bit-identical (sqrt and division are IEEE on both sides).
+//
+// A CTA owns one 1024-face block and a tile of phase entries; the block's
+// SoA columns are staged into shared memory by bulk TMA copies.
+#include "engine.h"
+#include "tma.cuh"
+
+namespace lcg {
+
+namespace {
+
+constexpr int kThreads64 = 128;
+constexpr int kBlock = 1024;
+
+struct Consts64 {
+    double c1, c2, c3, c4, base, mucrit, beam, spin, vfac, xcofm, rlens1;
+};
+
+// imu_bl (comp_light_flat.cpp:80-95)
+template <int LT>
+__device__ __forceinline__ double imu_bl(double mu, const Consts64 &L) {
+    const double m = (1.0 < mu) ? 1.0 : mu;
+    double im;
+    if constexpr (LT == 0) {
+        const double om = 1.0 - m;
+        im = 1.0 - om * (L.c1 + om * (L.c2 + om * (L.c3 + om * L.c4)));
+    } else {
+        const double msq = sqrt((m < 0.0) ? 0.0 : m);
+        im = L.base + msq * (L.c1 + msq * (L.c2 + msq * (L.c3 + msq * L.c4)));
+    }
+    return (double)(mu > 0.0) * im;
+}
+
+// s1_elem / s2_elem (comp_light_flat.cpp:109-168)
+template <int LT, bool BEAM, bool GLENS, int STAR>
+__device__ __forceinline__ double elem(double ex, double ey, double ez, double dx, double dy,
+                                       double dz, double px, double py, double pz, double flux,
+                                       const Consts64 &L) {
+    const double mu = ex * dx + ey * dy + ez * dz;
+    double magn = 1.0;
+    if constexpr (GLENS) {
+        const double d = -(px * ex + py * ey + pz * ez);
+        const double qx = px + d * ex, qy = py + d * ey, qz = pz + d * ez;
+        const double p = sqrt(qx * qx + qy * qy + qz * qz);
+        const double ph = 0.5 * p;
+        const double rd = L.rlens1 * d;
+        const double pd = (ph * ph > 25.0 * rd) ? p + rd / p : ph + sqrt(ph * ph + rd);
+        const double mg = pd * pd / (pd - ph) / ph / 4.0;
+        magn = d > 0.0 ? mg : 1.0;
+    }
+    double val;
+    if constexpr (!BEAM) {
+        if constexpr (STAR == 0) val = mu * flux * imu_bl<LT>(mu, L);
+        else val = mu * magn * flux * imu_bl<LT>(mu, L);
+    } else {
+        const double vx = -L.vfac * L.spin * py;
+        const double vy = STAR == 0 ? L.vfac * (L.spin * px - L.xcofm)
+                                    : L.vfac * (L.spin * (px - 1.0) + 1.0 - L.xcofm);
+        const double vr = -(ex * vx + ey * vy);
+        const double vn = dx * vx + dy * vy;
+        const double mud = mu - mu * vr - vn;
+        if constexpr (STAR == 0) val = mu * flux * (1.0 - L.beam * vr) * imu_bl<LT>(mud, L);
+        else val = mu * magn * flux * (1.0 - L.beam * vr) * imu_bl<LT>(mud, L);
+    }
+    if constexpr (GLENS) return mu > L.mucrit ? val : 0.0;
+    return (double)(mu > L.mucrit) * val;
+}
+
+template <int PPT, int LT, bool BEAM, bool GLENS, int STAR>
+__global__ void __launch_bounds__(kThreads64)
+    k_flux64(FluxConsts k, FlatDev f, PhaseDev ph, double *part, int64_t ldp, DevStatus *st) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ uint64_t bar;
+    constexpr bool need_pos = BEAM || GLENS;
+    const int tid = threadIdx.x;
+    const int64_t lo = (int64_t)blockIdx.y * kBlock;
+    const int64_t n = f.n, n0 = *f.n0;
+    const int64_t hi = (lo + kBlock < n) ? lo + kBlock : n;
+    const int64_t a1 = hi < n0 ? hi : n0;  // plain segment [lo, a1)
+    const int64_t b0 = lo > n0 ? lo : n0;  // one-range segment [b0, hi)
+    const bool need_ecl = hi > n0;
+    double *s_dx = reinterpret_cast<double *>(smem);
+    double *s_dy = s_dx + kBlock, *s_dz = s_dy + kBlock, *s_fl = s_dz + kBlock;
+    double *s_in = s_fl + kBlock, *s_out = s_in + kBlock;
+    double *s_px = s_out + kBlock, *s_py = s_px + kBlock, *s_pz = s_py + kBlock;
+    constexpr uint32_t col = kBlock * 8;
+
+    if (tid == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    if (tid == 0) {
+        uint32_t bytes = 4 * col + (need_ecl ? 2 * col : 0u) + (need_pos ? 3 * col : 0u);
+        mbar_arrive_expect_tx(&bar, bytes);
+        bulk_g2s(s_dx, f.dx + lo, col, &bar);
+        bulk_g2s(s_dy, f.dy + lo, col, &bar);
+        bulk_g2s(s_dz, f.dz + lo, col, &bar);
+        bulk_g2s(s_fl, f.flux + lo, col, &bar);
+        if (need_ecl) {
+            bulk_g2s(s_in, f.in1 + lo, col, &bar);
+            bulk_g2s(s_out, f.out1 + lo, col, &bar);
+        }
+        if (need_pos) {
+            bulk_g2s(s_px, f.px + lo, col, &bar);
+            bulk_g2s(s_py, f.py + lo, col, &bar);
+            bulk_g2s(s_pz, f.pz + lo, col, &bar);
+        }
+    }
+    double ex[PPT], ey[PPT], ez[PPT], pn[PPT], br[PPT];
+    const int64_t ebase = (int64_t)blockIdx.x * kThreads64 * PPT + tid;
+#pragma unroll
+    for (int j = 0; j < PPT; j++) {
+        const int64_t e = ebase + (int64_t)j * kThreads64;
+        const bool ok = e < ph.nent;
+        ex[j] = ok ? ph.ex[e] : 0.;
+        ey[j] = ok ? ph.ey[e] : 0.;
+        ez[j] = ok ? ph.ez[e] : 0.;
+        pn[j] = ok ? ph.phin[e] : 0.;
+        br[j] = 0.0;
+    }
+    const Consts64 L{k.c[0], k.c[1], k.c[2], k.c[3], k.base, k.mucrit,
+                     k.beam, k.spin, k.vfac, k.xcofm, k.rlens1};
+    if (!mbar_wait_bounded(&bar, 0)) {
+        if (tid == 0) {
+            if (atomicCAS(&st->code, 0, 6) == 0) st->face = (int32_t)lo;
+        }
+        mbar_wait_bounded(&bar, 0);
+        return;
+    }
+    for (int64_t i = lo; i < a1; i++) {
+        const int t = (int)(i - lo);
+        const double dx = s_dx[t], dy = s_dy[t], dz = s_dz[t], fl = s_fl[t];
+        double px = 0., py = 0., pz = 0.;
+        if constexpr (need_pos) { px = s_px[t]; py = s_py[t]; pz = s_pz[t]; }
+#pragma unroll
+        for (int j = 0; j < PPT; j++)
+            br[j] += elem<LT, BEAM, GLENS, STAR>(ex[j], ey[j], ez[j], dx, dy, dz, px, py, pz, fl, L);
+    }
+    for (int64_t i = b0; i < hi; i++) {
+        const int t = (int)(i - lo);
+        const double dx = s_dx[t], dy = s_dy[t], dz = s_dz[t], fl = s_fl[t];
+        const double ein = s_in[t], eout = s_out[t];
+        double px = 0., py = 0., pz = 0.;
+        if constexpr (need_pos) { px = s_px[t]; py = s_py[t]; pz = s_pz[t]; }
+#pragma unroll
+        for (int j = 0; j < PPT; j++) {
+            const double v =
+                elem<LT, BEAM, GLENS, STAR>(ex[j], ey[j], ez[j], dx, dy, dz, px, py, pz, fl, L);
+            const bool ecl = (pn[j] >= ein && pn[j] <= eout) || pn[j] <= eout - 1.0;
+            br[j] += ecl ? 0.0 : v;
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < PPT; j++) {
+        const int64_t e = ebase + (int64_t)j * kThreads64;
+        if (e < ph.nent) part[(int64_t)blockIdx.y * ldp + e] = br[j];
+    }
+}
+
+template <int PPT, int LT, bool BEAM, bool GLENS, int STAR>
+void launch_t(const FluxConsts &k, const FlatDev &f, const PhaseDev &ph, const FluxPlan &plan,
+              double *part, int64_t ldp, DevStatus *st, cudaStream_t s) {
+    constexpr bool need_pos = BEAM || GLENS;
+    const size_t smem = (size_t)kBlock * 8 * (need_pos ? 9 : 6);
+    auto kern = k_flux64<PPT, LT, BEAM, GLENS, STAR>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    dim3 grid((unsigned)plan.ntile, (unsigned)plan.nchunk);
+    kern<<<grid, kThreads64, smem, s>>>(k, f, ph, part, ldp, st);
+}
+
+template <int PPT, int LT>
+void launch_lt(int star, const FluxConsts &k, const FlatDev &f, const PhaseDev &ph,
+               const FluxPlan &plan, double *part, int64_t ldp, DevStatus *st, cudaStream_t s) {
+    const bool beam = k.beam_on != 0, glens = (star == 1) && k.glens;
+    if (star == 0) {
+        if (beam) launch_t<PPT, LT, true, false, 0>(k, f, ph, plan, part, ldp, st, s);
+        else launch_t<PPT, LT, false, false, 0>(k, f, ph, plan, part, ldp, st, s);
+    } else if (glens) {
+        if (beam) launch_t<PPT, LT, true, true, 1>(k, f, ph, plan, part, ldp, st, s);
+        else launch_t<PPT, LT, false, true, 1>(k, f, ph, plan, part, ldp, st, s);
+    } else {
+        if (beam) launch_t<PPT, LT, true, false, 1>(k, f, ph, plan, part, ldp, st, s);
+        else launch_t<PPT, LT, false, false, 1>(k, f, ph, plan, part, ldp, st, s);
+    }
+}
+
+template <int PPT>
+void launch_ppt(int star, const FluxConsts &k, const FlatDev &f, const PhaseDev &ph,
+                const FluxPlan &plan, double *part, int64_t ldp, DevStatus *st, cudaStream_t s) {
+    if (k.ltype == 1) launch_lt<PPT, 1>(star, k, f, ph, plan, part, ldp, st, s);
+    else launch_lt<PPT, 0>(star, k, f, ph, plan, part, ldp, st, s);
+}
+
+}  // namespace
+
+void launch_flux64(int star, const FluxConsts &k, const FlatDev &f, const PhaseDev &ph,
+                   const FluxPlan &plan, double *part, int64_t ldp, DevStatus *st,
+                   cudaStream_t s) {
+    switch (plan.ppt) {
+    case 4: launch_ppt<4>(star, k, f, ph, plan, part, ldp, st, s); break;
+    case 2: launch_ppt<2>(star, k, f, ph, plan, part, ldp, st, s); break;
+    default: launch_ppt<1>(star, k, f, ph, plan, part, ldp, st, s); break;
+    }
+}
+
+}  // namespace lcg

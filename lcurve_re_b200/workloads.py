@@ -1,0 +1,125 @@
+"""The benchmark workloads, as seeded synthetic inputs.
+
+No public dataset is involved: each workload is a binary-star model in the
+reference's JSON parameter format plus a synthetic light curve with the
+named shape (number of points, phase range, exposure subdivision) and
+Gaussian noise drawn from a seeded numpy Generator.
+
+  wd_dm_small    detached WD + dM eclipsing binary, nlat 40/80, 500 points
+  wd_dm_large    same physics, nlat 200/800, 5000 points x ndiv 5
+  mcmc_batch     256 models around wd_dm_small, nlat2f in 60..400, 2000 points
+  tiny_star      r1 in {0.002, 0.005, 0.01}, nlat 400/200, 10000 points near eclipse
+  surrogate_box  the prior box of the surrogate training set
+"""
+import numpy as np
+
+from . import abi
+from .model import Model, make_data
+
+SIGMA = 1.5e-3
+
+
+def _pp(v, vary=0):
+    return "%.17g 0.01 0.001 %d 1" % (v, vary)
+
+
+def base_parameters():
+    """Detached WD+dM eclipsing binary: q=0.25, i=86 deg, r1=0.015, r2=0.20,
+    T1=20000 K, T2=3200 K, 4-coefficient Claret limb darkening, gravity
+    darkening 0.25/0.08, irradiation absorb=0.5; wavelength 550 nm,
+    velocity_scale 300 km/s, no beaming, synchronous spins."""
+    p = {
+        "q": _pp(0.25, 1), "iangle": _pp(86.0, 1), "r1": _pp(0.015, 1), "r2": _pp(0.20, 1),
+        "cphi3": _pp(0.01), "cphi4": _pp(0.055), "spin1": _pp(1.0), "spin2": _pp(1.0),
+        "t1": _pp(20000.0, 1), "t2": _pp(3200.0, 1),
+        "ldc1_1": _pp(0.10), "ldc1_2": _pp(0.60), "ldc1_3": _pp(-0.45), "ldc1_4": _pp(0.15),
+        "ldc2_1": _pp(0.70), "ldc2_2": _pp(-0.60), "ldc2_3": _pp(1.00), "ldc2_4": _pp(-0.35),
+        "velocity_scale": _pp(300.0), "beam_factor1": _pp(0.0), "beam_factor2": _pp(0.0),
+        "t0": _pp(0.0, 1), "period": _pp(1.0), "pdot": _pp(0.0), "deltat": _pp(0.0),
+        "gravity_dark1": _pp(0.25), "gravity_dark2": _pp(0.08), "absorb": _pp(0.5, 1),
+        "slope": _pp(0.0), "quad": _pp(0.0), "cube": _pp(0.0), "third": _pp(0.0),
+        "delta_phase": "1e-07", "nlat1f": "40", "nlat2f": "80", "nlat1c": "40", "nlat2c": "80",
+        "npole": "1", "nlatfill": "0", "nlngfill": "0", "lfudge": "0", "llo": "0", "lhi": "0",
+        "phase1": "0.05", "phase2": "0.45", "wavelength": "550", "roche1": "1", "roche2": "1",
+        "eclipse1": "1", "eclipse2": "1", "glens1": "0", "use_radii": "1", "tperiod": "0.1",
+        "gdark_bolom1": "1", "gdark_bolom2": "1", "mucrit1": "0", "mucrit2": "0",
+        "limb1": "Claret", "limb2": "Claret", "mirror": "0", "add_disc": "0", "nrad": "40",
+        "opaque": "0", "add_spot": "0", "nspot": "0", "iscale": "0",
+    }
+    for k in ("rdisc1", "rdisc2", "height_disc", "beta_disc", "temp_disc", "texp_disc",
+              "lin_limb_disc", "quad_limb_disc", "temp_edge", "absorb_edge", "radius_spot",
+              "length_spot", "height_spot", "expon_spot", "epow_spot", "angle_spot", "yaw_spot",
+              "temp_spot", "tilt_spot", "cfrac_spot"):
+        p[k] = _pp(0.0)
+    return p
+
+
+def model(**over):
+    p = base_parameters()
+    for k, v in over.items():
+        if k in ("nlat1f", "nlat2f", "nlat1c", "nlat2c", "nlatfill", "nlngfill", "npole",
+                 "roche1", "roche2", "eclipse1", "eclipse2", "glens1", "use_radii", "mirror",
+                 "gdark_bolom1", "gdark_bolom2", "delta_phase", "phase1", "phase2", "wavelength",
+                 "tperiod", "mucrit1", "mucrit2", "llo", "lhi", "lfudge"):
+            p[k] = str(v)
+        elif k in ("limb1", "limb2"):
+            p[k] = v
+        else:
+            p[k] = _pp(float(v), 1 if k in ("q", "iangle", "r1", "r2", "t1", "t2", "t0", "absorb") else 0)
+    # keep coarse = fine unless given
+    for s in ("1", "2"):
+        if ("nlat%sf" % s) in over and ("nlat%sc" % s) not in over:
+            p["nlat%sc" % s] = str(over["nlat%sf" % s])
+    return Model({"model_parameters": p})
+
+
+def times(n, lo=-0.2, hi=1.2):
+    return np.linspace(lo, hi, n)
+
+
+def data(n, lo=-0.2, hi=1.2, ndiv=1, expose=0.0):
+    return make_data(times(n, lo, hi), expose=expose, flux=1.0, ferr=SIGMA, weight=1.0, ndiv=ndiv)
+
+
+def add_noise(d, calc, seed):
+    """flux = calc / median(calc) + sigma * N(0,1), from a seeded Generator."""
+    rng = np.random.default_rng(seed)
+    d = d.copy()
+    d["flux"] = calc / np.median(calc) + SIGMA * rng.standard_normal(calc.shape[0])
+    return d
+
+
+def wd_dm_small():
+    return model(), data(500)
+
+
+def wd_dm_large():
+    # ndiv 5 over one cadence of a 5000-point curve spanning 1.4 phases
+    return model(nlat1f=200, nlat2f=800), data(5000, ndiv=5, expose=1.4 / 5000)
+
+
+def tiny_star(r1=0.005, q=0.2, iangle=87.0):
+    return (model(r1=r1, q=q, iangle=iangle, nlat1f=400, nlat2f=200),
+            data(10000, lo=-0.03, hi=0.03))
+
+
+def mcmc_batch(nmodels=256, seed=2024):
+    """Models drawn around wd_dm_small: q~N(0.25,0.02), i~N(86,0.5),
+    r1,r2 x N(1,0.05), T1,T2 x N(1,0.03); nlat2f ~ U{60..400}, nlat1f = nlat2f/2."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(nmodels):
+        nl2 = int(rng.integers(60, 401))
+        out.append(model(q=0.25 + 0.02 * rng.standard_normal(),
+                         iangle=86.0 + 0.5 * rng.standard_normal(),
+                         r1=0.015 * (1 + 0.05 * rng.standard_normal()),
+                         r2=0.20 * (1 + 0.05 * rng.standard_normal()),
+                         t1=20000.0 * (1 + 0.03 * rng.standard_normal()),
+                         t2=3200.0 * (1 + 0.03 * rng.standard_normal()),
+                         nlat1f=nl2 // 2, nlat2f=nl2))
+    return out, data(2000)
+
+
+def elements(nface1, nface2, nent):
+    """Face x sub-phase pairs of one light curve (the flux roofline unit)."""
+    return (nface1 + nface2) * nent

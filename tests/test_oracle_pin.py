@@ -1,0 +1,67 @@
+"""Pins the C oracle (oracle/lcg_oracle.c) to the reference itself.
+
+The reference's CPU path is compiled from its own sources into
+oracle/_ref/liblcurve_ref.so (oracle/Makefile, -ffp-contract=off). Both are
+driven with the same lcg_model and data; with the same libm the oracle must
+reproduce the reference bit for bit: grids, eclipse phases, fluxes, the
+light curve and chi**2. The only exception is wdwarf, which the reference
+sums with an OpenMP SIMD reduction whose order is compiler-dependent.
+"""
+import numpy as np
+import pytest
+
+from cases import glens_case, small_cases
+
+CASES = small_cases() + [glens_case()]
+
+
+@pytest.mark.parametrize("name,model,data", CASES, ids=[c[0] for c in CASES])
+def test_light_curve_bit_exact(oracle, reference, name, model, data):
+    st_o, err_o, calc_o, sf_o, sc_o = oracle.light_curve(model, data)
+    st_r, err_r, calc_r, sf_r, sc_r = reference.light_curve(model, data)
+    assert st_o == st_r == 0, (err_o, err_r)
+    assert np.array_equal(calc_o, calc_r)
+    assert np.array_equal(sf_o, sf_r)
+    assert sc_o[1] == sc_r[1] and sc_o[2] == sc_r[2]  # chisq, wnok
+
+
+@pytest.mark.parametrize("name,model,data", CASES[:4], ids=[c[0] for c in CASES[:4]])
+def test_diagnostics(oracle, reference, name, model, data):
+    _, _, _, _, sc_o = oracle.light_curve(model, data, diagnostics=True)
+    _, _, _, _, sc_r = reference.light_curve(model, data, diagnostics=True)
+    np.testing.assert_allclose(sc_o[0], sc_r[0], rtol=1e-12)  # wdwarf: SIMD sum order
+    np.testing.assert_array_equal(sc_o[3:], sc_r[3:])         # logg1, logg2, rv1, rv2
+
+
+@pytest.mark.parametrize("name,model,data", CASES, ids=[c[0] for c in CASES])
+def test_grids_bit_exact(oracle, reference, name, model, data):
+    for star in (0, 1):
+        for fine in (True, False):
+            go = oracle.star_grid(model, star, fine)
+            gr = reference.star_grid(model, star, fine)
+            for k in go:
+                assert np.array_equal(go[k], gr[k]), (star, fine, k)
+
+
+def test_flux_sweep_bit_exact(oracle, reference):
+    from lcurve_re_b200 import workloads as W
+    m, d = W.wd_dm_small()
+    ph = oracle.phase_batch(m, d)
+    for star, ldc in ((0, m.to_c().ldc1), (1, m.to_c().ldc2)):
+        flat = oracle.flatten(oracle.star_grid(m, star))
+        for beam, glens in ((0.0, False), (1.5, False), (0.0, True), (0.7, True)):
+            kw = dict(ldc=list(ldc), ltype=1, mucrit=0.0, beam=beam, spin=1.1, vfac=1e-3,
+                      xcofm=0.2, glens1=glens, rlens1=2e-6)
+            a = oracle.sum_star_multi(star, flat, ph, **kw)
+            b = reference.sum_star_multi(star, flat, ph, **kw)
+            assert np.array_equal(a, b), (star, beam, glens)
+
+
+def test_errors_match(oracle, reference):
+    from lcurve_re_b200 import workloads as W
+    for over, code in (({"r2": 0.5}, 2), ({"r1": 0.9, "r2": 0.05}, 2)):
+        m = W.model(nlat1f=8, nlat2f=8, **over)
+        st_o, err_o, *_ = oracle.light_curve(m, W.data(20))
+        st_r, err_r, *_ = reference.light_curve(m, W.data(20))
+        assert st_o == st_r == code
+        assert err_o == err_r
