@@ -726,7 +726,13 @@ lcg_status check_model(lcg_ctx *c, const lcg_model *m) {
 }
 
 lcg_status finish_status(lcg_ctx *c) {
+    cudaError_t le = cudaGetLastError();
     cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (le != cudaSuccess) {
+        c->collect_timers();
+        c->has_geom = c->has_cont = false;
+        return c->cuda_fail(le, "kernel launch");
+    }
     c->collect_timers();
     if (e != cudaSuccess) return c->cuda_fail(e, "stream");
     DevStatus st{};
@@ -1043,7 +1049,8 @@ lcg_status lcg_light_curve(lcg_ctx *c, const lcg_model *mp, const lcg_datum *dat
     const Grid *gw = nullptr;
     int64_t wchunks = 0;
     if (diag) {
-        const bool fine = gi_type(c->gi, 0.5) == 1;
+        // star1c aliases star1f when copy1 (light_curve_comp.cpp:192-195)
+        const bool fine = c->copy1 || gi_type(c->gi, 0.5) == 1;
         gw = fine ? &g1f : &g1c;
         wchunks = fine ? sw[0].plan.nchunk : sw[1].plan.nchunk;
         wcol.resize((size_t)std::max<int64_t>(wchunks, 1));

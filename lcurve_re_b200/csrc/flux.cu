@@ -195,11 +195,8 @@ void launch_t(const FluxConsts &k, const FlatDev &f, const PhaseDev &ph, const F
               double *part, int64_t ldp, DevStatus *st, cudaStream_t s) {
     const size_t smem = (size_t)plan.chunk * ((BEAM || GLENS) ? 40 : 24);
     auto kern = k_flux_mixed<PPT, LT, BEAM, GLENS, STAR>;
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 40 * 4096);
-        attr_set = true;
-    }
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     dim3 grid((unsigned)plan.ntile, (unsigned)plan.nchunk);
     kern<<<grid, kThreads, smem, s>>>(k, f, ph, plan.chunk, part, ldp, st);
 }

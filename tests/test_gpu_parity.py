@@ -1,0 +1,179 @@
+"""Parity of the CUDA engine (through the C ABI) against the C oracle.
+
+Tolerances:
+  * FP64 flux sweep over the same FlatGrid and phases: bit-identical.
+  * grids: positions/normals within 1e-12 relative (device sin/cos of the
+    ring longitudes may differ from glibc by an ulp), float areas, gravities
+    and fluxes within 2 float ulps (4e-7 relative).
+  * eclipse flags identical away from the boundary band: a face may differ
+    only if its oracle phases put a boundary within 1e-9 of the other's.
+    Ingress/egress within 1e-9.
+  * light curves: FP64 mode per-point relative error <= 1e-6, mixed mode
+    <= 1e-5; chi**2 within 1e-6 relative in FP64 mode.
+"""
+import numpy as np
+import pytest
+
+from cases import glens_case, small_cases
+from lcurve_re_b200 import workloads as W
+from lcurve_re_b200.model import LcurveError
+
+pytestmark = pytest.mark.gpu
+
+CASES = small_cases() + [glens_case()]
+IDS = [c[0] for c in CASES]
+BAND = 1e-9
+
+
+def _noisy(oracle, model, data, seed=7):
+    st, err, calc, _, _ = oracle.light_curve(model, data, scale=False, rdata=False)
+    assert st == 0, err
+    if not np.all(np.isfinite(calc)) or np.median(calc) == 0:
+        return data
+    return W.add_noise(data, calc, seed)
+
+
+@pytest.mark.parametrize("star", [0, 1])
+def test_face_counts(engine_mixed, oracle, star):
+    for name, m, _ in CASES:
+        for fine in (True, False):
+            assert engine_mixed.face_count(m, star, fine) == oracle.face_count(m, star, fine), name
+
+
+@pytest.mark.parametrize("name,model,data", CASES, ids=IDS)
+def test_star_grid(engine_fp64, oracle, name, model, data):
+    for star in (0, 1):
+        go = oracle.star_grid(model, star)
+        gg = engine_fp64.star_grid(model, star)
+        np.testing.assert_allclose(gg["posn"], go["posn"], rtol=1e-12, atol=1e-14)
+        np.testing.assert_allclose(gg["dirn"], go["dirn"], rtol=1e-12, atol=1e-14)
+        for k in ("area", "gravity", "flux"):
+            np.testing.assert_allclose(gg[k], go[k], rtol=4e-7, atol=0, err_msg=k)
+        ne_o, ne_g = go["neclipse"], gg["neclipse"]
+        both = (ne_o == 1) & (ne_g == 1)
+        np.testing.assert_allclose(gg["ecl_in"][both], go["ecl_in"][both], atol=BAND, rtol=0)
+        np.testing.assert_allclose(gg["ecl_out"][both], go["ecl_out"][both], atol=BAND, rtol=0)
+        # a flag may differ only for a face grazing the eclipser (tiny interval)
+        diff = ne_o != ne_g
+        if diff.any():
+            width = np.where(ne_o == 1, go["ecl_out"] - go["ecl_in"],
+                             gg["ecl_out"] - gg["ecl_in"])
+            assert np.all(width[diff] < 1e-6), (name, star, int(diff.sum()))
+
+
+def test_flux_fp64_bit_exact(engine_fp64, oracle):
+    m, d = W.wd_dm_small()
+    ph = oracle.phase_batch(m, W.data(700, ndiv=3, expose=0.002))
+    for star, ldc in ((0, m.to_c().ldc1), (1, m.to_c().ldc2)):
+        flat = oracle.flatten(oracle.star_grid(m, star))
+        for beam, glens in ((0.0, False), (1.5, False), (0.0, True), (0.7, True)):
+            kw = dict(ldc=list(ldc), ltype=1, mucrit=0.0, beam=beam, spin=1.1, vfac=1e-3,
+                      xcofm=0.2, glens1=glens, rlens1=2e-6)
+            a = oracle.sum_star_multi(star, flat, ph, **kw)
+            b = engine_fp64.sum_star_multi(star, flat, ph, **kw)
+            assert np.array_equal(a, b), (star, beam, glens, np.max(np.abs(a - b) / np.abs(a)))
+
+
+def test_flux_mixed(engine_mixed, oracle):
+    m, d = W.wd_dm_small()
+    ph = oracle.phase_batch(m, W.data(700, ndiv=3, expose=0.002))
+    for star, ldc in ((0, m.to_c().ldc1), (1, m.to_c().ldc2)):
+        flat = oracle.flatten(oracle.star_grid(m, star))
+        for ltype in (0, 1):
+            a = oracle.sum_star_multi(star, flat, ph, ldc=list(ldc), ltype=ltype)
+            b = engine_mixed.sum_star_multi(star, flat, ph, ldc=list(ldc), ltype=ltype)
+            rel = np.abs(b - a) / np.max(np.abs(a))
+            assert rel.max() < 1e-5, (star, ltype, rel.max())
+
+
+@pytest.mark.parametrize("name,model,data", CASES, ids=IDS)
+def test_light_curve_fp64(engine_fp64, oracle, name, model, data):
+    d = _noisy(oracle, model, data)
+    st, err, co, sfo, sco = oracle.light_curve(model, d)
+    assert st == 0, err
+    sf = np.ones(5)
+    calc, wd, chisq, wnok, *_ = engine_fp64.light_curve_comp(model, d, scale=True, rdata=True,
+                                                             sfac=sf, diagnostics=False)
+    rel = np.abs(calc - co) / np.maximum(np.abs(co), 1e-300)
+    assert rel.max() <= 1e-6, (name, rel.max())
+    np.testing.assert_allclose(chisq, sco[1], rtol=1e-6)
+    assert wnok == sco[2]
+    np.testing.assert_allclose(sf, sfo, rtol=1e-6)
+
+
+@pytest.mark.parametrize("name,model,data", CASES, ids=IDS)
+def test_light_curve_mixed(engine_mixed, oracle, name, model, data):
+    d = _noisy(oracle, model, data)
+    st, err, co, sfo, sco = oracle.light_curve(model, d)
+    assert st == 0, err
+    calc, wd, chisq, wnok, *_ = engine_mixed.light_curve_comp(model, d, sfac=np.ones(5),
+                                                              diagnostics=False)
+    rel = np.abs(calc - co) / np.maximum(np.abs(co), 1e-300)
+    assert rel.max() <= 1e-5, (name, rel.max())
+
+
+def test_diagnostics(engine_fp64, oracle):
+    m, d = W.wd_dm_small()
+    d = _noisy(oracle, m, d)
+    _, _, _, _, sco = oracle.light_curve(m, d, diagnostics=True)
+    _, wd, chisq, wnok, logg1, logg2, rv1, rv2 = engine_fp64.light_curve_comp(
+        m, d, sfac=np.ones(5), diagnostics=True)
+    np.testing.assert_allclose([wd, logg1, logg2, rv1, rv2], sco[[0, 3, 4, 5, 6]], rtol=1e-9)
+
+
+def test_no_scale_paths(engine_fp64, oracle):
+    m, d = W.wd_dm_small()
+    d = _noisy(oracle, m, d)
+    for rdata in (True, False):
+        sf_in = np.array([2.5, 1, 1, 1, 1.0])
+        _, _, co, sfo, sco = oracle.light_curve(m, d, scale=False, rdata=rdata, sfac=sf_in)
+        sf = sf_in.copy()
+        calc, wd, chisq, wnok, *_ = engine_fp64.light_curve_comp(m, d, scale=False, rdata=rdata,
+                                                                 sfac=sf, diagnostics=False)
+        np.testing.assert_allclose(calc, co, rtol=1e-12)
+        assert np.array_equal(sf, sf_in)
+        if rdata:
+            np.testing.assert_allclose(chisq, sco[1], rtol=1e-9)
+
+
+def test_cache_reuse(engine_mixed):
+    m, d = W.wd_dm_small()
+    engine_mixed.set_profiling(True)
+    engine_mixed.stage_times(reset=True)
+    c1 = engine_mixed.light_curve_comp(m, d, diagnostics=False, no_cache=True)[0].copy()
+    c2 = engine_mixed.light_curve_comp(m, d, diagnostics=False)[0].copy()
+    assert np.array_equal(c1, c2)
+    t = engine_mixed.stage_times(reset=True)
+    assert t["grid"][1] == 2 and t["continuum"][1] == 2  # second call reused both
+    m2 = m.copy()
+    m2["t1"] = 21000.0  # continuum only
+    engine_mixed.light_curve_comp(m2, d, diagnostics=False)
+    t = engine_mixed.stage_times(reset=True)
+    assert t["grid"][1] == 0 and t["continuum"][1] == 2
+    engine_mixed.set_profiling(False)
+
+
+def test_errors(engine_mixed):
+    with pytest.raises(LcurveError, match="larger than its Roche lobe"):
+        engine_mixed.light_curve_comp(W.model(nlat1f=8, nlat2f=8, r2=0.5), W.data(10))
+    m = W.model(nlat1f=8, nlat2f=8)
+    m["add_disc"] = True
+    with pytest.raises(LcurveError) as ei:
+        engine_mixed.light_curve_comp(m, W.data(10))
+    assert ei.value.status == 5
+    # a failure leaves the context usable
+    calc = engine_mixed.light_curve_comp(W.model(nlat1f=8, nlat2f=8), W.data(10))[0]
+    assert np.all(np.isfinite(calc))
+
+
+def test_batch_equals_single(engine_mixed):
+    models, d = W.mcmc_batch(6, seed=3)
+    models = [W.model(nlat1f=int(m["nlat1f"]) // 4 + 4, nlat2f=int(m["nlat2f"]) // 4 + 8,
+                      q=m["q"], iangle=m["iangle"], r1=m["r1"], r2=m["r2"], t1=m["t1"],
+                      t2=m["t2"]) for m in models]
+    d = W.data(300)
+    calc, chisq, wnok, sfac, status = engine_mixed.light_curve_batch(models, d)
+    assert np.all(status == 0)
+    for i, m in enumerate(models):
+        c = engine_mixed.light_curve_comp(m, d, diagnostics=False, no_cache=True)[0]
+        np.testing.assert_allclose(calc[i], c, rtol=1e-12)
