@@ -1,0 +1,376 @@
+#!/usr/bin/env python
+"""Benchmark: light curves per second of the B200 engine.
+
+Workload (default wd_dm_large): the detached WD+dM binary at nlat 200/800
+(50,872 + 814,520 faces), 5000 points x ndiv 5 = 25,000 sub-exposure phases
+= 2.163e10 face-phase elements per light curve, synthetic seeded data. A
+step is one full light curve with the grids rebuilt (the cache disabled), as
+in an MCMC step whose geometry changes.
+
+  value  light curves/s with the points resident on the device
+         (lcg_set_data once, lcg_light_curve_resident per step)
+  e2e    the same through lcg_light_curve with pinned host buffers: the
+         points go host->device and the curve device->host every step
+  roofline  the flux sweep (the dominant kernel): 16 FLOP per element
+         (5 for mu, 8 for the Claret Horner form, 2 for
+         mu*flux*I, 1 accumulate) over its CUDA-event time, against the FP32
+         FMA peak measured live by lcg_measure_fp32_peak
+  cpu_baseline  lcurve_re's own CPU path (oracle/_ref, Release flags,
+         OpenMP on all host cores) on a bounded sample
+
+--impl reference times that reference CPU path alone (rank 0).
+Multi-GPU: one process per GPU; each rank evaluates its own light curves
+(independent replicas, no collective on the data path); value = all ranks'
+curves / the slowest rank's time.
+"""
+import argparse
+import datetime
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "light curves/s"
+FLOP_PER_ELEMENT = 16
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--workload", default="wd_dm_large",
+                    choices=("wd_dm_large", "wd_dm_small", "tiny_star"))
+    ap.add_argument("--precision", choices=("mixed", "fp64"), default="mixed")
+    ap.add_argument("--e2e-steps", type=int, default=100)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(name):
+    from lcurve_re_b200 import workloads as W
+    if name == "wd_dm_large":
+        m, d = W.wd_dm_large()
+        desc = "wd_dm_large: WD+dM q=0.25 i=86 r1=0.015 r2=0.20, nlat 200/800, 5000 pts x ndiv 5"
+    elif name == "wd_dm_small":
+        m, d = W.wd_dm_small()
+        desc = "wd_dm_small: WD+dM q=0.25 i=86 r1=0.015 r2=0.20, nlat 40/80, 500 pts"
+    else:
+        m, d = W.tiny_star()
+        desc = "tiny_star: r1=0.005 q=0.2 i=87, nlat 400/200, 10000 pts in +-0.03"
+    return m, d, desc
+
+
+def rank_info():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)),
+            int(os.environ.get("WORLD_SIZE", 1)))
+
+
+# ---- clocks ---------------------------------------------------------------------
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) >= 9:
+                rows.append(p)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+# ---- CPU baseline: the reference's own CPU path ------------------------------------
+class RefTimer:
+    """Times lcurve_re's CPU light_curve_comp (oracle/_ref Release build, OpenMP
+    over all host cores; the C port in oracle/ if that build is absent).
+
+    Bounded sample: one light curve costs t_grid + frac * t_sample, where
+    t_grid is a cold call on 1 point (the geometry perturbed by 1e-13 so the
+    reference's grid cache misses: grids, eclipses, continuum, FlatGrids) and
+    t_sample a warm call (cache hit) on 1/frac of the points."""
+
+    def __init__(self, model, data, frac=50):
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_lib as OL
+        self.kind = "reference"
+        if os.path.exists(OL.REF_RELEASE_SO):
+            self.lib = OL.Reference(OL.REF_RELEASE_SO)
+        else:
+            self.kind = "port"
+            self.lib = OL.Oracle()
+        self.model = model
+        self.n = data.shape[0]
+        step = max(1, frac)
+        self.sub = np.ascontiguousarray(data[::step])  # strided: covers eclipses too
+        self.ns = self.sub.shape[0]
+        self.frac = self.n / self.ns
+        self.one = np.ascontiguousarray(data[:1])
+        self.k = 0
+        st, err, *_ = self.lib.light_curve(model, self.one)
+        if st:
+            raise RuntimeError(err)
+
+    def cold_grid(self, reps=3):
+        ts = []
+        for _ in range(reps):
+            self.k += 1
+            m = self.model.copy()
+            m["q"] = m["q"] * (1 + 1e-13 * self.k)
+            t = time.perf_counter()
+            self.lib.light_curve(m, self.one)
+            ts.append(time.perf_counter() - t)
+        self.t_grid = float(np.median(ts))
+        self.lib.light_curve(self.model, self.sub)  # re-warm the cache on the model
+        return self.t_grid
+
+    def sample(self):
+        t = time.perf_counter()
+        self.lib.light_curve(self.model, self.sub)
+        return time.perf_counter() - t
+
+    def describe(self, reps, t_curve):
+        return ("every %dth point (%d of %d) per timed call (warm grids), x%.0f, plus a cold 1-point call for "
+                "grids+eclipses+continuum (%.3f s); %d calls; one light curve = %.3f s"
+                % (round(self.frac), self.ns, self.n, self.frac, self.t_grid, reps, t_curve))
+
+
+def cpu_reference_rate(model, data, budget_s=15.0):
+    r = RefTimer(model, data)
+    r.cold_grid()
+    t_probe = r.sample()
+    reps = int(max(3, min(50, budget_s // max(t_probe, 1e-3))))
+    ts = [r.sample() for _ in range(reps)]
+    t_curve = r.t_grid + r.frac * float(np.median(ts))
+    return {"value": 1.0 / t_curve, "unit": METRIC, "cores": os.cpu_count(), "kind": r.kind,
+            "sample": r.describe(reps, t_curve)}
+
+
+def run_reference(args):
+    rank, _, world = rank_info()
+    if rank != 0:
+        return 0
+    model, data, desc = workload(args.workload)
+    r = RefTimer(model, data)
+    r.cold_grid()
+    for _ in range(args.warmup):
+        r.sample()
+    ts = [r.t_grid + r.frac * r.sample() for _ in range(args.steps)]
+    mean_t = float(np.mean(ts))
+    v = 1.0 / mean_t
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean_t * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": desc, "precision": "fp64 (reference CPU)"},
+            "cpu_baseline": {"value": v, "unit": METRIC, "cores": os.cpu_count(), "kind": r.kind,
+                             "sample": r.describe(args.steps, mean_t)},
+            "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---- our arm -------------------------------------------------------------------------
+def run_ours(args):
+    import ctypes as C
+    import torch
+    rank, local, world = rank_info()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from lcurve_re_b200 import abi
+    from lcurve_re_b200 import workloads as W
+    from lcurve_re_b200.engine import Engine
+
+    model, data, desc = workload(args.workload)
+    eng = Engine(device=local, precision=args.precision)
+    lib, ctx = eng.lib, eng.ctx
+    # synthetic noisy data from the model itself (seeded per rank)
+    calc0 = eng.light_curve_comp(model, data, scale=False, rdata=False, diagnostics=False)[0]
+    data = W.add_noise(data, calc0, seed=1234 + rank)
+    n = data.shape[0]
+    mc = model.to_c()
+    flags = abi.FLAG_SCALE | abi.FLAG_RDATA | abi.FLAG_NO_CACHE
+    sfac = np.ones(5)
+    scal = np.zeros(abi.NOUT)
+    dptr = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    peak = eng.fp32_peak_tflops()
+
+    ext = torch.cuda.ExternalStream(eng.stream_ptr)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def check(st):
+        if st != abi.OK:
+            raise RuntimeError(lib.lcg_last_error(ctx).decode())
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    # ---- device-resident value
+    check(lib.lcg_set_data(ctx, data.ctypes.data, n))
+    for _ in range(args.warmup):
+        check(lib.lcg_light_curve_resident(ctx, C.byref(mc), flags, dptr(sfac), None, dptr(scal)))
+    e0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    e1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    eng.set_profiling(True)
+    eng.stage_times(reset=True)
+    eng.flux_elements(reset=True)
+    barrier()
+    lib.lcg_kernel_launches(1)
+    clocks = Clocks(local)
+    clocks.start()
+    with torch.cuda.stream(ext):
+        for k in range(args.steps):
+            flush.fill_(float(k))  # L2 flush, outside the timed span
+            e0[k].record(ext)
+            check(lib.lcg_light_curve_resident(ctx, C.byref(mc), flags, dptr(sfac), None,
+                                               dptr(scal)))
+            e1[k].record(ext)
+    barrier()
+    launches = int(lib.lcg_kernel_launches(1))
+    clk = clocks.stop()
+    total_ms = sum(a.elapsed_time(b) for a, b in zip(e0, e1))
+    st = eng.stage_times(reset=True)
+    elements = eng.flux_elements(reset=True)
+    eng.set_profiling(False)
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    value = world * args.steps / (total_ms / 1e3)
+    flux_ms, flux_n = st["flux"]
+    achieved = elements * FLOP_PER_ELEMENT / (flux_ms / 1e3) / 1e12 if flux_ms > 0 else None
+
+    # ---- end to end through lcg_light_curve with pinned host buffers
+    hdata = torch.empty(n * data.itemsize, dtype=torch.uint8, pin_memory=True).numpy()
+    hdata[:] = data.view(np.uint8).reshape(-1)
+    hcalc = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    ke = min(args.e2e_steps, args.steps)
+    for _ in range(2):
+        check(lib.lcg_light_curve(ctx, C.byref(mc), hdata.ctypes.data, n, flags, dptr(sfac),
+                                  dptr(hcalc), dptr(scal)))
+    f0 = [torch.cuda.Event(enable_timing=True) for _ in range(ke)]
+    f1 = [torch.cuda.Event(enable_timing=True) for _ in range(ke)]
+    barrier()
+    with torch.cuda.stream(ext):
+        for k in range(ke):
+            flush.fill_(float(k))
+            f0[k].record(ext)
+            check(lib.lcg_light_curve(ctx, C.byref(mc), hdata.ctypes.data, n, flags, dptr(sfac),
+                                      dptr(hcalc), dptr(scal)))
+            f1[k].record(ext)
+    barrier()
+    e2e_ms = sum(a.elapsed_time(b) for a, b in zip(f0, f1))
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * ke / (float(t.item()) / 1e3)
+    h2d = n * data.itemsize + (n + 1) * 8 + 5 * 8
+    d2h = n * 8 + 5 * 8 + 3 * 8 + 8
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_reference_rate(model, data)
+        except Exception as ex:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": METRIC, "cores": os.cpu_count(), "kind": "unavailable",
+                   "sample": str(ex)}
+
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "flux_mixed_wd_dm_large.txt")
+    if os.path.exists(prof) and args.workload == "wd_dm_large" and args.precision == "mixed":
+        for line in open(prof):
+            if line.startswith("dram_bytes_per_light_curve:"):
+                traffic = float(line.split(":")[1]) / 2  # two sweeps per curve
+
+    nf1 = eng.face_count(model, 0)
+    nf2 = eng.face_count(model, 1)
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 elements + f64 accumulation" if args.precision == "mixed" else "f64",
+        "data": "synthetic (seeded model + Gaussian noise sigma=1.5e-3)",
+        "config": {"workload": desc, "faces": [nf1, nf2], "sub_phases": int(data["ndiv"].sum()),
+                   "precision": args.precision, "grids": "rebuilt every step",
+                   "l2": "flushed by a 256 MiB write between timed steps (untimed)",
+                   "parallelism": "replicas x%d" % world},
+        "roofline": {"bound": "fp32", "kernel": "k_flux_mixed" if args.precision == "mixed"
+                     else "k_flux64",
+                     "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                     "peak_source": "measured live: FFMA-chain kernel (lcg_measure_fp32_peak)",
+                     "flop_per_element": FLOP_PER_ELEMENT,
+                     "flux_ms_per_step": flux_ms / args.steps,
+                     "flux_launches_per_step": flux_n / args.steps},
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "steps": ke},
+        "gpu_launches": launches,
+        "stage_ms_per_step": {k: v[0] / args.steps for k, v in st.items()},
+        "cpu_baseline": cpu,
+        "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

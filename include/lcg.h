@@ -175,6 +175,19 @@ lcg_status lcg_light_curve(lcg_ctx *ctx, const lcg_model *model,
                            const lcg_datum *data, int32_t n, int32_t flags,
                            double *sfac, double *calc, double *scalars);
 
+/* Resident-data form of lcg_light_curve for callers that evaluate many
+ * models over the same points (samplers, Jacobians): lcg_set_data copies the
+ * points to the device once; lcg_light_curve_resident then evaluates a model
+ * over them. calc may be NULL, leaving the curve on the device only
+ * (lcg_device_calc). lcg_light_curve is lcg_set_data followed by
+ * lcg_light_curve_resident. The reference passes the Data on every call
+ * (light_curve_comp.cpp:119); these two split that call. */
+lcg_status lcg_set_data(lcg_ctx *ctx, const lcg_datum *data, int32_t n);
+lcg_status lcg_light_curve_resident(lcg_ctx *ctx, const lcg_model *model, int32_t flags,
+                                    double *sfac, double *calc, double *scalars);
+/* Device pointer to the last light curve computed on ctx (n doubles). */
+const double *lcg_device_calc(lcg_ctx *ctx);
+
 /* nmodels light curves over the same data points, one per model.
  *   calc[nmodels*n], chisq[nmodels], wnok[nmodels], sfac[nmodels*5] out;
  *   status[nmodels] out: the per-model status (a failed model does not fail
@@ -241,6 +254,10 @@ void lcg_stage_times(lcg_ctx *ctx, double *ms, int64_t *launches,
 /* Elements (face x sub-phase pairs) summed by the flux stage since the last
  * reset: the algorithmic unit of the flux roofline. */
 int64_t lcg_flux_elements(lcg_ctx *ctx, int32_t reset);
+
+/* Kernels launched by this library in this process (all contexts) since the
+ * last reset. */
+int64_t lcg_kernel_launches(int32_t reset);
 
 /* Measures the device's FP32 FMA throughput in TFLOP/s (2 FLOP per FMA)
  * with a register-resident FFMA chain kernel; the denominator of the flux

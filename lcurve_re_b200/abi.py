@@ -105,6 +105,10 @@ PROTOTYPES = {
     "lcg_stage_times": (None, [P, D, I64, C.c_int32]),
     "lcg_flux_elements": (C.c_int64, [P, C.c_int32]),
     "lcg_measure_fp32_peak": (C.c_int, [P, D]),
+    "lcg_set_data": (C.c_int, [P, P, C.c_int32]),
+    "lcg_light_curve_resident": (C.c_int, [P, C.POINTER(LcgModel), C.c_int32, D, D, D]),
+    "lcg_device_calc": (P, [P]),
+    "lcg_kernel_launches": (C.c_int64, [C.c_int32]),
 }
 
 

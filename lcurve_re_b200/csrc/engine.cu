@@ -15,6 +15,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <string>
 #include <vector>
 
@@ -26,6 +27,7 @@ using namespace lcg;
 namespace {
 
 thread_local std::string g_create_error;
+std::atomic<long long> g_launches{0};
 
 template <class T>
 struct DBuf {
@@ -396,6 +398,10 @@ struct lcg_ctx {
     DBuf<uint8_t> ptype;
     std::vector<int64_t> h_off;
     std::vector<double> h_diag;
+    // resident light-curve points (lcg_set_data)
+    int32_t data_n = 0;
+    int64_t data_nent = 0;
+    double data_xmin = 0., data_xmax = 0.;
     // profiling
     bool profiling = false;
     std::vector<Timer> pending[LCG_NSTAGE];
@@ -747,6 +753,8 @@ lcg_status finish_status(lcg_ctx *c) {
 
 }  // namespace
 
+void lcg::count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
 // ---- C ABI --------------------------------------------------------------------
 
 extern "C" {
@@ -858,6 +866,39 @@ int64_t lcg_flux_elements(lcg_ctx *c, int32_t reset) {
     return v;
 }
 
+lcg_status lcg_set_data(lcg_ctx *c, const lcg_datum *data, int32_t n) {
+    if (!c) return LCG_E_INVALID;
+    c->err.clear();
+    if (!data) return c->fail(LCG_E_INVALID, "null argument");
+    if (n < 1) return c->fail(LCG_E_INVALID, "light_curve_comp: no data points");
+    cudaSetDevice(c->device);
+    // per-point offsets of the sub-exposure entries and the time range used
+    // by the polynomial factor (light_curve_comp.cpp:351-356)
+    std::vector<int64_t> &off = c->h_off;
+    off.resize((size_t)n + 1);
+    off[0] = 0;
+    double xmin = data[0].time, xmax = data[0].time;
+    for (int i = 0; i < n; i++) {
+        off[i + 1] = off[i] + (data[i].ndiv > 0 ? data[i].ndiv : 0);
+        if (i > 0) {
+            xmin = data[i].time > xmin ? xmin : data[i].time;
+            xmax = data[i].time < xmax ? xmax : data[i].time;
+        }
+    }
+    cudaError_t e;
+    if ((e = c->data.ensure(n)) || (e = c->off.ensure(n + 1)))
+        return c->cuda_fail(e, "data buffers");
+    cudaMemcpyAsync(c->data.p, data, (size_t)n * sizeof(DatumRec), cudaMemcpyHostToDevice,
+                    c->stream);
+    cudaMemcpyAsync(c->off.p, off.data(), (size_t)(n + 1) * sizeof(int64_t),
+                    cudaMemcpyHostToDevice, c->stream);
+    c->data_n = n;
+    c->data_nent = off[n];
+    c->data_xmin = xmin;
+    c->data_xmax = xmax;
+    return LCG_OK;
+}
+
 lcg_status lcg_light_curve(lcg_ctx *c, const lcg_model *mp, const lcg_datum *data, int32_t n,
                            int32_t flags, double *sfac, double *calc, double *scalars) {
     if (!c) return LCG_E_INVALID;
@@ -865,8 +906,22 @@ lcg_status lcg_light_curve(lcg_ctx *c, const lcg_model *mp, const lcg_datum *dat
     lcg_status rc = check_model(c, mp);
     if (rc) return rc;
     if (!data || !calc || !sfac || !scalars) return c->fail(LCG_E_INVALID, "null argument");
-    if (n < 1) return c->fail(LCG_E_INVALID, "light_curve_comp: no data points");
+    if ((rc = lcg_set_data(c, data, n))) return rc;
+    return lcg_light_curve_resident(c, mp, flags, sfac, calc, scalars);
+}
+
+const double *lcg_device_calc(lcg_ctx *c) { return c ? c->calc.p : nullptr; }
+
+lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t flags, double *sfac,
+                                    double *calc, double *scalars) {
+    if (!c) return LCG_E_INVALID;
+    c->err.clear();
+    lcg_status rc = check_model(c, mp);
+    if (rc) return rc;
+    if (!sfac || !scalars) return c->fail(LCG_E_INVALID, "null argument");
+    if (c->data_n < 1) return c->fail(LCG_E_INVALID, "no data: call lcg_set_data first");
     cudaSetDevice(c->device);
+    const int32_t n = c->data_n;
     const lcg_model &m = *mp;
     const int mixed = c->precision == LCG_PREC_MIXED;
     cudaError_t e;
@@ -936,32 +991,17 @@ lcg_status lcg_light_curve(lcg_ctx *c, const lcg_model *mp, const lcg_datum *dat
         c->cached_mixed_pos = (int)need_pos;
     }
 
-    // data, offsets, phases
-    std::vector<int64_t> &off = c->h_off;
-    off.resize((size_t)n + 1);
-    off[0] = 0;
-    double xmin = data[0].time, xmax = data[0].time;
-    for (int i = 0; i < n; i++) {
-        off[i + 1] = off[i] + (data[i].ndiv > 0 ? data[i].ndiv : 0);
-        if (i > 0) {
-            xmin = data[i].time > xmin ? xmin : data[i].time;
-            xmax = data[i].time < xmax ? xmax : data[i].time;
-        }
-    }
-    const int64_t nent = off[n];
+    // phase entries (light_curve_comp.cpp:358-455) over the resident points
+    const int64_t nent = c->data_nent;
+    const double xmin = c->data_xmin, xmax = c->data_xmax;
     const bool diag = (flags & LCG_FLAG_DIAGNOSTICS) != 0;
     const int64_t nall = nent + (diag ? 1 : 0);  // + the phase-0.5 entry of wdwarf
     const int64_t ldp = ((nall + 3) / 4) * 4;
-    if ((e = c->data.ensure(n)) || (e = c->off.ensure(n + 1)) || (e = c->pex.ensure(nall)) ||
-        (e = c->pey.ensure(nall)) || (e = c->pez.ensure(nall)) || (e = c->pphin.ensure(nall)) ||
-        (e = c->pw1.ensure(nall)) || (e = c->pw2.ensure(nall)) || (e = c->pef.ensure(nall)) ||
-        (e = c->ptype.ensure(nall)) || (e = c->calc.ensure(n)) ||
+    if ((e = c->pex.ensure(nall)) || (e = c->pey.ensure(nall)) || (e = c->pez.ensure(nall)) ||
+        (e = c->pphin.ensure(nall)) || (e = c->pw1.ensure(nall)) || (e = c->pw2.ensure(nall)) ||
+        (e = c->pef.ensure(nall)) || (e = c->ptype.ensure(nall)) || (e = c->calc.ensure(n)) ||
         (e = c->scratch.ensure(3 * (size_t)n)))
         return c->cuda_fail(e, "phase buffers");
-    cudaMemcpyAsync(c->data.p, data, (size_t)n * sizeof(DatumRec), cudaMemcpyHostToDevice,
-                    c->stream);
-    cudaMemcpyAsync(c->off.p, off.data(), (size_t)(n + 1) * sizeof(int64_t),
-                    cudaMemcpyHostToDevice, c->stream);
     PhaseDev ph{c->pex.p, c->pey.p, c->pez.p, c->pphin.p, c->pw1.p, c->pw2.p,
                 c->pef.p, c->ptype.p, nall};
     const double ri = deg2rad(m.iangle);
@@ -1039,8 +1079,9 @@ lcg_status lcg_light_curve(lcg_ctx *c, const lcg_model *mp, const lcg_datum *dat
                         c->stream);
     }
     double hout[4] = {0, 0, 0, 0};
-    cudaMemcpyAsync(calc, c->calc.p, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost,
-                    c->stream);
+    if (calc)
+        cudaMemcpyAsync(calc, c->calc.p, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost,
+                        c->stream);
     cudaMemcpyAsync(sfac, c->sfac.p, 5 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
     cudaMemcpyAsync(hout, c->out.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
 
@@ -1134,10 +1175,12 @@ lcg_status lcg_light_curve_batch(lcg_ctx *c, const lcg_model *models, int32_t nm
     if (!c) return LCG_E_INVALID;
     if (!models || nmodels < 0 || !sfac || !calc || !status)
         return c->fail(LCG_E_INVALID, "null argument");
+    lcg_status rs = lcg_set_data(c, data, n);
+    if (rs) return rs;
     for (int32_t i = 0; i < nmodels; i++) {
         double sc[LCG_NOUT] = {0};
-        lcg_status rc = lcg_light_curve(c, models + i, data, n, flags & ~LCG_FLAG_DIAGNOSTICS,
-                                        sfac + 5 * (size_t)i, calc + (size_t)i * n, sc);
+        lcg_status rc = lcg_light_curve_resident(c, models + i, flags & ~LCG_FLAG_DIAGNOSTICS,
+                                                 sfac + 5 * (size_t)i, calc + (size_t)i * n, sc);
         status[i] = rc;
         if (rc) {
             memset(calc + (size_t)i * n, 0, (size_t)n * sizeof(double));
@@ -1287,6 +1330,10 @@ lcg_status lcg_sum_star_multi(lcg_ctx *c, int32_t star, int64_t n, int64_t n0, c
         out[j] = o;
     }
     return LCG_OK;
+}
+
+int64_t lcg_kernel_launches(int32_t reset) {
+    return reset ? g_launches.exchange(0) : g_launches.load();
 }
 
 lcg_status lcg_measure_fp32_peak(lcg_ctx *c, double *tflops) {

@@ -9,6 +9,10 @@
 
 namespace lcg {
 
+// Number of kernels this library has launched (all contexts); read by
+// lcg_kernel_launches.
+void count_launch();
+
 // One latitude ring of a star grid (set_star_grid.cpp:280-320), computed on
 // the host with the reference's libm so ring sizes match exactly.
 struct RingRec {

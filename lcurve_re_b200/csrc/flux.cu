@@ -199,6 +199,7 @@ void launch_t(const FluxConsts &k, const FlatDev &f, const PhaseDev &ph, const F
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     dim3 grid((unsigned)plan.ntile, (unsigned)plan.nchunk);
     kern<<<grid, kThreads, smem, s>>>(k, f, ph, plan.chunk, part, ldp, st);
+    count_launch();
 }
 
 template <int PPT, int LT>

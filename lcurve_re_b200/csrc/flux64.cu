@@ -172,6 +172,7 @@ void launch_t(const FluxConsts &k, const FlatDev &f, const PhaseDev &ph, const F
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     dim3 grid((unsigned)plan.ntile, (unsigned)plan.nchunk);
     kern<<<grid, kThreads64, smem, s>>>(k, f, ph, part, ldp, st);
+    count_launch();
 }
 
 template <int PPT, int LT>

@@ -500,17 +500,20 @@ inline unsigned nblocks(int64_t n, int t) { return (unsigned)((n + t - 1) / t); 
 
 void launch_pack_flat(FlatDev f, int64_t n0, int need_pos, cudaStream_t s) {
     k_pack_flat<<<nblocks(f.n > 0 ? f.n : 1, 256), 256, 0, s>>>(f, n0, need_pos);
+    count_launch();
 }
 
 void launch_pack_phases(PhaseDev ph, cudaStream_t s) {
     if (ph.nent <= 0) return;
     k_pack_phases<<<nblocks(ph.nent, 256), 256, 0, s>>>(ph);
+    count_launch();
 }
 
 void launch_grid(const GridParams &p, const RingRec *rings, GridDev g, DevStatus *st,
                  cudaStream_t s) {
     if (p.nhalf <= 0) return;
     k_grid<<<nblocks(p.nhalf, 128), 128, 0, s>>>(p, rings, g, st);
+    count_launch();
 }
 
 void launch_eclipse(const EclParams &p, int32_t eclipse_on, GridDev g, int32_t *queue,
@@ -518,17 +521,20 @@ void launch_eclipse(const EclParams &p, int32_t eclipse_on, GridDev g, int32_t *
     if (g.n <= 0) return;
     cudaMemsetAsync(counters, 0, 2 * sizeof(int32_t), s);
     k_ecl_pre<<<nblocks(g.n, 256), 256, 0, s>>>(p, eclipse_on, g, queue, counters);
+    count_launch();
     if (eclipse_on && p.comp_roche) {
         unsigned nb = (unsigned)nsm * 4u;
         const unsigned need = nblocks(g.n, 128);
         if (need < nb) nb = need;
         k_ecl_roche<<<nb, 128, 0, s>>>(p, g, queue, counters, st);
+        count_launch();
     }
 }
 
 void launch_continuum(const ContParams &p, GridDev g, cudaStream_t s) {
     if (g.n <= 0) return;
     k_continuum<<<nblocks(g.n, 256), 256, 0, s>>>(p, g);
+    count_launch();
 }
 
 void launch_flatten(GridDev g, FlatDev f, int32_t *blockcnt, int mixed, int need_pos,
@@ -540,14 +546,18 @@ void launch_flatten(GridDev g, FlatDev f, int32_t *blockcnt, int mixed, int need
         return;
     }
     k_flat_count<<<nb, kFlatBlock, 0, s>>>(g, blockcnt);
+    count_launch();
     k_flat_scan<<<1, 1024, 0, s>>>(blockcnt, (int32_t)nb, g.n, f.n0);
+    count_launch();
     k_flat_scatter<<<nb, kFlatBlock, 0, s>>>(g, f, blockcnt, mixed, need_pos);
+    count_launch();
 }
 
 void launch_phases(const PhaseParams &p, const DatumRec *data, const int64_t *off, int32_t n,
                    PhaseDev ph, cudaStream_t s) {
     if (n <= 0) return;
     k_phases<<<nblocks(n, 128), 128, 0, s>>>(p, data, off, n, ph);
+    count_launch();
 }
 
 void launch_scatter(const ScatterParams &p, const double *part1f, const double *part1c,
@@ -557,17 +567,20 @@ void launch_scatter(const ScatterParams &p, const double *part1f, const double *
     if (n <= 0) return;
     k_scatter<<<nblocks(n, 128), 128, 0, s>>>(p, part1f, part1c, part2f, part2c, ph, data, off,
                                               n, calc);
+    count_launch();
 }
 
 void launch_finalize(int32_t flags, const DatumRec *data, int32_t n, double *calc,
                      double *scratch, double *sfac_io, double *out, cudaStream_t s) {
     k_finalize<<<1, 1024, 0, s>>>(flags, data, n, calc, scratch, sfac_io, out);
+    count_launch();
 }
 
 void launch_diagnostics(int star, GridDev g, double *out, cudaStream_t s) {
     const int64_t nblk = (g.n + 8191) / 8192;
     if (nblk <= 0) return;
     k_diag<<<nblocks(nblk, 64), 64, 0, s>>>(star, g, out);
+    count_launch();
 }
 
 }  // namespace lcg
