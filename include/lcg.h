@@ -237,6 +237,31 @@ lcg_status lcg_sum_star_multi(lcg_ctx *ctx, int32_t star, int64_t n,
                               double xcofm, int32_t glens1, double rlens1,
                               double *out);
 
+/* Allocation-free form of the FP64 sweep of lcg_sum_star_multi, for callers
+ * in which this library must not allocate device memory: programs whose
+ * device memory is already claimed by another framework's pooling allocator
+ * (a cudaMalloc from here would fail), or latency-critical loops in which an
+ * allocation would synchronise the device. No counterpart in the reference.
+ *   All arrays are DEVICE arrays owned by the caller (same meaning as in
+ *   lcg_sum_star_multi; in1/out1 of length n-n0); ldc is a host array of 4.
+ *   Runs on `stream` (a cudaStream_t; NULL = the legacy default stream) on
+ *   the device that owns `out`; returns without waiting for the GPU.
+ *   No beaming or lensing in this form; FP64 arithmetic of the reference.
+ * Scratch: a fixed 16 MiB device array inside the library (held by every GPU
+ * that loads it, until exit): ceil(n/1024) * nent must not exceed 2,097,152
+ * and ceil(n/1024) must not exceed 65,535, else LCG_E_CAPACITY is returned
+ * and nothing runs. The first call on a device looks up that array's
+ * address (set-up, no allocation); make it before any stream capture. All
+ * calls share the array: calls that overlap on the GPU race and must be
+ * ordered by the caller. Calls no cudaMalloc/cudaFree. */
+lcg_status lcg_sum_star_multi_noalloc(void *stream, int32_t star, int64_t n, int64_t n0,
+                                      const double *dx, const double *dy, const double *dz,
+                                      const double *flux, const double *in1,
+                                      const double *out1, int32_t nent, const double *ex,
+                                      const double *ey, const double *ez, const double *phin,
+                                      const double *ldc, int32_t ltype, double mucrit,
+                                      double *out);
+
 /* ---- measurement ------------------------------------------------------- */
 
 /* Stage timings recorded with CUDA events on the context's stream when

@@ -29,6 +29,7 @@ SOURCES = {
     "flux64.cu": ["--fmad=false"],
     "engine.cu": ["--fmad=false"],
     "flux.cu": ["--fmad=true"],
+    "noalloc.cu": ["--fmad=false"],
 }
 HEADERS = ["roche.cuh", "eclipse.cuh", "engine.h", "tma.cuh"]
 
