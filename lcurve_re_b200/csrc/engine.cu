@@ -19,7 +19,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/lcg.h"
+#include "lcg.h"
 #include "engine.h"
 
 using namespace lcg;
@@ -324,7 +324,9 @@ struct Grid {
     DBuf<float4> geo, pos;
     DBuf<uint2> ecl;
     DBuf<double> fdx, fdy, fdz, fpx, fpy, fpz, fflux, fin, fout;
+    DBuf<float> fp;
     int64_t n = 0, npad = 0;
+    int fast = 0;  // flat records built for the fast mixed sweep
     StarSetup setup;
 
     cudaError_t alloc_points(int64_t nf) {
@@ -338,13 +340,18 @@ struct Grid {
             return e;
         return cudaSuccess;
     }
-    cudaError_t alloc_flat(int mixed, int need_pos) {
+    cudaError_t alloc_flat(int mixed, int need_pos, int fast_on) {
         npad = ((n + 4095) / 4096) * 4096;
         if (npad == 0) npad = 4096;
         cudaError_t e = n0.ensure(1);
         if (e) return e;
         if (mixed) {
-            if ((e = geo.ensure(npad)) || (e = ecl.ensure(npad))) return e;
+            if ((e = ecl.ensure(npad))) return e;
+            if (fast_on) {
+                if ((e = fp.ensure(8 * npad))) return e;
+            } else if ((e = geo.ensure(npad))) {
+                return e;
+            }
             if (need_pos && (e = pos.ensure(npad))) return e;
         } else {
             DBuf<double> *d[] = {&fdx, &fdy, &fdz, &fpx, &fpy, &fpz, &fflux, &fin, &fout};
@@ -359,14 +366,14 @@ struct Grid {
     }
     FlatDev flat() const {
         return FlatDev{n, npad, n0.p, geo.p, ecl.p, pos.p, fdx.p, fdy.p, fdz.p,
-                       fpx.p, fpy.p, fpz.p, fflux.p, fin.p, fout.p};
+                       fpx.p, fpy.p, fpz.p, fflux.p, fin.p, fout.p, fp.p};
     }
     void release() {
         DBuf<double> *d[] = {&px, &py, &pz, &nx, &ny, &nz, &ein, &eout, &fdx, &fdy,
                              &fdz, &fpx, &fpy, &fpz, &fflux, &fin, &fout};
         for (auto *b : d) b->release();
         area.release(); grav.release(); flux.release(); necl.release(); rings.release();
-        n0.release(); geo.release(); pos.release(); ecl.release();
+        n0.release(); geo.release(); pos.release(); ecl.release(); fp.release();
     }
 };
 
@@ -393,7 +400,7 @@ struct lcg_ctx {
     DBuf<DatumRec> data;
     DBuf<int64_t> off;
     DBuf<double> pex, pey, pez, pphin, pw1, pw2, part1f, part1c, part2f, part2c, calc, scratch,
-        sfac, out, diag;
+        sfac, out, diag, osum;
     DBuf<float4> pef;
     DBuf<uint8_t> ptype;
     std::vector<int64_t> h_off;
@@ -634,14 +641,40 @@ lcg_status build_geometry(lcg_ctx *c, const lcg_model &m, int star, int fine, Gr
     return LCG_OK;
 }
 
-lcg_status flatten(lcg_ctx *c, Grid &g, int need_pos) {
+// Fast mixed-sweep records apply without beaming or lensing and with
+// mucrit <= 0, where the reference's masks reduce to mu > 0.
+FastCoef fast_coef(const lcg_model &m, int star, int mixed) {
+    FastCoef f{};
+    const double beam = star == kStar1 ? m.beam_factor1 : m.beam_factor2;
+    const double mucrit = star == kStar1 ? m.mucrit1 : m.mucrit2;
+    const bool glens = star == kStar2 && m.glens1;
+    f.on = mixed && beam == 0.0 && !glens && mucrit <= 0.0;
+    f.ltype = star == kStar1 ? m.limb1 : m.limb2;
+    f.cosi = cos(deg2rad(m.iangle));
+    const double *c = star == kStar1 ? m.ldc1 : m.ldc2;
+    f.p[0] = 1.0 - (c[0] + c[1] + c[2] + c[3]);
+    if (f.ltype == LCG_LIMB_CLARET) {
+        for (int k = 0; k < 4; k++) f.p[k + 1] = c[k];
+    } else {  // 1 - sum_k c_k (1 - mu)^k in powers of mu
+        f.p[1] = c[0] + 2. * c[1] + 3. * c[2] + 4. * c[3];
+        f.p[2] = -(c[1] + 3. * c[2] + 6. * c[3]);
+        f.p[3] = c[2] + 4. * c[3];
+        f.p[4] = -c[3];
+    }
+    return f;
+}
+
+lcg_status flatten(lcg_ctx *c, Grid &g, int need_pos, const FastCoef &fc) {
     const int mixed = c->precision == LCG_PREC_MIXED;
     cudaError_t e;
-    if ((e = g.alloc_flat(mixed, need_pos)) != cudaSuccess) return c->cuda_fail(e, "flat grid");
+    if ((e = g.alloc_flat(mixed, need_pos, fc.on)) != cudaSuccess)
+        return c->cuda_fail(e, "flat grid");
+    g.fast = fc.on;
     if ((e = c->blockcnt.ensure((g.n + 1023) / 1024 + 1)) != cudaSuccess)
         return c->cuda_fail(e, "partition");
     StageScope t(c, LCG_STAGE_FLATTEN);
-    launch_flatten(g.dev(), g.flat(), c->blockcnt.p, mixed, need_pos, c->status.p, c->stream);
+    launch_flatten(g.dev(), g.flat(), c->blockcnt.p, mixed, need_pos, fc, c->status.p,
+                   c->stream);
     return LCG_OK;
 }
 
@@ -662,7 +695,7 @@ lcg_status sweep_one(lcg_ctx *c, const lcg_model &m, Grid &g, int star, double p
     PhaseDev ph{c->pex.p, c->pey.p, c->pez.p, c->pphin.p, nullptr, nullptr, c->pef.p, nullptr, 1};
     const int mixed = c->precision == LCG_PREC_MIXED;
     if (mixed) launch_pack_phases(ph, c->stream);
-    FluxPlan plan = plan_flux(mixed, g.n, 1, c->nsm);
+    FluxPlan plan = plan_flux(mixed, g.fast, g.n, 1, c->nsm);
     if ((err = c->part1f.ensure((size_t)std::max<int64_t>(plan.nchunk, 1) * 4)))
         return c->cuda_fail(err, "partials");
     FluxConsts k = flux_consts(m, star, 1.0, rlens1);
@@ -826,7 +859,7 @@ void lcg_destroy(lcg_ctx *c) {
     for (Grid *g : gs) g->release();
     DBuf<double> *d[] = {&c->pex, &c->pey, &c->pez, &c->pphin, &c->pw1, &c->pw2, &c->part1f,
                          &c->part1c, &c->part2f, &c->part2c, &c->calc, &c->scratch, &c->sfac,
-                         &c->out, &c->diag};
+                         &c->out, &c->diag, &c->osum};
     for (auto *b : d) b->release();
     c->status.release(); c->queue.release(); c->counters.release(); c->blockcnt.release();
     c->data.release(); c->off.release(); c->pef.release(); c->ptype.release();
@@ -982,7 +1015,8 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
                 StageScope t(c, LCG_STAGE_CONTINUUM);
                 launch_continuum(cp, gl[k]->dev(), c->stream);
             }
-            if ((rc = flatten(c, *gl[k], need_pos))) return rc;
+            if ((rc = flatten(c, *gl[k], need_pos, fast_coef(m, stars[k], c->precision == LCG_PREC_MIXED))))
+                return rc;
         }
         c->gi = Ginterp{m.phase1, m.phase2, 1., 1., 1., 1.};
         if (!c->copy1 || !c->copy2) {
@@ -1048,7 +1082,7 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
     for (int k = 0; k < 4; k++) {
         if (!use_sw[k]) continue;
         Sweep &s = sw[k];
-        s.plan = plan_flux(mixed, s.g->n, s.nent, c->nsm);
+        s.plan = plan_flux(mixed, s.g->fast, s.g->n, s.nent, c->nsm);
         if ((e = s.part->ensure((size_t)std::max<int64_t>(s.plan.nchunk, 1) * ldp)))
             return c->cuda_fail(e, "flux partials");
         PhaseDev phk = ph;
@@ -1065,18 +1099,20 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
         ScatterParams sp{};
         sp.copy1 = c->copy1;
         sp.copy2 = c->copy2;
-        sp.nchunk1f = sw[0].plan.nchunk;
-        sp.nchunk1c = c->copy1 ? 0 : sw[1].plan.nchunk;
-        sp.nchunk2f = sw[2].plan.nchunk;
-        sp.nchunk2c = c->copy2 ? 0 : sw[3].plan.nchunk;
-        sp.ldp = ldp;
         sp.third = m.third;
+        if ((e = c->osum.ensure(4 * (size_t)ldp))) return c->cuda_fail(e, "entry sums");
+        ReduceParams rp{};
+        rp.ldp = ldp;
+        for (int k = 0; k < 4; k++) {
+            rp.part[k] = use_sw[k] ? sw[k].part->p : nullptr;
+            rp.nchunk[k] = use_sw[k] ? sw[k].plan.nchunk : 0;
+            rp.nent[k] = use_sw[k] ? sw[k].nent : 0;
+            rp.osum[k] = c->osum.p + k * ldp;
+        }
         StageScope t(c, LCG_STAGE_REDUCE);
-        launch_scatter(sp, c->part1f.p, c->part1c.p, c->part2f.p, c->part2c.p, ph, c->data.p,
-                       c->off.p, n, c->calc.p, c->stream);
+        launch_scatter(sp, rp, ph, c->data.p, c->off.p, n, c->calc.p, c->stream);
         cudaMemcpyAsync(c->sfac.p, sfac, 5 * sizeof(double), cudaMemcpyHostToDevice, c->stream);
-        launch_finalize(flags & 3, c->data.p, n, c->calc.p, c->scratch.p, c->sfac.p, c->out.p,
-                        c->stream);
+        launch_finalize(flags & 3, c->data.p, n, c->calc.p, c->sfac.p, c->out.p, c->stream);
     }
     double hout[4] = {0, 0, 0, 0};
     if (calc)
@@ -1085,20 +1121,13 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
     cudaMemcpyAsync(sfac, c->sfac.p, 5 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
     cudaMemcpyAsync(hout, c->out.p, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
 
-    // diagnostics: wdwarf partial column, logg / rv block sums
-    std::vector<double> wcol;
-    const Grid *gw = nullptr;
-    int64_t wchunks = 0;
+    // diagnostics: wdwarf's phase-0.5 sum, logg / rv block sums
+    double wsum = 0.;
     if (diag) {
         // star1c aliases star1f when copy1 (light_curve_comp.cpp:192-195)
         const bool fine = c->copy1 || gi_type(c->gi, 0.5) == 1;
-        gw = fine ? &g1f : &g1c;
-        wchunks = fine ? sw[0].plan.nchunk : sw[1].plan.nchunk;
-        wcol.resize((size_t)std::max<int64_t>(wchunks, 1));
-        const double *src = (fine ? c->part1f.p : c->part1c.p) + nent;
-        if (wchunks > 0)
-            cudaMemcpy2DAsync(wcol.data(), sizeof(double), src, (size_t)ldp * sizeof(double),
-                              sizeof(double), (size_t)wchunks, cudaMemcpyDeviceToHost, c->stream);
+        cudaMemcpyAsync(&wsum, c->osum.p + (fine ? 0 : 1) * ldp + nent, sizeof(double),
+                        cudaMemcpyDeviceToHost, c->stream);
         const int64_t nb1 = (g1f.n + 8191) / 8192, nb2 = (g2f.n + 8191) / 8192;
         if ((e = c->diag.ensure(4 * (size_t)(nb1 + nb2))))
             return c->cuda_fail(e, "diagnostics");
@@ -1118,9 +1147,7 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
     }
     const double sc = sfac[0];
     if (diag) {
-        double o = 0.0;
-        for (int64_t k = 0; k < wchunks; k++) o += wcol[(size_t)k];
-        double wd = 1.0 * gi_scale1(c->gi, 0.5) * o;
+        double wd = 1.0 * gi_scale1(c->gi, 0.5) * wsum;
         scalars[LCG_OUT_WDWARF] = wd / 1 * sc;
         // comp_gravity1/2 (comp_gravity.cpp:20-155), comp_radius1/2 (comp_radius.cpp)
         const int64_t nb1 = (g1f.n + 8191) / 8192, nb2 = (g2f.n + 8191) / 8192;
@@ -1165,7 +1192,6 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
         scalars[LCG_OUT_LOGG1] = scalars[LCG_OUT_LOGG2] = 0.0;
         scalars[LCG_OUT_RV1] = scalars[LCG_OUT_RV2] = 0.0;
     }
-    (void)gw;
     return LCG_OK;
 }
 
@@ -1264,6 +1290,7 @@ lcg_status lcg_sum_star_multi(lcg_ctx *c, int32_t star, int64_t n, int64_t n0, c
     Grid &g = star == kStar1 ? c->g1c : c->g2c;  // scratch slot
     c->has_geom = c->has_cont = false;
     g.n = n;
+    g.fast = 0;
     const bool need_pos = beam != 0. || (star == kStar2 && glens1);
     g.npad = ((n + 4095) / 4096) * 4096;
     if (g.npad == 0) g.npad = 4096;
@@ -1308,7 +1335,7 @@ lcg_status lcg_sum_star_multi(lcg_ctx *c, int32_t star, int64_t n, int64_t n0, c
     k.vfac = vfac;
     k.xcofm = xcofm;
     k.rlens1 = rlens1;
-    FluxPlan plan = plan_flux(mixed, n, nent, c->nsm);
+    FluxPlan plan = plan_flux(mixed, 0, n, nent, c->nsm);
     const int64_t ldp = ((nent + 3) / 4) * 4;
     if ((e = c->part1f.ensure((size_t)std::max<int64_t>(plan.nchunk, 1) * std::max<int64_t>(ldp, 1))))
         return c->cuda_fail(e, "partials");

@@ -71,10 +71,26 @@ struct DevStatus {
 struct FlatDev {
     int64_t n, npad;
     int64_t *n0;  // device scalar, written by the partition
-    float4 *geo;  // mixed
+    float4 *geo;  // mixed, general: (nx, ny, nz, flux)
     uint2 *ecl;
     float4 *pos;  // (px,py,pz,0): beaming and lensing only
     double *dx, *dy, *dz, *px, *py, *pz, *flux, *in1, *out1;  // FP64
+    // mixed, fast: per PAIR of faces (a, b) four float4
+    //   (nx_a, nx_b, ny_a, ny_b) (cz_a, cz_b, f0_a, f0_b) (f1_a, f1_b, f2_a, f2_b) (f3_a, f3_b, f4_a, f4_b)
+    // with cz = cos(i) nz and f_k = flux * p_k, so each float2 operand of the
+    // packed FP32x2 arithmetic is an aligned register pair
+    float *fp;
+};
+
+// Face records of the fast mixed sweep (no beaming, no lensing, mucrit <= 0):
+// the constant z term of mu = e.n and the face flux times the intensity
+// polynomial, so mu costs 2 FMA and Horner yields flux * I directly.
+//   Claret: I = p0 + p1 t + p2 t^2 + p3 t^3 + p4 t^4, t = sqrt(mu), p = (1 - sum c, c1..c4)
+//   poly:   I = 1 - sum_k c_k (1-mu)^k expanded in powers of t = mu
+struct FastCoef {
+    int32_t on, ltype;
+    double cosi;
+    double p[5];
 };
 
 // Sub-exposure phase entries of all data points (light_curve_comp.cpp:416-455).
@@ -99,9 +115,16 @@ struct FluxConsts {
 
 struct ScatterParams {
     int32_t copy1, copy2;
-    int64_t nchunk1f, nchunk1c, nchunk2f, nchunk2c;  // partial rows per sweep
-    int64_t ldp;                                     // row stride of partials
     double third;
+};
+
+// The four sweeps' chunk partials (1f, 1c, 2f, 2c; NULL when a sweep did not
+// run) and their per-entry sums.
+struct ReduceParams {
+    const double *part[4];
+    int64_t nchunk[4], nent[4];
+    int64_t ldp;  // row stride of the partials
+    double *osum[4];
 };
 
 // ---- launchers (geometry.cu) ------------------------------------------------
@@ -111,17 +134,16 @@ void launch_eclipse(const EclParams &p, int32_t eclipse_on, GridDev g, int32_t *
                     int32_t *counters, DevStatus *st, int nsm, cudaStream_t s);
 void launch_continuum(const ContParams &p, GridDev g, cudaStream_t s);
 void launch_flatten(GridDev g, FlatDev f, int32_t *blockcnt, int mixed, int need_pos,
-                    DevStatus *st, cudaStream_t s);
+                    const FastCoef &fc, DevStatus *st, cudaStream_t s);
 void launch_phases(const PhaseParams &p, const DatumRec *data, const int64_t *off, int32_t n,
                    PhaseDev ph, cudaStream_t s);
-void launch_scatter(const ScatterParams &p, const double *part1f, const double *part1c,
-                    const double *part2f, const double *part2c, const PhaseDev &ph,
+void launch_scatter(const ScatterParams &p, const ReduceParams &r, const PhaseDev &ph,
                     const DatumRec *data, const int64_t *off, int32_t n, double *calc,
                     cudaStream_t s);
 // finalize: scale / chi**2 (re_scale.cpp:16-42, light_curve_comp.cpp:557-585).
 // out[0] = chisq, out[1] = wnok, out[2] = 1 when they were computed.
 void launch_finalize(int32_t flags, const DatumRec *data, int32_t n, double *calc,
-                     double *scratch, double *sfac_io, double *out, cudaStream_t s);
+                     double *sfac_io, double *out, cudaStream_t s);
 // flux-weighted gravity / volume-averaged radius sums (comp_gravity.cpp,
 // comp_radius.cpp): out[0..3] = sum f*g, sum f, sum solid angle, sum volume
 void launch_diagnostics(int star, GridDev g, double *out, cudaStream_t s);
@@ -131,13 +153,14 @@ void launch_pack_phases(PhaseDev ph, cudaStream_t s);
 
 // ---- launchers (flux.cu, flux64.cu) -----------------------------------------
 struct FluxPlan {
+    int fast;       // fast mixed sweep (FlatDev::fa/fb records)
     int ppt;        // phase entries per thread
     int threads;    // threads per CTA
     int64_t chunk;  // faces per CTA
     int64_t nchunk;
     int64_t ntile;  // phase tiles
 };
-FluxPlan plan_flux(int mixed, int64_t nface, int64_t nent, int nsm);
+FluxPlan plan_flux(int mixed, int fast, int64_t nface, int64_t nent, int nsm);
 void launch_flux(int mixed, int star, const FluxConsts &k, const FlatDev &f,
                  const PhaseDev &ph, const FluxPlan &plan, double *part, int64_t ldp,
                  DevStatus *st, cudaStream_t s);

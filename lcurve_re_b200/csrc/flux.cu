@@ -227,6 +227,138 @@ void launch_ppt(int star, const FluxConsts &k, const FlatDev &f, const PhaseDev 
     else launch_ppt_lt<PPT, 0>(star, k, f, ph, plan, part, ldp, st, s);
 }
 
+// ---- fast path: no beaming, no lensing, mucrit <= 0 ---------------------------
+//
+// Two faces per instruction with Blackwell's packed FP32x2 FMA: per pair of
+// faces and phase entry
+//   mu  = fma2(ex, nx, fma2(ey, ny, cos(i) nz))        2 FFMA2
+//   m   = max(mu, 0) per face                          2 FMNMX  (I(mu) = 0 for mu <= 0)
+//   t   = sqrt(m) (Claret) or m (polynomial)           2 MUFU / 0
+//   fI  = flux * I(t), Horner on per-face coefficients 4 FFMA2
+//   s  += m * fI                                       1 FFMA2
+// one-range faces add the fixed-point eclipse test (IADD, ISETP, FSEL per face).
+// Phase entries are dealt to the tiles round-robin so every tile is equally full.
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+
+template <int PPT, int LT, bool ECL>
+__device__ __forceinline__ void sweep_pairs(const float4 *sp, const uint4 *se, int64_t q0,
+                                            int64_t lo, int64_t hi, const float2 *ex,
+                                            const float2 *ey, const uint32_t *pf, float *acc) {
+    constexpr int kFoldPairs = kFold / 2;
+    for (int64_t b = lo; b < hi; b += kFoldPairs) {
+        const int cnt = (int)((b + kFoldPairs < hi) ? kFoldPairs : hi - b);
+        const float4 *rp = sp + 4 * (b - q0);
+        const uint4 *ep = se + (b - q0);
+        float2 s[PPT];
+#pragma unroll
+        for (int j = 0; j < PPT; j++) s[j] = f2(0.f, 0.f);
+#pragma unroll 2
+        for (int i = 0; i < cnt; i++) {
+            const float4 P0 = rp[4 * i], P1 = rp[4 * i + 1], P2 = rp[4 * i + 2], P3 = rp[4 * i + 3];
+            const float2 nx = f2(P0.x, P0.y), ny = f2(P0.z, P0.w), cz = f2(P1.x, P1.y);
+            const float2 p0 = f2(P1.z, P1.w), p1 = f2(P2.x, P2.y), p2 = f2(P2.z, P2.w);
+            const float2 p3 = f2(P3.x, P3.y), p4 = f2(P3.z, P3.w);
+            uint4 E = make_uint4(0u, 0u, 0u, 0u);
+            if constexpr (ECL) E = ep[i];
+#pragma unroll
+            for (int j = 0; j < PPT; j++) {
+                const float2 mu = __ffma2_rn(ex[j], nx, __ffma2_rn(ey[j], ny, cz));
+                float ma = fmaxf(mu.x, 0.f), mb = fmaxf(mu.y, 0.f);
+                if constexpr (ECL) {
+                    ma = ((pf[j] - E.x) >= E.y) ? ma : 0.f;
+                    mb = ((pf[j] - E.z) >= E.w) ? mb : 0.f;
+                }
+                const float2 m = f2(ma, mb);
+                float2 t;
+                if constexpr (LT == 1) t = f2(sqrt_approx(ma), sqrt_approx(mb));
+                else t = m;
+                const float2 fI =
+                    __ffma2_rn(t, __ffma2_rn(t, __ffma2_rn(t, __ffma2_rn(t, p4, p3), p2), p1), p0);
+                s[j] = __ffma2_rn(m, fI, s[j]);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < PPT; j++) acc[j] += s[j].x + s[j].y;
+    }
+}
+
+template <int PPT, int LT>
+__global__ void __launch_bounds__(kThreads, 2)
+    k_flux_fast(FlatDev f, PhaseDev ph, int64_t chunk, int64_t ntile, double *part, int64_t ldp,
+                DevStatus *st) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ uint64_t bar;
+    const int tid = threadIdx.x;
+    const int64_t c0 = (int64_t)blockIdx.y * chunk;
+    const int64_t n = f.n, n0 = *f.n0;
+    const int64_t cend = (c0 + chunk < n) ? c0 + chunk : n;
+    const bool need_ecl = cend > n0;
+    float4 *sp = reinterpret_cast<float4 *>(smem);
+    uint4 *se = reinterpret_cast<uint4 *>(smem + chunk * 32);
+    if (tid == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    if (tid == 0) {
+        const uint32_t bytes = (uint32_t)(chunk * 32) + (need_ecl ? (uint32_t)(chunk * 8) : 0u);
+        mbar_arrive_expect_tx(&bar, bytes);
+        bulk_g2s(sp, f.fp + 8 * c0, (uint32_t)(chunk * 32), &bar);
+        if (need_ecl) bulk_g2s(se, f.ecl + c0, (uint32_t)(chunk * 8), &bar);
+    }
+    float2 ex[PPT], ey[PPT];
+    uint32_t pf[PPT];
+#pragma unroll
+    for (int j = 0; j < PPT; j++) {
+        const int64_t e = blockIdx.x + ntile * ((int64_t)j * kThreads + tid);
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (e < ph.nent) v = ph.ef[e];
+        ex[j] = f2(v.x, v.x);
+        ey[j] = f2(v.y, v.y);
+        pf[j] = __float_as_uint(v.w);
+    }
+    if (!mbar_wait_bounded(&bar, 0)) {
+        if (tid == 0) {
+            if (atomicCAS(&st->code, 0, 6) == 0) st->face = (int32_t)c0;
+        }
+        mbar_wait_bounded(&bar, 0);
+        return;
+    }
+    // two-level FP32 sums: runs of <= 64 faces, then the runs of the chunk;
+    // the chunk partial goes out in FP64 and chunks are added in FP64
+    float acc[PPT];
+#pragma unroll
+    for (int j = 0; j < PPT; j++) acc[j] = 0.f;
+    // pairs: the pair holding face n0 and those after it take the eclipse
+    // test (a never-eclipsed face in that pair has an empty range); faces past
+    // n in the last pair carry zero coefficients
+    const int64_t q0 = c0 >> 1, qend = (cend + 1) >> 1, qn0 = n0 >> 1;
+    const int64_t qa = qn0 < qend ? qn0 : qend;
+    sweep_pairs<PPT, LT, false>(sp, se, q0, q0, qa > q0 ? qa : q0, ex, ey, pf, acc);
+    sweep_pairs<PPT, LT, true>(sp, se, q0, qa > q0 ? qa : q0, qend, ex, ey, pf, acc);
+#pragma unroll
+    for (int j = 0; j < PPT; j++) {
+        const int64_t e = blockIdx.x + ntile * ((int64_t)j * kThreads + tid);
+        if (e < ph.nent) part[(int64_t)blockIdx.y * ldp + e] = (double)acc[j];
+    }
+}
+
+template <int PPT, int LT>
+void launch_fast_t(const FlatDev &f, const PhaseDev &ph, const FluxPlan &plan, double *part,
+                   int64_t ldp, DevStatus *st, cudaStream_t s) {
+    const size_t smem = (size_t)plan.chunk * 40;  // 32 B records + 8 B eclipse ranges
+    auto kern = k_flux_fast<PPT, LT>;
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    dim3 grid((unsigned)plan.ntile, (unsigned)plan.nchunk);
+    kern<<<grid, kThreads, smem, s>>>(f, ph, plan.chunk, plan.ntile, part, ldp, st);
+    count_launch();
+}
+
+template <int PPT>
+void launch_fast_ppt(int ltype, const FlatDev &f, const PhaseDev &ph, const FluxPlan &plan,
+                     double *part, int64_t ldp, DevStatus *st, cudaStream_t s) {
+    if (ltype == 1) launch_fast_t<PPT, 1>(f, ph, plan, part, ldp, st, s);
+    else launch_fast_t<PPT, 0>(f, ph, plan, part, ldp, st, s);
+}
+
 // 8 independent FFMA chains per thread keep the FP32 pipes full.
 __global__ void __launch_bounds__(256) k_fma_probe(float *sink, int iters) {
     float a0 = threadIdx.x * 1e-3f, a1 = a0 + 1.f, a2 = a0 + 2.f, a3 = a0 + 3.f;
@@ -250,9 +382,31 @@ void launch_fma_probe(float *sink, int blocks, int iters, double *gflop, cudaStr
     *gflop = 2.0 * 8 * 16 * (double)iters * 256.0 * blocks * 1e-9;
 }
 
-FluxPlan plan_flux(int mixed, int64_t nface, int64_t nent, int nsm) {
+FluxPlan plan_flux(int mixed, int fast, int64_t nface, int64_t nent, int nsm) {
     FluxPlan p;
-    if (mixed) {
+    p.fast = mixed && fast;
+    if (p.fast) {
+        // entries per thread: the fewest idle lanes, weighed against the per-face
+        // shared-memory loads that a larger PPT amortises
+        p.threads = kThreads;
+        const int cand[] = {4, 2, 1};  // PPT 8 spills with the face loop unrolled by 2
+        double best = 1e300;
+        p.ppt = 1;
+        for (int c : cand) {
+            const int64_t nt = (nent + (int64_t)kThreads * c - 1) / ((int64_t)kThreads * c);
+            const double cost = (double)nt * kThreads * c * (8.0 + 8.0 / c) / (double)(nent > 0 ? nent : 1);
+            if (cost < best - 1e-9) {
+                best = cost;
+                p.ppt = c;
+            }
+        }
+        p.ntile = (nent + (int64_t)kThreads * p.ppt - 1) / ((int64_t)kThreads * p.ppt);
+        if (p.ntile < 1) p.ntile = 1;
+        const int64_t want = ((int64_t)nsm * 4 + p.ntile - 1) / p.ntile;
+        int64_t chunk = 1024;  // 40 B per face: 40 KB of shared memory per CTA
+        while (chunk > 64 && (nface + chunk - 1) / chunk < want) chunk >>= 1;
+        p.chunk = chunk;
+    } else if (mixed) {
         p.threads = kThreads;
         p.ppt = nent >= 16384 ? 8 : (nent >= 2048 ? 4 : 1);
         p.ntile = (nent + (int64_t)kThreads * p.ppt - 1) / ((int64_t)kThreads * p.ppt);
@@ -280,6 +434,17 @@ void launch_flux(int mixed, int star, const FluxConsts &k, const FlatDev &f,
     if (plan.nchunk == 0 || ph.nent == 0) return;
     if (!mixed) {
         launch_flux64(star, k, f, ph, plan, part, ldp, st, s);
+        return;
+    }
+    if (plan.fast) {
+        switch (plan.ppt) {
+        case 16: launch_fast_ppt<16>(k.ltype, f, ph, plan, part, ldp, st, s); break;
+        case 12: launch_fast_ppt<12>(k.ltype, f, ph, plan, part, ldp, st, s); break;
+        case 8: launch_fast_ppt<8>(k.ltype, f, ph, plan, part, ldp, st, s); break;
+        case 4: launch_fast_ppt<4>(k.ltype, f, ph, plan, part, ldp, st, s); break;
+        case 2: launch_fast_ppt<2>(k.ltype, f, ph, plan, part, ldp, st, s); break;
+        default: launch_fast_ppt<1>(k.ltype, f, ph, plan, part, ldp, st, s); break;
+        }
         return;
     }
     switch (plan.ppt) {

@@ -266,7 +266,7 @@ __device__ __forceinline__ uint32_t phase_fx(double ph) {
 }
 
 __global__ void k_flat_scatter(GridDev g, FlatDev f, const int32_t *__restrict__ blockoff,
-                               int mixed, int need_pos) {
+                               int mixed, int need_pos, FastCoef fc) {
     __shared__ int32_t warp_tot[32];
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
     const int64_t i = blockIdx.x * (int64_t)kFlatBlock + t;
@@ -284,7 +284,20 @@ __global__ void k_flat_scatter(GridDev g, FlatDev f, const int32_t *__restrict__
     const int64_t dest = flag ? n0 + boff + rank
                               : blockIdx.x * (int64_t)kFlatBlock - boff + (t - rank);
     if (mixed) {
-        f.geo[dest] = make_float4((float)g.nx[i], (float)g.ny[i], (float)g.nz[i], g.flux[i]);
+        if (fc.on) {
+            const double fl = (double)g.flux[i];
+            float *r = f.fp + 16 * (dest >> 1) + (dest & 1);
+            r[0] = (float)g.nx[i];
+            r[2] = (float)g.ny[i];
+            r[4] = (float)(fc.cosi * g.nz[i]);
+            r[6] = (float)(fl * fc.p[0]);
+            r[8] = (float)(fl * fc.p[1]);
+            r[10] = (float)(fl * fc.p[2]);
+            r[12] = (float)(fl * fc.p[3]);
+            r[14] = (float)(fl * fc.p[4]);
+        } else {
+            f.geo[dest] = make_float4((float)g.nx[i], (float)g.ny[i], (float)g.nz[i], g.flux[i]);
+        }
         uint2 e = make_uint2(0u, 0u);
         if (flag) {
             const double in1 = g.ein[i], out1 = g.eout[i];
@@ -343,16 +356,34 @@ __global__ void k_phases(PhaseParams p, const DatumRec *__restrict__ data,
     }
 }
 
-__device__ __forceinline__ double chunk_sum(const double *__restrict__ part, int64_t nchunk,
-                                            int64_t ldp, int64_t e) {
+// Sum of the chunk partials of every phase entry, chunks in order (for the
+// FP64 sweep: the reference's block order). One thread per (sweep, entry);
+// consecutive threads read consecutive entries of a chunk row.
+__global__ void k_reduce_chunks(ReduceParams p) {
+    const int s = blockIdx.y;
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const double *__restrict__ part = p.part[s];
+    if (!part || e >= p.nent[s]) return;
+    const int64_t nc = p.nchunk[s], ldp = p.ldp;
     double o = 0.0;
-    for (int64_t c = 0; c < nchunk; c++) o += part[c * ldp + e];
-    return o;
+    int64_t c = 0;
+    for (; c + 8 <= nc; c += 8) {
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) v[u] = part[(c + u) * ldp + e];
+#pragma unroll
+        for (int u = 0; u < 8; u++) o += v[u];
+    }
+    for (; c < nc; c++) o += part[c * ldp + e];
+    p.osum[s][e] = o;
 }
 
-__global__ void k_scatter(ScatterParams p, const double *__restrict__ part1f,
-                          const double *__restrict__ part1c, const double *__restrict__ part2f,
-                          const double *__restrict__ part2c, PhaseDev ph,
+// Per data point: weighted sub-exposure sums of the four sweeps in the
+// reference's order (pb1f, pb1c, pb2f, pb2c, light_curve_comp.cpp:476-480),
+// then third light.
+__global__ void k_scatter(ScatterParams p, const double *__restrict__ o1f,
+                          const double *__restrict__ o1c, const double *__restrict__ o2f,
+                          const double *__restrict__ o2c, PhaseDev ph,
                           const DatumRec *__restrict__ data, const int64_t *__restrict__ off,
                           int32_t n, double *calc) {
     const int np = blockIdx.x * blockDim.x + threadIdx.x;
@@ -360,84 +391,84 @@ __global__ void k_scatter(ScatterParams p, const double *__restrict__ part1f,
     const int64_t e0 = off[np], e1 = e0 + (data[np].ndiv > 0 ? data[np].ndiv : 0);
     double c = 0.;
     for (int64_t e = e0; e < e1; e++)
-        if (p.copy1 || ph.type[e] == 1) c += ph.w1[e] * chunk_sum(part1f, p.nchunk1f, p.ldp, e);
+        if (p.copy1 || ph.type[e] == 1) c += ph.w1[e] * o1f[e];
     if (!p.copy1)
         for (int64_t e = e0; e < e1; e++)
-            if (ph.type[e] != 1) c += ph.w1[e] * chunk_sum(part1c, p.nchunk1c, p.ldp, e);
+            if (ph.type[e] != 1) c += ph.w1[e] * o1c[e];
     for (int64_t e = e0; e < e1; e++)
-        if (p.copy2 || ph.type[e] == 3) c += ph.w2[e] * chunk_sum(part2f, p.nchunk2f, p.ldp, e);
+        if (p.copy2 || ph.type[e] == 3) c += ph.w2[e] * o2f[e];
     if (!p.copy2)
         for (int64_t e = e0; e < e1; e++)
-            if (ph.type[e] != 3) c += ph.w2[e] * chunk_sum(part2c, p.nchunk2c, p.ldp, e);
+            if (ph.type[e] != 3) c += ph.w2[e] * o2c[e];
     calc[np] = c + p.third;
 }
 
-// One block. Terms are formed in parallel, the sums run in point order in
-// one thread so they equal the reference's serial loops.
-__global__ void k_finalize(int32_t flags, const DatumRec *__restrict__ data, int32_t n,
-                           double *calc, double *scratch, double *sfac_io, double *out) {
-    __shared__ double s_scale;
+// Fixed-shape tree over the 1024 threads of the block: deterministic.
+__device__ __forceinline__ double block_sum(double v, double *sh) {
+    const int t = threadIdx.x;
+    sh[t] = v;
+    __syncthreads();
+    for (int w = 512; w > 0; w >>= 1) {
+        if (t < w) sh[t] += sh[t + w];
+        __syncthreads();
+    }
+    const double r = sh[0];
+    __syncthreads();
+    return r;
+}
+
+// One block of 1024 threads: thread t takes points t, t+1024, ... in order,
+// the block sums them in a fixed tree.
+__global__ void __launch_bounds__(1024) k_finalize(int32_t flags, const DatumRec *__restrict__ data,
+                                                   int32_t n, double *calc, double *sfac_io,
+                                                   double *out) {
+    __shared__ double sh[1024];
     const bool scale = flags & 1, rdata = flags & 2;
-    double *t0 = scratch, *t1 = scratch + n, *t2 = scratch + 2 * (int64_t)n;
+    const int t = threadIdx.x;
     if (scale) {
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        double a = 0., b = 0., w = 0.;
+        for (int i = t; i < n; i += 1024) {
             const DatumRec d = data[i];
             if (d.weight > 0.) {
                 const double wgt = d.weight / sq(d.ferr);
-                t0[i] = wgt * d.flux * calc[i];
-                t1[i] = wgt * calc[i] * calc[i];
-                t2[i] = d.weight;
+                a += wgt * d.flux * calc[i];
+                b += wgt * calc[i] * calc[i];
+                w += d.weight;
             }
         }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double sdy = 0., syy = 0., wnok = 0.;
-            for (int i = 0; i < n; i++) {
-                if (data[i].weight > 0.) {
-                    sdy += t0[i];
-                    syy += t1[i];
-                    wnok += t2[i];
-                }
-            }
-            s_scale = wnok > 0.0 ? sdy / syy : 1.;
+        const double sdy = block_sum(a, sh), syy = block_sum(b, sh), wnok = block_sum(w, sh);
+        const bool ok = wnok > 0.0;
+        const double sc = ok ? sdy / syy : 1.;
+        if (t == 0) {
             out[1] = wnok;
-        }
-        __syncthreads();
-        const double sc = s_scale;
-        const bool ok = out[1] > 0.0;
-        if (ok)
-            for (int i = threadIdx.x; i < n; i += blockDim.x) calc[i] = calc[i] * sc;
-        if (threadIdx.x == 0)
             for (int k = 0; k < 5; k++) sfac_io[k] = sc;
+        }
         if (!ok) {
-            if (threadIdx.x == 0) {
+            if (t == 0) {
                 out[0] = 0.;
                 out[2] = 1.;
             }
             return;
         }
+        for (int i = t; i < n; i += 1024) calc[i] = calc[i] * sc;
     } else {
         const double sc = sfac_io[0];
-        for (int i = threadIdx.x; i < n; i += blockDim.x) calc[i] *= sc;
+        for (int i = t; i < n; i += 1024) calc[i] *= sc;
         if (!rdata) {
-            if (threadIdx.x == 0) out[2] = 0.;
+            if (t == 0) out[2] = 0.;
             return;
         }
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double cs = 0., w = 0.;
+    for (int i = t; i < n; i += 1024) {
         const DatumRec d = data[i];
-        if (d.weight > 0.) t0[i] = d.weight * sq((d.flux - calc[i]) / d.ferr);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double chisq = 0., wnok = 0.;
-        for (int i = 0; i < n; i++) {
-            if (data[i].weight > 0.) {
-                chisq += t0[i];
-                wnok += data[i].weight;
-            }
+        if (d.weight > 0.) {
+            cs += d.weight * sq((d.flux - calc[i]) / d.ferr);
+            w += d.weight;
         }
+    }
+    const double chisq = block_sum(cs, sh), wnok = block_sum(w, sh);
+    if (t == 0) {
         out[0] = chisq;
         if (!scale) out[1] = wnok;
         out[2] = 1.;
@@ -538,18 +569,20 @@ void launch_continuum(const ContParams &p, GridDev g, cudaStream_t s) {
 }
 
 void launch_flatten(GridDev g, FlatDev f, int32_t *blockcnt, int mixed, int need_pos,
-                    DevStatus *st, cudaStream_t s) {
+                    const FastCoef &fc, DevStatus *st, cudaStream_t s) {
     (void)st;
     const unsigned nb = nblocks(g.n, kFlatBlock);
     if (nb == 0) {
         cudaMemsetAsync(f.n0, 0, sizeof(int64_t), s);
         return;
     }
+    if (mixed && fc.on && f.npad > g.n)  // padding faces must add nothing
+        cudaMemsetAsync(f.fp + 8 * g.n, 0, (size_t)(f.npad - g.n) * 8 * sizeof(float), s);
     k_flat_count<<<nb, kFlatBlock, 0, s>>>(g, blockcnt);
     count_launch();
     k_flat_scan<<<1, 1024, 0, s>>>(blockcnt, (int32_t)nb, g.n, f.n0);
     count_launch();
-    k_flat_scatter<<<nb, kFlatBlock, 0, s>>>(g, f, blockcnt, mixed, need_pos);
+    k_flat_scatter<<<nb, kFlatBlock, 0, s>>>(g, f, blockcnt, mixed, need_pos, fc);
     count_launch();
 }
 
@@ -560,19 +593,25 @@ void launch_phases(const PhaseParams &p, const DatumRec *data, const int64_t *of
     count_launch();
 }
 
-void launch_scatter(const ScatterParams &p, const double *part1f, const double *part1c,
-                    const double *part2f, const double *part2c, const PhaseDev &ph,
+void launch_scatter(const ScatterParams &p, const ReduceParams &r, const PhaseDev &ph,
                     const DatumRec *data, const int64_t *off, int32_t n, double *calc,
                     cudaStream_t s) {
     if (n <= 0) return;
-    k_scatter<<<nblocks(n, 128), 128, 0, s>>>(p, part1f, part1c, part2f, part2c, ph, data, off,
-                                              n, calc);
+    int64_t nmax = 0;
+    for (int k = 0; k < 4; k++)
+        if (r.part[k] && r.nent[k] > nmax) nmax = r.nent[k];
+    if (nmax > 0) {
+        k_reduce_chunks<<<dim3(nblocks(nmax, 256), 4), 256, 0, s>>>(r);
+        count_launch();
+    }
+    k_scatter<<<nblocks(n, 128), 128, 0, s>>>(p, r.osum[0], r.osum[1], r.osum[2], r.osum[3], ph,
+                                              data, off, n, calc);
     count_launch();
 }
 
 void launch_finalize(int32_t flags, const DatumRec *data, int32_t n, double *calc,
-                     double *scratch, double *sfac_io, double *out, cudaStream_t s) {
-    k_finalize<<<1, 1024, 0, s>>>(flags, data, n, calc, scratch, sfac_io, out);
+                     double *sfac_io, double *out, cudaStream_t s) {
+    k_finalize<<<1, 1024, 0, s>>>(flags, data, n, calc, sfac_io, out);
     count_launch();
 }
 

@@ -30,7 +30,7 @@
 
 #include <mutex>
 
-#include "../../include/lcg.h"
+#include "lcg.h"
 
 namespace {
 
