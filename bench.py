@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", default="wd_dm_large",
-                    choices=("wd_dm_large", "wd_dm_small", "tiny_star"))
+                    choices=("wd_dm_large", "wd_dm_small", "tiny_star", "mcmc_batch"))
     ap.add_argument("--precision", choices=("mixed", "fp64"), default="mixed")
     ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -365,10 +365,249 @@ def run_ours(args):
     return 0
 
 
+# ---- batched workload: 256 models per step -------------------------------------------
+BATCH_DESC = ("mcmc_batch: 256 models around wd_dm_small (q~N(0.25,0.02), i~N(86,0.5), r1,r2 "
+              "x N(1,0.05), T1,T2 x N(1,0.03); nlat2f ~ U{60..400}, nlat1f = nlat2f/2), "
+              "2000 points")
+
+
+def batch_workload():
+    """The 256 models, a second set with every q scaled by 1 + 1e-4 (so that
+    alternating steps rebuild every grid, as an MCMC step does), and noisy data
+    from the first model's curve."""
+    from lcurve_re_b200 import workloads as W
+    ms, d = W.mcmc_batch(256)
+    alt = []
+    for m in ms:
+        c = m.to_c()
+        alt.append(W.model(q=c.q * (1 + 1e-4), iangle=c.iangle, r1=c.r1, r2=c.r2, t1=c.t1,
+                           t2=c.t2, nlat1f=c.nlat1f, nlat2f=c.nlat2f))
+    return ms, alt, d
+
+
+def cpu_batch_rate(models, data, sample=8, budget_s=20.0):
+    """The reference CPU path on the first `sample` models of the batch (each
+    a cold call: grids rebuilt), scaled to the batch by total face count."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as OL
+    kind = "reference"
+    if os.path.exists(OL.REF_RELEASE_SO):
+        lib = OL.Reference(OL.REF_RELEASE_SO)
+    else:
+        kind = "port"
+        lib = OL.Oracle()
+    counter = OL.Oracle()
+    face_count_host = lambda m: counter.face_count(m, 0) + counter.face_count(m, 1)
+    t_used, k = 0.0, 0
+    f_used = 0
+    for m in models[:sample]:
+        t = time.perf_counter()
+        st, err, *_ = lib.light_curve(m, data)
+        t_used += time.perf_counter() - t
+        if st:
+            raise RuntimeError(err)
+        f_used += face_count_host(m)
+        k += 1
+        if t_used > budget_s:
+            break
+    f_all = sum(face_count_host(m) for m in models)
+    t_batch = t_used * f_all / f_used
+    v = len(models) / t_batch
+    return {"value": v, "unit": METRIC, "cores": os.cpu_count(), "kind": kind,
+            "sample": "%d of %d models, full %d points each, cold grids (%.2f s); scaled to the "
+                      "batch by total faces (%d of %d)" % (k, len(models), data.shape[0], t_used,
+                                                           f_used, f_all)}
+
+
+def run_batch(args):
+    import ctypes as C
+    import torch
+    rank, local, world = rank_info()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from lcurve_re_b200 import abi
+    from lcurve_re_b200 import workloads as W
+    from lcurve_re_b200.engine import Engine
+
+    ms, alt, data = batch_workload()
+    eng = Engine(device=local, precision="mixed")
+    lib, ctx = eng.lib, eng.ctx
+    calc0 = eng.light_curve_comp(ms[0], data, scale=False, rdata=False, diagnostics=False)[0]
+    data = W.add_noise(data, calc0, seed=1234 + rank)
+    n, nm = data.shape[0], len(ms)
+    A = (abi.LcgModel * nm)(*[m.to_c() for m in ms])
+    B = (abi.LcgModel * nm)(*[m.to_c() for m in alt])
+    flags = abi.FLAG_SCALE | abi.FLAG_RDATA
+    sfac = np.ones(5 * nm)
+    chisq = np.zeros(nm)
+    wnok = np.zeros(nm)
+    status = np.zeros(nm, dtype=np.int32)
+    dptr = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    i32 = status.ctypes.data_as(C.POINTER(C.c_int32))
+    peak = eng.fp32_peak_tflops()
+    ext = torch.cuda.ExternalStream(eng.stream_ptr)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+
+    def check(st):
+        if st != abi.OK:
+            raise RuntimeError(lib.lcg_last_error(ctx).decode())
+        if np.any(status != 0):
+            raise RuntimeError("model status %s" % np.unique(status))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def step(k, calc_out=None):
+        check(lib.lcg_light_curve_batch_resident(ctx, A if k % 2 == 0 else B, nm, flags,
+                                                 dptr(sfac), calc_out, dptr(chisq), dptr(wnok),
+                                                 i32))
+
+    # ---- device-resident value (CUDA graph path)
+    check(lib.lcg_set_data(ctx, data.ctypes.data, n))
+    for k in range(args.warmup):
+        step(k)
+    e0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    e1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    barrier()
+    lib.lcg_kernel_launches(1)
+    clocks = Clocks(local)
+    clocks.start()
+    with torch.cuda.stream(ext):
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            e0[k].record(ext)
+            step(k)
+            e1[k].record(ext)
+    barrier()
+    launches = int(lib.lcg_kernel_launches(1))
+    clk = clocks.stop()
+    total_ms = sum(a.elapsed_time(b) for a, b in zip(e0, e1))
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    value = world * nm * args.steps / (total_ms / 1e3)
+
+    # ---- stage breakdown and the flux roofline (profiled, untimed)
+    eng.set_profiling(True)
+    eng.stage_times(reset=True)
+    eng.flux_elements(reset=True)
+    kp = 4
+    with torch.cuda.stream(ext):
+        for k in range(kp):
+            flush.fill_(float(k))
+            step(k)
+    barrier()
+    st = eng.stage_times(reset=True)
+    elements = eng.flux_elements(reset=True)
+    eng.set_profiling(False)
+    flux_ms, flux_n = st["flux"]
+    achieved = elements * FLOP_PER_ELEMENT / (flux_ms / 1e3) / 1e12 if flux_ms > 0 else None
+
+    # ---- end to end: lcg_light_curve_batch with pinned host data and curves
+    hdata = torch.empty(n * data.itemsize, dtype=torch.uint8, pin_memory=True).numpy()
+    hdata[:] = data.view(np.uint8).reshape(-1)
+    hcalc = torch.empty(nm * n, dtype=torch.float64, pin_memory=True).numpy()
+    ke = min(args.e2e_steps, args.steps)
+
+    def step_e2e(k):
+        check(lib.lcg_light_curve_batch(ctx, A if k % 2 == 0 else B, nm, hdata.ctypes.data, n,
+                                        flags, dptr(sfac), dptr(hcalc), dptr(chisq), dptr(wnok),
+                                        i32))
+    for k in range(2):
+        step_e2e(k)
+    f0 = [torch.cuda.Event(enable_timing=True) for _ in range(ke)]
+    f1 = [torch.cuda.Event(enable_timing=True) for _ in range(ke)]
+    barrier()
+    with torch.cuda.stream(ext):
+        for k in range(ke):
+            flush.fill_(float(k))
+            f0[k].record(ext)
+            step_e2e(k)
+            f1[k].record(ext)
+    barrier()
+    e2e_ms = sum(a.elapsed_time(b) for a, b in zip(f0, f1))
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * nm * ke / (float(t.item()) / 1e3)
+    h2d = n * data.itemsize + (n + 1) * 8 + nm * C.sizeof(abi.LcgModel)
+    d2h = nm * (n * 8 + 5 * 8 + 3 * 8 + 8)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_batch_rate(ms, data)
+        except Exception as ex:
+            cpu = {"value": None, "unit": METRIC, "cores": os.cpu_count(), "kind": "unavailable",
+                   "sample": str(ex)}
+    faces = [eng.face_count(m, 0) + eng.face_count(m, 1) for m in ms]
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 elements + f64 accumulation",
+        "data": "synthetic (seeded models + Gaussian noise sigma=1.5e-3)",
+        "config": {"workload": BATCH_DESC, "models_per_step": nm, "faces_per_step": int(sum(faces)),
+                   "points": n, "precision": "mixed",
+                   "grids": "every model's grids rebuilt every step (q alternates by 1e-4)",
+                   "l2": "flushed by a 256 MiB write between timed steps (untimed)",
+                   "graph": "one CUDA graph per step", "parallelism": "replicas x%d" % world},
+        "roofline": {"bound": "fp32", "kernel": "k_flux_batch", "achieved": achieved,
+                     "peak": peak, "unit": "TFLOP/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": None,
+                     "peak_source": "measured live: FFMA-chain kernel (lcg_measure_fp32_peak)",
+                     "flop_per_element": FLOP_PER_ELEMENT,
+                     "flux_ms_per_step": flux_ms / kp},
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "steps": ke},
+        "gpu_launches": launches,
+        "stage_ms_per_step": {k: v[0] / kp for k, v in st.items()},
+        "cpu_baseline": cpu,
+        "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def run_reference_batch(args):
+    rank, _, world = rank_info()
+    if rank != 0:
+        return 0
+    from lcurve_re_b200 import workloads as W
+    ms, alt, data = batch_workload()
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as OL
+    calc0 = OL.Oracle().light_curve(ms[0], data, scale=False, rdata=False)[2]
+    data = W.add_noise(data, calc0, seed=1234)
+    vals = [cpu_batch_rate(ms, data, sample=2, budget_s=8.0) for _ in range(args.warmup + args.steps)]
+    vals = vals[args.warmup:]
+    v = float(np.mean([x["value"] for x in vals]))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 256 / v * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": BATCH_DESC, "precision": "fp64 (reference CPU)"},
+            "cpu_baseline": dict(vals[-1], value=v),
+            "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
-        return run_reference(args)
+        return run_reference_batch(args) if args.workload == "mcmc_batch" else run_reference(args)
+    if args.workload == "mcmc_batch":
+        return run_batch(args)
     return run_ours(args)
 
 

@@ -39,7 +39,7 @@
 extern "C" {
 #endif
 
-#define LCG_ABI_VERSION 1
+#define LCG_ABI_VERSION 2
 
 typedef enum lcg_status {
     LCG_OK = 0,
@@ -133,7 +133,10 @@ typedef struct lcg_options {
     int32_t device;        /* CUDA device ordinal                          */
     int32_t precision;     /* LCG_PREC_FP64 or LCG_PREC_MIXED              */
     int32_t verbose;       /* print per-stage timings at destroy when > 0  */
-    int32_t reserved[5];
+    int32_t eclipse_warp;  /* Roche eclipse candidates up to which one warp
+                              bisects each face (the rest: one thread per
+                              face); 0 automatic, -1 never                 */
+    int32_t reserved[4];
 } lcg_options;
 
 typedef struct lcg_ctx lcg_ctx;
@@ -192,12 +195,26 @@ const double *lcg_device_calc(lcg_ctx *ctx);
  *   calc[nmodels*n], chisq[nmodels], wnok[nmodels], sfac[nmodels*5] out;
  *   status[nmodels] out: the per-model status (a failed model does not fail
  *   the batch; its calc row is zero). sfac is read when SCALE is clear.
- * Returns LCG_OK unless the batch as a whole could not run. */
+ * Returns LCG_OK unless the batch as a whole could not run.
+ * On a mixed-precision context, models without beaming, lensing, mucrit > 0,
+ * separate coarse grids or infill are evaluated together: every stage runs
+ * once for the whole batch (one CUDA graph, replayed while the batch keeps
+ * its size and grid resolutions), and a model's grids are rebuilt only when
+ * its geometry parameters changed since the previous batch call on ctx (its
+ * continuum only when its brightness parameters did). Other models are
+ * evaluated one by one. LCG_FLAG_DIAGNOSTICS is ignored. */
 lcg_status lcg_light_curve_batch(lcg_ctx *ctx, const lcg_model *models,
                                  int32_t nmodels, const lcg_datum *data,
                                  int32_t n, int32_t flags, double *sfac,
                                  double *calc, double *chisq, double *wnok,
                                  int32_t *status);
+
+/* lcg_light_curve_batch over the points of lcg_set_data. calc, chisq and
+ * wnok may be NULL. */
+lcg_status lcg_light_curve_batch_resident(lcg_ctx *ctx, const lcg_model *models,
+                                          int32_t nmodels, int32_t flags, double *sfac,
+                                          double *calc, double *chisq, double *wnok,
+                                          int32_t *status);
 
 /* ---- stage-level seams, for parity tests and integrations -------------- */
 

@@ -5,7 +5,7 @@ test (tests/test_abi.py) checks sizes and offsets against the header.
 """
 import ctypes as C
 
-LCG_ABI_VERSION = 1
+LCG_ABI_VERSION = 2
 
 # lcg_status
 OK, E_INVALID, E_LOBE, E_ROCHE, E_NOCONVERGE, E_UNSUPPORTED, E_CUDA, E_NOMEM, E_CAPACITY = range(9)
@@ -66,7 +66,7 @@ class LcgDatum(C.Structure):
 class LcgOptions(C.Structure):
     _fields_ = [
         ("device", C.c_int32), ("precision", C.c_int32), ("verbose", C.c_int32),
-        ("reserved", C.c_int32 * 5),
+        ("eclipse_warp", C.c_int32), ("reserved", C.c_int32 * 4),
     ]
 
 
@@ -106,6 +106,8 @@ PROTOTYPES = {
     "lcg_flux_elements": (C.c_int64, [P, C.c_int32]),
     "lcg_measure_fp32_peak": (C.c_int, [P, D]),
     "lcg_set_data": (C.c_int, [P, P, C.c_int32]),
+    "lcg_light_curve_batch_resident": (C.c_int, [P, C.POINTER(LcgModel), C.c_int32, C.c_int32,
+                                                 D, D, D, D, I32]),
     "lcg_light_curve_resident": (C.c_int, [P, C.POINTER(LcgModel), C.c_int32, D, D, D]),
     "lcg_device_calc": (P, [P]),
     "lcg_kernel_launches": (C.c_int64, [C.c_int32]),

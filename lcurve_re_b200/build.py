@@ -30,8 +30,9 @@ SOURCES = {
     "engine.cu": ["--fmad=false"],
     "flux.cu": ["--fmad=true"],
     "noalloc.cu": ["--fmad=false"],
+    "batch_host.cu": ["--fmad=false"],
 }
-HEADERS = ["roche.cuh", "eclipse.cuh", "engine.h", "tma.cuh"]
+HEADERS = ["roche.cuh", "eclipse.cuh", "engine.h", "tma.cuh", "context.h"]
 
 
 def nvcc():

@@ -1,0 +1,608 @@
+// batch_host.cu — batched evaluation of many models over the resident points
+// (lcg_light_curve_batch_resident).
+//
+// The MCMC and Levenberg-Marquardt callers evaluate light_curve_comp for
+// many parameter vectors over one data set (mcmc_solver.cpp:1062-1070,
+// levmarq_solver.cpp:789-886). One model's grids keep a B200 busy only at
+// the largest resolutions, so here all models of a batch go through every
+// stage together:
+//   * layout: the two star grids of model m are slots 2m and 2m+1; their
+//     faces are concatenated in one set of point arrays, their flat records
+//     start at multiples of 1024 faces, and their flux work is a list of
+//     (chunk, phase tile) CTAs over all slots;
+//   * the ring tables of grids without infill depend on nlat alone and are
+//     computed once per nlat (set_star_grid.cpp:241-320, numface.cpp);
+//   * per call, only the slots whose geometry (GeomKey) changed go through
+//     grid + eclipse, and only those whose continuum (ContKey) changed
+//     through continuum + partition (the per-model form of the exact-reuse
+//     cache, light_curve_comp.cpp:34-117);
+//   * the work lists and per-model parameters are one host table copied in
+//     one transfer, and the whole sequence is one CUDA graph, captured once
+//     per layout and replayed.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <map>
+#include <thread>
+#include <vector>
+
+#include "context.h"
+
+namespace lcg {
+namespace eng {
+
+namespace {
+
+constexpr int64_t kSlotAlign = 1024;  // flat records and partition blocks
+
+struct RingSet {
+    int32_t ring0, nrings;
+    int64_t nface, ntiled, nhalf;  // numface, the tiling's faces, half-faces
+};
+
+inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Runs f(i) for i in [0, n) on up to 16 host threads.
+template <class F>
+void parallel_for(int n, F f) {
+    int nt = (int)std::min<unsigned>(16u, std::max(1u, std::thread::hardware_concurrency()));
+    if (n < 32 || nt < 2) {
+        for (int i = 0; i < n; i++) f(i);
+        return;
+    }
+    nt = std::min(nt, n / 8);
+    std::vector<std::thread> th;
+    th.reserve(nt);
+    for (int t = 0; t < nt; t++)
+        th.emplace_back([&, t] {
+            for (int i = t; i < n; i += nt) f(i);
+        });
+    for (auto &x : th) x.join();
+}
+
+}  // namespace
+
+struct BatchState {
+    // layout key
+    int32_t nmodels = -1, n = 0, flags = 0, want_calc = 0;
+    int64_t nent = 0;
+    const void *data_p = nullptr;
+    std::vector<int32_t> nlat;  // nlat1f, nlat2f per model
+    // layout
+    int32_t nslots = 0;
+    int64_t nfaces = 0, nflat = 0, nblk = 0, ldp = 0;
+    FluxPlan plan{};
+    std::vector<int64_t> face0, flat0, blk0, chunk_pre;
+    std::vector<RingSet> slot_rings;
+    // ring pool, one table per nlat
+    std::map<int32_t, RingSet> ringsets;
+    std::vector<RingRec> h_rings;
+    DBuf<RingRec> rings;
+    // per-model exact-reuse keys
+    std::vector<lcg_model> key;
+    std::vector<uint8_t> key_ok;
+    // host table (pinned) and its device copy
+    unsigned char *h_tab = nullptr;
+    size_t tab_bytes = 0;
+    DBuf<unsigned char> d_tab;
+    size_t o_slots = 0, o_models = 0, o_face0 = 0, o_chunk = 0, o_counts = 0, o_geo_slot = 0,
+           o_geo_half = 0, o_geo_face = 0, o_cont_slot = 0, o_cont_face = 0, o_cont_blk = 0;
+    // device arrays
+    DBuf<double> px, py, pz, nx, ny, nz, ein, eout;
+    DBuf<float> area, grav, flux, fp;
+    DBuf<uint8_t> necl;
+    DBuf<uint2> ecl;
+    DBuf<int64_t> n0;
+    DBuf<int32_t> blockcnt, queue, counters;
+    DBuf<DevStatus> st;
+    DBuf<float4> ef;
+    DBuf<double> w1, w2, part, osum, calc, sfac, out;
+    // results (pinned): calc, sfac, out, status
+    unsigned char *h_res = nullptr;
+    size_t res_bytes = 0, r_calc = 0, r_sfac = 0, r_out = 0, r_st = 0;
+    cudaGraphExec_t exec = nullptr;
+    int64_t graph_kernels = 0;  // kernels per graph launch
+
+    template <class T>
+    T *tab(size_t off) { return reinterpret_cast<T *>(h_tab + off); }
+    template <class T>
+    T *res(size_t off) { return reinterpret_cast<T *>(h_res + off); }
+
+    void drop_graph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        exec = nullptr;
+    }
+    void free_all() {
+        drop_graph();
+        DBuf<double> *d[] = {&px, &py, &pz, &nx, &ny, &nz, &ein, &eout,
+                             &w1, &w2, &part, &osum, &calc, &sfac, &out};
+        for (auto *b : d) b->release();
+        area.release(); grav.release(); flux.release(); fp.release(); necl.release();
+        ecl.release(); n0.release(); blockcnt.release(); queue.release(); counters.release();
+        st.release(); ef.release(); rings.release(); d_tab.release();
+        if (h_tab) cudaFreeHost(h_tab);
+        if (h_res) cudaFreeHost(h_res);
+        h_tab = h_res = nullptr;
+    }
+
+    BatchDev dev() {
+        BatchDev b{};
+        unsigned char *d = d_tab.p;
+        b.slots = reinterpret_cast<const SlotDev *>(d + o_slots);
+        b.models = reinterpret_cast<const ModelDev *>(d + o_models);
+        b.face0 = reinterpret_cast<const int64_t *>(d + o_face0);
+        b.chunk_pre = reinterpret_cast<const int64_t *>(d + o_chunk);
+        b.rings = rings.p;
+        b.nslots = nslots;
+        b.nmodels = nmodels;
+        b.g = GridDev{px.p, py.p, pz.p, nx.p, ny.p, nz.p, area.p, grav.p, flux.p,
+                      necl.p, ein.p, eout.p, nfaces};
+        b.fp = fp.p;
+        b.ecl = ecl.p;
+        b.n0 = n0.p;
+        b.blockcnt = blockcnt.p;
+        b.queue = queue.p;
+        b.counters = counters.p;
+        b.st = st.p;
+        b.counts = reinterpret_cast<const int32_t *>(d + o_counts);
+        b.geo_slot = reinterpret_cast<const int32_t *>(d + o_geo_slot);
+        b.geo_half = reinterpret_cast<const int64_t *>(d + o_geo_half);
+        b.geo_face = reinterpret_cast<const int64_t *>(d + o_geo_face);
+        b.cont_slot = reinterpret_cast<const int32_t *>(d + o_cont_slot);
+        b.cont_face = reinterpret_cast<const int64_t *>(d + o_cont_face);
+        b.cont_blk = reinterpret_cast<const int64_t *>(d + o_cont_blk);
+        return b;
+    }
+    BatchPhases phases() { return BatchPhases{ef.p, w1.p, w2.p, ldp, nent}; }
+};
+
+void batch_release(BatchState *b) {
+    if (!b) return;
+    b->free_all();
+    delete b;
+}
+
+namespace {
+
+// Face count and ring table of a grid without infill (numface.cpp:14-52,
+// set_star_grid.cpp:241-320), added to the pool once per nlat.
+void ring_set(BatchState &B, int32_t nlat, RingSet &out) {
+    auto it = B.ringsets.find(nlat);
+    if (it != B.ringsets.end()) {
+        out = it->second;
+        return;
+    }
+    StarSetup s{};
+    s.nhalf = 0;
+    int nface = 0;
+    add_rings(kStar1, s, nface, 0., kPi, kPi / nlat, 0, 0);
+    RingSet r{(int32_t)B.h_rings.size(), (int32_t)s.rings.size(),
+              numface(nlat, false, 0., 0., 0, 0), nface, s.nhalf};
+    B.h_rings.insert(B.h_rings.end(), s.rings.begin(), s.rings.end());
+    B.ringsets[nlat] = r;
+    out = r;
+}
+
+// Lays out slots, records, flux chunks and the host table for a batch of
+// nmodels with the given grid resolutions, and (re)allocates everything.
+lcg_status relayout(lcg_ctx *c, BatchState &B, const lcg_model *models, int32_t nmodels,
+                    int32_t flags, int want_calc) {
+    B.drop_graph();
+    B.nmodels = nmodels;
+    B.n = c->data_n;
+    B.nent = c->data_nent;
+    B.data_p = c->data.p;
+    B.flags = flags;
+    B.want_calc = want_calc;
+    B.nslots = 2 * nmodels;
+    B.nlat.resize(2 * (size_t)nmodels);
+    B.slot_rings.resize(B.nslots);
+    B.face0.assign(B.nslots + 1, 0);
+    B.flat0.assign(B.nslots + 1, 0);
+    B.blk0.assign(B.nslots + 1, 0);
+    B.chunk_pre.assign(B.nslots + 1, 0);
+    const size_t nring_before = B.h_rings.size();
+    for (int32_t m = 0; m < nmodels; m++) {
+        B.nlat[2 * m] = models[m].nlat1f;
+        B.nlat[2 * m + 1] = models[m].nlat2f;
+        for (int k = 0; k < 2; k++) {
+            const int s = 2 * m + k;
+            RingSet r;
+            ring_set(B, B.nlat[s], r);
+            B.slot_rings[s] = r;
+            B.face0[s + 1] = B.face0[s] + r.nface;
+            B.flat0[s + 1] = B.flat0[s] + (int64_t)align_up((size_t)r.nface, kSlotAlign);
+            B.blk0[s + 1] = B.blk0[s] + (r.nface + kSlotAlign - 1) / kSlotAlign;
+        }
+    }
+    B.nfaces = B.face0[B.nslots];
+    B.nflat = B.flat0[B.nslots];
+    B.nblk = B.blk0[B.nslots];
+    if (B.nfaces >= (int64_t)0x7fffffff)
+        return c->fail(LCG_E_CAPACITY, "batch: %lld faces exceed the 2^31 face index",
+                       (long long)B.nfaces);
+    // flux plan: the single-grid plan for entries per thread and phase tiles;
+    // then the largest chunk (dividing 1024) that still fills the SMs
+    B.plan = plan_flux(1, 1, B.nfaces, B.nent, c->nsm);
+    int64_t chunk = 1024, total = 0;
+    const int64_t want = (int64_t)c->nsm * 4;
+    for (;;) {
+        total = 0;
+        for (int s = 0; s < B.nslots; s++)
+            total += (B.slot_rings[s].nface + chunk - 1) / chunk;
+        if (chunk <= 64 || total * B.plan.ntile >= want) break;
+        chunk >>= 1;
+    }
+    B.plan.chunk = chunk;
+    B.plan.nchunk = total;
+    if (total * B.plan.ntile >= (int64_t)0x7fffffff)
+        return c->fail(LCG_E_CAPACITY, "batch: too many flux tiles");
+    for (int s = 0; s < B.nslots; s++)
+        B.chunk_pre[s + 1] = B.chunk_pre[s] + (B.slot_rings[s].nface + chunk - 1) / chunk;
+    B.ldp = ((B.nent + 3) / 4) * 4;
+
+    // host table sections
+    size_t o = 0;
+    auto sect = [&](size_t bytes) {
+        const size_t at = o;
+        o = align_up(o + bytes, 256);
+        return at;
+    };
+    const size_t ns = (size_t)B.nslots;
+    B.o_slots = sect(ns * sizeof(SlotDev));
+    B.o_models = sect((size_t)nmodels * sizeof(ModelDev));
+    B.o_face0 = sect((ns + 1) * 8);
+    B.o_chunk = sect((ns + 1) * 8);
+    B.o_counts = sect(8);
+    B.o_geo_slot = sect(ns * 4);
+    B.o_geo_half = sect((ns + 1) * 8);
+    B.o_geo_face = sect((ns + 1) * 8);
+    B.o_cont_slot = sect(ns * 4);
+    B.o_cont_face = sect((ns + 1) * 8);
+    B.o_cont_blk = sect((ns + 1) * 8);
+    B.tab_bytes = o;
+    if (B.h_tab) cudaFreeHost(B.h_tab);
+    B.h_tab = nullptr;
+    cudaError_t e;
+    if ((e = cudaHostAlloc((void **)&B.h_tab, B.tab_bytes, cudaHostAllocDefault)))
+        return c->cuda_fail(e, "batch table");
+    memset(B.h_tab, 0, B.tab_bytes);
+    memcpy(B.tab<int64_t>(B.o_face0), B.face0.data(), (ns + 1) * 8);
+    memcpy(B.tab<int64_t>(B.o_chunk), B.chunk_pre.data(), (ns + 1) * 8);
+
+    // results
+    const size_t nm = (size_t)nmodels;
+    o = 0;
+    B.r_calc = sect(want_calc ? nm * (size_t)B.n * 8 : 0);
+    B.r_sfac = sect(nm * 5 * 8);
+    B.r_out = sect(nm * 3 * 8);
+    B.r_st = sect(nm * sizeof(DevStatus));
+    B.res_bytes = o;
+    if (B.h_res) cudaFreeHost(B.h_res);
+    B.h_res = nullptr;
+    if ((e = cudaHostAlloc((void **)&B.h_res, B.res_bytes, cudaHostAllocDefault)))
+        return c->cuda_fail(e, "batch results");
+
+    // device arrays
+    const size_t nf = (size_t)B.nfaces;
+    DBuf<double> *d[] = {&B.px, &B.py, &B.pz, &B.nx, &B.ny, &B.nz, &B.ein, &B.eout};
+    for (auto *b : d)
+        if ((e = b->ensure(nf))) return c->cuda_fail(e, "batch grids");
+    if ((e = B.area.ensure(nf)) || (e = B.grav.ensure(nf)) || (e = B.flux.ensure(nf)) ||
+        (e = B.necl.ensure(nf)) || (e = B.queue.ensure(nf)) ||
+        (e = B.fp.ensure(8 * (size_t)B.nflat)) || (e = B.ecl.ensure((size_t)B.nflat)) ||
+        (e = B.n0.ensure(ns)) || (e = B.blockcnt.ensure((size_t)B.nblk)) ||
+        (e = B.counters.ensure(2)) || (e = B.st.ensure(nm)) ||
+        (e = B.ef.ensure(nm * (size_t)B.ldp)) || (e = B.w1.ensure(nm * (size_t)B.ldp)) ||
+        (e = B.w2.ensure(nm * (size_t)B.ldp)) ||
+        (e = B.part.ensure((size_t)std::max<int64_t>(B.plan.nchunk, 1) * (size_t)B.ldp)) ||
+        (e = B.osum.ensure(ns * (size_t)B.ldp)) || (e = B.calc.ensure(nm * (size_t)B.n)) ||
+        (e = B.sfac.ensure(nm * 5)) || (e = B.out.ensure(nm * 3)) ||
+        (e = B.d_tab.ensure(B.tab_bytes)))
+        return c->cuda_fail(e, "batch buffers");
+    if (B.h_rings.size() != nring_before || !B.rings.p) {
+        if ((e = B.rings.ensure(B.h_rings.size()))) return c->cuda_fail(e, "ring pool");
+        cudaMemcpyAsync(B.rings.p, B.h_rings.data(), B.h_rings.size() * sizeof(RingRec),
+                        cudaMemcpyHostToDevice, c->stream);
+    }
+    // an odd pad record or a never-built slot must read as zeros
+    cudaMemsetAsync(B.fp.p, 0, 8 * (size_t)B.nflat * sizeof(float), c->stream);
+    cudaMemsetAsync(B.ecl.p, 0, (size_t)B.nflat * sizeof(uint2), c->stream);
+    cudaMemsetAsync(B.n0.p, 0, ns * sizeof(int64_t), c->stream);
+    B.key.assign(nm, lcg_model{});
+    B.key_ok.assign(nm, 0);
+    for (int s = 0; s < B.nslots; s++) {
+        SlotDev &S = B.tab<SlotDev>(B.o_slots)[s];
+        S.face0 = B.face0[s];
+        S.nface = B.slot_rings[s].nface;
+        S.ntiled = B.slot_rings[s].ntiled;
+        S.flat0 = B.flat0[s];
+        S.blk0 = B.blk0[s];
+        S.ring0 = B.slot_rings[s].ring0;
+        S.model = s / 2;
+    }
+    return LCG_OK;
+}
+
+bool same_layout(const BatchState &B, const lcg_ctx *c, const lcg_model *models,
+                 int32_t nmodels, int32_t flags, int want_calc) {
+    if (B.nmodels != nmodels || B.n != c->data_n || B.nent != c->data_nent ||
+        B.data_p != (const void *)c->data.p || B.flags != flags || B.want_calc != want_calc)
+        return false;
+    for (int32_t m = 0; m < nmodels; m++)
+        if (B.nlat[2 * m] != models[m].nlat1f || B.nlat[2 * m + 1] != models[m].nlat2f)
+            return false;
+    return true;
+}
+
+// Models the batched path covers: the fast mixed sweep applies to both stars
+// and each star has a single grid (coarse = fine, no infill).
+bool batchable(const lcg_model &m) {
+    return m.beam_factor1 == 0. && m.beam_factor2 == 0. && !m.glens1 && m.mucrit1 <= 0. &&
+           m.mucrit2 <= 0. && m.nlat1c == m.nlat1f && m.nlat2c == m.nlat2f &&
+           (!m.npole || (m.nlatfill == 0 && m.nlngfill == 0));
+}
+
+// The stages of one batch on the context's stream.
+void enqueue(lcg_ctx *c, BatchState &B, bool timed) {
+    cudaStream_t s = c->stream;
+    const BatchDev b = B.dev();
+    const BatchPhases ph = B.phases();
+    cudaMemcpyAsync(B.d_tab.p, B.h_tab, B.tab_bytes, cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(B.st.p, 0, (size_t)B.nmodels * sizeof(DevStatus), s);
+    auto stage = [&](int id, auto &&fn) {
+        Timer t;
+        if (timed) c->stage_begin(id, t);
+        fn();
+        if (timed) c->stage_end(id, t);
+    };
+    stage(LCG_STAGE_GRID, [&] { launch_batch_grid(b, c->nsm, s); });
+    stage(LCG_STAGE_ECLIPSE, [&] { launch_batch_eclipse(b, c->nsm, c->eclipse_warp, s); });
+    stage(LCG_STAGE_CONTINUUM, [&] { launch_batch_continuum(b, c->nsm, s); });
+    stage(LCG_STAGE_FLATTEN, [&] { launch_batch_flatten(b, c->nsm, s); });
+    stage(LCG_STAGE_PHASES, [&] { launch_batch_phases(b, c->data.p, c->off.p, B.n, ph, s); });
+    stage(LCG_STAGE_FLUX, [&] { launch_batch_flux(b, ph, B.plan, B.part.p, B.ldp, s); });
+    stage(LCG_STAGE_REDUCE, [&] {
+        launch_batch_reduce(b, ph, B.part.p, B.ldp, B.osum.p, c->data.p, c->off.p, B.n,
+                            B.flags & 3, B.calc.p, B.sfac.p, B.out.p, s);
+    });
+    const size_t nm = (size_t)B.nmodels;
+    if (B.want_calc)
+        cudaMemcpyAsync(B.h_res + B.r_calc, B.calc.p, nm * (size_t)B.n * 8,
+                        cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(B.h_res + B.r_sfac, B.sfac.p, nm * 5 * 8, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(B.h_res + B.r_out, B.out.p, nm * 3 * 8, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(B.h_res + B.r_st, B.st.p, nm * sizeof(DevStatus), cudaMemcpyDeviceToHost,
+                    s);
+}
+
+}  // namespace
+}  // namespace eng
+}  // namespace lcg
+
+using namespace lcg;
+using namespace lcg::eng;
+
+extern "C" lcg_status lcg_light_curve_batch_resident(lcg_ctx *c, const lcg_model *models,
+                                                     int32_t nmodels, int32_t flags,
+                                                     double *sfac, double *calc, double *chisq,
+                                                     double *wnok, int32_t *status) {
+    if (!c) return LCG_E_INVALID;
+    c->err.clear();
+    if (!models || nmodels < 0 || !sfac || !status) return c->fail(LCG_E_INVALID, "null argument");
+    if (c->data_n < 1) return c->fail(LCG_E_INVALID, "no data: call lcg_set_data first");
+    if (nmodels == 0) return LCG_OK;
+    cudaSetDevice(c->device);
+    const int32_t n = c->data_n;
+    flags &= ~LCG_FLAG_DIAGNOSTICS;
+
+    // which models go through the batch; the rest are evaluated one by one
+    std::vector<uint8_t> inb((size_t)nmodels, 0);
+    int32_t nb = 0;
+    for (int32_t m = 0; m < nmodels; m++) {
+        lcg_status rc = check_model(c, models + m);
+        status[m] = rc;
+        if (rc) continue;
+        if (c->precision == LCG_PREC_MIXED && batchable(models[m])) {
+            inb[m] = 1;
+            nb++;
+        }
+    }
+    c->err.clear();
+    if (nb > 0) {
+        if (!c->batch) c->batch = new BatchState();
+        BatchState &B = *c->batch;
+        const int want_calc = calc != nullptr;
+        lcg_status rc;
+        if (!same_layout(B, c, models, nmodels, flags, want_calc) &&
+            (rc = relayout(c, B, models, nmodels, flags, want_calc))) {
+            B.nmodels = -1;
+            return rc;
+        }
+        // per-model host setup; geometry and continuum only where changed
+        SlotDev *slots = B.tab<SlotDev>(B.o_slots);
+        ModelDev *md = B.tab<ModelDev>(B.o_models);
+        std::vector<uint8_t> geo((size_t)nmodels, 0), cont((size_t)nmodels, 0);
+        const double xmin = c->data_xmin, xmax = c->data_xmax;
+        parallel_for(nmodels, [&](int m) {
+            const lcg_model &M = models[m];
+            ModelDev &D = md[m];
+            SlotDev *S = slots + 2 * m;
+            D.live = 0;
+            S[0].live = S[1].live = 0;
+            if (!inb[m]) return;
+            // light_curve_comp.cpp:130-154
+            double r1, r2;
+            get_r1r2(M, r1, r2);
+            const double xl2 = xl12(M.q, M.spin2);
+            if (xl2 < 0) {
+                status[m] = LCG_E_NOCONVERGE;
+                return;
+            }
+            if (r2 >= 0 && r2 > 1. - xl2) {
+                status[m] = LCG_E_LOBE;
+                return;
+            }
+            const bool g = !B.key_ok[m] || !same_geometry(B.key[m], M);
+            const bool k = g || !same_continuum(B.key[m], M);
+            if (g) {
+                for (int star = 0; star < 2; star++) {
+                    StarSetup su{};
+                    Fail f{0, ""};
+                    if (!prepare_star(M, star, 1, su, f, false)) {
+                        status[m] = f.code;
+                        return;
+                    }
+                    SlotDev &X = S[star];
+                    const RingSet &R = B.slot_rings[2 * m + star];
+                    GridParams &gp = X.gp;
+                    gp.star = star;
+                    gp.roche = star == kStar1 ? M.roche1 : M.roche2;
+                    gp.npole = M.npole;
+                    gp.nrings = R.nrings;
+                    gp.nhalf = R.nhalf;
+                    gp.q = M.q;
+                    gp.spin = star == kStar1 ? M.spin1 : M.spin2;
+                    gp.rref = star == kStar1 ? su.rref1 : su.rref2;
+                    gp.pref = star == kStar1 ? su.pref1 : su.pref2;
+                    gp.acc = M.delta_phase / 10.;
+                    gp.gref = su.gref;
+                    gp.rad_sphere = star == kStar1 ? su.r1 : su.r2;
+                    EclParams &ep = X.ep;
+                    ep.comp_star = star == kStar1 ? kStar2 : kStar1;
+                    ep.comp_roche = star == kStar1 ? M.roche2 : M.roche1;
+                    ep.q = M.q;
+                    ep.comp_spin = star == kStar1 ? M.spin2 : M.spin1;
+                    ep.comp_rref = star == kStar1 ? su.rref2 : su.rref1;
+                    ep.comp_pref = star == kStar1 ? su.pref2 : su.pref1;
+                    ep.comp_r = star == kStar1 ? su.r2 : su.r1;
+                    const double ri = deg2rad(M.iangle);
+                    ep.cosi = cos(ri);
+                    ep.sini = sin(ri);
+                    ep.delta = M.delta_phase;
+                    X.eclipse_on = su.eclipse;
+                }
+            }
+            if (k) {
+                for (int star = 0; star < 2; star++) {
+                    S[star].cp = continuum_params(M, star);
+                    S[star].fc = fast_coef(M, star, 1);
+                }
+            }
+            PhaseParams &pp = D.pp;
+            pp.t0 = M.t0; pp.period = M.period; pp.pdot = M.pdot; pp.deltat = M.deltat;
+            pp.slope = M.slope; pp.quad = M.quad; pp.cube = M.cube;
+            pp.middle = (xmin + xmax) / 2.;
+            pp.range = (xmax - xmin) / 2.;
+            const double ri = deg2rad(M.iangle);
+            pp.cosi = cos(ri);
+            pp.sini = sin(ri);
+            pp.gi = Ginterp{M.phase1, M.phase2, 1., 1., 1., 1.};
+            D.third = M.third;
+            D.sfac0 = sfac[5 * (size_t)m];
+            D.live = 1;
+            S[0].live = S[1].live = 1;
+            geo[m] = g;
+            cont[m] = k;
+        });
+        // work lists
+        int32_t *counts = B.tab<int32_t>(B.o_counts);
+        int32_t *gs = B.tab<int32_t>(B.o_geo_slot), *cs = B.tab<int32_t>(B.o_cont_slot);
+        int64_t *gh = B.tab<int64_t>(B.o_geo_half), *gf = B.tab<int64_t>(B.o_geo_face);
+        int64_t *cf = B.tab<int64_t>(B.o_cont_face), *cb = B.tab<int64_t>(B.o_cont_blk);
+        int32_t ng = 0, nc = 0;
+        gh[0] = gf[0] = cf[0] = cb[0] = 0;
+        for (int32_t m = 0; m < nmodels; m++) {
+            if (!md[m].live) continue;
+            for (int star = 0; star < 2; star++) {
+                const int s = 2 * m + star;
+                const RingSet &R = B.slot_rings[s];
+                if (geo[m]) {
+                    gs[ng] = s;
+                    gh[ng + 1] = gh[ng] + R.nhalf;
+                    gf[ng + 1] = gf[ng] + R.nface;
+                    ng++;
+                }
+                if (cont[m]) {
+                    cs[nc] = s;
+                    cf[nc + 1] = cf[nc] + R.nface;
+                    cb[nc + 1] = cb[nc] + (R.nface + kSlotAlign - 1) / kSlotAlign;
+                    nc++;
+                }
+            }
+        }
+        counts[0] = ng;
+        counts[1] = nc;
+
+        cudaError_t e;
+        if (c->profiling) {
+            enqueue(c, B, true);
+        } else {
+            if (!B.exec) {
+                cudaGraph_t graph = nullptr;
+                if ((e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal)))
+                    return c->cuda_fail(e, "batch capture");
+                const int64_t k0 = lcg_kernel_launches(0);
+                enqueue(c, B, false);
+                B.graph_kernels = lcg_kernel_launches(0) - k0;
+                count_launches(-B.graph_kernels);  // counted when the graph runs
+                e = cudaStreamEndCapture(c->stream, &graph);
+                if (e == cudaSuccess) e = cudaGraphInstantiate(&B.exec, graph, 0);
+                if (graph) cudaGraphDestroy(graph);
+                if (e) {
+                    B.exec = nullptr;
+                    return c->cuda_fail(e, "batch graph");
+                }
+            }
+            if ((e = cudaGraphLaunch(B.exec, c->stream))) return c->cuda_fail(e, "batch launch");
+            count_launches(B.graph_kernels);
+        }
+        if ((e = cudaStreamSynchronize(c->stream))) {
+            c->collect_timers();
+            B.nmodels = -1;  // relayout (and re-key every model) next time
+            return c->cuda_fail(e, "batch");
+        }
+        c->collect_timers();
+        const DevStatus *dst = B.res<DevStatus>(B.r_st);
+        const double *hs = B.res<double>(B.r_sfac), *ho = B.res<double>(B.r_out);
+        const double *hc = B.res<double>(B.r_calc);
+        for (int32_t m = 0; m < nmodels; m++) {
+            if (!inb[m]) continue;
+            if (!md[m].live || dst[m].code) {
+                if (!status[m]) status[m] = dst[m].code;
+                B.key_ok[m] = 0;
+                if (calc) memset(calc + (size_t)m * n, 0, (size_t)n * sizeof(double));
+                continue;
+            }
+            B.key[m] = models[m];
+            B.key_ok[m] = 1;
+            if (calc) memcpy(calc + (size_t)m * n, hc + (size_t)m * n, (size_t)n * sizeof(double));
+            for (int k = 0; k < 5; k++) sfac[5 * (size_t)m + k] = hs[5 * (size_t)m + k];
+            if (ho[3 * m + 2] != 0.) {
+                if (chisq) chisq[m] = ho[3 * m];
+                if (wnok) wnok[m] = ho[3 * m + 1];
+            }
+        }
+        c->flux_elements += B.nfaces * B.nent;
+    }
+    // the rest, one at a time
+    for (int32_t m = 0; m < nmodels; m++) {
+        if (inb[m] || status[m]) continue;
+        double sc[LCG_NOUT] = {0};
+        if (chisq) sc[LCG_OUT_CHISQ] = chisq[m];
+        if (wnok) sc[LCG_OUT_WNOK] = wnok[m];
+        lcg_status rc = lcg_light_curve_resident(c, models + m, flags, sfac + 5 * (size_t)m,
+                                                 calc ? calc + (size_t)m * n : nullptr, sc);
+        status[m] = rc;
+        if (rc) {
+            if (calc) memset(calc + (size_t)m * n, 0, (size_t)n * sizeof(double));
+            if (rc == LCG_E_CUDA || rc == LCG_E_NOMEM) return rc;
+            continue;
+        }
+        if (chisq) chisq[m] = sc[LCG_OUT_CHISQ];
+        if (wnok) wnok[m] = sc[LCG_OUT_WNOK];
+    }
+    c->err.clear();
+    return LCG_OK;
+}

@@ -391,3 +391,115 @@ __device__ bool ingress_egress(int star, double q, double spin, double cosi, dou
 }
 
 }  // namespace lcg
+
+namespace lcg {
+
+// Warp-cooperative Roche::ingress_egress, for grids with few eclipse
+// candidates, where one thread per face leaves the GPU idle. Lane 0 runs the
+// sphere test and pot_min; then lanes 0-15 bisect the ingress and lanes 16-31
+// the egress. Each half evaluates at once the 15 midpoints of the next four
+// bisection steps (a complete binary tree of brackets in heap order: child 2n
+// is "not hidden", pout = mid; child 2n+1 is "hidden", pin = mid) and then
+// follows the path the results select. Each midpoint is computed from the
+// same bracket by the same arithmetic as the sequential loop
+// (ingress_egress.cpp:61-86), and fblink has no state, so the phases are
+// identical to the sequential ones; only failures on the taken path count.
+// All 32 lanes must call this with the same face.
+__device__ bool ingress_egress_warp(int star, double q, double spin, double cosi, double sini,
+                                    double delta, V3 r, double rref, double pref,
+                                    double &ingress, double &egress, int &st) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int half = lane >> 4;
+    const int node = (lane & 15) + 1;  // 1..16; node 16 has nothing to evaluate
+    const V3 cofm = star == kStar1 ? v3(0., 0., 0.) : v3(1., 0., 0.);
+    double phi1 = 0., phi2 = 0., lam1 = 0., lam2 = 0., phi = 0., lam = 0., ACC = 0.;
+    int ok = 0, s0 = 0;
+    if (lane == 0) {
+        if (sphere_eclipse_ph(cosi, sini, r, cofm, rref, phi1, phi2, lam1, lam2)) {
+            ACC = 2. * sqrt(2. * kTwoPi * (lam2 - lam1) * delta);
+            ok = pot_min(star, q, spin, cosi, sini, r, phi1, phi2, lam1, lam2, rref, pref, ACC, phi,
+                         lam, s0) ? 1 : 0;
+        }
+    }
+    ok = __shfl_sync(full, ok, 0);
+    s0 = __shfl_sync(full, s0, 0);
+    if (s0) {
+        st = s0;
+        return false;
+    }
+    if (!ok) return false;
+    phi = __shfl_sync(full, phi, 0);
+    phi1 = __shfl_sync(full, phi1, 0);
+    phi2 = __shfl_sync(full, phi2, 0);
+    ACC = __shfl_sync(full, ACC, 0);
+    double pin = phi, pout = half ? phi2 : phi1;
+    const int depth = 31 - __clz(node);
+    int fail = 0;  // uniform within a half: the status of a failed node on its path
+    for (int round = 0;; round++) {
+        const bool live = fabs(pin - pout) > delta && fail == 0;
+        if (!__any_sync(full, live)) break;
+        if (round >= 100) {  // uniform: every lane counts the same rounds
+            st = kEclNoConverge;
+            return false;
+        }
+        // this lane's bracket: replay the path below the root
+        double a = pin, b = pout;
+        bool valid = node < 16 && live;
+        for (int lev = depth - 1; lev >= 0 && valid; lev--) {
+            if (!(fabs(a - b) > delta)) {
+                valid = false;
+                break;
+            }
+            const double mid = (a + b) / 2.;
+            if ((node >> lev) & 1) a = mid;
+            else b = mid;
+        }
+        if (valid && !(fabs(a - b) > delta)) valid = false;
+        int ls = 0;
+        bool hidden = false;
+        if (valid)
+            hidden = fblink(star, q, spin, ACC, set_earth(cosi, sini, (a + b) / 2.), r, rref, pref,
+                            ls);
+        const unsigned res = __ballot_sync(full, hidden);
+        const unsigned bad = __ballot_sync(full, ls != 0);
+        // follow the taken path (the same in every lane of a half)
+        int bad_src = -1;
+        if (live) {
+            int n = 1;
+            for (int lev = 0; lev < 4; lev++) {
+                if (!(fabs(pin - pout) > delta)) break;
+                const int src = half * 16 + n - 1;
+                if ((bad >> src) & 1u) {
+                    bad_src = src;
+                    break;
+                }
+                const double mid = (pin + pout) / 2.;
+                const int h = (res >> src) & 1u;
+                if (h) pin = mid;
+                else pout = mid;
+                n = 2 * n + h;
+            }
+        }
+        const int code = __shfl_sync(full, ls, bad_src >= 0 ? bad_src : lane);
+        if (bad_src >= 0) fail = code;
+    }
+    // the sequential routine bisects the ingress first: its failure wins
+    const int fail_i = __shfl_sync(full, fail, 0), fail_e = __shfl_sync(full, fail, 16);
+    if (fail_i || fail_e) {
+        st = fail_i ? fail_i : fail_e;
+        return false;
+    }
+    const double other_pin = __shfl_xor_sync(full, pin, 16);
+    const double other_pout = __shfl_xor_sync(full, pout, 16);
+    const double pin_i = half ? other_pin : pin, pout_i = half ? other_pout : pout;
+    const double pin_e = half ? pin : other_pin, pout_e = half ? pout : other_pout;
+    ingress = (pin_i + pout_i) / 2.;
+    ingress = ingress - floor(ingress);
+    egress = (pin_e + pout_e) / 2.;
+    egress = egress - floor(egress);
+    if (egress < ingress) egress++;
+    return true;
+}
+
+}  // namespace lcg

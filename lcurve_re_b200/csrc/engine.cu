@@ -19,37 +19,20 @@
 #include <string>
 #include <vector>
 
-#include "lcg.h"
-#include "engine.h"
+#include "context.h"
 
 using namespace lcg;
+using namespace lcg::eng;
 
 namespace {
 
 thread_local std::string g_create_error;
 std::atomic<long long> g_launches{0};
 
-template <class T>
-struct DBuf {
-    T *p = nullptr;
-    size_t cap = 0;
-    cudaError_t ensure(size_t n) {
-        if (n == 0) n = 1;
-        if (n <= cap) return cudaSuccess;
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-        cudaError_t e = cudaMalloc((void **)&p, n * sizeof(T));
-        if (e != cudaSuccess) return e;
-        cap = n;
-        return cudaSuccess;
-    }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        cap = 0;
-    }
-};
+}  // namespace
+
+namespace lcg {
+namespace eng {
 
 // ---- per-model host setup ---------------------------------------------------
 
@@ -116,19 +99,6 @@ int numface(int nlat, bool infill, double thelo, double thehi, int nlatfill, int
     return nface;
 }
 
-struct StarSetup {
-    double r1, r2, rl1, rl2, ffac1, ffac2, rref1, pref1, rref2, pref2, gref;
-    int infill, nlat, nlatfill, nlngfill, eclipse;
-    double thelo, thehi;
-    int nface;
-    int64_t nhalf;
-    std::vector<RingRec> rings;
-};
-
-struct Fail {
-    int code;
-    std::string msg;
-};
 
 // Appends the rings of one add_faces call (set_star_grid.cpp:241-320).
 bool add_rings(int star, StarSetup &s, int &nface, double tlo, double thi, double dtheta,
@@ -188,7 +158,7 @@ bool add_rings(int star, StarSetup &s, int &nface, double tlo, double thi, doubl
 }
 
 // set_star_grid.cpp:49-223 up to the tiling.
-bool prepare_star(const lcg_model &m, int star, int fine, StarSetup &s, Fail &f) {
+bool prepare_star(const lcg_model &m, int star, int fine, StarSetup &s, Fail &f, bool tiling) {
     double r1, r2;
     get_r1r2(m, r1, r2);
     s.eclipse = star == kStar1 ? m.eclipse1 : m.eclipse2;
@@ -273,7 +243,7 @@ bool prepare_star(const lcg_model &m, int star, int fine, StarSetup &s, Fail &f)
     s.infill = infill;
     s.thelo = thelo;
     s.thehi = thehi;
-    s.nface = numface(s.nlat, infill, thelo, thehi, s.nlatfill, s.nlngfill);
+    s.nface = tiling ? numface(s.nlat, infill, thelo, thehi, s.nlatfill, s.nlngfill) : 0;
 
     const double ACC = m.delta_phase / 10.;
     V3 posn, dvec;
@@ -290,6 +260,7 @@ bool prepare_star(const lcg_model &m, int star, int fine, StarSetup &s, Fail &f)
         return false;
     }
     s.gref = gref;
+    if (!tiling) return true;
 
     s.rings.clear();
     s.nhalf = 0;
@@ -302,169 +273,11 @@ bool prepare_star(const lcg_model &m, int star, int fine, StarSetup &s, Fail &f)
     } else {
         add_rings(star, s, nface, 0., kPi, dtheta, 0, 0);
     }
-    if (nface != s.nface) {
-        char b[160];
-        snprintf(b, sizeof b, "set_star_grid: ring tiling gives %d faces but numface gives %d",
-                 nface, s.nface);
-        f = {LCG_E_INVALID, b};
-        return false;
-    }
+    // the ring tiling can differ from numface by a face or two (nlat 153, 297,
+    // 315, 333, 339, 813, ...); the grid keeps numface faces (GridDev)
+    s.ntiled = nface;
     return true;
 }
-
-// ---- the context ------------------------------------------------------------
-
-struct Grid {
-    DBuf<double> px, py, pz, nx, ny, nz, ein, eout;
-    DBuf<float> area, grav, flux;
-    DBuf<uint8_t> necl;
-    DBuf<RingRec> rings;
-    // flat
-    DBuf<int64_t> n0;
-    DBuf<float4> geo, pos;
-    DBuf<uint2> ecl;
-    DBuf<double> fdx, fdy, fdz, fpx, fpy, fpz, fflux, fin, fout;
-    DBuf<float> fp;
-    int64_t n = 0, npad = 0;
-    int fast = 0;  // flat records built for the fast mixed sweep
-    StarSetup setup;
-
-    cudaError_t alloc_points(int64_t nf) {
-        n = nf;
-        cudaError_t e = cudaSuccess;
-        DBuf<double> *d[] = {&px, &py, &pz, &nx, &ny, &nz, &ein, &eout};
-        for (auto *b : d)
-            if ((e = b->ensure(nf)) != cudaSuccess) return e;
-        if ((e = area.ensure(nf)) || (e = grav.ensure(nf)) || (e = flux.ensure(nf)) ||
-            (e = necl.ensure(nf)))
-            return e;
-        return cudaSuccess;
-    }
-    cudaError_t alloc_flat(int mixed, int need_pos, int fast_on) {
-        npad = ((n + 4095) / 4096) * 4096;
-        if (npad == 0) npad = 4096;
-        cudaError_t e = n0.ensure(1);
-        if (e) return e;
-        if (mixed) {
-            if ((e = ecl.ensure(npad))) return e;
-            if (fast_on) {
-                if ((e = fp.ensure(8 * npad))) return e;
-            } else if ((e = geo.ensure(npad))) {
-                return e;
-            }
-            if (need_pos && (e = pos.ensure(npad))) return e;
-        } else {
-            DBuf<double> *d[] = {&fdx, &fdy, &fdz, &fpx, &fpy, &fpz, &fflux, &fin, &fout};
-            for (auto *b : d)
-                if ((e = b->ensure(npad)) != cudaSuccess) return e;
-        }
-        return cudaSuccess;
-    }
-    GridDev dev() const {
-        return GridDev{px.p, py.p, pz.p, nx.p, ny.p, nz.p, area.p, grav.p, flux.p,
-                       necl.p, ein.p, eout.p, n};
-    }
-    FlatDev flat() const {
-        return FlatDev{n, npad, n0.p, geo.p, ecl.p, pos.p, fdx.p, fdy.p, fdz.p,
-                       fpx.p, fpy.p, fpz.p, fflux.p, fin.p, fout.p, fp.p};
-    }
-    void release() {
-        DBuf<double> *d[] = {&px, &py, &pz, &nx, &ny, &nz, &ein, &eout, &fdx, &fdy,
-                             &fdz, &fpx, &fpy, &fpz, &fflux, &fin, &fout};
-        for (auto *b : d) b->release();
-        area.release(); grav.release(); flux.release(); necl.release(); rings.release();
-        n0.release(); geo.release(); pos.release(); ecl.release(); fp.release();
-    }
-};
-
-struct Timer {
-    cudaEvent_t a = nullptr, b = nullptr;
-};
-
-}  // namespace
-
-struct lcg_ctx {
-    int device = 0, precision = LCG_PREC_MIXED, verbose = 0, nsm = 148;
-    cudaStream_t stream = nullptr;
-    std::string err;
-    // exact-reuse cache
-    bool has_geom = false, has_cont = false;
-    lcg_model key{};
-    int cached_mixed_pos = -1;
-    bool copy1 = true, copy2 = true;
-    Ginterp gi{};
-    Grid g1f, g2f, g1c, g2c;
-    // work buffers
-    DBuf<DevStatus> status;
-    DBuf<int32_t> queue, counters, blockcnt;
-    DBuf<DatumRec> data;
-    DBuf<int64_t> off;
-    DBuf<double> pex, pey, pez, pphin, pw1, pw2, part1f, part1c, part2f, part2c, calc, scratch,
-        sfac, out, diag, osum;
-    DBuf<float4> pef;
-    DBuf<uint8_t> ptype;
-    std::vector<int64_t> h_off;
-    std::vector<double> h_diag;
-    // resident light-curve points (lcg_set_data)
-    int32_t data_n = 0;
-    int64_t data_nent = 0;
-    double data_xmin = 0., data_xmax = 0.;
-    // profiling
-    bool profiling = false;
-    std::vector<Timer> pending[LCG_NSTAGE];
-    double stage_ms[LCG_NSTAGE] = {0};
-    int64_t stage_n[LCG_NSTAGE] = {0};
-    int64_t flux_elements = 0;
-
-    lcg_status fail(int code, const char *fmt, ...) {
-        char b[512];
-        va_list ap;
-        va_start(ap, fmt);
-        vsnprintf(b, sizeof b, fmt, ap);
-        va_end(ap);
-        err = b;
-        return (lcg_status)code;
-    }
-    lcg_status cuda_fail(cudaError_t e, const char *what) {
-        return fail(e == cudaErrorMemoryAllocation ? LCG_E_NOMEM : LCG_E_CUDA, "%s: %s", what,
-                    cudaGetErrorString(e));
-    }
-    void stage_begin(int s, Timer &t) {
-        if (!profiling) return;
-        cudaEventCreate(&t.a);
-        cudaEventCreate(&t.b);
-        cudaEventRecord(t.a, stream);
-        (void)s;
-    }
-    void stage_end(int s, Timer &t) {
-        if (!profiling) return;
-        cudaEventRecord(t.b, stream);
-        pending[s].push_back(t);
-    }
-    void collect_timers() {
-        for (int s = 0; s < LCG_NSTAGE; s++) {
-            for (auto &t : pending[s]) {
-                float ms = 0.f;
-                cudaEventElapsedTime(&ms, t.a, t.b);
-                stage_ms[s] += ms;
-                stage_n[s] += 1;
-                cudaEventDestroy(t.a);
-                cudaEventDestroy(t.b);
-            }
-            pending[s].clear();
-        }
-    }
-};
-
-namespace {
-
-struct StageScope {
-    lcg_ctx *c;
-    int s;
-    Timer t;
-    StageScope(lcg_ctx *c_, int s_) : c(c_), s(s_) { c->stage_begin(s, t); }
-    ~StageScope() { c->stage_end(s, t); }
-};
 
 const char *status_text(int code) {
     switch (code) {
@@ -600,6 +413,7 @@ lcg_status build_geometry(lcg_ctx *c, const lcg_model &m, int star, int fine, Gr
     const StarSetup &s = g.setup;
     cudaError_t e;
     if ((e = g.alloc_points(s.nface)) != cudaSuccess) return c->cuda_fail(e, "grid allocation");
+    g.ntiled = s.ntiled;
     if ((e = g.rings.ensure(s.rings.size())) != cudaSuccess) return c->cuda_fail(e, "rings");
     cudaMemcpyAsync(g.rings.p, s.rings.data(), s.rings.size() * sizeof(RingRec),
                     cudaMemcpyHostToDevice, c->stream);
@@ -636,7 +450,7 @@ lcg_status build_geometry(lcg_ctx *c, const lcg_model &m, int star, int fine, Gr
     {
         StageScope t(c, LCG_STAGE_ECLIPSE);
         launch_eclipse(ep, s.eclipse, g.dev(), c->queue.p, c->counters.p, c->status.p, c->nsm,
-                       c->stream);
+                       c->eclipse_warp, c->stream);
     }
     return LCG_OK;
 }
@@ -784,9 +598,11 @@ lcg_status finish_status(lcg_ctx *c) {
     return LCG_OK;
 }
 
-}  // namespace
+}  // namespace eng
+}  // namespace lcg
 
 void lcg::count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void lcg::count_launches(int64_t k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
 
 // ---- C ABI --------------------------------------------------------------------
 
@@ -831,6 +647,7 @@ lcg_status lcg_create(lcg_ctx **out, const lcg_options *opt) {
     c->device = o.device;
     c->precision = o.precision == LCG_PREC_FP64 ? LCG_PREC_FP64 : LCG_PREC_MIXED;
     c->verbose = o.verbose;
+    c->eclipse_warp = o.eclipse_warp;
     c->nsm = prop.multiProcessorCount;
     if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess ||
         (e = c->status.ensure(1)) != cudaSuccess || (e = c->counters.ensure(2)) != cudaSuccess ||
@@ -863,6 +680,8 @@ void lcg_destroy(lcg_ctx *c) {
     for (auto *b : d) b->release();
     c->status.release(); c->queue.release(); c->counters.release(); c->blockcnt.release();
     c->data.release(); c->off.release(); c->pef.release(); c->ptype.release();
+    batch_release(c->batch);
+    c->batch = nullptr;
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -1203,20 +1022,8 @@ lcg_status lcg_light_curve_batch(lcg_ctx *c, const lcg_model *models, int32_t nm
         return c->fail(LCG_E_INVALID, "null argument");
     lcg_status rs = lcg_set_data(c, data, n);
     if (rs) return rs;
-    for (int32_t i = 0; i < nmodels; i++) {
-        double sc[LCG_NOUT] = {0};
-        lcg_status rc = lcg_light_curve_resident(c, models + i, flags & ~LCG_FLAG_DIAGNOSTICS,
-                                                 sfac + 5 * (size_t)i, calc + (size_t)i * n, sc);
-        status[i] = rc;
-        if (rc) {
-            memset(calc + (size_t)i * n, 0, (size_t)n * sizeof(double));
-            if (rc == LCG_E_CUDA || rc == LCG_E_NOMEM) return rc;
-        }
-        if (chisq) chisq[i] = sc[LCG_OUT_CHISQ];
-        if (wnok) wnok[i] = sc[LCG_OUT_WNOK];
-    }
-    c->err.clear();
-    return LCG_OK;
+    return lcg_light_curve_batch_resident(c, models, nmodels, flags, sfac, calc, chisq, wnok,
+                                          status);
 }
 
 lcg_status lcg_star_face_count(lcg_ctx *c, const lcg_model *m, int32_t star, int32_t fine,

@@ -12,6 +12,7 @@ namespace lcg {
 // Number of kernels this library has launched (all contexts); read by
 // lcg_kernel_launches.
 void count_launch();
+void count_launches(int64_t k);
 
 // One latitude ring of a star grid (set_star_grid.cpp:280-320), computed on
 // the host with the reference's libm so ring sizes match exactly.
@@ -21,12 +22,15 @@ struct RingRec {
 };
 
 // Point-order star grid on the device (the reference's vector<Point>).
+// n is the reference's face count (numface, the length of its vector);
+// faces [ntiled, n) are default Points (no tiled face lands there) and the
+// tiling's faces past n are dropped, as the reference's vector holds them.
 struct GridDev {
     double *px, *py, *pz, *nx, *ny, *nz;
     float *area, *grav, *flux;
     uint8_t *necl;
     double *ein, *eout;
-    int64_t n;
+    int64_t n, ntiled;
 };
 
 struct GridParams {
@@ -127,11 +131,81 @@ struct ReduceParams {
     double *osum[4];
 };
 
+// ---- batched evaluation -----------------------------------------------------
+// A batch evaluates many models over the same resident points. Each model has
+// two star grids ("slots" 2m and 2m+1); the faces of all slots live in one set
+// of point arrays, the flat records of slot s start at a multiple of 1024
+// faces, and every stage walks a work list of slots instead of launching per
+// grid. Only the fast mixed sweep is batched (no beaming, lensing, mucrit > 0,
+// coarse grids or infill).
+struct SlotDev {
+    GridParams gp;
+    EclParams ep;
+    ContParams cp;
+    FastCoef fc;
+    int64_t face0;  // first face in the batch point arrays
+    int64_t nface, ntiled;
+    int64_t flat0;  // first face of the slot's flat records (a multiple of 1024)
+    int64_t blk0;   // first 1024-face partition block
+    int32_t ring0;  // first ring of the slot's table in the ring pool
+    int32_t model, eclipse_on, live;
+};
+
+struct ModelDev {
+    PhaseParams pp;
+    double third;
+    double sfac0;  // the scale when it is not fitted
+    int32_t live;
+    int32_t pad_;
+};
+
+struct BatchDev {
+    const SlotDev *slots;
+    const ModelDev *models;
+    const int64_t *face0;      // nslots + 1 face offsets (candidate -> slot)
+    const int64_t *chunk_pre;  // nslots + 1 flux-chunk offsets
+    const RingRec *rings;
+    int32_t nslots, nmodels;
+    GridDev g;  // every face of the batch
+    float *fp;  // fast sweep records (FlatDev::fp layout per slot)
+    uint2 *ecl;
+    int64_t *n0;  // per slot
+    int32_t *blockcnt, *queue, *counters;
+    DevStatus *st;  // per model
+    // work lists: counts[0] geometry slots, counts[1] continuum slots; each
+    // list has its slots and prefix sums (count + 1 entries) of its units
+    const int32_t *counts;
+    const int32_t *geo_slot;
+    const int64_t *geo_half, *geo_face;
+    const int32_t *cont_slot;
+    const int64_t *cont_face, *cont_blk;
+};
+
+// k such that pre[k] <= u < pre[k + 1], over count entries.
+__host__ __device__ __forceinline__ int find_seg(const int64_t *__restrict__ pre, int count,
+                                                 int64_t u) {
+    int lo = 0, hi = count - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pre[mid] <= u) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Per-model phase rows of a batch: entry e of model m at m * ldp + e.
+struct BatchPhases {
+    float4 *ef;
+    double *w1, *w2;
+    int64_t ldp, nent;
+};
+
 // ---- launchers (geometry.cu) ------------------------------------------------
 void launch_grid(const GridParams &p, const RingRec *rings, GridDev g, DevStatus *st,
                  cudaStream_t s);
 void launch_eclipse(const EclParams &p, int32_t eclipse_on, GridDev g, int32_t *queue,
-                    int32_t *counters, DevStatus *st, int nsm, cudaStream_t s);
+                    int32_t *counters, DevStatus *st, int nsm, int32_t warp_mode,
+                    cudaStream_t s);
 void launch_continuum(const ContParams &p, GridDev g, cudaStream_t s);
 void launch_flatten(GridDev g, FlatDev f, int32_t *blockcnt, int mixed, int need_pos,
                     const FastCoef &fc, DevStatus *st, cudaStream_t s);
@@ -151,6 +225,21 @@ void launch_diagnostics(int star, GridDev g, double *out, cudaStream_t s);
 void launch_pack_flat(FlatDev f, int64_t n0, int need_pos, cudaStream_t s);
 void launch_pack_phases(PhaseDev ph, cudaStream_t s);
 
+// batched stages (geometry.cu): grid + eclipse of the geometry list;
+// continuum + partition of the continuum list; phases; reduction, scatter and
+// scale / chi**2 of every model. Grids are fixed by the layout (persistent
+// loops over device-side counts), so a captured graph replays any work lists.
+void launch_batch_grid(const BatchDev &b, int nsm, cudaStream_t s);
+void launch_batch_eclipse(const BatchDev &b, int nsm, int32_t warp_mode, cudaStream_t s);
+void launch_batch_continuum(const BatchDev &b, int nsm, cudaStream_t s);
+void launch_batch_flatten(const BatchDev &b, int nsm, cudaStream_t s);
+void launch_batch_phases(const BatchDev &b, const DatumRec *data, const int64_t *off, int32_t n,
+                         const BatchPhases &ph, cudaStream_t s);
+void launch_batch_reduce(const BatchDev &b, const BatchPhases &ph, const double *part,
+                         int64_t ldp, double *osum, const DatumRec *data, const int64_t *off,
+                         int32_t n, int32_t flags, double *calc, double *sfac, double *out,
+                         cudaStream_t s);
+
 // ---- launchers (flux.cu, flux64.cu) -----------------------------------------
 struct FluxPlan {
     int fast;       // fast mixed sweep (FlatDev::fa/fb records)
@@ -164,6 +253,10 @@ FluxPlan plan_flux(int mixed, int fast, int64_t nface, int64_t nent, int nsm);
 void launch_flux(int mixed, int star, const FluxConsts &k, const FlatDev &f,
                  const PhaseDev &ph, const FluxPlan &plan, double *part, int64_t ldp,
                  DevStatus *st, cudaStream_t s);
+// Batched fast mixed sweep: one CTA per (flux chunk of any slot, phase tile);
+// plan.chunk divides 1024, plan.nchunk is the batch's total chunk count.
+void launch_batch_flux(const BatchDev &b, const BatchPhases &ph, const FluxPlan &plan,
+                       double *part, int64_t ldp, cudaStream_t s);
 // FP32 FMA throughput probe: fills *gflop with the FLOPs it executed.
 void launch_fma_probe(float *sink, int blocks, int iters, double *gflop, cudaStream_t s);
 void launch_flux64(int star, const FluxConsts &k, const FlatDev &f, const PhaseDev &ph,

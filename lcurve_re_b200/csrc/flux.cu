@@ -340,6 +340,86 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
 }
 
+// The batched fast sweep: CTA w takes phase tile w % ntile of batch chunk
+// w / ntile; the chunk's slot gives its records, its model's phase row and
+// its limb-darkening law. Same per-element arithmetic and sums as
+// k_flux_fast.
+template <int PPT>
+__global__ void __launch_bounds__(kThreads, 2)
+    k_flux_batch(BatchDev b, BatchPhases ph, int64_t chunk, int64_t ntile, double *part,
+                 int64_t ldp) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ uint64_t bar;
+    const int tid = threadIdx.x;
+    const int64_t tile = blockIdx.x % ntile, gc = blockIdx.x / ntile;
+    const int s = find_seg(b.chunk_pre, b.nslots, gc);
+    const SlotDev &S = b.slots[s];
+    const int64_t c0 = (gc - b.chunk_pre[s]) * chunk;
+    const int64_t n = S.nface, n0 = b.n0[s];
+    const int64_t cend = (c0 + chunk < n) ? c0 + chunk : n;
+    const int model = S.model, ltype = S.fc.ltype;
+    const bool need_ecl = cend > n0;
+    float4 *sp = reinterpret_cast<float4 *>(smem);
+    uint4 *se = reinterpret_cast<uint4 *>(smem + chunk * 32);
+    if (tid == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    if (tid == 0) {
+        const uint32_t bytes = (uint32_t)(chunk * 32) + (need_ecl ? (uint32_t)(chunk * 8) : 0u);
+        mbar_arrive_expect_tx(&bar, bytes);
+        bulk_g2s(sp, b.fp + 8 * (S.flat0 + c0), (uint32_t)(chunk * 32), &bar);
+        if (need_ecl) bulk_g2s(se, b.ecl + S.flat0 + c0, (uint32_t)(chunk * 8), &bar);
+    }
+    const float4 *ef = ph.ef + model * ph.ldp;
+    float2 ex[PPT], ey[PPT];
+    uint32_t pf[PPT];
+#pragma unroll
+    for (int j = 0; j < PPT; j++) {
+        const int64_t e = tile + ntile * ((int64_t)j * kThreads + tid);
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (e < ph.nent) v = ef[e];
+        ex[j] = f2(v.x, v.x);
+        ey[j] = f2(v.y, v.y);
+        pf[j] = __float_as_uint(v.w);
+    }
+    if (!mbar_wait_bounded(&bar, 0)) {
+        if (tid == 0) {
+            if (atomicCAS(&b.st[model].code, 0, 6) == 0) b.st[model].face = (int32_t)c0;
+        }
+        mbar_wait_bounded(&bar, 0);
+        return;
+    }
+    float acc[PPT];
+#pragma unroll
+    for (int j = 0; j < PPT; j++) acc[j] = 0.f;
+    const int64_t q0 = c0 >> 1, qend = (cend + 1) >> 1, qn0 = n0 >> 1;
+    const int64_t qa = qn0 < qend ? qn0 : qend;
+    const int64_t qb = qa > q0 ? qa : q0;
+    if (ltype == 1) {
+        sweep_pairs<PPT, 1, false>(sp, se, q0, q0, qb, ex, ey, pf, acc);
+        sweep_pairs<PPT, 1, true>(sp, se, q0, qb, qend, ex, ey, pf, acc);
+    } else {
+        sweep_pairs<PPT, 0, false>(sp, se, q0, q0, qb, ex, ey, pf, acc);
+        sweep_pairs<PPT, 0, true>(sp, se, q0, qb, qend, ex, ey, pf, acc);
+    }
+#pragma unroll
+    for (int j = 0; j < PPT; j++) {
+        const int64_t e = tile + ntile * ((int64_t)j * kThreads + tid);
+        if (e < ph.nent) part[gc * ldp + e] = (double)acc[j];
+    }
+}
+
+template <int PPT>
+void launch_batch_t(const BatchDev &b, const BatchPhases &ph, const FluxPlan &plan, double *part,
+                    int64_t ldp, cudaStream_t s) {
+    const size_t smem = (size_t)plan.chunk * 40;
+    auto kern = k_flux_batch<PPT>;
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const int64_t nblk = plan.nchunk * plan.ntile;
+    kern<<<(unsigned)nblk, kThreads, smem, s>>>(b, ph, plan.chunk, plan.ntile, part, ldp);
+    count_launch();
+}
+
 template <int PPT, int LT>
 void launch_fast_t(const FlatDev &f, const PhaseDev &ph, const FluxPlan &plan, double *part,
                    int64_t ldp, DevStatus *st, cudaStream_t s) {
@@ -380,6 +460,16 @@ __global__ void __launch_bounds__(256) k_fma_probe(float *sink, int iters) {
 void launch_fma_probe(float *sink, int blocks, int iters, double *gflop, cudaStream_t s) {
     k_fma_probe<<<blocks, 256, 0, s>>>(sink, iters);
     *gflop = 2.0 * 8 * 16 * (double)iters * 256.0 * blocks * 1e-9;
+}
+
+void launch_batch_flux(const BatchDev &b, const BatchPhases &ph, const FluxPlan &plan,
+                       double *part, int64_t ldp, cudaStream_t s) {
+    if (plan.nchunk <= 0 || ph.nent <= 0) return;
+    switch (plan.ppt) {
+    case 4: launch_batch_t<4>(b, ph, plan, part, ldp, s); break;
+    case 2: launch_batch_t<2>(b, ph, plan, part, ldp, s); break;
+    default: launch_batch_t<1>(b, ph, plan, part, ldp, s); break;
+    }
 }
 
 FluxPlan plan_flux(int mixed, int fast, int64_t nface, int64_t nent, int nsm) {

@@ -20,10 +20,9 @@ __device__ __forceinline__ void set_status(DevStatus *st, int code, int64_t face
     if (atomicCAS(&st->code, 0, code) == 0) st->face = (int32_t)face;
 }
 
-__global__ void k_grid(GridParams p, const RingRec *__restrict__ rings, GridDev g,
-                       DevStatus *st) {
-    const int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (h >= p.nhalf) return;
+// One half-face h of a grid and its mirror partner.
+__device__ __forceinline__ void grid_half(const GridParams &p, const RingRec *__restrict__ rings,
+                                          GridDev g, int64_t h, DevStatus *st) {
     int lo = 0, hi = p.nrings - 1;
     while (lo < hi) {
         int mid = (lo + hi + 1) >> 1;
@@ -64,13 +63,17 @@ __global__ void k_grid(GridParams p, const RingRec *__restrict__ rings, GridDev 
     }
     const double area = (R.span / R.nphi * rad * R.sint) * (R.latspan / R.nl * rad) / dot(dirn, dvec);
     const float af = (float)area, gf = (float)(gravity / p.gref);
+    // a tiled face past the reference's face count is dropped (its vector
+    // ends there, set_star_grid.cpp:162-166)
     int64_t i = R.off + np;
-    g.px[i] = posn.x; g.py[i] = posn.y; g.pz[i] = posn.z;
-    g.nx[i] = dvec.x; g.ny[i] = dvec.y; g.nz[i] = dvec.z;
-    g.area[i] = af;
-    g.grav[i] = gf;
+    if (i < g.n) {
+        g.px[i] = posn.x; g.py[i] = posn.y; g.pz[i] = posn.z;
+        g.nx[i] = dvec.x; g.ny[i] = dvec.y; g.nz[i] = dvec.z;
+        g.area[i] = af;
+        g.grav[i] = gf;
+    }
     const int np2 = R.nphi - 1 - np;
-    if (np2 != np) {
+    if (np2 != np && R.off + np2 < g.n) {
         i = R.off + np2;
         if (p.npole) {
             g.px[i] = posn.x; g.py[i] = -posn.y; g.pz[i] = posn.z;
@@ -84,13 +87,26 @@ __global__ void k_grid(GridParams p, const RingRec *__restrict__ rings, GridDev 
     }
 }
 
-// Sphere test of every face; Roche eclipsers queue their candidates.
-__global__ void k_ecl_pre(EclParams p, int32_t eclipse_on, GridDev g, int32_t *queue,
-                          int32_t *counters) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const bool in = i < g.n;
+__global__ void k_grid(GridParams p, const RingRec *__restrict__ rings, GridDev g,
+                       DevStatus *st) {
+    const int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (h < p.nhalf) grid_half(p, rings, g, h, st);
+}
+
+// Sphere test of face i: a spherical eclipser sets the range directly; a
+// Roche eclipser makes the face a candidate.
+__device__ __forceinline__ bool ecl_pre_face(const EclParams &p, int32_t eclipse_on, GridDev g,
+                                             int64_t i) {
     bool cand = false;
-    if (in) {
+    if (i >= g.ntiled) {
+        // a default Point (lcurve.h:53-54): no face of the tiling lands here
+        g.px[i] = g.py[i] = g.pz[i] = 0.;
+        g.nx[i] = g.ny[i] = g.nz[i] = 0.;
+        g.area[i] = 0.f;
+        g.grav[i] = 1.f;
+        g.necl[i] = 0;
+        g.ein[i] = g.eout[i] = 0.;
+    } else {
         g.necl[i] = 0;
         g.ein[i] = 0.;
         g.eout[i] = 0.;
@@ -109,6 +125,12 @@ __global__ void k_ecl_pre(EclParams p, int32_t eclipse_on, GridDev g, int32_t *q
             }
         }
     }
+    return cand;
+}
+
+// Appends the candidates of a full warp to the queue (warp-aggregated).
+__device__ __forceinline__ void queue_push(bool cand, int32_t item, int32_t *queue,
+                                           int32_t *counters) {
     const unsigned mask = __ballot_sync(0xffffffffu, cand);
     if (mask) {
         const int lane = threadIdx.x & 31;
@@ -116,21 +138,60 @@ __global__ void k_ecl_pre(EclParams p, int32_t eclipse_on, GridDev g, int32_t *q
         int base = 0;
         if (lane == leader) base = atomicAdd(&counters[0], __popc(mask));
         base = __shfl_sync(0xffffffffu, base, leader);
-        if (cand) queue[base + __popc(mask & ((1u << lane) - 1u))] = (int32_t)i;
+        if (cand) queue[base + __popc(mask & ((1u << lane) - 1u))] = item;
     }
 }
 
-// Each warp takes 32 consecutive candidates at a time, so neighbouring faces
-// (similar iteration counts) run in lockstep.
+// Sphere test of every face; Roche eclipsers queue their candidates.
+__global__ void k_ecl_pre(EclParams p, int32_t eclipse_on, GridDev g, int32_t *queue,
+                          int32_t *counters) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const bool cand = i < g.n && ecl_pre_face(p, eclipse_on, g, i);
+    queue_push(cand, (int32_t)i, queue, counters);
+}
+
+// Ingress/egress of the queued candidates. Up to warp_max candidates, one
+// warp bisects each face (ingress_egress_warp): few candidates leave most of
+// the GPU idle otherwise. Beyond that, one thread per face, each warp taking
+// 32 consecutive candidates at a time so that neighbouring faces (similar
+// iteration counts) run in lockstep. The count is read on the device, so the
+// choice needs no host round trip.
 __global__ void __launch_bounds__(128) k_ecl_roche(EclParams p, GridDev g,
                                                    const int32_t *__restrict__ queue,
-                                                   int32_t *counters, DevStatus *st) {
+                                                   int32_t *counters, DevStatus *st,
+                                                   int32_t warp_max) {
+    const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int total = counters[0];
+    if (total <= warp_max) {
+        for (;;) {
+            int k = 0;
+            if (lane == 0) k = atomicAdd(&counters[1], 1);
+            k = __shfl_sync(full, k, 0);
+            if (k >= total) break;
+            const int32_t i = queue[k];
+            const V3 pos = v3(g.px[i], g.py[i], g.pz[i]);
+            double ing = 0., egr = 0.;
+            int s = 0;
+            const bool ecl = ingress_egress_warp(p.comp_star, p.q, p.comp_spin, p.cosi, p.sini,
+                                                 p.delta, pos, p.comp_rref, p.comp_pref, ing,
+                                                 egr, s);
+            if (lane == 0) {
+                if (s) {
+                    set_status(st, s, i);
+                } else if (ecl) {
+                    g.necl[i] = 1;
+                    g.ein[i] = ing;
+                    g.eout[i] = egr;
+                }
+            }
+        }
+        return;
+    }
     for (;;) {
         int base = 0;
         if (lane == 0) base = atomicAdd(&counters[1], 32);
-        base = __shfl_sync(0xffffffffu, base, 0);
+        base = __shfl_sync(full, base, 0);
         if (base >= total) break;
         const int k = base + lane;
         if (k < total) {
@@ -151,9 +212,11 @@ __global__ void __launch_bounds__(128) k_ecl_roche(EclParams p, GridDev g,
     }
 }
 
-__global__ void k_continuum(ContParams p, GridDev g) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= g.n) return;
+__device__ __forceinline__ void continuum_face(const ContParams &p, GridDev g, int64_t i) {
+    if (i >= g.ntiled) {  // default Point: zero area, zero flux
+        g.flux[i] = 0.f;
+        return;
+    }
     const V3 pos = v3(g.px[i], g.py[i], g.pz[i]);
     const V3 dir = v3(g.nx[i], g.ny[i], g.nz[i]);
     const V3 cofm_other = p.star == kStar1 ? v3(1., 0., 0.) : v3(0., 0., 0.);
@@ -226,6 +289,11 @@ __global__ void k_continuum(ContParams p, GridDev g) {
     g.flux[i] = f;
 }
 
+__global__ void k_continuum(ContParams p, GridDev g) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < g.n) continuum_face(p, g, i);
+}
+
 constexpr int kFlatBlock = 1024;
 
 __global__ void k_flat_count(GridDev g, int32_t *blockcnt) {
@@ -237,7 +305,8 @@ __global__ void k_flat_count(GridDev g, int32_t *blockcnt) {
 
 // Single block: exclusive scan of the per-block eclipse counts; n0 = faces
 // never eclipsed.
-__global__ void k_flat_scan(int32_t *blockcnt, int32_t nb, int64_t n, int64_t *n0) {
+__device__ __forceinline__ void scan_blocks(int32_t *blockcnt, int32_t nb, int64_t n,
+                                            int64_t *n0) {
     __shared__ int32_t part[1024];
     __shared__ int64_t carry;
     if (threadIdx.x == 0) carry = 0;
@@ -259,10 +328,39 @@ __global__ void k_flat_scan(int32_t *blockcnt, int32_t nb, int64_t n, int64_t *n
         __syncthreads();
     }
     if (threadIdx.x == 0) *n0 = n - carry;
+    __syncthreads();
+}
+
+__global__ void k_flat_scan(int32_t *blockcnt, int32_t nb, int64_t n, int64_t *n0) {
+    scan_blocks(blockcnt, nb, n, n0);
 }
 
 __device__ __forceinline__ uint32_t phase_fx(double ph) {
     return (uint32_t)((unsigned long long)llrint(ph * 4294967296.0) & 0xffffffffull);
+}
+
+// Eclipse range [in1, out1] as 32-bit fixed-point phase (start, width + 1).
+__device__ __forceinline__ uint2 ecl_fx(double in1, double out1) {
+    long long w64 = llrint((out1 - in1) * 4294967296.0);
+    if (w64 < 0) w64 = 0;
+    if (w64 > 4294967294ll) w64 = 4294967294ll;
+    return make_uint2(phase_fx(in1), (uint32_t)(w64 + 1));
+}
+
+// Face i's record of the fast mixed sweep at flat position dest (pairs of
+// faces interleaved, FlatDev::fp).
+__device__ __forceinline__ void fast_record(float *fp, int64_t dest, GridDev g, int64_t i,
+                                            const FastCoef &fc) {
+    const double fl = (double)g.flux[i];
+    float *r = fp + 16 * (dest >> 1) + (dest & 1);
+    r[0] = (float)g.nx[i];
+    r[2] = (float)g.ny[i];
+    r[4] = (float)(fc.cosi * g.nz[i]);
+    r[6] = (float)(fl * fc.p[0]);
+    r[8] = (float)(fl * fc.p[1]);
+    r[10] = (float)(fl * fc.p[2]);
+    r[12] = (float)(fl * fc.p[3]);
+    r[14] = (float)(fl * fc.p[4]);
 }
 
 __global__ void k_flat_scatter(GridDev g, FlatDev f, const int32_t *__restrict__ blockoff,
@@ -285,28 +383,11 @@ __global__ void k_flat_scatter(GridDev g, FlatDev f, const int32_t *__restrict__
                               : blockIdx.x * (int64_t)kFlatBlock - boff + (t - rank);
     if (mixed) {
         if (fc.on) {
-            const double fl = (double)g.flux[i];
-            float *r = f.fp + 16 * (dest >> 1) + (dest & 1);
-            r[0] = (float)g.nx[i];
-            r[2] = (float)g.ny[i];
-            r[4] = (float)(fc.cosi * g.nz[i]);
-            r[6] = (float)(fl * fc.p[0]);
-            r[8] = (float)(fl * fc.p[1]);
-            r[10] = (float)(fl * fc.p[2]);
-            r[12] = (float)(fl * fc.p[3]);
-            r[14] = (float)(fl * fc.p[4]);
+            fast_record(f.fp, dest, g, i, fc);
         } else {
             f.geo[dest] = make_float4((float)g.nx[i], (float)g.ny[i], (float)g.nz[i], g.flux[i]);
         }
-        uint2 e = make_uint2(0u, 0u);
-        if (flag) {
-            const double in1 = g.ein[i], out1 = g.eout[i];
-            long long w64 = llrint((out1 - in1) * 4294967296.0);
-            if (w64 < 0) w64 = 0;
-            if (w64 > 4294967294ll) w64 = 4294967294ll;
-            e = make_uint2(phase_fx(in1), (uint32_t)(w64 + 1));
-        }
-        f.ecl[dest] = e;
+        f.ecl[dest] = flag ? ecl_fx(g.ein[i], g.eout[i]) : make_uint2(0u, 0u);
         if (need_pos) f.pos[dest] = make_float4((float)g.px[i], (float)g.py[i], (float)g.pz[i], 0.f);
     } else {
         f.dx[dest] = g.nx[i]; f.dy[dest] = g.ny[i]; f.dz[dest] = g.nz[i];
@@ -317,31 +398,45 @@ __global__ void k_flat_scatter(GridDev g, FlatDev f, const int32_t *__restrict__
     }
 }
 
-__global__ void k_phases(PhaseParams p, const DatumRec *__restrict__ data,
-                         const int64_t *__restrict__ off, int32_t n, PhaseDev ph) {
-    const int np = blockIdx.x * blockDim.x + threadIdx.x;
-    if (np >= n) return;
-    const DatumRec d = data[np];
-    double phase = (d.time - p.t0) / p.period;
+// Orbital phase of one point (4 Newton steps with pdot, the deltat shift)
+// and its polynomial scale factor (light_curve_comp.cpp:358-376).
+__device__ __forceinline__ void point_phase(const PhaseParams &p, const DatumRec &d,
+                                            double &phase, double &slfac) {
+    phase = (d.time - p.t0) / p.period;
     for (int it = 0; it < 4; it++)
         phase -= (p.t0 + phase * (p.period + p.pdot * phase) - d.time) /
                  (p.period + 2. * p.pdot * phase);
     phase += p.deltat / p.period / 2. * (cos(2. * kPi * phase) - 1.);
     const double frac = (d.time - p.middle) / p.range;
-    const double slfac = 1. + frac * (p.slope + frac * (p.quad + frac * p.cube));
+    slfac = 1. + frac * (p.slope + frac * (p.quad + frac * p.cube));
+}
+
+// Phase and trapezoid weight of sub-exposure nd (light_curve_comp.cpp:416-455).
+__device__ __forceinline__ void sub_exposure(double phase, double expose, int ndiv, int nd,
+                                             double &phi, double &wgt) {
+    if (ndiv == 1) {
+        phi = phase;
+        wgt = 1.0;
+    } else {
+        phi = phase + expose * (nd - (ndiv - 1) / 2.0) / (ndiv - 1);
+        wgt = (nd == 0 || nd == ndiv - 1) ? 0.5 : 1.0;
+    }
+}
+
+__global__ void k_phases(PhaseParams p, const DatumRec *__restrict__ data,
+                         const int64_t *__restrict__ off, int32_t n, PhaseDev ph) {
+    const int np = blockIdx.x * blockDim.x + threadIdx.x;
+    if (np >= n) return;
+    const DatumRec d = data[np];
+    double phase, slfac;
+    point_phase(p, d, phase, slfac);
     const double expose = d.expose / p.period;
     const int ndiv = d.ndiv;
     const double norm = (ndiv - 1 > 1) ? ndiv - 1 : 1;
     int64_t e = off[np];
     for (int nd = 0; nd < ndiv; ++nd, ++e) {
         double phi, wgt;
-        if (ndiv == 1) {
-            phi = phase;
-            wgt = 1.0;
-        } else {
-            phi = phase + expose * (nd - (ndiv - 1) / 2.0) / (ndiv - 1);
-            wgt = (nd == 0 || nd == ndiv - 1) ? 0.5 : 1.0;
-        }
+        sub_exposure(phase, expose, ndiv, nd, phi, wgt);
         const V3 earth = set_earth(p.cosi, p.sini, phi);
         const double phin = phi - floor(phi);
         ph.ex[e] = earth.x;
@@ -419,10 +514,9 @@ __device__ __forceinline__ double block_sum(double v, double *sh) {
 
 // One block of 1024 threads: thread t takes points t, t+1024, ... in order,
 // the block sums them in a fixed tree.
-__global__ void __launch_bounds__(1024) k_finalize(int32_t flags, const DatumRec *__restrict__ data,
-                                                   int32_t n, double *calc, double *sfac_io,
-                                                   double *out) {
-    __shared__ double sh[1024];
+__device__ __forceinline__ void finalize_block(int32_t flags, const DatumRec *__restrict__ data,
+                                               int32_t n, double *calc, double *sfac_io,
+                                               double *out, double *sh) {
     const bool scale = flags & 1, rdata = flags & 2;
     const int t = threadIdx.x;
     if (scale) {
@@ -475,6 +569,13 @@ __global__ void __launch_bounds__(1024) k_finalize(int32_t flags, const DatumRec
     }
 }
 
+__global__ void __launch_bounds__(1024) k_finalize(int32_t flags, const DatumRec *__restrict__ data,
+                                                   int32_t n, double *calc, double *sfac_io,
+                                                   double *out) {
+    __shared__ double sh[1024];
+    finalize_block(flags, data, n, calc, sfac_io, out, sh);
+}
+
 // comp_gravity / comp_radius blocked sums: one thread per 8192-point block,
 // serial inside the block; the host merges the blocks in order.
 __global__ void k_diag(int star, GridDev g, double *blk) {
@@ -525,6 +626,265 @@ __global__ void k_pack_phases(PhaseDev ph) {
                            __uint_as_float(phase_fx(ph.phin[e])));
 }
 
+// ---- batched stages ---------------------------------------------------------
+
+// The slot's view of the batch point arrays.
+__device__ __forceinline__ GridDev slot_grid(const GridDev &g, int64_t face0, int64_t nface,
+                                             int64_t ntiled) {
+    return GridDev{g.px + face0, g.py + face0, g.pz + face0, g.nx + face0, g.ny + face0,
+                   g.nz + face0, g.area + face0, g.grav + face0, g.flux + face0, g.necl + face0,
+                   g.ein + face0, g.eout + face0, nface, ntiled};
+}
+
+__global__ void __launch_bounds__(128) k_grid_b(BatchDev b) {
+    const int nk = b.counts[0];
+    if (nk <= 0) return;
+    const int64_t total = b.geo_half[nk];
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < total; u += stride) {
+        const int k = find_seg(b.geo_half, nk, u);
+        const SlotDev &S = b.slots[b.geo_slot[k]];
+        grid_half(S.gp, b.rings + S.ring0, slot_grid(b.g, S.face0, S.nface, S.ntiled), u - b.geo_half[k],
+                  b.st + S.model);
+    }
+}
+
+// Sphere pre-test of the geometry list's faces; candidates are queued by
+// their batch face index. Whole warps step together (queue_push votes).
+__global__ void k_ecl_pre_b(BatchDev b) {
+    const int nk = b.counts[0];
+    if (nk <= 0) return;
+    const int64_t total = b.geo_face[nk];
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int lane = threadIdx.x & 31;
+    for (int64_t u0 = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31); u0 < total;
+         u0 += stride) {
+        const int64_t u = u0 + lane;
+        bool cand = false;
+        int32_t item = 0;
+        if (u < total) {
+            const int k = find_seg(b.geo_face, nk, u);
+            const SlotDev &S = b.slots[b.geo_slot[k]];
+            const int64_t i = u - b.geo_face[k];
+            cand = ecl_pre_face(S.ep, S.eclipse_on, slot_grid(b.g, S.face0, S.nface, S.ntiled), i);
+            item = (int32_t)(S.face0 + i);
+        }
+        queue_push(cand, item, b.queue, b.counters);
+    }
+}
+
+// k_ecl_roche over the batch queue: each candidate finds its slot by its
+// face index.
+__global__ void __launch_bounds__(128) k_ecl_roche_b(BatchDev b, int32_t warp_max) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int total = b.counters[0];
+    const GridDev g = b.g;
+    if (total <= warp_max) {
+        for (;;) {
+            int k = 0;
+            if (lane == 0) k = atomicAdd(&b.counters[1], 1);
+            k = __shfl_sync(full, k, 0);
+            if (k >= total) break;
+            const int32_t i = b.queue[k];
+            const SlotDev &S = b.slots[find_seg(b.face0, b.nslots, i)];
+            const EclParams &p = S.ep;
+            const V3 pos = v3(g.px[i], g.py[i], g.pz[i]);
+            double ing = 0., egr = 0.;
+            int s = 0;
+            const bool ecl = ingress_egress_warp(p.comp_star, p.q, p.comp_spin, p.cosi, p.sini,
+                                                 p.delta, pos, p.comp_rref, p.comp_pref, ing,
+                                                 egr, s);
+            if (lane == 0) {
+                if (s) {
+                    set_status(b.st + S.model, s, i - S.face0);
+                } else if (ecl) {
+                    g.necl[i] = 1;
+                    g.ein[i] = ing;
+                    g.eout[i] = egr;
+                }
+            }
+        }
+        return;
+    }
+    for (;;) {
+        int base = 0;
+        if (lane == 0) base = atomicAdd(&b.counters[1], 32);
+        base = __shfl_sync(full, base, 0);
+        if (base >= total) break;
+        const int k = base + lane;
+        if (k < total) {
+            const int32_t i = b.queue[k];
+            const SlotDev &S = b.slots[find_seg(b.face0, b.nslots, i)];
+            const EclParams &p = S.ep;
+            const V3 pos = v3(g.px[i], g.py[i], g.pz[i]);
+            double ing = 0., egr = 0.;
+            int s = 0;
+            const bool ecl = ingress_egress(p.comp_star, p.q, p.comp_spin, p.cosi, p.sini,
+                                            p.delta, pos, p.comp_rref, p.comp_pref, ing, egr, s);
+            if (s) {
+                set_status(b.st + S.model, s, i - S.face0);
+            } else if (ecl) {
+                g.necl[i] = 1;
+                g.ein[i] = ing;
+                g.eout[i] = egr;
+            }
+        }
+    }
+}
+
+__global__ void k_continuum_b(BatchDev b) {
+    const int nk = b.counts[1];
+    if (nk <= 0) return;
+    const int64_t total = b.cont_face[nk];
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t u = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; u < total; u += stride) {
+        const int k = find_seg(b.cont_face, nk, u);
+        const SlotDev &S = b.slots[b.cont_slot[k]];
+        continuum_face(S.cp, slot_grid(b.g, S.face0, S.nface, S.ntiled), u - b.cont_face[k]);
+    }
+}
+
+// Partition counts per 1024-face block of the continuum list's slots; a
+// CTA takes whole blocks.
+__global__ void __launch_bounds__(kFlatBlock) k_flat_count_b(BatchDev b) {
+    const int nk = b.counts[1];
+    if (nk <= 0) return;
+    const int64_t total = b.cont_blk[nk];
+    for (int64_t B = blockIdx.x; B < total; B += gridDim.x) {
+        const int k = find_seg(b.cont_blk, nk, B);
+        const SlotDev &S = b.slots[b.cont_slot[k]];
+        const int64_t lb = B - b.cont_blk[k];
+        const int64_t i = lb * kFlatBlock + threadIdx.x;
+        const int flag = (i < S.nface) && b.g.necl[S.face0 + i] == 1;
+        const int c = __syncthreads_count(flag);
+        if (threadIdx.x == 0) b.blockcnt[S.blk0 + lb] = c;
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_flat_scan_b(BatchDev b) {
+    const int nk = b.counts[1];
+    for (int k = blockIdx.x; k < nk; k += gridDim.x) {
+        const int s = b.cont_slot[k];
+        const SlotDev &S = b.slots[s];
+        const int32_t nb = (int32_t)((S.nface + kFlatBlock - 1) / kFlatBlock);
+        scan_blocks(b.blockcnt + S.blk0, nb, S.nface, b.n0 + s);
+    }
+}
+
+// Stable partition into fast sweep records; the record after an odd last
+// face is zeroed (the sweep reads faces in pairs).
+__global__ void __launch_bounds__(kFlatBlock) k_flat_scatter_b(BatchDev b) {
+    __shared__ int32_t warp_tot[32];
+    const int nk = b.counts[1];
+    if (nk <= 0) return;
+    const int64_t total = b.cont_blk[nk];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    for (int64_t B = blockIdx.x; B < total; B += gridDim.x) {
+        const int k = find_seg(b.cont_blk, nk, B);
+        const int s = b.cont_slot[k];
+        const SlotDev &S = b.slots[s];
+        const int64_t lb = B - b.cont_blk[k];
+        const int64_t i = lb * kFlatBlock + t, n = S.nface;
+        const bool in = i < n;
+        const int flag = in && b.g.necl[S.face0 + i] == 1;
+        const unsigned m = __ballot_sync(0xffffffffu, flag);
+        if (lane == 0) warp_tot[w] = __popc(m);
+        __syncthreads();
+        int before = 0;
+        for (int q = 0; q < w; q++) before += warp_tot[q];
+        __syncthreads();
+        const int rank = before + __popc(m & ((1u << lane) - 1u));
+        float *fp = b.fp + 8 * S.flat0;
+        uint2 *ecl = b.ecl + S.flat0;
+        if (in) {
+            const GridDev g = slot_grid(b.g, S.face0, n, S.ntiled);
+            const int64_t n0 = b.n0[s];
+            const int64_t boff = b.blockcnt[S.blk0 + lb];
+            const int64_t dest = flag ? n0 + boff + rank : lb * kFlatBlock - boff + (t - rank);
+            fast_record(fp, dest, g, i, S.fc);
+            ecl[dest] = flag ? ecl_fx(g.ein[i], g.eout[i]) : make_uint2(0u, 0u);
+        } else if (i == n && (n & 1)) {
+            float *r = fp + 16 * (n >> 1) + 1;
+            for (int q = 0; q < 16; q += 2) r[q] = 0.f;
+            ecl[n] = make_uint2(0u, 0u);
+        }
+    }
+}
+
+__global__ void k_phases_b(BatchDev b, const DatumRec *__restrict__ data,
+                           const int64_t *__restrict__ off, int32_t n, BatchPhases ph) {
+    const int np = blockIdx.x * blockDim.x + threadIdx.x;
+    const int m = blockIdx.y;
+    if (np >= n) return;
+    const PhaseParams &p = b.models[m].pp;
+    const DatumRec d = data[np];
+    double phase, slfac;
+    point_phase(p, d, phase, slfac);
+    const double expose = d.expose / p.period;
+    const int ndiv = d.ndiv;
+    const double norm = (ndiv - 1 > 1) ? ndiv - 1 : 1;
+    int64_t e = m * ph.ldp + off[np];
+    for (int nd = 0; nd < ndiv; ++nd, ++e) {
+        double phi, wgt;
+        sub_exposure(phase, expose, ndiv, nd, phi, wgt);
+        const V3 earth = set_earth(p.cosi, p.sini, phi);
+        const double phin = phi - floor(phi);
+        ph.w1[e] = slfac * wgt * gi_scale1(p.gi, phi) / norm;
+        ph.w2[e] = slfac * wgt * gi_scale2(p.gi, phi) / norm;
+        ph.ef[e] = make_float4((float)earth.x, (float)earth.y, (float)earth.z,
+                               __uint_as_float(phase_fx(phin)));
+    }
+}
+
+// Chunk partials of each slot summed in chunk order, per phase entry.
+__global__ void k_reduce_b(BatchDev b, const double *__restrict__ part, int64_t ldp, int64_t nent,
+                           double *osum) {
+    const int s = blockIdx.y;
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= nent) return;
+    const int64_t c0 = b.chunk_pre[s], c1 = b.chunk_pre[s + 1];
+    double o = 0.0;
+    int64_t c = c0;
+    for (; c + 8 <= c1; c += 8) {
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) v[u] = part[(c + u) * ldp + e];
+#pragma unroll
+        for (int u = 0; u < 8; u++) o += v[u];
+    }
+    for (; c < c1; c++) o += part[c * ldp + e];
+    osum[s * ldp + e] = o;
+}
+
+// Per model and point: star 1 then star 2 sub-exposure sums, third light.
+__global__ void k_scatter_b(BatchDev b, BatchPhases ph, const double *__restrict__ osum,
+                            const DatumRec *__restrict__ data, const int64_t *__restrict__ off,
+                            int32_t n, double *calc) {
+    const int np = blockIdx.x * blockDim.x + threadIdx.x;
+    const int m = blockIdx.y;
+    if (np >= n) return;
+    const int64_t row = m * ph.ldp;
+    const double *o1 = osum + (2 * (int64_t)m) * ph.ldp, *o2 = o1 + ph.ldp;
+    const int64_t e0 = off[np], e1 = e0 + (data[np].ndiv > 0 ? data[np].ndiv : 0);
+    double c = 0.;
+    for (int64_t e = e0; e < e1; e++) c += ph.w1[row + e] * o1[e];
+    for (int64_t e = e0; e < e1; e++) c += ph.w2[row + e] * o2[e];
+    calc[m * (int64_t)n + np] = c + b.models[m].third;
+}
+
+__global__ void __launch_bounds__(1024) k_finalize_b(BatchDev b, int32_t flags,
+                                                     const DatumRec *__restrict__ data,
+                                                     int32_t n, double *calc, double *sfac,
+                                                     double *out) {
+    __shared__ double sh[1024];
+    const int m = blockIdx.x;
+    double *sf = sfac + 5 * (int64_t)m;
+    if (threadIdx.x == 0) sf[0] = b.models[m].sfac0;
+    __syncthreads();
+    finalize_block(flags, data, n, calc + m * (int64_t)n, sf, out + 3 * (int64_t)m, sh);
+}
+
 inline unsigned nblocks(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 }  // namespace
@@ -548,16 +908,20 @@ void launch_grid(const GridParams &p, const RingRec *rings, GridDev g, DevStatus
 }
 
 void launch_eclipse(const EclParams &p, int32_t eclipse_on, GridDev g, int32_t *queue,
-                    int32_t *counters, DevStatus *st, int nsm, cudaStream_t s) {
+                    int32_t *counters, DevStatus *st, int nsm, int32_t warp_mode,
+                    cudaStream_t s) {
     if (g.n <= 0) return;
     cudaMemsetAsync(counters, 0, 2 * sizeof(int32_t), s);
     k_ecl_pre<<<nblocks(g.n, 256), 256, 0, s>>>(p, eclipse_on, g, queue, counters);
     count_launch();
     if (eclipse_on && p.comp_roche) {
+        // 4 blocks of 4 warps per SM; no more warps than faces
         unsigned nb = (unsigned)nsm * 4u;
-        const unsigned need = nblocks(g.n, 128);
+        const unsigned need = nblocks(g.n, 4);
         if (need < nb) nb = need;
-        k_ecl_roche<<<nb, 128, 0, s>>>(p, g, queue, counters, st);
+        const int32_t warps = (int32_t)nb * 4;
+        const int32_t warp_max = warp_mode < 0 ? -1 : warp_mode > 0 ? warp_mode : 2 * warps;
+        k_ecl_roche<<<nb, 128, 0, s>>>(p, g, queue, counters, st, warp_max);
         count_launch();
     }
 }
@@ -576,8 +940,13 @@ void launch_flatten(GridDev g, FlatDev f, int32_t *blockcnt, int mixed, int need
         cudaMemsetAsync(f.n0, 0, sizeof(int64_t), s);
         return;
     }
-    if (mixed && fc.on && f.npad > g.n)  // padding faces must add nothing
-        cudaMemsetAsync(f.fp + 8 * g.n, 0, (size_t)(f.npad - g.n) * 8 * sizeof(float), s);
+    if (mixed && fc.on && f.npad > g.n) {
+        // padding faces must add nothing: zero from the pair holding face n
+        // (records interleave the two faces of a pair; the scatter below
+        // rewrites face n-1's half when n is odd)
+        const int64_t z0 = 16 * (g.n >> 1);
+        cudaMemsetAsync(f.fp + z0, 0, (size_t)(8 * f.npad - z0) * sizeof(float), s);
+    }
     k_flat_count<<<nb, kFlatBlock, 0, s>>>(g, blockcnt);
     count_launch();
     k_flat_scan<<<1, 1024, 0, s>>>(blockcnt, (int32_t)nb, g.n, f.n0);
@@ -619,6 +988,61 @@ void launch_diagnostics(int star, GridDev g, double *out, cudaStream_t s) {
     const int64_t nblk = (g.n + 8191) / 8192;
     if (nblk <= 0) return;
     k_diag<<<nblocks(nblk, 64), 64, 0, s>>>(star, g, out);
+    count_launch();
+}
+
+// ---- batched launchers -------------------------------------------------------
+
+void launch_batch_grid(const BatchDev &b, int nsm, cudaStream_t s) {
+    k_grid_b<<<nsm * 8, 128, 0, s>>>(b);
+    count_launch();
+}
+
+void launch_batch_eclipse(const BatchDev &b, int nsm, int32_t warp_mode, cudaStream_t s) {
+    cudaMemsetAsync(b.counters, 0, 2 * sizeof(int32_t), s);
+    k_ecl_pre_b<<<nsm * 4, 256, 0, s>>>(b);
+    count_launch();
+    const int32_t warps = nsm * 16;
+    const int32_t warp_max = warp_mode < 0 ? -1 : warp_mode > 0 ? warp_mode : 2 * warps;
+    k_ecl_roche_b<<<nsm * 4, 128, 0, s>>>(b, warp_max);
+    count_launch();
+}
+
+void launch_batch_continuum(const BatchDev &b, int nsm, cudaStream_t s) {
+    k_continuum_b<<<nsm * 4, 256, 0, s>>>(b);
+    count_launch();
+}
+
+void launch_batch_flatten(const BatchDev &b, int nsm, cudaStream_t s) {
+    k_flat_count_b<<<nsm * 2, kFlatBlock, 0, s>>>(b);
+    count_launch();
+    k_flat_scan_b<<<nsm, 1024, 0, s>>>(b);
+    count_launch();
+    k_flat_scatter_b<<<nsm * 2, kFlatBlock, 0, s>>>(b);
+    count_launch();
+}
+
+void launch_batch_phases(const BatchDev &b, const DatumRec *data, const int64_t *off, int32_t n,
+                         const BatchPhases &ph, cudaStream_t s) {
+    if (n <= 0 || b.nmodels <= 0) return;
+    k_phases_b<<<dim3(nblocks(n, 128), (unsigned)b.nmodels), 128, 0, s>>>(b, data, off, n, ph);
+    count_launch();
+}
+
+void launch_batch_reduce(const BatchDev &b, const BatchPhases &ph, const double *part,
+                         int64_t ldp, double *osum, const DatumRec *data, const int64_t *off,
+                         int32_t n, int32_t flags, double *calc, double *sfac, double *out,
+                         cudaStream_t s) {
+    if (n <= 0 || b.nmodels <= 0) return;
+    if (ph.nent > 0) {
+        k_reduce_b<<<dim3(nblocks(ph.nent, 256), (unsigned)b.nslots), 256, 0, s>>>(
+            b, part, ldp, ph.nent, osum);
+        count_launch();
+    }
+    k_scatter_b<<<dim3(nblocks(n, 128), (unsigned)b.nmodels), 128, 0, s>>>(b, ph, osum, data,
+                                                                             off, n, calc);
+    count_launch();
+    k_finalize_b<<<b.nmodels, 1024, 0, s>>>(b, flags, data, n, calc, sfac, out);
     count_launch();
 }
 

@@ -49,13 +49,14 @@ def _as_data(d):
 class Engine:
     """One engine context: a CUDA stream, device buffers and the grid cache."""
 
-    def __init__(self, device=0, precision="mixed", verbose=0):
+    def __init__(self, device=0, precision="mixed", verbose=0, eclipse_warp=0):
         self.lib = load_library()
         opt = abi.LcgOptions()
         self.lib.lcg_default_options(C.byref(opt))
         opt.device = device
         opt.precision = {"mixed": abi.PREC_MIXED, "fp64": abi.PREC_FP64}[precision]
         opt.verbose = verbose
+        opt.eclipse_warp = eclipse_warp
         ctx = C.c_void_p()
         st = self.lib.lcg_create(C.byref(ctx), C.byref(opt))
         if st != abi.OK:
@@ -124,6 +125,30 @@ class Engine:
             self.ctx, ms, nm, d.ctypes.data, n, flags, _dptr(sf), _dptr(calc), _dptr(chisq),
             _dptr(wnok), status.ctypes.data_as(C.POINTER(C.c_int32))))
         return calc, chisq, wnok, sf.reshape(nm, 5), status
+
+    def set_data(self, data):
+        """Copies the points to the device once (lcg_set_data) for the
+        resident calls."""
+        d = _as_data(data)
+        self._check(self.lib.lcg_set_data(self.ctx, d.ctypes.data, d.shape[0]))
+        self._n = d.shape[0]
+
+    def light_curve_batch_resident(self, models, scale=True, rdata=True, sfac=None, calc=True):
+        """lcg_light_curve_batch over the points of set_data; calc=False
+        returns only chi**2 (calc is None)."""
+        ms = models if isinstance(models, C.Array) else \
+            (abi.LcgModel * len(models))(*[_as_model(m) for m in models])
+        nm, n = len(ms), self._n
+        sf = np.ones(5 * nm) if sfac is None else np.ascontiguousarray(sfac, dtype=np.float64)
+        out = np.zeros((nm, n)) if calc else None
+        chisq = np.zeros(nm)
+        wnok = np.zeros(nm)
+        status = np.zeros(nm, dtype=np.int32)
+        flags = (abi.FLAG_SCALE if scale else 0) | (abi.FLAG_RDATA if rdata else 0)
+        self._check(self.lib.lcg_light_curve_batch_resident(
+            self.ctx, ms, nm, flags, _dptr(sf), _dptr(out) if calc else None, _dptr(chisq),
+            _dptr(wnok), status.ctypes.data_as(C.POINTER(C.c_int32))))
+        return out, chisq, wnok, sf.reshape(nm, 5), status
 
     # -- stage seams ---------------------------------------------------------
     def face_count(self, model, star, fine=True):

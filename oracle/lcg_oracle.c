@@ -1017,12 +1017,11 @@ static int add_faces(const lcg_model *m, const grid_setup *s, int star,
         ring_geometry(star, infill, nlat, nlat1, nlat2, nlngfill, tlo, thi, dtheta, nt, &g);
         *nface += g.nphi;
     }
-    if (*nface > cap) {
-        free(off);
-        return seterr(e, LCG_E_INVALID,
-                      "set_star_grid: ring tiling gives more faces than numface (%d > %d)",
-                      *nface, cap);
-    }
+    /* The reference sizes its vector by numface (set_star_grid.cpp:162-166)
+     * and writes each face at off[nt] + np (:490, :508). For a few nlat
+     * (153, 297, 315, 333, 339, ...) the ring tiling has one or two faces
+     * more than numface; those writes land past the vector's end and are not
+     * part of the grid it goes on to use. Only faces below cap are kept. */
     const double ACC = m->delta_phase / 10.;
     const double q = m->q;
     const int roche_solve = (star == LCG_STAR1 && m->roche1) || (star == LCG_STAR2 && m->roche2);
@@ -1069,13 +1068,15 @@ static int add_faces(const lcg_model *m, const grid_setup *s, int star,
             const int i1 = off[nt] + np;
             double ein = 0., eout = 0.;
             int ecl = face_eclipse(m, s, star, posn, &ein, &eout, &le);
-            o->posn[3 * i1] = posn.x; o->posn[3 * i1 + 1] = posn.y; o->posn[3 * i1 + 2] = posn.z;
-            o->dirn[3 * i1] = dvec.x; o->dirn[3 * i1 + 1] = dvec.y; o->dirn[3 * i1 + 2] = dvec.z;
-            o->area[i1] = (float)area;
-            o->gravity[i1] = (float)(gravity / s->gref);
-            o->necl[i1] = ecl;
-            o->ein[i1] = ecl ? ein : 0.;
-            o->eout[i1] = ecl ? eout : 0.;
+            if (i1 < cap) {
+                o->posn[3 * i1] = posn.x; o->posn[3 * i1 + 1] = posn.y; o->posn[3 * i1 + 2] = posn.z;
+                o->dirn[3 * i1] = dvec.x; o->dirn[3 * i1 + 1] = dvec.y; o->dirn[3 * i1 + 2] = dvec.z;
+                o->area[i1] = (float)area;
+                o->gravity[i1] = (float)(gravity / s->gref);
+                o->necl[i1] = ecl;
+                o->ein[i1] = ecl ? ein : 0.;
+                o->eout[i1] = ecl ? eout : 0.;
+            }
             const int np2 = g.nphi - 1 - np;
             if (np2 != np) {
                 v3 dirn2 = dirn, posn2 = posn, dvec2 = dvec;
@@ -1085,6 +1086,7 @@ static int add_faces(const lcg_model *m, const grid_setup *s, int star,
                 const int i2 = off[nt] + np2;
                 ein = eout = 0.;
                 ecl = face_eclipse(m, s, star, posn2, &ein, &eout, &le);
+                if (i2 >= cap) continue;
                 o->posn[3 * i2] = posn2.x; o->posn[3 * i2 + 1] = posn2.y; o->posn[3 * i2 + 2] = posn2.z;
                 o->dirn[3 * i2] = dvec2.x; o->dirn[3 * i2 + 1] = dvec2.y; o->dirn[3 * i2 + 2] = dvec2.z;
                 o->area[i2] = (float)area;
@@ -1125,10 +1127,15 @@ static int build_grid(const lcg_model *m, const grid_setup *s, int star,
         st = add_faces(m, s, star, o, &nface, cap, 0., PI_, dtheta, 0, 0, e);
     }
     if (st) return st;
-    if (nface != nface_expected)
-        return seterr(e, LCG_E_INVALID,
-                      "set_star_grid: ring tiling gives fewer faces than numface (%d < %d)",
-                      nface, nface_expected);
+    /* fewer tiled faces than numface (nlat 813, 879, ...): the rest of the
+     * reference's vector holds default Points (lcurve.h:53-54) */
+    for (int i = nface; i < nface_expected; i++) {
+        for (int k = 0; k < 3; k++) o->posn[3 * i + k] = o->dirn[3 * i + k] = 0.;
+        o->area[i] = 0.f;
+        o->gravity[i] = 1.f;
+        o->necl[i] = 0;
+        o->ein[i] = o->eout[i] = 0.;
+    }
     return LCG_OK;
 }
 

@@ -61,6 +61,25 @@ def test_star_grid(engine_fp64, oracle, name, model, data):
             assert np.all(width[diff] < 1e-6), (name, star, int(diff.sum()))
 
 
+def test_eclipse_warp_and_thread_modes_agree(oracle):
+    """The warp-per-face bisection evaluates the same midpoints as the
+    thread-per-face one: flags and phases are bit-identical, whichever the
+    candidate count selects."""
+    from lcurve_re_b200.engine import Engine
+    warp = Engine(precision="fp64", eclipse_warp=1 << 30)
+    thread = Engine(precision="fp64", eclipse_warp=-1)
+    try:
+        cases = [(n, m) for n, m, _ in CASES] + [("wd_dm_small", W.wd_dm_small()[0])]
+        for name, m in cases:
+            for star in (0, 1):
+                a, b = warp.star_grid(m, star), thread.star_grid(m, star)
+                for k in ("neclipse", "ecl_in", "ecl_out"):
+                    assert np.array_equal(a[k], b[k]), (name, star, k)
+    finally:
+        warp.close()
+        thread.close()
+
+
 def test_flux_fp64_bit_exact(engine_fp64, oracle):
     m, d = W.wd_dm_small()
     ph = oracle.phase_batch(m, W.data(700, ndiv=3, expose=0.002))
@@ -167,6 +186,7 @@ def test_errors(engine_mixed):
 
 
 def test_batch_equals_single(engine_mixed):
+    # the batch chunks each grid's flux sum differently: 2e-6 (mixed mode)
     models, d = W.mcmc_batch(6, seed=3)
     models = [W.model(nlat1f=int(m["nlat1f"]) // 4 + 4, nlat2f=int(m["nlat2f"]) // 4 + 8,
                       q=m["q"], iangle=m["iangle"], r1=m["r1"], r2=m["r2"], t1=m["t1"],
@@ -176,4 +196,48 @@ def test_batch_equals_single(engine_mixed):
     assert np.all(status == 0)
     for i, m in enumerate(models):
         c = engine_mixed.light_curve_comp(m, d, diagnostics=False, no_cache=True)[0]
-        np.testing.assert_allclose(calc[i], c, rtol=1e-12)
+        np.testing.assert_allclose(calc[i], c, rtol=2e-6)
+
+
+def test_context_history_does_not_leak(oracle):
+    """A context that has evaluated a larger grid gives a smaller one (with an
+    odd face count, so the last face pair is half padding) the result of a
+    fresh context, bit for bit."""
+    from lcurve_re_b200.engine import Engine
+    nl = next(k for k in range(17, 60) if oracle.face_count(W.model(nlat2f=k), 1) % 2)
+    small = W.model(nlat1f=12, nlat2f=nl)
+    big = W.model(nlat1f=40, nlat2f=90, nlat1c=20, nlat2c=45)
+    d = W.data(200)
+    for prec in ("mixed", "fp64"):
+        fresh = Engine(precision=prec)
+        used = Engine(precision=prec)
+        try:
+            a = fresh.light_curve_comp(small, d)[0]
+            used.light_curve_comp(big, d)
+            b = used.light_curve_comp(small, d)[0]
+            assert np.array_equal(a, b), (prec, np.max(np.abs(a - b) / np.abs(a)))
+        finally:
+            fresh.close()
+            used.close()
+
+
+@pytest.mark.parametrize("over,star", [({"nlat1f": 20, "nlat2f": 153}, 1),
+                                       ({"nlat1f": 813, "nlat2f": 40, "eclipse1": 0}, 0)],
+                         ids=["tiling_long_153", "tiling_short_813"])
+def test_tiling_mismatch_keeps_the_reference_face_count(engine_fp64, oracle, over, star):
+    """numface and the ring tiling disagree by two faces at these nlat: the
+    grid keeps numface faces, dropping the extra tiled faces (153) or ending
+    in default Points (813), as the reference's vector does."""
+    m = W.model(**over)
+    go = oracle.star_grid(m, star)
+    gg = engine_fp64.star_grid(m, star)
+    assert gg["posn"].shape == go["posn"].shape
+    np.testing.assert_allclose(gg["posn"], go["posn"], rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(gg["dirn"], go["dirn"], rtol=1e-12, atol=1e-14)
+    for k in ("area", "gravity", "flux"):
+        np.testing.assert_allclose(gg[k], go[k], rtol=4e-7, atol=0, err_msg=k)
+    d = W.data(100)
+    st, err, co, _, _ = oracle.light_curve(m, d)
+    assert st == 0, err
+    calc = engine_fp64.light_curve_comp(m, d, sfac=np.ones(5), diagnostics=False)[0]
+    assert np.max(np.abs(calc - co) / np.abs(co)) <= 1e-6

@@ -65,3 +65,17 @@ def test_errors_match(oracle, reference):
         st_r, err_r, *_ = reference.light_curve(m, W.data(20))
         assert st_o == st_r == code
         assert err_o == err_r
+
+
+def test_short_tiling_ends_in_default_points(oracle, reference):
+    """At nlat 813 the ring tiling has two faces fewer than numface: the
+    reference's grid ends in two default Points (zero position, normal, area
+    and flux, gravity 1, never eclipsed)."""
+    from lcurve_re_b200 import workloads as W
+    m = W.model(nlat1f=813, nlat2f=40, eclipse1=0)
+    go = oracle.star_grid(m, 0)
+    gr = reference.star_grid(m, 0)
+    for k in go:
+        assert np.array_equal(go[k], gr[k]), k
+    assert np.all(go["area"][-2:] == 0) and np.all(go["gravity"][-2:] == 1)
+    assert np.all(go["posn"][-2:] == 0) and np.all(go["flux"][-2:] == 0)
