@@ -49,7 +49,17 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", default="wd_dm_large",
-                    choices=("wd_dm_large", "wd_dm_small", "tiny_star", "mcmc_batch"))
+                    choices=("wd_dm_large", "wd_dm_small", "tiny_star", "mcmc_batch",
+                             "surrogate_da"))
+    ap.add_argument("--train-curves", type=int, default=200000)
+    ap.add_argument("--epochs", type=int, default=60)
+    ap.add_argument("--chains", type=int, default=512)
+    ap.add_argument("--mcmc-steps", type=int, default=2000)
+    ap.add_argument("--burn", type=int, default=400)
+    ap.add_argument("--ncoef", type=int, default=64)
+    ap.add_argument("--local-curves", type=int, default=65536)
+    ap.add_argument("--refine-epochs", type=int, default=150)
+    ap.add_argument("--da-scale", type=float, default=1.6)
     ap.add_argument("--precision", choices=("mixed", "fp64"), default="mixed")
     ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -602,8 +612,178 @@ def run_reference_batch(args):
     return 0
 
 
+# ---- learned surrogate + delayed acceptance ---------------------------------------------
+def _peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+def _bf16_peak():
+    p = _peaks()
+    for k in ("bf16_tflops", "bf16_dense_tflops"):
+        if isinstance(p.get(k), (int, float)):
+            return float(p[k]), "measured (MEASURED_PEAKS.json %s)" % k
+    return 1590.0, "fallback 1.59 PFLOP/s"
+
+
+def run_surrogate(args):
+    """cfg4: the surrogate trained on engine curves over the prior box, then
+    plain vs delayed-acceptance Metropolis (same proposals, same start) on
+    wd_dm_small data; effective samples per second of sampling."""
+    import torch
+    rank, local, world = rank_info()
+    torch.cuda.set_device(local)
+    from lcurve_re_b200 import surrogate as S
+    from lcurve_re_b200 import workloads as W
+    from lcurve_re_b200.engine import Engine
+    from lcurve_re_b200.sampler import ExactChi2, delayed_acceptance, ess_total, metropolis
+
+    eng = Engine(device=local, precision="mixed")
+    clocks = Clocks(local)
+    clocks.start()
+    # training curves from the batched engine
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    theta, curves = S.training_set(eng, args.train_curves, seed=100 + rank, batch=2048)
+    t_gen = time.perf_counter() - t0
+    sur = S.Surrogate(ncoef=args.ncoef, batch=4096, seed=rank)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    losses = sur.fit(theta, curves, epochs=args.epochs)
+    ev1.record()
+    torch.cuda.synchronize()
+    t_fit = ev0.elapsed_time(ev1) / 1e3
+    nsteps_fit = args.epochs * (args.train_curves // sur.net.B)
+    train_flop = nsteps_fit * sur.net.B * sur.net.flops_per_sample(train=True)
+    # held-out accuracy
+    th_h, cu_h = S.training_set(eng, 2048, seed=999, batch=2048)
+    pred = sur.curves(th_h)
+    rel_err = float(np.sqrt(np.mean((pred - cu_h) ** 2)))
+    # data: wd_dm_small physics at the even points of the grid
+    idx = np.arange(0, S.NGRID, 2)
+    truth = np.array([0.25, 86.0, 0.015, 0.20, 20000.0, 3200.0, 0.08, 0.5, 0.0])
+    calc = eng.light_curve_comp(S.ModelFactory()(truth[None])[0], W.data(S.NGRID, -0.2, 1.2),
+                                scale=False, rdata=False, sfac=np.ones(5), diagnostics=False)[0]
+    data = W.add_noise(W.data(S.NGRID, -0.2, 1.2)[idx], calc[idx], 1234 + rank)
+    exact = ExactChi2(eng, data)
+    sur_chi = S.SurrogateChi2(sur, data, idx)
+    rng = np.random.default_rng(7 + rank)
+    scale0 = (S.BOX[:, 1] - S.BOX[:, 0]) * 1e-3
+    theta0 = truth + rng.standard_normal((args.chains, 9)) * scale0
+    # burn-in with plain Metropolis, then the adapted proposal (2.38^2 / d)
+    cov = np.diag(scale0 ** 2)
+    for k in range(2):
+        ch, theta0, _, acc_b, _ = metropolis(exact, theta0, cov, args.burn // 2, seed=11 + k)
+        samp = ch[ch.shape[0] // 2:].reshape(-1, 9)
+        cov = np.cov(samp.T) * 2.38 ** 2 / 9 + np.diag((scale0 * 1e-3) ** 2)
+    # refinement: the same network trained again on engine curves around the
+    # burn-in posterior (Gaussian, 3x its spread, inside the box)
+    samp = ch[ch.shape[0] // 2:].reshape(-1, 9)
+    th_loc = S.local_draws(samp.mean(0), np.cov(samp.T), args.local_curves, seed=5 + rank)
+    t0 = time.perf_counter()
+    _, cu_loc = S.training_set(eng, 0, theta=th_loc, batch=2048)
+    sur_loc = S.Surrogate(ncoef=args.ncoef, batch=4096, seed=rank + 1)
+    losses_loc = sur_loc.fit(th_loc, cu_loc, epochs=args.refine_epochs)
+    t_ref = time.perf_counter() - t0
+    th_lh = S.local_draws(samp.mean(0), np.cov(samp.T), 2048, seed=77 + rank)
+    _, cu_lh = S.training_set(eng, 0, theta=th_lh, batch=2048)
+    loc_err = float(np.sqrt(np.mean((sur_loc.curves(th_lh) - cu_lh) ** 2)))
+    glob_err_loc = float(np.sqrt(np.mean((sur.curves(th_lh) - cu_lh) ** 2)))
+    exact = ExactChi2(eng, data)
+    sur_loc_chi = S.SurrogateChi2(sur_loc, data, idx)
+    # inference throughput of the network alone (the DA screening pass)
+    xin = torch.rand(args.chains, 9, device="cuda") * 2 - 1
+    for _ in range(3):
+        sur.net.forward(xin)
+    ev0.record()
+    for _ in range(50):
+        sur.net.forward(xin)
+    ev1.record()
+    torch.cuda.synchronize()
+    t_inf = ev0.elapsed_time(ev1) / 1e3 / 50
+    lib = eng.lib
+    lib.lcg_kernel_launches(1)
+    e_plain0 = exact.evals
+    chp, _, _, accp, wall_p = metropolis(exact, theta0, cov, args.mcmc_steps, seed=21)
+    launches_plain = int(lib.lcg_kernel_launches(1))
+    # delayed acceptance can afford bolder proposals: the surrogate screens them
+    cov_da = cov * args.da_scale ** 2
+    n_plain = exact.evals - e_plain0
+    exact_g = ExactChi2(eng, data, curves=True)
+    chg, _, _, accg, wall_g, stg = delayed_acceptance(exact_g, sur_chi, theta0, cov_da,
+                                                       args.mcmc_steps, seed=21)
+    exact2 = ExactChi2(eng, data, curves=True)
+    lib.lcg_kernel_launches(1)
+    chd, _, _, accd, wall_d, st = delayed_acceptance(exact2, sur_loc_chi, theta0, cov_da,
+                                                      args.mcmc_steps, seed=21)
+    launches_da = int(lib.lcg_kernel_launches(1))
+    clk = clocks.stop()
+    ess_g, _ = ess_total(chg)
+    shift_g = np.abs(chg.reshape(-1, 9).mean(0) - chp.reshape(-1, 9).mean(0)) / \
+        chp.reshape(-1, 9).std(0)
+    ess_p, per_p = ess_total(chp)
+    ess_d, per_d = ess_total(chd)
+    sp, sd = chp.reshape(-1, 9), chd.reshape(-1, 9)
+    shift = np.abs(sd.mean(0) - sp.mean(0)) / sp.std(0)
+    peak, peak_src = _bf16_peak()
+    train_tflops = train_flop / t_fit / 1e12
+    line = {
+        "metric": "MCMC effective samples/s", "value": ess_d / wall_d,
+        "unit": "effective samples/s", "n_gpus": world, "steps": args.mcmc_steps,
+        "warmup": args.burn, "ms_per_step": wall_d / args.mcmc_steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16 tensor-core MLP (fp32 accumulate) + f32/f64 engine",
+        "data": "synthetic (wd_dm_small physics at 500 points + noise sigma=1.5e-3)",
+        "config": {"workload": "surrogate_da: %d chains x %d steps, 9 parameters; surrogate "
+                               "9 -> 4x256 GELU -> 64 PCA coefficients of a %d-point curve, "
+                               "%d training curves" % (args.chains, args.mcmc_steps, S.NGRID,
+                                                       args.train_curves),
+                   "ess": "Geyer initial positive sequence, min over parameters of the sum "
+                          "over chains (new_scripts/mcmc_solver.cpp:80-115)"},
+        "plain": {"ess": ess_p, "ess_per_s": ess_p / wall_p, "wall_s": wall_p,
+                  "acceptance": accp, "exact_evals": n_plain},
+        "delayed_acceptance": {"surrogate": "refined around the burn-in posterior",
+                               "ess": ess_d, "ess_per_s": ess_d / wall_d, "wall_s": wall_d,
+                               "acceptance": accd, "exact_evals": exact2.evals, **st},
+        "delayed_acceptance_global": {"surrogate": "prior box only",
+                                      "ess": ess_g, "ess_per_s": ess_g / wall_g,
+                                      "wall_s": wall_g, "acceptance": accg,
+                                      "exact_evals": exact_g.evals,
+                                      "posterior_mean_shift_sigma_max": float(shift_g.max()),
+                                      **stg},
+        "ess_per_s_ratio": (ess_d / wall_d) / (ess_p / wall_p),
+        "posterior_mean_shift_sigma_max": float(shift.max()),
+        "surrogate": {"train_curves": args.train_curves, "curve_generation_s": t_gen,
+                      "curves_per_s": args.train_curves / t_gen, "fit_s": t_fit,
+                      "epochs": args.epochs, "final_loss": losses[-1],
+                      "heldout_rms_curve_error": rel_err, "pca_max_error": sur.pca_max_err,
+                      "inference_ms_per_batch": t_inf * 1e3,
+                      "refined": {"curves": args.local_curves, "seconds": t_ref,
+                                  "final_loss": losses_loc[-1],
+                                  "local_rms_curve_error": loc_err,
+                                  "global_net_local_rms_curve_error": glob_err_loc,
+                                  "pca_max_error": sur_loc.pca_max_err}},
+        "roofline": {"bound": "tensor", "kernel": "k_gemm (training, all layers)",
+                     "achieved": train_tflops, "peak": peak, "unit": "TFLOP/s",
+                     "frac": train_tflops / peak, "traffic": None, "peak_source": peak_src,
+                     "flop_per_sample_train": sur.net.flops_per_sample(train=True)},
+        "gpu_launches": launches_da,
+        "gpu_launches_plain": launches_plain,
+        "da_proposal_scale": args.da_scale,
+        "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    eng.close()
+    return 0
+
+
 def main():
     args = parse()
+    if args.impl == "ours" and args.workload == "surrogate_da":
+        return run_surrogate(args)
     if args.impl == "reference":
         return run_reference_batch(args) if args.workload == "mcmc_batch" else run_reference(args)
     if args.workload == "mcmc_batch":

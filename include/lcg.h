@@ -306,6 +306,59 @@ int64_t lcg_kernel_launches(int32_t reset);
  * roofline. */
 lcg_status lcg_measure_fp32_peak(lcg_ctx *ctx, double *tflops);
 
+/* ---- surrogate network kernels (no reference counterpart) -------------
+ * The delayed-acceptance sampler screens proposals with a small MLP whose
+ * training and inference run on these kernels. Device pointers, all on the
+ * caller's stream; BF16 matrices are row-major.
+ *
+ * lcg_mlp_gemm: D[m x n] = A[m x k] * B[n x k]^T on the tensor cores (BF16
+ * in, FP32 accumulate), m a multiple of 128, k of 64, n of 64; A, B 16-byte
+ * aligned. epi selects the fused epilogue:
+ *   LCG_EPI_GELU    z = D + bias (BF16), y = GELU(z) (BF16), yt = y^T
+ *                   (BF16, row stride ldt; may be NULL)
+ *   LCG_EPI_LINEAR  out = D + bias (FP32)
+ *   LCG_EPI_DGELU   y = D * GELU'(z) with z read (BF16), yt = y^T
+ *   LCG_EPI_F32     out = D (FP32)
+ * Rows >= mvalid are not stored. *err (may be NULL) is set if a pipeline
+ * wait timed out. */
+enum { LCG_EPI_GELU = 0, LCG_EPI_LINEAR = 1, LCG_EPI_DGELU = 2, LCG_EPI_F32 = 3 };
+lcg_status lcg_mlp_gemm(void *stream, int32_t epi, int32_t m, int32_t n, int32_t k,
+                        const void *a, const void *b, const float *bias, void *z, void *y,
+                        void *yt, float *out, int32_t mvalid, int32_t ldt, int32_t *err);
+/* Adam step on FP32 master weights [rows x cols] (moments m1, m2), writing
+ * the BF16 weights and their BF16 transpose (either may be NULL). */
+lcg_status lcg_mlp_adam(void *stream, float *w, float *m1, float *m2, const float *g,
+                        int32_t rows, int32_t cols, float lr, float beta1, float beta2,
+                        float eps, int32_t step, void *w_bf16, void *wt_bf16);
+/* out[c] = sum over the first rvalid rows of the BF16 [rows x cols] g. */
+lcg_status lcg_mlp_colsum(void *stream, const void *g_bf16, int32_t rows, int32_t cols,
+                          int32_t rvalid, float *out);
+/* Gradient of the mean squared error of out against target ([rows x cols]
+ * FP32, first rvalid rows), as BF16 and its BF16 transpose (row stride ldt),
+ * and the per-row squared-error sums (may be NULL). cols <= 256. */
+lcg_status lcg_mlp_mse_grad(void *stream, const float *out, const float *target, int32_t rows,
+                            int32_t cols, int32_t rvalid, int32_t ldt, void *g_bf16,
+                            void *gt_bf16, float *loss_rows);
+/* Input layer in FP32 (kin <= 16): z = x w^T + b, y = GELU(z) as BF16 [m x n]
+ * (z and yt = y^T, row stride ldt, may be NULL); rows >= mvalid are zero. */
+lcg_status lcg_mlp_input(void *stream, const float *x, int32_t kin, const float *w,
+                         const float *b, int32_t m, int32_t n, int32_t mvalid, void *z, void *y,
+                         void *yt, int32_t ldt);
+/* dw[n x kin] = g^T x over the first mvalid rows (g BF16 [m x n], x FP32). */
+lcg_status lcg_mlp_input_grad(void *stream, const void *g_bf16, const float *x, int32_t kin,
+                              int32_t m, int32_t n, int32_t mvalid, float *dw);
+/* Per row r of coef [m x ncoef]: the surrogate curve s(c) = mean + c * basis
+ * (basis [ncoef x npts]) at the data points, or, with an anchor (exact curves
+ * [m x npts] at the points coef_x [m x ncoef] describes), the anchored curve
+ * anchor * s(coef) / s(coef_x); then chi**2 of the data after the optimal
+ * scale s = sum(w f y / e^2) / sum(w f^2 / e^2), as re_scale does
+ * (chisq[m]; scale[m] may be NULL; coef_x and anchor NULL for none). */
+lcg_status lcg_mlp_pca_chisq(void *stream, const float *coef, int32_t m, int32_t ncoef,
+                             const float *basis, const float *mean, int32_t npts,
+                             const double *flux, const double *ferr, const double *weight,
+                             const float *coef_x, const double *anchor, double *chisq,
+                             double *scale);
+
 #ifdef __cplusplus
 }
 #endif

@@ -31,6 +31,7 @@ SOURCES = {
     "flux.cu": ["--fmad=true"],
     "noalloc.cu": ["--fmad=false"],
     "batch_host.cu": ["--fmad=false"],
+    "mlp.cu": ["--fmad=true"],
 }
 HEADERS = ["roche.cuh", "eclipse.cuh", "engine.h", "tma.cuh", "context.h"]
 

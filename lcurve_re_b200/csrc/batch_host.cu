@@ -79,9 +79,12 @@ struct BatchState {
     std::map<int32_t, RingSet> ringsets;
     std::vector<RingRec> h_rings;
     DBuf<RingRec> rings;
-    // per-model exact-reuse keys
+    // per-model exact-reuse keys: the last model evaluated in each position,
+    // its input scale and the data version its results belong to
     std::vector<lcg_model> key;
     std::vector<uint8_t> key_ok;
+    std::vector<double> key_sfac0;
+    int64_t data_version = -1;
     // host table (pinned) and its device copy
     unsigned char *h_tab = nullptr;
     size_t tab_bytes = 0;
@@ -312,6 +315,7 @@ lcg_status relayout(lcg_ctx *c, BatchState &B, const lcg_model *models, int32_t 
     cudaMemsetAsync(B.n0.p, 0, ns * sizeof(int64_t), c->stream);
     B.key.assign(nm, lcg_model{});
     B.key_ok.assign(nm, 0);
+    B.key_sfac0.assign(nm, 0.);
     for (int s = 0; s < B.nslots; s++) {
         SlotDev &S = B.tab<SlotDev>(B.o_slots)[s];
         S.face0 = B.face0[s];
@@ -424,14 +428,28 @@ extern "C" lcg_status lcg_light_curve_batch_resident(lcg_ctx *c, const lcg_model
         SlotDev *slots = B.tab<SlotDev>(B.o_slots);
         ModelDev *md = B.tab<ModelDev>(B.o_models);
         std::vector<uint8_t> geo((size_t)nmodels, 0), cont((size_t)nmodels, 0);
+        std::vector<uint8_t> reuse((size_t)nmodels, 0);
         const double xmin = c->data_xmin, xmax = c->data_xmax;
-        parallel_for(nmodels, [&](int m) {
+        const bool same_data = B.data_version == c->data_version;
+        // the same model as last time in its position, on the same points:
+        // its previous results stand and nothing runs for it
+        std::vector<int> todo;
+        todo.reserve((size_t)nmodels);
+        for (int32_t m = 0; m < nmodels; m++) {
+            md[m].live = 0;
+            slots[2 * m].live = slots[2 * m + 1].live = 0;
+            if (!inb[m]) continue;
+            if (same_data && B.key_ok[m] && memcmp(&B.key[m], models + m, sizeof(lcg_model)) == 0 &&
+                ((flags & LCG_FLAG_SCALE) || B.key_sfac0[m] == sfac[5 * (size_t)m]))
+                reuse[m] = 1;
+            else
+                todo.push_back(m);
+        }
+        parallel_for((int)todo.size(), [&](int j) {
+            const int m = todo[(size_t)j];
             const lcg_model &M = models[m];
             ModelDev &D = md[m];
             SlotDev *S = slots + 2 * m;
-            D.live = 0;
-            S[0].live = S[1].live = 0;
-            if (!inb[m]) return;
             // light_curve_comp.cpp:130-154
             double r1, r2;
             get_r1r2(M, r1, r2);
@@ -567,9 +585,10 @@ extern "C" lcg_status lcg_light_curve_batch_resident(lcg_ctx *c, const lcg_model
         const DevStatus *dst = B.res<DevStatus>(B.r_st);
         const double *hs = B.res<double>(B.r_sfac), *ho = B.res<double>(B.r_out);
         const double *hc = B.res<double>(B.r_calc);
+        B.data_version = c->data_version;
         for (int32_t m = 0; m < nmodels; m++) {
             if (!inb[m]) continue;
-            if (!md[m].live || dst[m].code) {
+            if (!reuse[m] && (!md[m].live || dst[m].code)) {
                 if (!status[m]) status[m] = dst[m].code;
                 B.key_ok[m] = 0;
                 if (calc) memset(calc + (size_t)m * n, 0, (size_t)n * sizeof(double));
@@ -577,6 +596,7 @@ extern "C" lcg_status lcg_light_curve_batch_resident(lcg_ctx *c, const lcg_model
             }
             B.key[m] = models[m];
             B.key_ok[m] = 1;
+            B.key_sfac0[m] = sfac[5 * (size_t)m];
             if (calc) memcpy(calc + (size_t)m * n, hc + (size_t)m * n, (size_t)n * sizeof(double));
             for (int k = 0; k < 5; k++) sfac[5 * (size_t)m + k] = hs[5 * (size_t)m + k];
             if (ho[3 * m + 2] != 0.) {
@@ -584,7 +604,9 @@ extern "C" lcg_status lcg_light_curve_batch_resident(lcg_ctx *c, const lcg_model
                 if (wnok) wnok[m] = ho[3 * m + 1];
             }
         }
-        c->flux_elements += B.nfaces * B.nent;
+        for (int32_t m = 0; m < nmodels; m++)
+            if (md[m].live)
+                c->flux_elements += (B.face0[2 * m + 2] - B.face0[2 * m]) * B.nent;
     }
     // the rest, one at a time
     for (int32_t m = 0; m < nmodels; m++) {

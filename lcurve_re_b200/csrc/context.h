@@ -159,6 +159,7 @@ struct lcg_ctx {
     std::vector<double> h_diag;
     // resident light-curve points (lcg_set_data)
     int32_t data_n = 0;
+    int64_t data_version = 0;  // bumped by every lcg_set_data
     int64_t data_nent = 0;
     double data_xmin = 0., data_xmax = 0.;
     // profiling

@@ -7,7 +7,10 @@
 // includes this is compiled with --fmad=false), so the eclipse flags and
 // phases follow the reference decision for decision. Every loop that the
 // reference leaves unbounded carries an iteration cap; hitting one returns
-// kEclNoConverge instead of spinning.
+// kEclNoConverge instead of spinning. linmin, pot_min and fblink are
+// out-of-line functions: inlined into every caller they overflow the
+// instruction cache and the warps stall on instruction fetch (dbrent stays
+// inline in its two callers).
 #pragma once
 
 #include "roche.cuh"
@@ -135,7 +138,7 @@ __device__ double dbrent(double ax, double bx, double cx, const LineFn &f, doubl
 // Roche::linmin (pot_min.cpp:127-420). jammed starts false: the reference
 // leaves it unset on early returns whose pmin equals the starting potential,
 // where pot_min stops regardless of it.
-__device__ void linmin(int star, double q, double spin, double cosi, double sini, V3 p,
+__device__ __noinline__ void linmin(int star, double q, double spin, double cosi, double sini, V3 p,
                        double &phi, double &lam, double dphi, double dlam, double phi1,
                        double phi2, double lam1, double lam2, double pref, double acc,
                        double &pmin, bool &jammed, int &st) {
@@ -256,7 +259,7 @@ __device__ void linmin(int star, double q, double spin, double cosi, double sini
 
 // Roche::pot_min (pot_min.cpp:38-100): conjugate gradients in (phase,
 // lambda) for the lowest potential on the line-of-sight cone.
-__device__ bool pot_min(int star, double q, double spin, double cosi, double sini, V3 p,
+__device__ __noinline__ bool pot_min(int star, double q, double spin, double cosi, double sini, V3 p,
                         double phi1, double phi2, double lam1, double lam2, double rref,
                         double pref, double acc, double &phi, double &lam, int &st) {
     double dphi, dlam, gdphi, gdlam, hdphi, hdlam;
@@ -308,7 +311,7 @@ __device__ bool pot_min(int star, double q, double spin, double cosi, double sin
 }
 
 // Roche::fblink (fblink.cpp:34-104): is p hidden along earth by the star?
-__device__ bool fblink(int star, double q, double spin, double acc, V3 earth, V3 p,
+__device__ __noinline__ bool fblink(int star, double q, double spin, double acc, V3 earth, V3 p,
                        double rref, double pref, int &st) {
     const V3 cofm = star == kStar1 ? v3(0., 0., 0.) : v3(1., 0., 0.);
     double lam1, lam2;

@@ -745,6 +745,7 @@ lcg_status lcg_set_data(lcg_ctx *c, const lcg_datum *data, int32_t n) {
     cudaMemcpyAsync(c->off.p, off.data(), (size_t)(n + 1) * sizeof(int64_t),
                     cudaMemcpyHostToDevice, c->stream);
     c->data_n = n;
+    c->data_version++;
     c->data_nent = off[n];
     c->data_xmin = xmin;
     c->data_xmax = xmax;

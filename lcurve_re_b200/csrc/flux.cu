@@ -237,7 +237,12 @@ void launch_ppt(int star, const FluxConsts &k, const FlatDev &f, const PhaseDev 
 //   fI  = flux * I(t), Horner on per-face coefficients 4 FFMA2
 //   s  += m * fI                                       1 FFMA2
 // one-range faces add the fixed-point eclipse test (IADD, ISETP, FSEL per face).
-// Phase entries are dealt to the tiles round-robin so every tile is equally full.
+// Each thread holds PPT consecutive phase entries, so a warp covers 32 * PPT
+// consecutive entries: a narrow arc of the orbit for time-ordered points.
+// A face pair that faces away (mu <= 0) or is eclipsed at every entry of the
+// warp adds exactly zero to every sum, so the warp skips its intensity
+// (a vote per pair); nearly half the pairs fall out this way, and the sums
+// are bit-identical to evaluating them.
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 
 template <int PPT, int LT, bool ECL>
@@ -254,12 +259,12 @@ __device__ __forceinline__ void sweep_pairs(const float4 *sp, const uint4 *se, i
         for (int j = 0; j < PPT; j++) s[j] = f2(0.f, 0.f);
 #pragma unroll 2
         for (int i = 0; i < cnt; i++) {
-            const float4 P0 = rp[4 * i], P1 = rp[4 * i + 1], P2 = rp[4 * i + 2], P3 = rp[4 * i + 3];
+            const float4 P0 = rp[4 * i], P1 = rp[4 * i + 1];
             const float2 nx = f2(P0.x, P0.y), ny = f2(P0.z, P0.w), cz = f2(P1.x, P1.y);
-            const float2 p0 = f2(P1.z, P1.w), p1 = f2(P2.x, P2.y), p2 = f2(P2.z, P2.w);
-            const float2 p3 = f2(P3.x, P3.y), p4 = f2(P3.z, P3.w);
             uint4 E = make_uint4(0u, 0u, 0u, 0u);
             if constexpr (ECL) E = ep[i];
+            float2 m[PPT];
+            bool vis = false;
 #pragma unroll
             for (int j = 0; j < PPT; j++) {
                 const float2 mu = __ffma2_rn(ex[j], nx, __ffma2_rn(ey[j], ny, cz));
@@ -268,13 +273,21 @@ __device__ __forceinline__ void sweep_pairs(const float4 *sp, const uint4 *se, i
                     ma = ((pf[j] - E.x) >= E.y) ? ma : 0.f;
                     mb = ((pf[j] - E.z) >= E.w) ? mb : 0.f;
                 }
-                const float2 m = f2(ma, mb);
+                m[j] = f2(ma, mb);
+                vis = vis || ma > 0.f || mb > 0.f;
+            }
+            if (!__any_sync(0xffffffffu, vis)) continue;
+            const float4 P2 = rp[4 * i + 2], P3 = rp[4 * i + 3];
+            const float2 p0 = f2(P1.z, P1.w), p1 = f2(P2.x, P2.y), p2 = f2(P2.z, P2.w);
+            const float2 p3 = f2(P3.x, P3.y), p4 = f2(P3.z, P3.w);
+#pragma unroll
+            for (int j = 0; j < PPT; j++) {
                 float2 t;
-                if constexpr (LT == 1) t = f2(sqrt_approx(ma), sqrt_approx(mb));
-                else t = m;
+                if constexpr (LT == 1) t = f2(sqrt_approx(m[j].x), sqrt_approx(m[j].y));
+                else t = m[j];
                 const float2 fI =
                     __ffma2_rn(t, __ffma2_rn(t, __ffma2_rn(t, __ffma2_rn(t, p4, p3), p2), p1), p0);
-                s[j] = __ffma2_rn(m, fI, s[j]);
+                s[j] = __ffma2_rn(m[j], fI, s[j]);
             }
         }
 #pragma unroll
@@ -307,7 +320,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     uint32_t pf[PPT];
 #pragma unroll
     for (int j = 0; j < PPT; j++) {
-        const int64_t e = blockIdx.x + ntile * ((int64_t)j * kThreads + tid);
+        const int64_t e = (int64_t)blockIdx.x * (kThreads * PPT) + tid * PPT + j;
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
         if (e < ph.nent) v = ph.ef[e];
         ex[j] = f2(v.x, v.x);
@@ -335,7 +348,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     sweep_pairs<PPT, LT, true>(sp, se, q0, qa > q0 ? qa : q0, qend, ex, ey, pf, acc);
 #pragma unroll
     for (int j = 0; j < PPT; j++) {
-        const int64_t e = blockIdx.x + ntile * ((int64_t)j * kThreads + tid);
+        const int64_t e = (int64_t)blockIdx.x * (kThreads * PPT) + tid * PPT + j;
         if (e < ph.nent) part[(int64_t)blockIdx.y * ldp + e] = (double)acc[j];
     }
 }
@@ -354,6 +367,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     const int64_t tile = blockIdx.x % ntile, gc = blockIdx.x / ntile;
     const int s = find_seg(b.chunk_pre, b.nslots, gc);
     const SlotDev &S = b.slots[s];
+    if (!S.live) return;  // not evaluated this call (unchanged or failed)
     const int64_t c0 = (gc - b.chunk_pre[s]) * chunk;
     const int64_t n = S.nface, n0 = b.n0[s];
     const int64_t cend = (c0 + chunk < n) ? c0 + chunk : n;
@@ -374,7 +388,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     uint32_t pf[PPT];
 #pragma unroll
     for (int j = 0; j < PPT; j++) {
-        const int64_t e = tile + ntile * ((int64_t)j * kThreads + tid);
+        const int64_t e = tile * (kThreads * PPT) + tid * PPT + j;
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
         if (e < ph.nent) v = ef[e];
         ex[j] = f2(v.x, v.x);
@@ -403,7 +417,7 @@ __global__ void __launch_bounds__(kThreads, 2)
     }
 #pragma unroll
     for (int j = 0; j < PPT; j++) {
-        const int64_t e = tile + ntile * ((int64_t)j * kThreads + tid);
+        const int64_t e = tile * (kThreads * PPT) + tid * PPT + j;
         if (e < ph.nent) part[gc * ldp + e] = (double)acc[j];
     }
 }

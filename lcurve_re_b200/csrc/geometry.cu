@@ -156,7 +156,7 @@ __global__ void k_ecl_pre(EclParams p, int32_t eclipse_on, GridDev g, int32_t *q
 // 32 consecutive candidates at a time so that neighbouring faces (similar
 // iteration counts) run in lockstep. The count is read on the device, so the
 // choice needs no host round trip.
-__global__ void __launch_bounds__(128) k_ecl_roche(EclParams p, GridDev g,
+__global__ void __launch_bounds__(128, 4) k_ecl_roche(EclParams p, GridDev g,
                                                    const int32_t *__restrict__ queue,
                                                    int32_t *counters, DevStatus *st,
                                                    int32_t warp_max) {
@@ -675,7 +675,7 @@ __global__ void k_ecl_pre_b(BatchDev b) {
 
 // k_ecl_roche over the batch queue: each candidate finds its slot by its
 // face index.
-__global__ void __launch_bounds__(128) k_ecl_roche_b(BatchDev b, int32_t warp_max) {
+__global__ void __launch_bounds__(128, 4) k_ecl_roche_b(BatchDev b, int32_t warp_max) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int total = b.counters[0];
@@ -816,7 +816,7 @@ __global__ void k_phases_b(BatchDev b, const DatumRec *__restrict__ data,
                            const int64_t *__restrict__ off, int32_t n, BatchPhases ph) {
     const int np = blockIdx.x * blockDim.x + threadIdx.x;
     const int m = blockIdx.y;
-    if (np >= n) return;
+    if (np >= n || !b.models[m].live) return;
     const PhaseParams &p = b.models[m].pp;
     const DatumRec d = data[np];
     double phase, slfac;
@@ -842,7 +842,7 @@ __global__ void k_reduce_b(BatchDev b, const double *__restrict__ part, int64_t 
                            double *osum) {
     const int s = blockIdx.y;
     const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (e >= nent) return;
+    if (e >= nent || !b.slots[s].live) return;
     const int64_t c0 = b.chunk_pre[s], c1 = b.chunk_pre[s + 1];
     double o = 0.0;
     int64_t c = c0;
@@ -863,7 +863,7 @@ __global__ void k_scatter_b(BatchDev b, BatchPhases ph, const double *__restrict
                             int32_t n, double *calc) {
     const int np = blockIdx.x * blockDim.x + threadIdx.x;
     const int m = blockIdx.y;
-    if (np >= n) return;
+    if (np >= n || !b.models[m].live) return;
     const int64_t row = m * ph.ldp;
     const double *o1 = osum + (2 * (int64_t)m) * ph.ldp, *o2 = o1 + ph.ldp;
     const int64_t e0 = off[np], e1 = e0 + (data[np].ndiv > 0 ? data[np].ndiv : 0);
@@ -879,6 +879,7 @@ __global__ void __launch_bounds__(1024) k_finalize_b(BatchDev b, int32_t flags,
                                                      double *out) {
     __shared__ double sh[1024];
     const int m = blockIdx.x;
+    if (!b.models[m].live) return;  // keeps the previous call's results
     double *sf = sfac + 5 * (int64_t)m;
     if (threadIdx.x == 0) sf[0] = b.models[m].sfac0;
     __syncthreads();

@@ -1,0 +1,196 @@
+"""Random-walk Metropolis over many parallel chains, plain or with delayed
+acceptance screened by a surrogate, and the effective-sample-size
+estimator of the reference sampler.
+
+The likelihood is exp(-chi**2 / 2) with chi**2 from a callable over a batch
+of parameter vectors (one row per chain): the exact GPU engine
+(ExactChi2: every chain's model in one lcg_light_curve_batch_resident call)
+or the surrogate (surrogate.SurrogateChi2). The prior is uniform over a box.
+
+Delayed acceptance (Christen & Fox 2005): a proposal y from x first passes
+the approximation's test with probability g(x, y) = min(1, pi*_x(y) / pi*_x(x));
+only then is the exact chi**2 computed, and y is accepted with probability
+min(1, pi(y) g(y, x) / (pi(x) g(x, y))), which leaves the exact posterior
+invariant for any approximation, including one that depends on the current
+state. Two are supported: the surrogate's own chi**2 (pi* = exp(-chi_s/2)),
+and the anchored one, chi**2 of exact(x) * s(y) / s(x), which needs the exact
+curve at the current state (ExactChi2 keeps the curves it computed) and, for
+g(y, x), at the proposal. Chains whose proposal the approximation rejects
+pass the engine the model it evaluated for them last, so the batched engine
+skips them entirely.
+"""
+import time
+
+import numpy as np
+
+from .surrogate import ModelFactory, in_box
+
+
+def ess_geyer(x):
+    """Geyer's initial-positive-sequence ESS of one chain, as the reference
+    sampler computes it (new_scripts/mcmc_solver.cpp:80-115): autocorrelations
+    summed in consecutive pairs up to the first negative pair sum, lags up to
+    min(n/2, 10000). Autocovariances come from an FFT (the same sums)."""
+    x = np.asarray(x, np.float64)
+    n = x.shape[0]
+    if n < 4:
+        return float(n)
+    xc = x - x.mean()
+    c0 = float(np.dot(xc, xc)) / n
+    if c0 < 1e-30:
+        return float(n)
+    size = 1 << int(np.ceil(np.log2(2 * n)))
+    f = np.fft.rfft(xc, size)
+    acov = np.fft.irfft(f * np.conj(f), size)[:n]  # acov[k] = sum_i xc[i] xc[i+k]
+    rho = acov / (n * c0)
+    tau = 1.0
+    max_lag = min(n // 2, 10000)
+    for lag in range(1, max_lag, 2):
+        r1 = rho[lag]
+        r2 = rho[lag + 1] if lag + 1 < n else 0.0
+        if r1 + r2 < 0.0:
+            break
+        tau += 2.0 * (r1 + r2)
+    return n / max(tau, 1.0)
+
+
+def ess_total(chain):
+    """chain [steps x chains x params]: per parameter, the sum over chains
+    of ess_geyer; the minimum over parameters (the reference reports the
+    minimum)."""
+    steps, nc, npar = chain.shape
+    per = np.array([[ess_geyer(chain[:, c, k]) for c in range(nc)] for k in range(npar)])
+    return float(per.sum(axis=1).min()), per.sum(axis=1)
+
+
+class ExactChi2:
+    """chi**2 of the resident data for each row of theta, from the batched
+    engine (scale fitted, as re_scale does). Failed models get +inf."""
+
+    def __init__(self, engine, data, factory=None, curves=False):
+        self.engine = engine
+        self.fac = factory or ModelFactory()
+        engine.set_data(data)
+        self.evals = 0
+        self.calls = 0
+        self._last = None
+        self.keep_curves = curves
+        self.curves = None  # the last call's light curves (scaled), when kept
+
+    def __call__(self, theta):
+        theta = np.asarray(theta, np.float64)
+        ms = self.fac(theta)
+        calc, chisq, _, _, st = self.engine.light_curve_batch_resident(
+            ms, calc=self.keep_curves)
+        self.curves = calc
+        if self._last is None or self._last.shape != theta.shape:
+            self.evals += theta.shape[0]
+        else:
+            self.evals += int(np.any(theta != self._last, axis=1).sum())
+        self._last = theta.copy()
+        self.calls += 1
+        out = chisq.copy()
+        out[st != 0] = np.inf
+        return out
+
+
+def _proposal(rng, theta, chol):
+    return theta + rng.standard_normal(theta.shape) @ chol.T
+
+
+def metropolis(exact, theta0, cov, steps, seed=0, box_check=in_box, record=True):
+    """Plain random-walk Metropolis on every chain at once. Returns
+    (chain [steps x chains x params] or None, final theta, final chi**2,
+    acceptance rate, wall seconds)."""
+    rng = np.random.default_rng(seed)
+    chol = np.linalg.cholesky(cov)
+    theta = np.array(theta0, np.float64)
+    chi = exact(theta)
+    last = theta.copy()
+    chain = np.empty((steps,) + theta.shape) if record else None
+    acc = 0
+    t0 = time.perf_counter()
+    for s in range(steps):
+        prop = _proposal(rng, theta, chol)
+        ok = box_check(prop)
+        ev = np.where(ok[:, None], prop, last)
+        chi_p = exact(ev)
+        chi_p[~ok] = np.inf
+        a = np.log(rng.random(theta.shape[0])) < -(chi_p - chi) / 2
+        theta[a] = prop[a]
+        chi[a] = chi_p[a]
+        last = ev
+        acc += int(a.sum())
+        if record:
+            chain[s] = theta
+    wall = time.perf_counter() - t0
+    return chain, theta, chi, acc / (steps * theta.shape[0]), wall
+
+
+def delayed_acceptance(exact, sur, theta0, cov, steps, seed=0, box_check=in_box, record=True):
+    """Delayed-acceptance Metropolis: the approximation screens, the exact
+    model judges every step that passes. sur is either a chi**2 callable
+    (state-independent approximation) or an anchored one with
+    state(theta) -> s and chi2(s_y, s_x, anchor) -> chi**2 of
+    anchor * s(y) / s(x); the anchored form needs exact.curves. Returns
+    (chain, final theta, final chi**2, acceptance rate, wall seconds, stats)."""
+    rng = np.random.default_rng(seed)
+    chol = np.linalg.cholesky(cov)
+    theta = np.array(theta0, np.float64)
+    anchored = hasattr(sur, "state")
+    chi = exact(theta)
+    if anchored:
+        f = np.array(exact.curves, np.float64)
+        sx = sur.state(theta)
+    else:
+        chi_s = sur(theta)
+    last = theta.copy()
+    chain = np.empty((steps,) + theta.shape) if record else None
+    acc = stage1 = 0
+    nc = theta.shape[0]
+    t0 = time.perf_counter()
+    for s in range(steps):
+        prop = _proposal(rng, theta, chol)
+        ok = box_check(prop)
+        if anchored:
+            sy = sur.state(prop)
+            chi_a = sur.chi2(sy, sx, f)       # chi**2 of exact(x) s(y) / s(x)
+            chi_a[~ok] = np.inf
+            log_g = np.minimum(0.0, -(chi_a - chi) / 2)
+        else:
+            chi_sp = np.full(nc, np.inf)
+            if ok.any():
+                chi_sp[ok] = sur(prop[ok])
+            log_g = np.minimum(0.0, -(chi_sp - chi_s) / 2)
+        a1 = ok & (np.log(rng.random(nc)) < log_g)
+        u2 = np.log(rng.random(nc))
+        if a1.any():
+            ev = np.where(a1[:, None], prop, last)
+            chi_p = exact(ev)
+            last = ev
+            if anchored:
+                fp = np.array(exact.curves, np.float64)
+                chi_r = sur.chi2(sx, sy, fp)  # chi**2 of exact(y) s(x) / s(y)
+                log_g_rev = np.minimum(0.0, -(chi_r - chi_p) / 2)
+            else:
+                log_g_rev = np.minimum(0.0, -(chi_s - chi_sp) / 2)
+            with np.errstate(invalid="ignore"):
+                log_rho = -(chi_p - chi) / 2 + log_g_rev - log_g
+            a2 = a1 & (u2 < log_rho)
+            theta[a2] = prop[a2]
+            chi[a2] = chi_p[a2]
+            if anchored:
+                f[a2] = fp[a2]
+                idx = np.nonzero(a2)[0]
+                if idx.size:
+                    sx[idx] = sy[idx]
+            else:
+                chi_s[a2] = chi_sp[a2]
+            acc += int(a2.sum())
+            stage1 += int(a1.sum())
+        if record:
+            chain[s] = theta
+    wall = time.perf_counter() - t0
+    n = steps * nc
+    return chain, theta, chi, acc / n, wall, {"stage1_rate": stage1 / n,
+                                              "stage2_rate": acc / max(stage1, 1)}

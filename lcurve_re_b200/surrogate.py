@@ -1,0 +1,254 @@
+"""Learned surrogate of the light curve over the MCMC prior box.
+
+The surrogate maps the nine sampled parameters (q, iangle, r1, r2, t1, t2,
+gravity_dark2, absorb, t0) to the light curve on a fixed grid of phases
+(1000 points in [-0.2, 1.2]): an MLP (lcurve_re_b200.mlp) predicts the
+curve's coefficients on its leading principal components. Curves are
+normalised to unit mean, since the sampler's chi**2 fits the scale factor
+anyway (re_scale.cpp:16-42).
+
+Training data come from the GPU engine itself: uniform draws over the box,
+evaluated by the batched engine (lcg_light_curve_batch) at the wd_dm_small
+resolution (nlat 40/80). The box is the mcmc_batch distribution's mean
++- 3 sigma, with gravity_dark2 in [0.05, 0.11], absorb in [0.3, 0.7] and t0
+in [-0.005, 0.005].
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import abi
+from . import workloads as W
+from .mlp import MLP
+
+PARAMS = ("q", "iangle", "r1", "r2", "t1", "t2", "gravity_dark2", "absorb", "t0")
+BOX = np.array([
+    (0.19, 0.31),        # q: 0.25 +- 3 x 0.02
+    (84.5, 87.5),        # iangle: 86 +- 3 x 0.5
+    (0.01275, 0.01725),  # r1: 0.015 x (1 +- 3 x 0.05)
+    (0.17, 0.23),        # r2: 0.20 x (1 +- 3 x 0.05)
+    (18200.0, 21800.0),  # t1: 20000 x (1 +- 3 x 0.03)
+    (2912.0, 3488.0),    # t2: 3200 x (1 +- 3 x 0.03)
+    (0.05, 0.11),        # gravity_dark2
+    (0.3, 0.7),          # absorb
+    (-0.005, 0.005),     # t0
+])
+NGRID = 1000
+NCOEF = 64
+
+
+def grid_times(n=NGRID):
+    return np.linspace(-0.2, 1.2, n)
+
+
+def to_unit(theta):
+    """Parameters -> [-1, 1]^9 over the box."""
+    lo, hi = BOX[:, 0], BOX[:, 1]
+    return (np.asarray(theta, np.float64) - (lo + hi) / 2) / ((hi - lo) / 2)
+
+
+def from_unit(u):
+    lo, hi = BOX[:, 0], BOX[:, 1]
+    return (lo + hi) / 2 + np.asarray(u, np.float64) * (hi - lo) / 2
+
+
+def in_box(theta):
+    t = np.asarray(theta)
+    return np.all((t >= BOX[:, 0]) & (t <= BOX[:, 1]), axis=-1)
+
+
+class ModelFactory:
+    """lcg_model arrays for parameter vectors: the base model (wd_dm_small's
+    physics and grids) with the nine sampled fields replaced, written through
+    a structured-array view of the ctypes array (no per-model parsing)."""
+
+    def __init__(self, base=None):
+        self.base = (base if base is not None else W.model()).to_c()
+
+    def __call__(self, theta, out=None):
+        theta = np.atleast_2d(np.asarray(theta, np.float64))
+        n = theta.shape[0]
+        arr = out if out is not None else (abi.LcgModel * n)()
+        view = np.ctypeslib.as_array(arr)
+        view[:] = np.frombuffer(bytes(self.base), dtype=view.dtype)[0]
+        for k, name in enumerate(PARAMS):
+            view[name] = theta[:, k]
+        return arr
+
+
+def training_set(engine, n, seed=0, batch=2048, npts=NGRID, theta=None):
+    """n uniform draws over the box (or the given parameter vectors) and
+    their unit-mean light curves on the phase grid, from the batched GPU
+    engine. Returns (theta [n x 9], curves [n x npts] float32)."""
+    rng = np.random.default_rng(seed)
+    if theta is None:
+        theta = BOX[:, 0] + rng.random((n, len(PARAMS))) * (BOX[:, 1] - BOX[:, 0])
+    theta = np.asarray(theta, np.float64)
+    n = theta.shape[0]
+    engine.set_data(W.data(npts, -0.2, 1.2))
+    fac = ModelFactory()
+    curves = np.empty((n, npts), np.float32)
+    for i0 in range(0, n, batch):
+        i1 = min(n, i0 + batch)
+        ms = fac(theta[i0:i1])
+        calc, _, _, _, st = engine.light_curve_batch_resident(ms, scale=False, rdata=False,
+                                                              sfac=np.ones(5 * (i1 - i0)))
+        if np.any(st != 0):
+            raise RuntimeError("training curves failed: statuses %s" % np.unique(st))
+        curves[i0:i1] = calc / calc.mean(axis=1, keepdims=True)
+    return theta, curves
+
+
+class Surrogate:
+    """PCA of the training curves + the MLP that predicts their coefficients."""
+
+    def __init__(self, ncoef=NCOEF, batch=4096, seed=0, device="cuda"):
+        import torch
+        self.torch = torch
+        self.ncoef = ncoef
+        self.net = MLP(nin=len(PARAMS), nout=ncoef, batch=batch, device=device, seed=seed)
+        self.dev = self.net.dev
+
+    # -- fitting ---------------------------------------------------------------
+    def fit_pca(self, curves):
+        torch = self.torch
+        y = torch.as_tensor(curves, device=self.dev, dtype=torch.float64)
+        self.mean = y.mean(dim=0)
+        yc = y - self.mean
+        cov = yc.T @ yc / y.shape[0]
+        evals, evecs = torch.linalg.eigh(cov)
+        order = torch.argsort(evals, descending=True)[:self.ncoef]
+        self.basis = evecs[:, order].T.contiguous()          # [ncoef x npts]
+        coef = yc @ self.basis.T                              # [n x ncoef]
+        self.cscale = float(coef[:, 0].std())                 # targets = coef / cscale
+        resid = yc - coef @ self.basis
+        return float(resid.abs().max()), coef / self.cscale
+
+    def fit(self, theta, curves, epochs=60, lr=2e-3, lr_min=2e-5, seed=1, log=None):
+        """PCA, then Adam on the MSE of the scaled coefficients with a cosine
+        learning-rate schedule. Returns the per-epoch mean losses."""
+        torch = self.torch
+        pca_err, target = self.fit_pca(curves)
+        self.pca_max_err = pca_err
+        x = torch.as_tensor(to_unit(theta), device=self.dev, dtype=torch.float32)
+        t = target.to(torch.float32)
+        B = self.net.B
+        n = (x.shape[0] // B) * B
+        if n == 0:
+            raise ValueError("fewer training curves than one batch")
+        steps = epochs * (n // B)
+        g = torch.Generator(device=self.dev).manual_seed(seed)
+        losses, k = [], 0
+        for ep in range(epochs):
+            perm = torch.randperm(x.shape[0], generator=g, device=self.dev)[:n]
+            tot = 0.0
+            for i0 in range(0, n, B):
+                idx = perm[i0:i0 + B]
+                rate = lr_min + 0.5 * (lr - lr_min) * (1 + np.cos(np.pi * k / steps))
+                self.net.forward(x[idx], train=True)
+                tot += self.net.backward(t[idx].contiguous())
+                self.net.step(rate)
+                k += 1
+            losses.append(tot / (n // B))
+            if log:
+                log("epoch %d loss %.3e" % (ep, losses[-1]))
+        self.net.check()
+        return losses
+
+    # -- prediction --------------------------------------------------------------
+    def coefficients(self, theta):
+        """Scaled PCA coefficients [n x ncoef] (device tensor) for parameter
+        vectors theta [n x 9]."""
+        torch = self.torch
+        x = torch.as_tensor(to_unit(theta), device=self.dev, dtype=torch.float32)
+        outs = []
+        for i0 in range(0, x.shape[0], self.net.B):
+            outs.append(self.net.forward(x[i0:i0 + self.net.B]).clone())
+        return torch.cat(outs)
+
+    def curves(self, theta):
+        c = self.coefficients(theta).to(self.torch.float64) * self.cscale
+        return (self.mean + c @ self.basis).cpu().numpy()
+
+    def head(self, index):
+        """The chi**2 head restricted to the grid points index: (basis
+        [ncoef x p] FP32 scaled by cscale, mean [p] FP32)."""
+        torch = self.torch
+        idx = torch.as_tensor(index, device=self.dev)
+        return ((self.basis[:, idx] * self.cscale).to(torch.float32).contiguous(),
+                self.mean[idx].to(torch.float32).contiguous())
+
+    def save(self):
+        st = self.net.state()
+        st.update(mean=self.mean.cpu().numpy(), basis=self.basis.cpu().numpy(),
+                  cscale=np.array(self.cscale))
+        return st
+
+    def load(self, st):
+        torch = self.torch
+        self.net.load_state(st)
+        self.mean = torch.as_tensor(st["mean"], device=self.dev)
+        self.basis = torch.as_tensor(st["basis"], device=self.dev)
+        self.cscale = float(st["cscale"])
+
+
+def local_draws(mean, cov, n, seed=0, widen=3.0):
+    """n parameter vectors around a posterior estimate: Gaussian with the
+    covariance widened by `widen` in each direction, kept inside the box
+    (the region a surrogate is refined on after burn-in)."""
+    rng = np.random.default_rng(seed)
+    L = np.linalg.cholesky(np.asarray(cov) * widen ** 2)
+    out = np.empty((0, len(PARAMS)))
+    while out.shape[0] < n:
+        t = np.asarray(mean) + rng.standard_normal((2 * n, len(PARAMS))) @ L.T
+        out = np.vstack([out, t[in_box(t)]])
+    return out[:n]
+
+
+class SurrogateChi2:
+    """chi**2 of the data under the surrogate, on the GPU: the MLP forward
+    pass, then lcg_mlp_pca_chisq (curve at the data points, optimal scale,
+    chi**2). The data points must lie on the surrogate's phase grid.
+
+    Called with parameters, it is the surrogate's own chi**2. The anchored
+    form (state / chi2) predicts the curve at y from an exact curve at x as
+    exact(x) * s(y) / s(x), so only the surrogate's relative change between
+    nearby points has to be right (the delayed-acceptance sampler's
+    state-dependent approximation)."""
+
+    def __init__(self, sur, data, index):
+        torch = sur.torch
+        self.sur, self.torch = sur, torch
+        self.basis, self.mean = sur.head(index)
+        d = np.ascontiguousarray(data)
+        self.flux = torch.as_tensor(d["flux"].copy(), device=sur.dev)
+        self.ferr = torch.as_tensor(d["ferr"].copy(), device=sur.dev)
+        self.wgt = torch.as_tensor(d["weight"].copy(), device=sur.dev)
+        self.npts = d.shape[0]
+        self.lib = sur.net.lib
+
+    def __call__(self, theta):
+        return self.chi2(self.state(theta))
+
+    def state(self, theta):
+        """The surrogate's coefficients at theta (device tensor)."""
+        return self.sur.coefficients(theta).contiguous()
+
+    def chi2(self, coef, coef_x=None, anchor=None):
+        """chi**2 of s(coef), or of anchor * s(coef) / s(coef_x) (anchor: exact
+        curves at the data points, one row per chain)."""
+        torch = self.torch
+        m = coef.shape[0]
+        chi = torch.empty(m, dtype=torch.float64, device=self.sur.dev)
+        an = None
+        if anchor is not None:
+            an = torch.as_tensor(np.ascontiguousarray(anchor, np.float64), device=self.sur.dev)
+        p = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
+        st = self.lib.lcg_mlp_pca_chisq(C.c_void_p(torch.cuda.current_stream().cuda_stream),
+                                        p(coef), m, coef.shape[1], p(self.basis), p(self.mean),
+                                        self.npts, p(self.flux), p(self.ferr), p(self.wgt),
+                                        p(coef_x.contiguous() if coef_x is not None else None),
+                                        p(an), p(chi), None)
+        if st != abi.OK:
+            raise RuntimeError("lcg_mlp_pca_chisq failed")
+        return chi.cpu().numpy()

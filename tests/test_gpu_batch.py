@@ -168,3 +168,40 @@ def test_batch_on_fp64_context_runs_one_by_one(data, oracle):
             assert _rel(calc[i], o_calc) < 1e-6
     finally:
         e.close()
+
+
+def test_batch_skips_models_that_did_not_change(data):
+    """A model identical to the previous call's model in its position (on the
+    same points) is not evaluated again: its previous results come back and
+    no flux work is done for it."""
+    ms = _models(k=6, seed=51)
+    e = Engine(precision="mixed")
+    try:
+        e.set_data(data)
+        first = e.light_curve_batch_resident(ms)
+        e.flux_elements(reset=True)
+        again = e.light_curve_batch_resident(ms)
+        assert e.flux_elements(reset=True) == 0
+        for k in range(4):
+            assert np.array_equal(first[k], again[k])
+        ms2 = list(ms)
+        ms2[3] = W.model(**{**_kw(ms[3]), "t2": 3300.0})
+        part = e.light_curve_batch_resident(ms2)
+        nent = data.shape[0] * 3  # ndiv = 3
+        faces = e.face_count(ms2[3], 0) + e.face_count(ms2[3], 1)
+        assert e.flux_elements(reset=True) == faces * nent
+        f = Engine(precision="mixed")
+        try:
+            f.set_data(data)
+            fresh = f.light_curve_batch_resident(ms2)
+        finally:
+            f.close()
+        assert np.array_equal(part[0], fresh[0]) and np.array_equal(part[1], fresh[1])
+        # new points (same size) invalidate every stored result
+        d2 = data.copy()
+        d2["flux"] = d2["flux"] * 1.01
+        e.set_data(d2)
+        moved = e.light_curve_batch_resident(ms2)
+        assert not np.array_equal(moved[1], part[1])
+    finally:
+        e.close()
