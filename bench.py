@@ -227,6 +227,7 @@ def run_reference(args):
 def run_ours(args):
     import ctypes as C
     import torch
+    from lcurve_re_b200.replicas import max_over_ranks
     rank, local, world = rank_info()
     torch.cuda.set_device(local)
     dist = None
@@ -290,10 +291,7 @@ def run_ours(args):
     st = eng.stage_times(reset=True)
     elements = eng.flux_elements(reset=True)
     eng.set_profiling(False)
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, dist, device="cuda")
     value = world * args.steps / (total_ms / 1e3)
     flux_ms, flux_n = st["flux"]
     achieved = elements * FLOP_PER_ELEMENT / (flux_ms / 1e3) / 1e12 if flux_ms > 0 else None
@@ -318,10 +316,7 @@ def run_ours(args):
             f1[k].record(ext)
     barrier()
     e2e_ms = sum(a.elapsed_time(b) for a, b in zip(f0, f1))
-    t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * ke / (float(t.item()) / 1e3)
+    e2e_value = world * ke / (max_over_ranks(e2e_ms, dist, device="cuda") / 1e3)
     h2d = n * data.itemsize + (n + 1) * 8 + 5 * 8
     d2h = n * 8 + 5 * 8 + 3 * 8 + 8
 
@@ -432,6 +427,7 @@ def cpu_batch_rate(models, data, sample=8, budget_s=20.0):
 def run_batch(args):
     import ctypes as C
     import torch
+    from lcurve_re_b200.replicas import max_over_ranks
     rank, local, world = rank_info()
     torch.cuda.set_device(local)
     dist = None
@@ -497,10 +493,7 @@ def run_batch(args):
     launches = int(lib.lcg_kernel_launches(1))
     clk = clocks.stop()
     total_ms = sum(a.elapsed_time(b) for a, b in zip(e0, e1))
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, dist, device="cuda")
     value = world * nm * args.steps / (total_ms / 1e3)
 
     # ---- stage breakdown and the flux roofline (profiled, untimed)
@@ -542,10 +535,7 @@ def run_batch(args):
             f1[k].record(ext)
     barrier()
     e2e_ms = sum(a.elapsed_time(b) for a, b in zip(f0, f1))
-    t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * nm * ke / (float(t.item()) / 1e3)
+    e2e_value = world * nm * ke / (max_over_ranks(e2e_ms, dist, device="cuda") / 1e3)
     h2d = n * data.itemsize + (n + 1) * 8 + nm * C.sizeof(abi.LcgModel)
     d2h = nm * (n * 8 + 5 * 8 + 3 * 8 + 8)
 

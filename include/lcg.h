@@ -188,6 +188,18 @@ lcg_status lcg_light_curve(lcg_ctx *ctx, const lcg_model *model,
 lcg_status lcg_set_data(lcg_ctx *ctx, const lcg_datum *data, int32_t n);
 lcg_status lcg_light_curve_resident(lcg_ctx *ctx, const lcg_model *model, int32_t flags,
                                     double *sfac, double *calc, double *scalars);
+/* Lcurve::light_curve_comp_fast (light_curve_comp_fast.cpp:6-84): with more
+ * than max_model_points points, the curve is computed at max_model_points
+ * points picked uniformly by index (both ends included), interpolated
+ * linearly in time to every point, and, with LCG_FLAG_RDATA, chi**2 and wnok
+ * are recomputed over all points; otherwise it is lcg_light_curve. The scale
+ * fitted (LCG_FLAG_SCALE) is the subsample's. max_model_points >= 2. The
+ * sampler and Levenberg-Marquardt callers use it (mcmc_solver.cpp:1066,
+ * levmarq_solver.cpp:679). */
+lcg_status lcg_light_curve_fast(lcg_ctx *ctx, const lcg_model *model,
+                                const lcg_datum *data, int32_t n, int32_t flags,
+                                int32_t max_model_points, double *sfac, double *calc,
+                                double *scalars);
 /* Device pointer to the last light curve computed on ctx (n doubles). */
 const double *lcg_device_calc(lcg_ctx *ctx);
 

@@ -158,6 +158,10 @@ struct lcg_ctx {
     std::vector<int64_t> h_off;
     std::vector<double> h_diag;
     // resident light-curve points (lcg_set_data)
+    // light_curve_comp_fast: all points, sample indices, interpolated curve
+    DBuf<DatumRec> fdata;
+    DBuf<int64_t> fidx;
+    DBuf<double> fcalc, fout;
     int32_t data_n = 0;
     int64_t data_version = 0;  // bumped by every lcg_set_data
     int64_t data_nent = 0;

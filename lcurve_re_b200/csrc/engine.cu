@@ -680,6 +680,7 @@ void lcg_destroy(lcg_ctx *c) {
     for (auto *b : d) b->release();
     c->status.release(); c->queue.release(); c->counters.release(); c->blockcnt.release();
     c->data.release(); c->off.release(); c->pef.release(); c->ptype.release();
+    c->fdata.release(); c->fidx.release(); c->fcalc.release(); c->fout.release();
     batch_release(c->batch);
     c->batch = nullptr;
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -764,6 +765,51 @@ lcg_status lcg_light_curve(lcg_ctx *c, const lcg_model *mp, const lcg_datum *dat
 }
 
 const double *lcg_device_calc(lcg_ctx *c) { return c ? c->calc.p : nullptr; }
+
+lcg_status lcg_light_curve_fast(lcg_ctx *c, const lcg_model *mp, const lcg_datum *data,
+                                int32_t n, int32_t flags, int32_t max_model_points, double *sfac,
+                                double *calc, double *scalars) {
+    if (!c) return LCG_E_INVALID;
+    c->err.clear();
+    if (n <= max_model_points)
+        return lcg_light_curve(c, mp, data, n, flags, sfac, calc, scalars);
+    if (!data || !calc || !sfac || !scalars) return c->fail(LCG_E_INVALID, "null argument");
+    if (max_model_points < 2)
+        return c->fail(LCG_E_INVALID, "light_curve_comp_fast: max_model_points must be >= 2");
+    // points uniform in index, both ends included (light_curve_comp_fast.cpp:32-37)
+    const int32_t m = max_model_points;
+    std::vector<int64_t> idx((size_t)m);
+    std::vector<lcg_datum> sub((size_t)m);
+    for (int32_t i = 0; i < m; i++) {
+        idx[(size_t)i] = (int64_t)((size_t)i * (size_t)(n - 1) / (size_t)(m - 1));
+        sub[(size_t)i] = data[idx[(size_t)i]];
+    }
+    lcg_status rc;
+    if ((rc = lcg_set_data(c, sub.data(), m))) return rc;
+    if ((rc = lcg_light_curve_resident(c, mp, flags, sfac, nullptr, scalars))) return rc;
+    cudaError_t e;
+    if ((e = c->fdata.ensure(n)) || (e = c->fidx.ensure(m)) || (e = c->fcalc.ensure(n)) ||
+        (e = c->fout.ensure(2)))
+        return c->cuda_fail(e, "interpolation buffers");
+    cudaMemcpyAsync(c->fdata.p, data, (size_t)n * sizeof(DatumRec), cudaMemcpyHostToDevice,
+                    c->stream);
+    cudaMemcpyAsync(c->fidx.p, idx.data(), (size_t)m * sizeof(int64_t), cudaMemcpyHostToDevice,
+                    c->stream);
+    const int32_t rdata = (flags & LCG_FLAG_RDATA) != 0;
+    launch_interp(c->fdata.p, n, c->fidx.p, m, c->calc.p, c->fcalc.p, rdata, c->fout.p,
+                  c->stream);
+    double out[2] = {0., 0.};
+    cudaMemcpyAsync(calc, c->fcalc.p, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost,
+                    c->stream);
+    if (rdata)
+        cudaMemcpyAsync(out, c->fout.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if ((rc = finish_status(c))) return rc;
+    if (rdata) {
+        scalars[LCG_OUT_CHISQ] = out[0];
+        scalars[LCG_OUT_WNOK] = out[1];
+    }
+    return LCG_OK;
+}
 
 lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t flags, double *sfac,
                                     double *calc, double *scalars) {

@@ -221,6 +221,10 @@ void launch_finalize(int32_t flags, const DatumRec *data, int32_t n, double *cal
 // flux-weighted gravity / volume-averaged radius sums (comp_gravity.cpp,
 // comp_radius.cpp): out[0..3] = sum f*g, sum f, sum solid angle, sum volume
 void launch_diagnostics(int star, GridDev g, double *out, cudaStream_t s);
+// light_curve_comp_fast interpolation of the model at sampled points mc
+// (sample indices idx, m of them) to all n points; chi**2, wnok -> out[0..1].
+void launch_interp(const DatumRec *data, int32_t n, const int64_t *idx, int32_t m,
+                   const double *mc, double *calc, int32_t rdata, double *out, cudaStream_t s);
 
 void launch_pack_flat(FlatDev f, int64_t n0, int need_pos, cudaStream_t s);
 void launch_pack_phases(PhaseDev ph, cudaStream_t s);

@@ -576,6 +576,49 @@ __global__ void __launch_bounds__(1024) k_finalize(int32_t flags, const DatumRec
     finalize_block(flags, data, n, calc, sfac_io, out, sh);
 }
 
+// light_curve_comp_fast's interpolation (light_curve_comp_fast.cpp:46-83):
+// point i takes the model at the sampled points around it (sample indices
+// idx[0..m), ascending), linearly in time; with rdata, chi**2 and wnok over
+// all points (out[0], out[1]). One block of 1024 threads, fixed-order tree.
+__global__ void __launch_bounds__(1024) k_interp(const DatumRec *__restrict__ data, int32_t n,
+                                                 const int64_t *__restrict__ idx, int32_t m,
+                                                 const double *__restrict__ mc, double *calc,
+                                                 int32_t rdata, double *out) {
+    __shared__ double sh[1024];
+    const int t = threadIdx.x;
+    double cs = 0., w = 0.;
+    for (int i = t; i < n; i += 1024) {
+        int lo = 0, hi = m;  // first sample index >= i
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (idx[mid] < i) lo = mid + 1;
+            else hi = mid;
+        }
+        double c;
+        if (lo == 0) {
+            c = mc[0];
+        } else if (lo == m) {
+            c = mc[m - 1];
+        } else {
+            const int64_t i1 = idx[lo - 1], i2 = idx[lo];
+            const double tt = (data[i].time - data[i1].time) / (data[i2].time - data[i1].time);
+            c = mc[lo - 1] * (1.0 - tt) + mc[lo] * tt;
+        }
+        calc[i] = c;
+        const DatumRec d = data[i];
+        if (d.weight > 0.) {
+            w += d.weight;
+            cs += d.weight * sq((d.flux - c) / d.ferr);
+        }
+    }
+    if (!rdata) return;
+    const double chisq = block_sum(cs, sh), wnok = block_sum(w, sh);
+    if (t == 0) {
+        out[0] = chisq;
+        out[1] = wnok;
+    }
+}
+
 // comp_gravity / comp_radius blocked sums: one thread per 8192-point block,
 // serial inside the block; the host merges the blocks in order.
 __global__ void k_diag(int star, GridDev g, double *blk) {
@@ -982,6 +1025,13 @@ void launch_scatter(const ScatterParams &p, const ReduceParams &r, const PhaseDe
 void launch_finalize(int32_t flags, const DatumRec *data, int32_t n, double *calc,
                      double *sfac_io, double *out, cudaStream_t s) {
     k_finalize<<<1, 1024, 0, s>>>(flags, data, n, calc, sfac_io, out);
+    count_launch();
+}
+
+void launch_interp(const DatumRec *data, int32_t n, const int64_t *idx, int32_t m,
+                   const double *mc, double *calc, int32_t rdata, double *out, cudaStream_t s) {
+    if (n <= 0 || m <= 0) return;
+    k_interp<<<1, 1024, 0, s>>>(data, n, idx, m, mc, calc, rdata, out);
     count_launch();
 }
 

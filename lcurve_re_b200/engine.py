@@ -111,6 +111,25 @@ class Engine:
         return (calc, sc[abi.OUT_WDWARF], sc[abi.OUT_CHISQ], sc[abi.OUT_WNOK], sc[abi.OUT_LOGG1],
                 sc[abi.OUT_LOGG2], sc[abi.OUT_RV1], sc[abi.OUT_RV2])
 
+    def light_curve_comp_fast(self, model, data, max_model_points, scale=True, rdata=True,
+                              sfac=None, diagnostics=False):
+        """Lcurve::light_curve_comp_fast: above max_model_points points, the
+        curve at points uniform in index, interpolated in time. Returns
+        (calc, chisq, wnok); sfac updated in place."""
+        m = _as_model(model)
+        d = _as_data(data)
+        n = d.shape[0]
+        if sfac is None:
+            sfac = np.ones(5)
+        calc = np.empty(n)
+        sc = np.zeros(abi.NOUT)
+        flags = ((abi.FLAG_SCALE if scale else 0) | (abi.FLAG_RDATA if rdata else 0) |
+                 (abi.FLAG_DIAGNOSTICS if diagnostics else 0))
+        self._check(self.lib.lcg_light_curve_fast(self.ctx, C.byref(m), d.ctypes.data, n, flags,
+                                                  max_model_points, _dptr(sfac), _dptr(calc),
+                                                  _dptr(sc)))
+        return calc, sc[abi.OUT_CHISQ], sc[abi.OUT_WNOK]
+
     def light_curve_batch(self, models, data, scale=True, rdata=True, sfac=None):
         ms = (abi.LcgModel * len(models))(*[_as_model(m) for m in models])
         d = _as_data(data)

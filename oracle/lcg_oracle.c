@@ -2021,3 +2021,63 @@ done:
     copyerr(&e, err, errlen);
     return e.st;
 }
+
+/* ---- light_curve_comp_fast (light_curve_comp_fast.cpp:6-84) ---------------
+ * Above max_pts points, the curve is computed on max_pts points picked
+ * uniformly by index (both ends included), interpolated linearly in time to
+ * every point, and chi**2 / wnok are recomputed over all points (serial sums
+ * in point order) when rdata is set. */
+int lco_light_curve_fast(const lcg_model *m, const lcg_datum *data, int32_t n,
+                         int32_t flags, int32_t max_pts, double *sfac, double *calc,
+                         double *scalars, char *err, int errlen) {
+    if (n <= max_pts)
+        return lco_light_curve(m, data, n, flags, sfac, calc, scalars, err, errlen);
+    if (max_pts < 2) {
+        if (err && errlen > 0) snprintf(err, (size_t)errlen, "light_curve_comp_fast: max_model_points < 2");
+        return LCG_E_INVALID;
+    }
+    size_t *idx = (size_t *)malloc(sizeof(size_t) * (size_t)max_pts);
+    lcg_datum *sub = (lcg_datum *)malloc(sizeof(lcg_datum) * (size_t)max_pts);
+    double *mc = (double *)malloc(sizeof(double) * (size_t)max_pts);
+    for (int i = 0; i < max_pts; i++) {
+        idx[i] = (size_t)i * (size_t)(n - 1) / (size_t)(max_pts - 1);
+        sub[i] = data[idx[i]];
+    }
+    int st = lco_light_curve(m, sub, max_pts, flags, sfac, mc, scalars, err, errlen);
+    if (st == 0) {
+        for (int32_t i = 0; i < n; i++) {
+            /* first sample index >= i */
+            int lo = 0, hi = max_pts;
+            while (lo < hi) {
+                int mid = (lo + hi) / 2;
+                if (idx[mid] < (size_t)i) lo = mid + 1;
+                else hi = mid;
+            }
+            if (lo == 0) {
+                calc[i] = mc[0];
+            } else if (lo == max_pts) {
+                calc[i] = mc[max_pts - 1];
+            } else {
+                const size_t i1 = idx[lo - 1], i2 = idx[lo];
+                const double t = (data[i].time - data[i1].time) / (data[i2].time - data[i1].time);
+                calc[i] = mc[lo - 1] * (1.0 - t) + mc[lo] * t;
+            }
+        }
+        if (flags & LCG_FLAG_RDATA) {
+            double wnok = 0., chisq = 0.;
+            for (int32_t i = 0; i < n; i++) {
+                if (data[i].weight > 0.) {
+                    wnok += data[i].weight;
+                    const double d = (data[i].flux - calc[i]) / data[i].ferr;
+                    chisq += data[i].weight * (d * d);
+                }
+            }
+            scalars[LCG_OUT_WNOK] = wnok;
+            scalars[LCG_OUT_CHISQ] = chisq;
+        }
+    }
+    free(idx);
+    free(sub);
+    free(mc);
+    return st;
+}

@@ -66,6 +66,13 @@ int lco_light_curve(const lcg_model *m, const lcg_datum *data, int32_t n,
                     int32_t flags, double *sfac, double *calc,
                     double *scalars, char *err, int errlen);
 
+/* Lcurve::light_curve_comp_fast (light_curve_comp_fast.cpp:6-84): above
+ * max_pts points, evaluate on max_pts points uniform in index and
+ * interpolate linearly in time; chi**2 recomputed when rdata is set. */
+int lco_light_curve_fast(const lcg_model *m, const lcg_datum *data, int32_t n,
+                         int32_t flags, int32_t max_pts, double *sfac, double *calc,
+                         double *scalars, char *err, int errlen);
+
 /* Scalars derived once per model (light_curve_comp.cpp:130-138,
  * set_star_grid.cpp:63-108): r1, r2, rl1, rl2, rref1, pref1, rref2, pref2,
  * ffac1, ffac2, gref1, gref2. Returns a status. */

@@ -104,6 +104,38 @@ int fail(const std::exception &ex, char *err, int errlen, int code) {
 
 extern "C" {
 
+int lcref_light_curve_fast(const lcg_model *m, const lcg_datum *data, int32_t n,
+                           int32_t flags, int32_t max_pts, double *sfac, double *calc,
+                           double *scalars, char *err, int errlen) {
+    try {
+        Lcurve::Model mdl = to_model(*m);
+        Lcurve::Data d(n);
+        for (int i = 0; i < n; i++) {
+            d[i].time = data[i].time; d[i].expose = data[i].expose;
+            d[i].flux = data[i].flux; d[i].ferr = data[i].ferr;
+            d[i].weight = data[i].weight; d[i].ndiv = data[i].ndiv;
+        }
+        std::vector<double> sf(sfac, sfac + 5), c;
+        double wdwarf = scalars[LCG_OUT_WDWARF], chisq = scalars[LCG_OUT_CHISQ];
+        double wnok = scalars[LCG_OUT_WNOK], logg1, logg2, rv1, rv2;
+        Lcurve::light_curve_comp_fast(mdl, d, flags & LCG_FLAG_SCALE, flags & LCG_FLAG_RDATA,
+                                      flags & LCG_FLAG_INFO, sf, c, wdwarf, chisq, wnok, logg1,
+                                      logg2, rv1, rv2, max_pts,
+                                      (flags & LCG_FLAG_DIAGNOSTICS) != 0);
+        for (int i = 0; i < n; i++) calc[i] = c[i];
+        for (int k = 0; k < 5; k++) sfac[k] = sf[k];
+        scalars[LCG_OUT_WDWARF] = wdwarf; scalars[LCG_OUT_CHISQ] = chisq;
+        scalars[LCG_OUT_WNOK] = wnok;
+        return 0;
+    } catch (const Lcurve::Lcurve_Error &ex) {
+        return fail(ex, err, errlen, LCG_E_LOBE);
+    } catch (const Roche::Roche_Error &ex) {
+        return fail(ex, err, errlen, LCG_E_ROCHE);
+    } catch (const std::exception &ex) {
+        return fail(ex, err, errlen, LCG_E_INVALID);
+    }
+}
+
 int lcref_light_curve(const lcg_model *m, const lcg_datum *data, int32_t n,
                       int32_t flags, double *sfac, double *calc,
                       double *scalars, char *err, int errlen) {

@@ -69,6 +69,23 @@ class _Lib:
             C.byref(m), d.ctypes.data, n, flags, _d(sf), _d(calc), _d(sc), err, 512)
         return st, err.value.decode(), calc, sf, sc
 
+    def light_curve_fast(self, model, data, max_pts, scale=True, rdata=True, sfac=None):
+        """light_curve_comp_fast: (status, message, calc, sfac, scalars)."""
+        m = model.to_c() if hasattr(model, "to_c") else model
+        d = np.ascontiguousarray(data)
+        n = d.shape[0]
+        sf = np.ones(5) if sfac is None else np.array(sfac, dtype=np.float64)
+        calc = np.zeros(n)
+        sc = np.zeros(abi.NOUT)
+        flags = (1 if scale else 0) | (2 if rdata else 0)
+        err = C.create_string_buffer(512)
+        fn = getattr(self.lib, self.prefix + "light_curve_fast")
+        fn.restype = C.c_int
+        fn.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_int32, D, D, D,
+                       C.c_char_p, C.c_int]
+        st = fn(C.byref(m), d.ctypes.data, n, flags, max_pts, _d(sf), _d(calc), _d(sc), err, 512)
+        return st, err.value.decode(), calc, sf, sc
+
     def sum_star_multi(self, star, flat, phases, ldc, ltype, mucrit=0.0, beam=0.0, spin=1.0,
                        vfac=0.0, xcofm=0.0, glens1=False, rlens1=0.0):
         cols = [np.ascontiguousarray(flat[k], dtype=np.float64)

@@ -241,3 +241,26 @@ def test_tiling_mismatch_keeps_the_reference_face_count(engine_fp64, oracle, ove
     assert st == 0, err
     calc = engine_fp64.light_curve_comp(m, d, sfac=np.ones(5), diagnostics=False)[0]
     assert np.max(np.abs(calc - co) / np.abs(co)) <= 1e-6
+
+
+@pytest.mark.parametrize("npts,max_pts", [(500, 120), (2000, 37), (90, 200), (300, 2)])
+def test_light_curve_fast(engine_fp64, engine_mixed, oracle, npts, max_pts):
+    """light_curve_comp_fast on the device against the oracle (which is pinned
+    bit for bit to the reference's own function): FP64 1e-6, mixed 1e-5."""
+    m = W.model(nlat1f=16, nlat2f=24)
+    d = W.data(npts, ndiv=2, expose=0.003)
+    d["time"] = d["time"] + 0.0007 * np.sin(np.arange(npts))
+    d["flux"] = 1.0 + 1e-3 * np.cos(np.arange(npts))
+    d["weight"][5] = 0.0
+    for eng, tol in ((engine_fp64, 1e-6), (engine_mixed, 1e-5)):
+        for scale, rdata in ((True, True), (False, True)):
+            st, err, co, sfo, sco = oracle.light_curve_fast(m, d, max_pts, scale=scale,
+                                                            rdata=rdata)
+            assert st == 0, err
+            sf = np.ones(5)
+            calc, chisq, wnok = eng.light_curve_comp_fast(m, d, max_pts, scale=scale,
+                                                          rdata=rdata, sfac=sf)
+            assert np.max(np.abs(calc - co) / np.abs(co)) <= tol
+            np.testing.assert_allclose(chisq, sco[1], rtol=100 * tol)
+            assert wnok == sco[2]
+            np.testing.assert_allclose(sf, sfo, rtol=tol)

@@ -79,3 +79,22 @@ def test_short_tiling_ends_in_default_points(oracle, reference):
         assert np.array_equal(go[k], gr[k]), k
     assert np.all(go["area"][-2:] == 0) and np.all(go["gravity"][-2:] == 1)
     assert np.all(go["posn"][-2:] == 0) and np.all(go["flux"][-2:] == 0)
+
+
+@pytest.mark.parametrize("npts,max_pts", [(500, 120), (2000, 37), (90, 200), (300, 2)])
+def test_light_curve_fast_bit_exact(oracle, reference, npts, max_pts):
+    """light_curve_comp_fast: subsample by index, interpolate in time,
+    recompute chi**2 (light_curve_comp_fast.cpp:6-84)."""
+    from lcurve_re_b200 import workloads as W
+    m = W.model(nlat1f=16, nlat2f=24)
+    d = W.data(npts, ndiv=2, expose=0.003)
+    d["time"] = d["time"] + 0.0007 * np.sin(np.arange(npts))  # uneven spacing
+    d["flux"] = 1.0 + 1e-3 * np.cos(np.arange(npts))
+    d["weight"][5] = 0.0
+    for scale, rdata in ((True, True), (False, True), (True, False)):
+        a = oracle.light_curve_fast(m, d, max_pts, scale=scale, rdata=rdata)
+        b = reference.light_curve_fast(m, d, max_pts, scale=scale, rdata=rdata)
+        assert a[0] == b[0] == 0, (a[1], b[1])
+        assert np.array_equal(a[2], b[2])
+        assert np.array_equal(a[3], b[3])
+        assert np.array_equal(a[4][:3], b[4][:3])
