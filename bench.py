@@ -51,6 +51,8 @@ def parse():
     ap.add_argument("--workload", default="wd_dm_large",
                     choices=("wd_dm_large", "wd_dm_small", "tiny_star", "mcmc_batch",
                              "surrogate_da"))
+    ap.add_argument("--batch-models", type=int, default=256,
+                    help="models per step of mcmc_batch (256 is the benchmark)")
     ap.add_argument("--train-curves", type=int, default=200000)
     ap.add_argument("--epochs", type=int, default=60)
     ap.add_argument("--chains", type=int, default=512)
@@ -58,8 +60,9 @@ def parse():
     ap.add_argument("--burn", type=int, default=400)
     ap.add_argument("--ncoef", type=int, default=64)
     ap.add_argument("--local-curves", type=int, default=65536)
-    ap.add_argument("--refine-epochs", type=int, default=150)
-    ap.add_argument("--da-scale", type=float, default=1.6)
+    ap.add_argument("--refine-epochs", type=int, default=300)
+    ap.add_argument("--da-scale", type=float, default=2.6)
+    ap.add_argument("--local-widen", type=float, default=2.0)
     ap.add_argument("--precision", choices=("mixed", "fp64"), default="mixed")
     ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -329,7 +332,7 @@ def run_ours(args):
                    "sample": str(ex)}
 
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "flux_mixed_wd_dm_large.txt")
+    prof = os.path.join(ROOT, "profiles", "flux_fast_wd_dm_large.txt")
     if os.path.exists(prof) and args.workload == "wd_dm_large" and args.precision == "mixed":
         for line in open(prof):
             if line.startswith("dram_bytes_per_light_curve:"):
@@ -376,12 +379,12 @@ BATCH_DESC = ("mcmc_batch: 256 models around wd_dm_small (q~N(0.25,0.02), i~N(86
               "2000 points")
 
 
-def batch_workload():
-    """The 256 models, a second set with every q scaled by 1 + 1e-4 (so that
+def batch_workload(nmodels=256):
+    """The models, a second set with every q scaled by 1 + 1e-4 (so that
     alternating steps rebuild every grid, as an MCMC step does), and noisy data
     from the first model's curve."""
     from lcurve_re_b200 import workloads as W
-    ms, d = W.mcmc_batch(256)
+    ms, d = W.mcmc_batch(nmodels)
     alt = []
     for m in ms:
         c = m.to_c()
@@ -438,7 +441,7 @@ def run_batch(args):
     from lcurve_re_b200 import workloads as W
     from lcurve_re_b200.engine import Engine
 
-    ms, alt, data = batch_workload()
+    ms, alt, data = batch_workload(args.batch_models)
     eng = Engine(device=local, precision="mixed")
     lib, ctx = eng.lib, eng.ctx
     calc0 = eng.light_curve_comp(ms[0], data, scale=False, rdata=False, diagnostics=False)[0]
@@ -468,10 +471,17 @@ def run_batch(args):
         if dist is not None:
             dist.barrier()
 
+    # one running counter over every call, so each call's models differ from
+    # the previous call's (the engine skips models identical to the last call's)
+    calls = [0]
+
+    def models_now():
+        calls[0] += 1
+        return A if calls[0] % 2 else B
+
     def step(k, calc_out=None):
-        check(lib.lcg_light_curve_batch_resident(ctx, A if k % 2 == 0 else B, nm, flags,
-                                                 dptr(sfac), calc_out, dptr(chisq), dptr(wnok),
-                                                 i32))
+        check(lib.lcg_light_curve_batch_resident(ctx, models_now(), nm, flags, dptr(sfac),
+                                                 calc_out, dptr(chisq), dptr(wnok), i32))
 
     # ---- device-resident value (CUDA graph path)
     check(lib.lcg_set_data(ctx, data.ctypes.data, n))
@@ -519,7 +529,7 @@ def run_batch(args):
     ke = min(args.e2e_steps, args.steps)
 
     def step_e2e(k):
-        check(lib.lcg_light_curve_batch(ctx, A if k % 2 == 0 else B, nm, hdata.ctypes.data, n,
+        check(lib.lcg_light_curve_batch(ctx, models_now(), nm, hdata.ctypes.data, n,
                                         flags, dptr(sfac), dptr(hcalc), dptr(chisq), dptr(wnok),
                                         i32))
     for k in range(2):
@@ -669,15 +679,17 @@ def run_surrogate(args):
         samp = ch[ch.shape[0] // 2:].reshape(-1, 9)
         cov = np.cov(samp.T) * 2.38 ** 2 / 9 + np.diag((scale0 * 1e-3) ** 2)
     # refinement: the same network trained again on engine curves around the
-    # burn-in posterior (Gaussian, 3x its spread, inside the box)
+    # burn-in posterior (Gaussian, local_widen x its spread, inside the box)
     samp = ch[ch.shape[0] // 2:].reshape(-1, 9)
-    th_loc = S.local_draws(samp.mean(0), np.cov(samp.T), args.local_curves, seed=5 + rank)
+    th_loc = S.local_draws(samp.mean(0), np.cov(samp.T), args.local_curves, seed=5 + rank,
+                           widen=args.local_widen)
     t0 = time.perf_counter()
     _, cu_loc = S.training_set(eng, 0, theta=th_loc, batch=2048)
     sur_loc = S.Surrogate(ncoef=args.ncoef, batch=4096, seed=rank + 1)
     losses_loc = sur_loc.fit(th_loc, cu_loc, epochs=args.refine_epochs)
     t_ref = time.perf_counter() - t0
-    th_lh = S.local_draws(samp.mean(0), np.cov(samp.T), 2048, seed=77 + rank)
+    th_lh = S.local_draws(samp.mean(0), np.cov(samp.T), 2048, seed=77 + rank,
+                          widen=args.local_widen)
     _, cu_lh = S.training_set(eng, 0, theta=th_lh, batch=2048)
     loc_err = float(np.sqrt(np.mean((sur_loc.curves(th_lh) - cu_lh) ** 2)))
     glob_err_loc = float(np.sqrt(np.mean((sur.curves(th_lh) - cu_lh) ** 2)))

@@ -222,11 +222,17 @@ lcg_status lcg_light_curve_batch(lcg_ctx *ctx, const lcg_model *models,
                                  int32_t *status);
 
 /* lcg_light_curve_batch over the points of lcg_set_data. calc, chisq and
- * wnok may be NULL. */
+ * wnok may be NULL: a sampler that needs the curves of a few models only
+ * passes calc = NULL and fetches those rows with lcg_batch_curves. */
 lcg_status lcg_light_curve_batch_resident(lcg_ctx *ctx, const lcg_model *models,
                                           int32_t nmodels, int32_t flags, double *sfac,
                                           double *calc, double *chisq, double *wnok,
                                           int32_t *status);
+
+/* Rows (model indices) of the light curves of the last batch call on ctx,
+ * copied to out [count x n]; the rows of models that call skipped as
+ * unchanged hold their earlier curves. */
+lcg_status lcg_batch_curves(lcg_ctx *ctx, const int32_t *rows, int32_t count, double *out);
 
 /* ---- stage-level seams, for parity tests and integrations -------------- */
 

@@ -106,6 +106,7 @@ PROTOTYPES = {
     "lcg_flux_elements": (C.c_int64, [P, C.c_int32]),
     "lcg_measure_fp32_peak": (C.c_int, [P, D]),
     "lcg_set_data": (C.c_int, [P, P, C.c_int32]),
+    "lcg_batch_curves": (C.c_int, [P, I32, C.c_int32, D]),
     "lcg_light_curve_fast": (C.c_int, [P, C.POINTER(LcgModel), P, C.c_int32, C.c_int32,
                                        C.c_int32, D, D, D]),
     "lcg_mlp_gemm": (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, P, P, P, P, P,

@@ -106,6 +106,11 @@ struct BatchState {
     size_t res_bytes = 0, r_calc = 0, r_sfac = 0, r_out = 0, r_st = 0;
     cudaGraphExec_t exec = nullptr;
     int64_t graph_kernels = 0;  // kernels per graph launch
+    // lcg_batch_curves: selected rows gathered on the device, then one copy
+    DBuf<int32_t> rows;
+    DBuf<double> gathered;
+    double *h_rows = nullptr;
+    size_t h_rows_cap = 0;
 
     template <class T>
     T *tab(size_t off) { return reinterpret_cast<T *>(h_tab + off); }
@@ -124,6 +129,10 @@ struct BatchState {
         area.release(); grav.release(); flux.release(); fp.release(); necl.release();
         ecl.release(); n0.release(); blockcnt.release(); queue.release(); counters.release();
         st.release(); ef.release(); rings.release(); d_tab.release();
+        rows.release(); gathered.release();
+        if (h_rows) cudaFreeHost(h_rows);
+        h_rows = nullptr;
+        h_rows_cap = 0;
         if (h_tab) cudaFreeHost(h_tab);
         if (h_res) cudaFreeHost(h_res);
         h_tab = h_res = nullptr;
@@ -626,5 +635,38 @@ extern "C" lcg_status lcg_light_curve_batch_resident(lcg_ctx *c, const lcg_model
         if (wnok) wnok[m] = sc[LCG_OUT_WNOK];
     }
     c->err.clear();
+    return LCG_OK;
+}
+
+extern "C" lcg_status lcg_batch_curves(lcg_ctx *c, const int32_t *rows, int32_t count,
+                                       double *out) {
+    if (!c) return LCG_E_INVALID;
+    c->err.clear();
+    if (!rows || !out || count < 0) return c->fail(LCG_E_INVALID, "null argument");
+    BatchState *B = c->batch;
+    if (!B || B->nmodels <= 0) return c->fail(LCG_E_INVALID, "no batch has run on this context");
+    for (int32_t i = 0; i < count; i++)
+        if (rows[i] < 0 || rows[i] >= B->nmodels)
+            return c->fail(LCG_E_INVALID, "row %d outside the batch of %d", rows[i], B->nmodels);
+    if (count == 0) return LCG_OK;
+    cudaSetDevice(c->device);
+    const size_t n = (size_t)B->n, bytes = (size_t)count * n * sizeof(double);
+    cudaError_t e;
+    if ((e = B->rows.ensure((size_t)count)) || (e = B->gathered.ensure((size_t)count * n)))
+        return c->cuda_fail(e, "curve rows");
+    if (B->h_rows_cap < bytes) {
+        if (B->h_rows) cudaFreeHost(B->h_rows);
+        B->h_rows = nullptr;
+        B->h_rows_cap = 0;
+        if ((e = cudaHostAlloc((void **)&B->h_rows, bytes, cudaHostAllocDefault)))
+            return c->cuda_fail(e, "curve rows");
+        B->h_rows_cap = bytes;
+    }
+    cudaMemcpyAsync(B->rows.p, rows, (size_t)count * sizeof(int32_t), cudaMemcpyHostToDevice,
+                    c->stream);
+    launch_gather_rows(B->calc.p, B->n, B->rows.p, count, B->gathered.p, c->stream);
+    cudaMemcpyAsync(B->h_rows, B->gathered.p, bytes, cudaMemcpyDeviceToHost, c->stream);
+    if ((e = cudaStreamSynchronize(c->stream))) return c->cuda_fail(e, "curve rows");
+    memcpy(out, B->h_rows, bytes);
     return LCG_OK;
 }

@@ -223,6 +223,9 @@ void launch_finalize(int32_t flags, const DatumRec *data, int32_t n, double *cal
 void launch_diagnostics(int star, GridDev g, double *out, cudaStream_t s);
 // light_curve_comp_fast interpolation of the model at sampled points mc
 // (sample indices idx, m of them) to all n points; chi**2, wnok -> out[0..1].
+// dst row r = src row rows[r] (count rows of n doubles)
+void launch_gather_rows(const double *src, int32_t n, const int32_t *rows, int32_t count,
+                        double *dst, cudaStream_t s);
 void launch_interp(const DatumRec *data, int32_t n, const int64_t *idx, int32_t m,
                    const double *mc, double *calc, int32_t rdata, double *out, cudaStream_t s);
 

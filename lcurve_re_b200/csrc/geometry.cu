@@ -619,6 +619,14 @@ __global__ void __launch_bounds__(1024) k_interp(const DatumRec *__restrict__ da
     }
 }
 
+// dst row r = src row rows[r] (rows of n doubles).
+__global__ void k_gather_rows(const double *__restrict__ src, int32_t n,
+                              const int32_t *__restrict__ rows, double *dst) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    dst[(int64_t)blockIdx.y * n + i] = src[(int64_t)rows[blockIdx.y] * n + i];
+}
+
 // comp_gravity / comp_radius blocked sums: one thread per 8192-point block,
 // serial inside the block; the host merges the blocks in order.
 __global__ void k_diag(int star, GridDev g, double *blk) {
@@ -1032,6 +1040,13 @@ void launch_interp(const DatumRec *data, int32_t n, const int64_t *idx, int32_t 
                    const double *mc, double *calc, int32_t rdata, double *out, cudaStream_t s) {
     if (n <= 0 || m <= 0) return;
     k_interp<<<1, 1024, 0, s>>>(data, n, idx, m, mc, calc, rdata, out);
+    count_launch();
+}
+
+void launch_gather_rows(const double *src, int32_t n, const int32_t *rows, int32_t count,
+                        double *dst, cudaStream_t s) {
+    if (n <= 0 || count <= 0) return;
+    k_gather_rows<<<dim3(nblocks(n, 256), (unsigned)count), 256, 0, s>>>(src, n, rows, dst);
     count_launch();
 }
 

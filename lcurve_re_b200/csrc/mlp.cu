@@ -142,7 +142,8 @@ __global__ void __launch_bounds__(128) k_gemm(const __grid_constant__ CUtensorMa
     __syncthreads();
     fence_after_sync();
     const uint32_t tmem = tmem_base;
-    const int nk = k / kBK;
+    const int nk = k / kBK;          // k: the K slice of this CTA
+    const int k0 = blockIdx.z * k;   // split-K: slices along grid z
     if (tid == 0) {
         const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
                                ((uint32_t)(kBM >> 4) << 24);
@@ -150,8 +151,8 @@ __global__ void __launch_bounds__(128) k_gemm(const __grid_constant__ CUtensorMa
         auto load = [&](int kb) {
             const int s = kb & 1;
             mbar_arrive_expect_tx(&full[s], kABytes + kBBytes);
-            tma_load_2d(sa0 + s * kABytes, &ta, kb * kBK, m0, &full[s]);
-            tma_load_2d(sb0 + s * kBBytes, &tb, kb * kBK, n0, &full[s]);
+            tma_load_2d(sa0 + s * kABytes, &ta, k0 + kb * kBK, m0, &full[s]);
+            tma_load_2d(sb0 + s * kBBytes, &tb, k0 + kb * kBK, n0, &full[s]);
             issued++;
         };
         load(0);
@@ -248,6 +249,13 @@ __global__ void __launch_bounds__(128) k_gemm(const __grid_constant__ CUtensorMa
 #pragma unroll
                         for (int i = 0; i < 16; i++) o.yt[(size_t)(nb + i) * o.ldt + m] = gb[i];
                     }
+                }
+            } else if (EPI == kEpiF32 && gridDim.z > 1) {
+                // split-K: slices add into the output the launcher zeroed
+                if (store) {
+                    float *op = o.out + (size_t)m * N + nb;
+#pragma unroll
+                    for (int i = 0; i < 16; i++) atomicAdd(op + i, v[i]);
                 }
             } else {  // kEpiLinear, kEpiF32
                 if (store) {
@@ -475,14 +483,18 @@ bool make_map(CUtensorMap *map, const void *base, int32_t rows, int32_t cols, in
 
 template <int BN, int EPI>
 cudaError_t launch_gemm_t(const CUtensorMap &ta, const CUtensorMap &tb, int m, int n, int k,
-                          const GemmOut &o, cudaStream_t s) {
+                          int splits, const GemmOut &o, cudaStream_t s) {
     const size_t smem = 2 * (size_t)(kBM + BN) * kBK * 2 + 1024;
     auto kern = k_gemm<BN, EPI>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
-    dim3 grid((unsigned)(n / BN), (unsigned)(m / kBM));
-    kern<<<grid, 128, smem, s>>>(ta, tb, k, o);
+    if (splits > 1) {
+        e = cudaMemsetAsync(o.out, 0, (size_t)o.mvalid * n * sizeof(float), s);
+        if (e != cudaSuccess) return e;
+    }
+    dim3 grid((unsigned)(n / BN), (unsigned)(m / kBM), (unsigned)splits);
+    kern<<<grid, 128, smem, s>>>(ta, tb, k / splits, o);
     count_launch();
     return cudaGetLastError();
 }
@@ -499,8 +511,20 @@ lcg_status lcg_mlp_gemm(void *stream, int32_t epi, int32_t m, int32_t n, int32_t
                         void *yt, float *out, int32_t mvalid, int32_t ldt, int32_t *err) {
     if (!a || !b || m <= 0 || n <= 0 || k <= 0 || m % kBM || k % kBK || epi < 0 || epi > 3)
         return LCG_E_INVALID;
-    const int bn = (n % 256 == 0) ? 256 : (n % 64 == 0 ? 64 : 0);
-    if (!bn) return LCG_E_INVALID;
+    if (n % 64) return LCG_E_INVALID;
+    // 256-wide tiles unless that leaves most SMs idle; split K across CTAs for
+    // the weight gradients (FP32 output, long K, few tiles)
+    int nsm = 148, dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    int bn = (n % 256 == 0 && (n / 256) * (m / kBM) >= nsm / 2) ? 256 : 64;
+    int splits = 1;
+    if (epi == kEpiF32) {
+        const int tiles = (n / bn) * (m / kBM);
+        while (tiles * splits * 2 <= 2 * nsm && (k / kBK) % (splits * 2) == 0 &&
+               k / (splits * 2) >= 4 * kBK)
+            splits *= 2;
+    }
     if ((epi == kEpiGelu && (!z || !y)) || (epi == kEpiDGelu && (!z || !y)) ||
         ((epi == kEpiLinear || epi == kEpiF32) && !out) || ((yt != nullptr) && ldt < m))
         return LCG_E_INVALID;
@@ -514,17 +538,17 @@ lcg_status lcg_mlp_gemm(void *stream, int32_t epi, int32_t m, int32_t n, int32_t
     cudaError_t e;
     if (bn == 256) {
         switch (epi) {
-        case kEpiGelu: e = launch_gemm_t<256, kEpiGelu>(ta, tb, m, n, k, o, s); break;
-        case kEpiLinear: e = launch_gemm_t<256, kEpiLinear>(ta, tb, m, n, k, o, s); break;
-        case kEpiDGelu: e = launch_gemm_t<256, kEpiDGelu>(ta, tb, m, n, k, o, s); break;
-        default: e = launch_gemm_t<256, kEpiF32>(ta, tb, m, n, k, o, s); break;
+        case kEpiGelu: e = launch_gemm_t<256, kEpiGelu>(ta, tb, m, n, k, splits, o, s); break;
+        case kEpiLinear: e = launch_gemm_t<256, kEpiLinear>(ta, tb, m, n, k, splits, o, s); break;
+        case kEpiDGelu: e = launch_gemm_t<256, kEpiDGelu>(ta, tb, m, n, k, splits, o, s); break;
+        default: e = launch_gemm_t<256, kEpiF32>(ta, tb, m, n, k, splits, o, s); break;
         }
     } else {
         switch (epi) {
-        case kEpiGelu: e = launch_gemm_t<64, kEpiGelu>(ta, tb, m, n, k, o, s); break;
-        case kEpiLinear: e = launch_gemm_t<64, kEpiLinear>(ta, tb, m, n, k, o, s); break;
-        case kEpiDGelu: e = launch_gemm_t<64, kEpiDGelu>(ta, tb, m, n, k, o, s); break;
-        default: e = launch_gemm_t<64, kEpiF32>(ta, tb, m, n, k, o, s); break;
+        case kEpiGelu: e = launch_gemm_t<64, kEpiGelu>(ta, tb, m, n, k, splits, o, s); break;
+        case kEpiLinear: e = launch_gemm_t<64, kEpiLinear>(ta, tb, m, n, k, splits, o, s); break;
+        case kEpiDGelu: e = launch_gemm_t<64, kEpiDGelu>(ta, tb, m, n, k, splits, o, s); break;
+        default: e = launch_gemm_t<64, kEpiF32>(ta, tb, m, n, k, splits, o, s); break;
         }
     }
     return e == cudaSuccess ? LCG_OK : LCG_E_CUDA;

@@ -152,22 +152,39 @@ class Engine:
         self._check(self.lib.lcg_set_data(self.ctx, d.ctypes.data, d.shape[0]))
         self._n = d.shape[0]
 
-    def light_curve_batch_resident(self, models, scale=True, rdata=True, sfac=None, calc=True):
+    def light_curve_batch_resident(self, models, scale=True, rdata=True, sfac=None, calc=True,
+                                   buffers=None):
         """lcg_light_curve_batch over the points of set_data; calc=False
-        returns only chi**2 (calc is None)."""
+        returns only chi**2 (calc is None). buffers (a dict, kept by the
+        caller) lets repeated calls of one size reuse their output arrays."""
         ms = models if isinstance(models, C.Array) else \
             (abi.LcgModel * len(models))(*[_as_model(m) for m in models])
         nm, n = len(ms), self._n
-        sf = np.ones(5 * nm) if sfac is None else np.ascontiguousarray(sfac, dtype=np.float64)
-        out = np.zeros((nm, n)) if calc else None
-        chisq = np.zeros(nm)
-        wnok = np.zeros(nm)
-        status = np.zeros(nm, dtype=np.int32)
+        b = buffers if buffers is not None else {}
+        if b.get("shape") != (nm, n, bool(calc)):
+            b.clear()
+            b.update(shape=(nm, n, bool(calc)), out=np.zeros((nm, n)) if calc else None,
+                     chisq=np.zeros(nm), wnok=np.zeros(nm), status=np.zeros(nm, np.int32),
+                     sf=np.ones(5 * nm))
+        out, chisq, wnok, status = b["out"], b["chisq"], b["wnok"], b["status"]
+        if sfac is None:
+            sf = b["sf"]
+            sf[:] = 1.0
+        else:
+            sf = np.ascontiguousarray(sfac, dtype=np.float64)
         flags = (abi.FLAG_SCALE if scale else 0) | (abi.FLAG_RDATA if rdata else 0)
         self._check(self.lib.lcg_light_curve_batch_resident(
             self.ctx, ms, nm, flags, _dptr(sf), _dptr(out) if calc else None, _dptr(chisq),
             _dptr(wnok), status.ctypes.data_as(C.POINTER(C.c_int32))))
         return out, chisq, wnok, sf.reshape(nm, 5), status
+
+    def batch_curves(self, rows):
+        """Light curves of the given model indices from the last batch call."""
+        r = np.ascontiguousarray(rows, dtype=np.int32)
+        out = np.empty((r.shape[0], self._n))
+        self._check(self.lib.lcg_batch_curves(self.ctx, r.ctypes.data_as(C.POINTER(C.c_int32)),
+                                              r.shape[0], _dptr(out)))
+        return out
 
     # -- stage seams ---------------------------------------------------------
     def face_count(self, model, star, fine=True):

@@ -14,10 +14,10 @@ min(1, pi(y) g(y, x) / (pi(x) g(x, y))), which leaves the exact posterior
 invariant for any approximation, including one that depends on the current
 state. Two are supported: the surrogate's own chi**2 (pi* = exp(-chi_s/2)),
 and the anchored one, chi**2 of exact(x) * s(y) / s(x), which needs the exact
-curve at the current state (ExactChi2 keeps the curves it computed) and, for
-g(y, x), at the proposal. Chains whose proposal the approximation rejects
-pass the engine the model it evaluated for them last, so the batched engine
-skips them entirely.
+curve at the current state and, for g(y, x), at the proposal (ExactChi2.curves_of
+fetches just the rows it needs from the engine). Chains whose proposal the
+approximation rejects pass the engine the model it evaluated for them last,
+so the batched engine skips them entirely.
 """
 import time
 
@@ -74,15 +74,14 @@ class ExactChi2:
         self.evals = 0
         self.calls = 0
         self._last = None
-        self.keep_curves = curves
-        self.curves = None  # the last call's light curves (scaled), when kept
+        self.keep_curves = curves  # curves_of() available
+        self._buffers = {}  # the engine's output arrays, reused between calls
 
     def __call__(self, theta):
         theta = np.asarray(theta, np.float64)
         ms = self.fac(theta)
-        calc, chisq, _, _, st = self.engine.light_curve_batch_resident(
-            ms, calc=self.keep_curves)
-        self.curves = calc
+        _, chisq, _, _, st = self.engine.light_curve_batch_resident(
+            ms, calc=False, buffers=self._buffers)
         if self._last is None or self._last.shape != theta.shape:
             self.evals += theta.shape[0]
         else:
@@ -93,9 +92,29 @@ class ExactChi2:
         out[st != 0] = np.inf
         return out
 
+    def curves_of(self, rows):
+        """The last call's light curves (scaled) of the given chains."""
+        return self.engine.batch_curves(rows)
+
 
 def _proposal(rng, theta, chol):
     return theta + rng.standard_normal(theta.shape) @ chol.T
+
+
+def _take(x, idx):
+    """Rows idx of a numpy array or a device tensor."""
+    if isinstance(x, np.ndarray):
+        return x[idx]
+    import torch
+    return x[torch.as_tensor(idx, device=x.device)]
+
+
+def _put(dst, idx, src):
+    if isinstance(dst, np.ndarray):
+        dst[idx] = src
+    else:
+        import torch
+        dst[torch.as_tensor(idx, device=dst.device)] = src
 
 
 def metropolis(exact, theta0, cov, steps, seed=0, box_check=in_box, record=True):
@@ -132,15 +151,16 @@ def delayed_acceptance(exact, sur, theta0, cov, steps, seed=0, box_check=in_box,
     model judges every step that passes. sur is either a chi**2 callable
     (state-independent approximation) or an anchored one with
     state(theta) -> s and chi2(s_y, s_x, anchor) -> chi**2 of
-    anchor * s(y) / s(x); the anchored form needs exact.curves. Returns
+    anchor * s(y) / s(x); the anchored form needs exact.curves_of(rows). Returns
     (chain, final theta, final chi**2, acceptance rate, wall seconds, stats)."""
     rng = np.random.default_rng(seed)
     chol = np.linalg.cholesky(cov)
     theta = np.array(theta0, np.float64)
     anchored = hasattr(sur, "state")
+    place = getattr(sur, "anchor", lambda rows: np.array(rows, np.float64))
     chi = exact(theta)
     if anchored:
-        f = np.array(exact.curves, np.float64)
+        f = place(exact.curves_of(np.arange(theta.shape[0])))  # exact curves at the states
         sx = sur.state(theta)
     else:
         chi_s = sur(theta)
@@ -169,8 +189,11 @@ def delayed_acceptance(exact, sur, theta0, cov, steps, seed=0, box_check=in_box,
             chi_p = exact(ev)
             last = ev
             if anchored:
-                fp = np.array(exact.curves, np.float64)
-                chi_r = sur.chi2(sx, sy, fp)  # chi**2 of exact(y) s(x) / s(y)
+                # only the chains that reached the engine need their new curve
+                i1 = np.nonzero(a1)[0]
+                fp = place(exact.curves_of(i1))
+                chi_r = np.full(nc, np.inf)
+                chi_r[i1] = sur.chi2(_take(sx, i1), _take(sy, i1), fp)  # exact(y) s(x)/s(y)
                 log_g_rev = np.minimum(0.0, -(chi_r - chi_p) / 2)
             else:
                 log_g_rev = np.minimum(0.0, -(chi_s - chi_sp) / 2)
@@ -180,10 +203,10 @@ def delayed_acceptance(exact, sur, theta0, cov, steps, seed=0, box_check=in_box,
             theta[a2] = prop[a2]
             chi[a2] = chi_p[a2]
             if anchored:
-                f[a2] = fp[a2]
-                idx = np.nonzero(a2)[0]
-                if idx.size:
-                    sx[idx] = sy[idx]
+                i2 = np.nonzero(a2)[0]
+                if i2.size:
+                    _put(f, i2, _take(fp, np.nonzero(a2[i1])[0]))
+                    _put(sx, i2, _take(sy, i2))
             else:
                 chi_s[a2] = chi_sp[a2]
             acc += int(a2.sum())

@@ -64,16 +64,24 @@ class ModelFactory:
 
     def __init__(self, base=None):
         self.base = (base if base is not None else W.model()).to_c()
+        self.dtype = np.dtype(abi.LcgModel)  # the struct layout, parsed once
+        self.base_row = np.frombuffer(bytes(self.base), dtype=self.dtype)[0]
+        self._arr = None
 
     def __call__(self, theta, out=None):
+        """lcg_model array for the rows of theta. Without out, the array is
+        reused between calls of the same size (valid until the next call)."""
         theta = np.atleast_2d(np.asarray(theta, np.float64))
         n = theta.shape[0]
-        arr = out if out is not None else (abi.LcgModel * n)()
-        view = np.ctypeslib.as_array(arr)
-        view[:] = np.frombuffer(bytes(self.base), dtype=view.dtype)[0]
+        if out is None:
+            if self._arr is None or len(self._arr) != n:
+                self._arr = (abi.LcgModel * n)()
+            out = self._arr
+        view = np.frombuffer(out, dtype=self.dtype)
+        view[:] = self.base_row
         for k, name in enumerate(PARAMS):
             view[name] = theta[:, k]
-        return arr
+        return out
 
 
 def training_set(engine, n, seed=0, batch=2048, npts=NGRID, theta=None):
@@ -230,6 +238,10 @@ class SurrogateChi2:
     def __call__(self, theta):
         return self.chi2(self.state(theta))
 
+    def anchor(self, rows):
+        """Exact curves (host rows) as the device tensor chi2 takes."""
+        return self.torch.as_tensor(np.ascontiguousarray(rows, np.float64), device=self.sur.dev)
+
     def state(self, theta):
         """The surrogate's coefficients at theta (device tensor)."""
         return self.sur.coefficients(theta).contiguous()
@@ -242,7 +254,8 @@ class SurrogateChi2:
         chi = torch.empty(m, dtype=torch.float64, device=self.sur.dev)
         an = None
         if anchor is not None:
-            an = torch.as_tensor(np.ascontiguousarray(anchor, np.float64), device=self.sur.dev)
+            an = anchor if isinstance(anchor, torch.Tensor) else self.anchor(anchor)
+            an = an.contiguous()
         p = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
         st = self.lib.lcg_mlp_pca_chisq(C.c_void_p(torch.cuda.current_stream().cuda_stream),
                                         p(coef), m, coef.shape[1], p(self.basis), p(self.mean),

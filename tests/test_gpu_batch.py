@@ -205,3 +205,18 @@ def test_batch_skips_models_that_did_not_change(data):
         assert not np.array_equal(moved[1], part[1])
     finally:
         e.close()
+
+
+def test_batch_curves_returns_the_rows_of_the_last_call(data):
+    ms = _models(k=5, seed=61)
+    e = Engine(precision="mixed")
+    try:
+        e.set_data(data)
+        full = e.light_curve_batch_resident(ms)[0]
+        assert np.array_equal(e.batch_curves([3, 0, 3]), full[[3, 0, 3]])
+        e.light_curve_batch_resident(ms, calc=False)  # all reused: rows unchanged
+        assert np.array_equal(e.batch_curves(np.arange(5)), full)
+        with pytest.raises(Exception):
+            e.batch_curves([5])
+    finally:
+        e.close()

@@ -120,6 +120,9 @@ class _CurveExact:
         self.curves = t.copy()
         return np.sum(((t - MU) / SIG) ** 2, axis=1)
 
+    def curves_of(self, rows):
+        return self.curves[rows]
+
 
 def test_anchored_delayed_acceptance_samples_the_posterior():
     chains, steps = 64, 3000
