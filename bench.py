@@ -782,10 +782,76 @@ def run_surrogate(args):
     return 0
 
 
+def run_reference_da(args):
+    """The reference's own CPU path driving plain Metropolis on the same data
+    (wd_dm_small physics at 500 points): a few chains for a bounded number of
+    steps, so the run takes seconds; ESS/s by the same estimator."""
+    rank, _, world = rank_info()
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as OL
+    from lcurve_re_b200 import surrogate as S
+    from lcurve_re_b200 import workloads as W
+    from lcurve_re_b200.sampler import ess_total, metropolis
+    kind = "reference" if os.path.exists(OL.REF_RELEASE_SO) else "port"
+    lib = OL.Reference(OL.REF_RELEASE_SO) if kind == "reference" else OL.Oracle()
+    fac = S.ModelFactory()
+    idx = np.arange(0, S.NGRID, 2)
+    truth = np.array([0.25, 86.0, 0.015, 0.20, 20000.0, 3200.0, 0.08, 0.5, 0.0])
+    st, err, calc, _, _ = lib.light_curve(fac(truth[None])[0], W.data(S.NGRID, -0.2, 1.2),
+                                          scale=False, rdata=False)
+    data = W.add_noise(W.data(S.NGRID, -0.2, 1.2)[idx], calc[idx], 1234)
+
+    class RefChi2:
+        evals = 0
+
+        def __call__(self, theta):
+            out = np.empty(theta.shape[0])
+            for i, t in enumerate(theta):
+                st, err, _, _, sc = lib.light_curve(fac(t[None])[0], data)
+                out[i] = sc[1] if st == 0 else np.inf
+            RefChi2.evals += theta.shape[0]
+            return out
+
+    exact = RefChi2()
+    chains = 8
+    rng = np.random.default_rng(7)
+    scale0 = (S.BOX[:, 1] - S.BOX[:, 0]) * 1e-3
+    theta0 = truth + rng.standard_normal((chains, 9)) * scale0
+    cov = np.diag(scale0 ** 2)
+    burn = max(20, args.warmup * 10)
+    ch, theta0, _, _, _ = metropolis(exact, theta0, cov, burn, seed=11)
+    samp = ch[burn // 2:].reshape(-1, 9)
+    cov = np.cov(samp.T) * 2.38 ** 2 / 9 + np.diag((scale0 * 1e-3) ** 2)
+    steps = min(400, max(40, args.steps * 20))  # about half a minute of CPU
+    chp, _, _, acc, wall = metropolis(exact, theta0, cov, steps, seed=21)
+    ess, _ = ess_total(chp)
+    v = ess / wall
+    line = {"impl": "reference", "metric": "MCMC effective samples/s", "value": v,
+            "unit": "effective samples/s", "n_gpus": world, "steps": steps, "warmup": burn,
+            "ms_per_step": wall / steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (wd_dm_small physics at 500 points + noise sigma=1.5e-3)",
+            "config": {"workload": "surrogate_da reference arm: plain Metropolis, %d chains x "
+                                   "%d steps on the reference CPU path" % (chains, steps)},
+            "cpu_baseline": {"value": v, "unit": "effective samples/s", "cores": os.cpu_count(),
+                             "kind": kind,
+                             "sample": "%d chains x %d steps after %d burn-in steps, one light "
+                                       "curve per chain and step, acceptance %.2f"
+                                       % (chains, steps, burn, acc)},
+            "e2e": {"value": v, "unit": "effective samples/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "ours" and args.workload == "surrogate_da":
         return run_surrogate(args)
+    if args.impl == "reference" and args.workload == "surrogate_da":
+        return run_reference_da(args)
     if args.impl == "reference":
         return run_reference_batch(args) if args.workload == "mcmc_batch" else run_reference(args)
     if args.workload == "mcmc_batch":
