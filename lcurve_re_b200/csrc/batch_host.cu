@@ -99,7 +99,7 @@ struct BatchState {
     DBuf<int64_t> n0;
     DBuf<int32_t> blockcnt, queue, counters;
     DBuf<DevStatus> st;
-    DBuf<float4> ef;
+    DBuf<float4> ef, runb;
     DBuf<double> w1, w2, part, osum, calc, sfac, out;
     // results (pinned): calc, sfac, out, status
     unsigned char *h_res = nullptr;
@@ -128,7 +128,7 @@ struct BatchState {
         for (auto *b : d) b->release();
         area.release(); grav.release(); flux.release(); fp.release(); necl.release();
         ecl.release(); n0.release(); blockcnt.release(); queue.release(); counters.release();
-        st.release(); ef.release(); rings.release(); d_tab.release();
+        st.release(); ef.release(); runb.release(); rings.release(); d_tab.release();
         rows.release(); gathered.release();
         if (h_rows) cudaFreeHost(h_rows);
         h_rows = nullptr;
@@ -151,6 +151,7 @@ struct BatchState {
         b.g = GridDev{px.p, py.p, pz.p, nx.p, ny.p, nz.p, area.p, grav.p, flux.p,
                       necl.p, ein.p, eout.p, nfaces};
         b.fp = fp.p;
+        b.runb = runb.p;
         b.ecl = ecl.p;
         b.n0 = n0.p;
         b.blockcnt = blockcnt.p;
@@ -304,6 +305,7 @@ lcg_status relayout(lcg_ctx *c, BatchState &B, const lcg_model *models, int32_t 
     if ((e = B.area.ensure(nf)) || (e = B.grav.ensure(nf)) || (e = B.flux.ensure(nf)) ||
         (e = B.necl.ensure(nf)) || (e = B.queue.ensure(nf)) ||
         (e = B.fp.ensure(8 * (size_t)B.nflat)) || (e = B.ecl.ensure((size_t)B.nflat)) ||
+        (e = B.runb.ensure((size_t)B.nflat / 64)) ||
         (e = B.n0.ensure(ns)) || (e = B.blockcnt.ensure((size_t)B.nblk)) ||
         (e = B.counters.ensure(2)) || (e = B.st.ensure(nm)) ||
         (e = B.ef.ensure(nm * (size_t)B.ldp)) || (e = B.w1.ensure(nm * (size_t)B.ldp)) ||
@@ -321,6 +323,7 @@ lcg_status relayout(lcg_ctx *c, BatchState &B, const lcg_model *models, int32_t 
     // an odd pad record or a never-built slot must read as zeros
     cudaMemsetAsync(B.fp.p, 0, 8 * (size_t)B.nflat * sizeof(float), c->stream);
     cudaMemsetAsync(B.ecl.p, 0, (size_t)B.nflat * sizeof(uint2), c->stream);
+    cudaMemsetAsync(B.runb.p, 0, (size_t)B.nflat / 64 * sizeof(float4), c->stream);
     cudaMemsetAsync(B.n0.p, 0, ns * sizeof(int64_t), c->stream);
     B.key.assign(nm, lcg_model{});
     B.key_ok.assign(nm, 0);

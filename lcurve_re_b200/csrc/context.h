@@ -63,6 +63,7 @@ struct Grid {
     DBuf<uint2> ecl;
     DBuf<double> fdx, fdy, fdz, fpx, fpy, fpz, fflux, fin, fout;
     DBuf<float> fp;
+    DBuf<float4> runb;
     int64_t n = 0, npad = 0, ntiled = 0;
     int fast = 0;  // flat records built for the fast mixed sweep
     StarSetup setup;
@@ -87,7 +88,7 @@ struct Grid {
         if (mixed) {
             if ((e = ecl.ensure(npad))) return e;
             if (fast_on) {
-                if ((e = fp.ensure(8 * npad))) return e;
+                if ((e = fp.ensure(8 * npad)) || (e = runb.ensure(npad / 64))) return e;
             } else if ((e = geo.ensure(npad))) {
                 return e;
             }
@@ -105,7 +106,7 @@ struct Grid {
     }
     FlatDev flat() const {
         return FlatDev{n, npad, n0.p, geo.p, ecl.p, pos.p, fdx.p, fdy.p, fdz.p,
-                       fpx.p, fpy.p, fpz.p, fflux.p, fin.p, fout.p, fp.p};
+                       fpx.p, fpy.p, fpz.p, fflux.p, fin.p, fout.p, fp.p, runb.p};
     }
     void release() {
         DBuf<double> *d[] = {&px, &py, &pz, &nx, &ny, &nz, &ein, &eout, &fdx, &fdy,
@@ -113,6 +114,7 @@ struct Grid {
         for (auto *b : d) b->release();
         area.release(); grav.release(); flux.release(); necl.release(); rings.release();
         n0.release(); geo.release(); pos.release(); ecl.release(); fp.release();
+        runb.release();
     }
 };
 

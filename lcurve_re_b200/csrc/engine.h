@@ -84,6 +84,11 @@ struct FlatDev {
     // with cz = cos(i) nz and f_k = flux * p_k, so each float2 operand of the
     // packed FP32x2 arithmetic is an aligned register pair
     float *fp;
+    // per run of 32 pairs (64 faces) of fp: (ax, ay, R, C) bounding
+    // mu = ex nx + ey ny + cz <= ex ax + ey ay + |(ex, ey)| R + C for every face
+    // of the run (C includes a margin over FP32 rounding), so a warp can skip
+    // a run that faces away at all its phases
+    float4 *runb;
 };
 
 // Face records of the fast mixed sweep (no beaming, no lensing, mucrit <= 0):
@@ -168,6 +173,7 @@ struct BatchDev {
     int32_t nslots, nmodels;
     GridDev g;  // every face of the batch
     float *fp;  // fast sweep records (FlatDev::fp layout per slot)
+    float4 *runb;  // FlatDev::runb per slot, from flat0 / 64
     uint2 *ecl;
     int64_t *n0;  // per slot
     int32_t *blockcnt, *queue, *counters;
@@ -230,6 +236,9 @@ void launch_interp(const DatumRec *data, int32_t n, const int64_t *idx, int32_t 
                    const double *mc, double *calc, int32_t rdata, double *out, cudaStream_t s);
 
 void launch_pack_flat(FlatDev f, int64_t n0, int need_pos, cudaStream_t s);
+// run bounds of fast records: npairs pairs from fp, one float4 per 32 pairs
+void launch_run_bounds(const float *fp, int64_t npairs, float4 *runb, cudaStream_t s);
+void launch_batch_run_bounds(const BatchDev &b, int nsm, cudaStream_t s);
 void launch_pack_phases(PhaseDev ph, cudaStream_t s);
 
 // batched stages (geometry.cu): grid + eclipse of the geometry list;

@@ -248,10 +248,25 @@ __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b
 template <int PPT, int LT, bool ECL>
 __device__ __forceinline__ void sweep_pairs(const float4 *sp, const uint4 *se, int64_t q0,
                                             int64_t lo, int64_t hi, const float2 *ex,
-                                            const float2 *ey, const uint32_t *pf, float *acc) {
+                                            const float2 *ey, const float *exy,
+                                            const uint32_t *pf, const float4 *__restrict__ runb,
+                                            float *acc) {
     constexpr int kFoldPairs = kFold / 2;
     for (int64_t b = lo; b < hi; b += kFoldPairs) {
         const int cnt = (int)((b + kFoldPairs < hi) ? kFoldPairs : hi - b);
+        {
+            // the run bound (or the two, when the fold run straddles stored runs):
+            // negative at every phase entry of the warp -> the whole run adds zero
+            const float4 B0 = runb[b >> 5], B1 = runb[(b + cnt - 1) >> 5];
+            bool vis = false;
+#pragma unroll
+            for (int j = 0; j < PPT; j++) {
+                const float e0 = fmaf(ex[j].x, B0.x, fmaf(ey[j].x, B0.y, fmaf(exy[j], B0.z, B0.w)));
+                const float e1 = fmaf(ex[j].x, B1.x, fmaf(ey[j].x, B1.y, fmaf(exy[j], B1.z, B1.w)));
+                vis = vis || e0 >= 0.f || e1 >= 0.f;
+            }
+            if (!__any_sync(0xffffffffu, vis)) continue;
+        }
         const float4 *rp = sp + 4 * (b - q0);
         const uint4 *ep = se + (b - q0);
         float2 s[PPT];
@@ -317,6 +332,7 @@ __global__ void __launch_bounds__(kThreads, 2)
         if (need_ecl) bulk_g2s(se, f.ecl + c0, (uint32_t)(chunk * 8), &bar);
     }
     float2 ex[PPT], ey[PPT];
+    float exy[PPT];
     uint32_t pf[PPT];
 #pragma unroll
     for (int j = 0; j < PPT; j++) {
@@ -325,6 +341,7 @@ __global__ void __launch_bounds__(kThreads, 2)
         if (e < ph.nent) v = ph.ef[e];
         ex[j] = f2(v.x, v.x);
         ey[j] = f2(v.y, v.y);
+        exy[j] = sqrtf(fmaf(v.x, v.x, v.y * v.y));
         pf[j] = __float_as_uint(v.w);
     }
     if (!mbar_wait_bounded(&bar, 0)) {
@@ -344,8 +361,8 @@ __global__ void __launch_bounds__(kThreads, 2)
     // n in the last pair carry zero coefficients
     const int64_t q0 = c0 >> 1, qend = (cend + 1) >> 1, qn0 = n0 >> 1;
     const int64_t qa = qn0 < qend ? qn0 : qend;
-    sweep_pairs<PPT, LT, false>(sp, se, q0, q0, qa > q0 ? qa : q0, ex, ey, pf, acc);
-    sweep_pairs<PPT, LT, true>(sp, se, q0, qa > q0 ? qa : q0, qend, ex, ey, pf, acc);
+    sweep_pairs<PPT, LT, false>(sp, se, q0, q0, qa > q0 ? qa : q0, ex, ey, exy, pf, f.runb, acc);
+    sweep_pairs<PPT, LT, true>(sp, se, q0, qa > q0 ? qa : q0, qend, ex, ey, exy, pf, f.runb, acc);
 #pragma unroll
     for (int j = 0; j < PPT; j++) {
         const int64_t e = (int64_t)blockIdx.x * (kThreads * PPT) + tid * PPT + j;
@@ -384,7 +401,9 @@ __global__ void __launch_bounds__(kThreads, 2)
         if (need_ecl) bulk_g2s(se, b.ecl + S.flat0 + c0, (uint32_t)(chunk * 8), &bar);
     }
     const float4 *ef = ph.ef + model * ph.ldp;
+    const float4 *runb = b.runb + S.flat0 / 64;
     float2 ex[PPT], ey[PPT];
+    float exy[PPT];
     uint32_t pf[PPT];
 #pragma unroll
     for (int j = 0; j < PPT; j++) {
@@ -393,6 +412,7 @@ __global__ void __launch_bounds__(kThreads, 2)
         if (e < ph.nent) v = ef[e];
         ex[j] = f2(v.x, v.x);
         ey[j] = f2(v.y, v.y);
+        exy[j] = sqrtf(fmaf(v.x, v.x, v.y * v.y));
         pf[j] = __float_as_uint(v.w);
     }
     if (!mbar_wait_bounded(&bar, 0)) {
@@ -409,11 +429,11 @@ __global__ void __launch_bounds__(kThreads, 2)
     const int64_t qa = qn0 < qend ? qn0 : qend;
     const int64_t qb = qa > q0 ? qa : q0;
     if (ltype == 1) {
-        sweep_pairs<PPT, 1, false>(sp, se, q0, q0, qb, ex, ey, pf, acc);
-        sweep_pairs<PPT, 1, true>(sp, se, q0, qb, qend, ex, ey, pf, acc);
+        sweep_pairs<PPT, 1, false>(sp, se, q0, q0, qb, ex, ey, exy, pf, runb, acc);
+        sweep_pairs<PPT, 1, true>(sp, se, q0, qb, qend, ex, ey, exy, pf, runb, acc);
     } else {
-        sweep_pairs<PPT, 0, false>(sp, se, q0, q0, qb, ex, ey, pf, acc);
-        sweep_pairs<PPT, 0, true>(sp, se, q0, qb, qend, ex, ey, pf, acc);
+        sweep_pairs<PPT, 0, false>(sp, se, q0, q0, qb, ex, ey, exy, pf, runb, acc);
+        sweep_pairs<PPT, 0, true>(sp, se, q0, qb, qend, ex, ey, exy, pf, runb, acc);
     }
 #pragma unroll
     for (int j = 0; j < PPT; j++) {

@@ -619,6 +619,73 @@ __global__ void __launch_bounds__(1024) k_interp(const DatumRec *__restrict__ da
     }
 }
 
+// Bound of mu over one run of 32 face pairs of the fast records, one warp per
+// run (lane l reads pair l): with a = the mean of (nx, ny), R = the largest
+// |(nx, ny) - a| and C = the largest cz of the run's faces,
+//   mu = ex nx + ey ny + cz <= ex ax + ey ay + |(ex, ey)| R + C.
+// R and C are widened well past FP32 rounding (1e-6, 1e-5), so when the bound
+// is negative the computed mu of every face of the run is <= 0 and the run adds
+// exactly zero. All-zero records (padding) are left out; a run of padding only
+// gets C = -1.
+__device__ __forceinline__ void run_bound(const float *__restrict__ fp, int64_t npairs,
+                                          int64_t run, float4 *out) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int64_t q = run * 32 + lane;
+    float nx[2] = {0.f, 0.f}, ny[2] = {0.f, 0.f}, cz[2] = {0.f, 0.f};
+    bool use[2] = {false, false};
+    if (q < npairs) {
+        const float4 P0 = reinterpret_cast<const float4 *>(fp)[4 * q];
+        const float4 P1 = reinterpret_cast<const float4 *>(fp)[4 * q + 1];
+        nx[0] = P0.x; nx[1] = P0.y; ny[0] = P0.z; ny[1] = P0.w; cz[0] = P1.x; cz[1] = P1.y;
+        for (int k = 0; k < 2; k++) use[k] = nx[k] != 0.f || ny[k] != 0.f || cz[k] != 0.f;
+    }
+    float sx = 0.f, sy = 0.f, cnt = 0.f;
+    for (int k = 0; k < 2; k++)
+        if (use[k]) { sx += nx[k]; sy += ny[k]; cnt += 1.f; }
+    for (int o = 16; o > 0; o >>= 1) {
+        sx += __shfl_xor_sync(full, sx, o);
+        sy += __shfl_xor_sync(full, sy, o);
+        cnt += __shfl_xor_sync(full, cnt, o);
+    }
+    const float ax = cnt > 0.f ? sx / cnt : 0.f, ay = cnt > 0.f ? sy / cnt : 0.f;
+    float r = 0.f, c = -1.f;
+    for (int k = 0; k < 2; k++)
+        if (use[k]) {
+            r = fmaxf(r, sqrtf((nx[k] - ax) * (nx[k] - ax) + (ny[k] - ay) * (ny[k] - ay)));
+            c = fmaxf(c, cz[k]);
+        }
+    for (int o = 16; o > 0; o >>= 1) {
+        r = fmaxf(r, __shfl_xor_sync(full, r, o));
+        c = fmaxf(c, __shfl_xor_sync(full, c, o));
+    }
+    if (lane == 0)
+        *out = cnt > 0.f ? make_float4(ax, ay, r * (1.f + 1e-6f) + 1e-6f, c + 1e-5f)
+                         : make_float4(0.f, 0.f, 0.f, -1.f);
+}
+
+__global__ void k_run_bounds(const float *__restrict__ fp, int64_t npairs, float4 *runb) {
+    const int64_t run = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (run >= (npairs + 31) / 32) return;  // whole warps
+    run_bound(fp, npairs, run, runb + run);
+}
+
+// Run bounds of the continuum list's slots (16 runs per 1024-face block).
+__global__ void k_run_bounds_b(BatchDev b) {
+    const int nk = b.counts[1];
+    if (nk <= 0) return;
+    const int64_t total = b.cont_blk[nk] * 16;
+    const int64_t warps = (int64_t)gridDim.x * blockDim.x / 32;
+    for (int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; w < total;
+         w += warps) {
+        const int64_t B = w >> 4;
+        const int k = find_seg(b.cont_blk, nk, B);
+        const SlotDev &S = b.slots[b.cont_slot[k]];
+        const int64_t run = (B - b.cont_blk[k]) * 16 + (w & 15);
+        run_bound(b.fp + 8 * S.flat0, (S.nface + 1) / 2, run, b.runb + S.flat0 / 64 + run);
+    }
+}
+
 // dst row r = src row rows[r] (rows of n doubles).
 __global__ void k_gather_rows(const double *__restrict__ src, int32_t n,
                               const int32_t *__restrict__ rows, double *dst) {
@@ -1005,6 +1072,7 @@ void launch_flatten(GridDev g, FlatDev f, int32_t *blockcnt, int mixed, int need
     count_launch();
     k_flat_scatter<<<nb, kFlatBlock, 0, s>>>(g, f, blockcnt, mixed, need_pos, fc);
     count_launch();
+    if (mixed && fc.on) launch_run_bounds(f.fp, f.npad / 2, f.runb, s);
 }
 
 void launch_phases(const PhaseParams &p, const DatumRec *data, const int64_t *off, int32_t n,
@@ -1040,6 +1108,18 @@ void launch_interp(const DatumRec *data, int32_t n, const int64_t *idx, int32_t 
                    const double *mc, double *calc, int32_t rdata, double *out, cudaStream_t s) {
     if (n <= 0 || m <= 0) return;
     k_interp<<<1, 1024, 0, s>>>(data, n, idx, m, mc, calc, rdata, out);
+    count_launch();
+}
+
+void launch_run_bounds(const float *fp, int64_t npairs, float4 *runb, cudaStream_t s) {
+    const int64_t nruns = (npairs + 31) / 32;
+    if (nruns <= 0) return;
+    k_run_bounds<<<nblocks(nruns * 32, 256), 256, 0, s>>>(fp, npairs, runb);
+    count_launch();
+}
+
+void launch_batch_run_bounds(const BatchDev &b, int nsm, cudaStream_t s) {
+    k_run_bounds_b<<<nsm * 4, 256, 0, s>>>(b);
     count_launch();
 }
 
@@ -1086,6 +1166,7 @@ void launch_batch_flatten(const BatchDev &b, int nsm, cudaStream_t s) {
     count_launch();
     k_flat_scatter_b<<<nsm * 2, kFlatBlock, 0, s>>>(b);
     count_launch();
+    launch_batch_run_bounds(b, nsm, s);
 }
 
 void launch_batch_phases(const BatchDev &b, const DatumRec *data, const int64_t *off, int32_t n,
