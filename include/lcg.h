@@ -15,6 +15,9 @@
  *                             new_scripts/levmarq_solver.cpp:789-886)
  *   lcg_star_grid          <- Lcurve::set_star_grid + set_star_continuum
  *                             (src/lcurve_base/lcurve.h:528,550)
+ *   lcg_components         <- Lcurve::set_disc_grid, set_disc_edge,
+ *                             set_bright_spot_grid + their continua
+ *                             (src/lcurve_base/lcurve.h:539-561)
  *   lcg_sum_star_multi     <- Lcurve::flat_sum_star1_multi / _star2_multi
  *                             (src/lcurve_base/lcurve.h:299-307) and the
  *                             reference CUDA hooks cuda_sum_star{1,2}_multi
@@ -39,7 +42,7 @@
 extern "C" {
 #endif
 
-#define LCG_ABI_VERSION 2
+#define LCG_ABI_VERSION 3
 
 typedef enum lcg_status {
     LCG_OK = 0,
@@ -47,7 +50,7 @@ typedef enum lcg_status {
     LCG_E_LOBE = 2,         /* a star overfills its Roche lobe (Lcurve_Error) */
     LCG_E_ROCHE = 3,        /* radius / eclipse solve failed (Roche_Error)    */
     LCG_E_NOCONVERGE = 4,   /* an iteration cap was reached                   */
-    LCG_E_UNSUPPORTED = 5,  /* disc, bright spot or iscale models             */
+    LCG_E_UNSUPPORTED = 5,  /* a model or call this engine does not evaluate  */
     LCG_E_CUDA = 6,         /* CUDA runtime failure or no device              */
     LCG_E_NOMEM = 7,        /* device or host allocation failed               */
     LCG_E_CAPACITY = 8      /* a size exceeds a fixed capacity                */
@@ -118,6 +121,13 @@ typedef struct lcg_model {
     int32_t limb1, limb2;
     int32_t mirror, add_disc, opaque, add_spot, iscale;
     int32_t pad_;
+    /* accretion disc with its outer edge (read when add_disc is set) and the
+       bright spot (read when add_spot is set), model.cpp:211-230,353-357 */
+    double rdisc1, rdisc2, height_disc, beta_disc, temp_disc, texp_disc;
+    double lin_limb_disc, quad_limb_disc, temp_edge, absorb_edge;
+    double radius_spot, length_spot, height_spot, expon_spot, epow_spot;
+    double angle_spot, yaw_spot, temp_spot, tilt_spot, cfrac_spot;
+    int32_t nrad, nspot;
 } lcg_model;
 
 /* One light-curve point, byte-compatible with Lcurve::Datum
@@ -250,6 +260,18 @@ lcg_status lcg_star_grid(lcg_ctx *ctx, const lcg_model *model, int32_t star,
                          double *dirn, float *area, float *gravity,
                          float *flux, int32_t *neclipse, double *ecl_in,
                          double *ecl_out);
+
+/* One component grid of a model as light_curve_comp builds it: which = 0
+ * the accretion disc (set_disc_grid.cpp:27-127 with set_disc_continuum),
+ * 1 its outer rim (set_disc_grid.cpp:144-264 with set_edge_continuum),
+ * 2 the bright spot (set_bright_spot_grid.cpp:27-100). *n gets the element
+ * count; when it is <= cap the host arrays are filled: posn, dirn (3 per
+ * element), float area and flux, the number of eclipse ranges nr and the
+ * ranges in rin / rout (4 per element, in the reference's push order). */
+lcg_status lcg_components(lcg_ctx *ctx, const lcg_model *model, int32_t which,
+                          int32_t cap, int32_t *n, double *posn, double *dirn,
+                          float *area, float *flux, int32_t *nr, double *rin,
+                          double *rout);
 
 /* The blocked multi-phase flux sweep over one flattened grid: out[k] is the
  * unweighted flux sum for phase entry k (flat_sum_star{1,2}_multi).

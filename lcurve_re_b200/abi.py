@@ -5,7 +5,7 @@ test (tests/test_abi.py) checks sizes and offsets against the header.
 """
 import ctypes as C
 
-LCG_ABI_VERSION = 2
+LCG_ABI_VERSION = 3
 
 # lcg_status
 OK, E_INVALID, E_LOBE, E_ROCHE, E_NOCONVERGE, E_UNSUPPORTED, E_CUDA, E_NOMEM, E_CAPACITY = range(9)
@@ -25,6 +25,13 @@ OUT_WDWARF, OUT_CHISQ, OUT_WNOK, OUT_LOGG1, OUT_LOGG2, OUT_RV1, OUT_RV2 = range(
 NOUT = 7
 
 STAGES = ("grid", "eclipse", "continuum", "flatten", "phases", "flux", "reduce")
+
+
+# disc, edge and bright-spot parameters, in lcg_model order
+DISC_SPOT = ["rdisc1", "rdisc2", "height_disc", "beta_disc", "temp_disc", "texp_disc",
+             "lin_limb_disc", "quad_limb_disc", "temp_edge", "absorb_edge",
+             "radius_spot", "length_spot", "height_spot", "expon_spot", "epow_spot",
+             "angle_spot", "yaw_spot", "temp_spot", "tilt_spot", "cfrac_spot"]
 
 
 class LcgModel(C.Structure):
@@ -53,7 +60,7 @@ class LcgModel(C.Structure):
         ("limb1", C.c_int32), ("limb2", C.c_int32),
         ("mirror", C.c_int32), ("add_disc", C.c_int32), ("opaque", C.c_int32),
         ("add_spot", C.c_int32), ("iscale", C.c_int32), ("pad_", C.c_int32),
-    ]
+    ] + [(n, C.c_double) for n in DISC_SPOT] + [("nrad", C.c_int32), ("nspot", C.c_int32)]
 
 
 class LcgDatum(C.Structure):
@@ -97,6 +104,8 @@ PROTOTYPES = {
     "lcg_star_face_count": (C.c_int, [P, C.POINTER(LcgModel), C.c_int32, C.c_int32, I32]),
     "lcg_star_grid": (C.c_int, [P, C.POINTER(LcgModel), C.c_int32, C.c_int32, C.c_int32,
                                 D, D, F, F, F, I32, D, D]),
+    "lcg_components": (C.c_int, [P, C.POINTER(LcgModel), C.c_int32, C.c_int32, I32, D, D, F, F,
+                                 I32, D, D]),
     "lcg_sum_star_multi": (C.c_int, [P, C.c_int32, C.c_int64, C.c_int64, D, D, D, D, D, D, D, D,
                                      D, C.c_int32, D, D, D, D, D, C.c_int32, C.c_double,
                                      C.c_double, C.c_double, C.c_double, C.c_double,

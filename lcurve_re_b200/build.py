@@ -32,8 +32,9 @@ SOURCES = {
     "noalloc.cu": ["--fmad=false"],
     "batch_host.cu": ["--fmad=false"],
     "mlp.cu": ["--fmad=true"],
+    "components.cu": ["--fmad=false"],
 }
-HEADERS = ["roche.cuh", "eclipse.cuh", "engine.h", "tma.cuh", "context.h"]
+HEADERS = ["roche.cuh", "eclipse.cuh", "disc.cuh", "engine.h", "tma.cuh", "context.h"]
 
 
 def nvcc():

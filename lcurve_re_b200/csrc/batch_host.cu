@@ -354,8 +354,12 @@ bool same_layout(const BatchState &B, const lcg_ctx *c, const lcg_model *models,
 
 // Models the batched path covers: the fast mixed sweep applies to both stars
 // and each star has a single grid (coarse = fine, no infill).
+// Models the batched stages cover; the others (beaming, lensing, limb cut-off,
+// coarse grids, infill, disc / spot / iscale models) go one by one through the
+// single-model path.
 bool batchable(const lcg_model &m) {
-    return m.beam_factor1 == 0. && m.beam_factor2 == 0. && !m.glens1 && m.mucrit1 <= 0. &&
+    return !m.add_disc && !m.add_spot && !m.iscale &&
+           m.beam_factor1 == 0. && m.beam_factor2 == 0. && !m.glens1 && m.mucrit1 <= 0. &&
            m.mucrit2 <= 0. && m.nlat1c == m.nlat1f && m.nlat2c == m.nlat2f &&
            (!m.npole || (m.nlatfill == 0 && m.nlngfill == 0));
 }

@@ -64,6 +64,11 @@ struct Grid {
     DBuf<double> fdx, fdy, fdz, fpx, fpy, fpz, fflux, fin, fout;
     DBuf<float> fp;
     DBuf<float4> runb;
+    // opaque disc: per-face disc ranges, and the flat grid's several-range faces
+    DBuf<uint8_t> ndx, rn;
+    DBuf<double2> xr, rr;
+    DBuf<int32_t> ridx;
+    bool disc = false;  // ndx / xr hold this grid's disc ranges
     int64_t n = 0, npad = 0, ntiled = 0;
     int fast = 0;  // flat records built for the fast mixed sweep
     StarSetup setup;
@@ -83,8 +88,10 @@ struct Grid {
     cudaError_t alloc_flat(int mixed, int need_pos, int fast_on) {
         npad = ((n + 4095) / 4096) * 4096;
         if (npad == 0) npad = 4096;
-        cudaError_t e = n0.ensure(1);
+        cudaError_t e = n0.ensure(2);  // n0, n1
         if (e) return e;
+        if (disc && ((e = ridx.ensure(n)) || (e = rn.ensure(n)) || (e = rr.ensure(kRagRanges * n))))
+            return e;
         if (mixed) {
             if ((e = ecl.ensure(npad))) return e;
             if (fast_on) {
@@ -102,11 +109,13 @@ struct Grid {
     }
     GridDev dev() const {
         return GridDev{px.p, py.p, pz.p, nx.p, ny.p, nz.p, area.p, grav.p, flux.p,
-                       necl.p, ein.p, eout.p, n, ntiled};
+                       necl.p, ein.p, eout.p, n, ntiled, disc ? ndx.p : nullptr,
+                       disc ? xr.p : nullptr};
     }
     FlatDev flat() const {
         return FlatDev{n, npad, n0.p, geo.p, ecl.p, pos.p, fdx.p, fdy.p, fdz.p,
-                       fpx.p, fpy.p, fpz.p, fflux.p, fin.p, fout.p, fp.p, runb.p};
+                       fpx.p, fpy.p, fpz.p, fflux.p, fin.p, fout.p, fp.p, runb.p,
+                       n0.p ? n0.p + 1 : nullptr, ridx.p, rr.p, rn.p};
     }
     void release() {
         DBuf<double> *d[] = {&px, &py, &pz, &nx, &ny, &nz, &ein, &eout, &fdx, &fdy,
@@ -114,7 +123,8 @@ struct Grid {
         for (auto *b : d) b->release();
         area.release(); grav.release(); flux.release(); necl.release(); rings.release();
         n0.release(); geo.release(); pos.release(); ecl.release(); fp.release();
-        runb.release();
+        runb.release(); ndx.release(); rn.release(); xr.release(); rr.release(); ridx.release();
+        disc = false;
     }
 };
 
@@ -157,6 +167,12 @@ struct lcg_ctx {
         sfac, out, diag, osum;
     DBuf<float4> pef;
     DBuf<uint8_t> ptype;
+    // disc, rim and bright spot of the last model; iscale components
+    DBuf<lcg::ElemRec> elem;
+    DBuf<double4> epos;
+    DBuf<lcg::DiscRing> drings;
+    DBuf<double> csum, fcomp, iwork;
+    lcg::CompParams comp{};
     std::vector<int64_t> h_off;
     std::vector<double> h_diag;
     // resident light-curve points (lcg_set_data)
@@ -243,6 +259,11 @@ ContParams continuum_params(const lcg_model &m, int star);
 FluxConsts flux_consts(const lcg_model &m, int star, double spin, double rlens1);
 FastCoef fast_coef(const lcg_model &m, int star, int mixed);
 lcg_status check_model(lcg_ctx *c, const lcg_model *m);
+// Disc, rim and spot of a model: counts, ring table and element constants
+// (set_disc_grid.cpp, set_bright_spot_grid.cpp); false with f set on a
+// reference error.
+bool comp_setup(const lcg_model &m, CompParams &p, std::vector<DiscRing> &rings, Fail &f);
+bool bright_spot_position(double q, double rad, double *pos, Fail &f);
 lcg_status finish_status(lcg_ctx *c);
 
 }  // namespace eng

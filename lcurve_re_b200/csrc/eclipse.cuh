@@ -16,6 +16,9 @@
 #include "roche.cuh"
 
 namespace lcg {
+// internal linkage: every translation unit that includes this header gets
+// its own copy of these device functions
+namespace {
 
 enum {
     kEclOk = 0,
@@ -393,9 +396,11 @@ __device__ bool ingress_egress(int star, double q, double spin, double cosi, dou
     return true;
 }
 
+}  // namespace
 }  // namespace lcg
 
 namespace lcg {
+namespace {
 
 // Warp-cooperative Roche::ingress_egress, for grids with few eclipse
 // candidates, where one thread per face leaves the GPU idle. Lane 0 runs the
@@ -505,4 +510,5 @@ __device__ bool ingress_egress_warp(int star, double q, double spin, double cosi
     return true;
 }
 
+}  // namespace
 }  // namespace lcg

@@ -484,7 +484,7 @@ lcg_status flatten(lcg_ctx *c, Grid &g, int need_pos, const FastCoef &fc) {
     if ((e = g.alloc_flat(mixed, need_pos, fc.on)) != cudaSuccess)
         return c->cuda_fail(e, "flat grid");
     g.fast = fc.on;
-    if ((e = c->blockcnt.ensure((g.n + 1023) / 1024 + 1)) != cudaSuccess)
+    if ((e = c->blockcnt.ensure(2 * ((g.n + 1023) / 1024) + 1)) != cudaSuccess)
         return c->cuda_fail(e, "partition");
     StageScope t(c, LCG_STAGE_FLATTEN);
     launch_flatten(g.dev(), g.flat(), c->blockcnt.p, mixed, need_pos, fc, c->status.p,
@@ -514,6 +514,9 @@ lcg_status sweep_one(lcg_ctx *c, const lcg_model &m, Grid &g, int star, double p
         return c->cuda_fail(err, "partials");
     FluxConsts k = flux_consts(m, star, 1.0, rlens1);
     launch_flux(mixed, star, k, g.flat(), ph, plan, c->part1f.p, 4, c->status.p, c->stream);
+    if (g.disc)
+        launch_flux_ragged(star, k, g.flat(), g.dev(), ph, plan.chunk, plan.nchunk, c->part1f.p, 4,
+                           c->stream);
     std::vector<double> col((size_t)std::max<int64_t>(plan.nchunk, 1));
     if (plan.nchunk)
         cudaMemcpy2DAsync(col.data(), 8, c->part1f.p, 4 * 8, 8, (size_t)plan.nchunk,
@@ -566,9 +569,8 @@ lcg_status ginterp_scales(lcg_ctx *c, const lcg_model &m, double rlens1) {
 
 lcg_status check_model(lcg_ctx *c, const lcg_model *m) {
     if (!m) return c->fail(LCG_E_INVALID, "null model");
-    if (m->add_disc || m->add_spot || m->iscale)
-        return c->fail(LCG_E_UNSUPPORTED,
-                       "disc, bright-spot and iscale models are not supported by this engine");
+    if (m->add_disc && m->nrad < 1)
+        return c->fail(LCG_E_INVALID, "nrad = %d: the disc needs at least one radius", m->nrad);
     if (!(m->q > 0.))
         return c->fail(LCG_E_INVALID, "Roche::xl12(double, double): q = %f <= 0.", m->q);
     if (!(m->delta_phase > 0.))
@@ -593,6 +595,11 @@ lcg_status finish_status(lcg_ctx *c) {
     if (e != cudaSuccess) return c->cuda_fail(e, "status");
     if (st.code) {
         c->has_geom = c->has_cont = false;
+        if (st.face < 0)  // a disc, rim or spot element (components.cu)
+            return c->fail(st.code, "%s (disc, rim or spot element %d)",
+                           st.code == 3 ? "disc or star eclipse of a component failed"
+                                        : status_text(st.code),
+                           -st.face - 1);
         return c->fail(st.code, "%s (face %d)", status_text(st.code), st.face);
     }
     return LCG_OK;
@@ -843,6 +850,11 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
         rlens1 = 4. * gm / (1. + m.q) / a / (kC * kC);
     }
     const bool need_pos = m.beam_factor1 != 0. || m.beam_factor2 != 0. || m.glens1;
+    // disc / rim / bright spot; an opaque disc also eclipses the stars;
+    // iscale fits one scale factor per component (light_curve_comp.cpp:272-414)
+    const bool comps = m.add_disc || m.add_spot;
+    const bool opaque = m.add_disc && m.opaque;
+    const bool iscale = m.iscale != 0;
     cudaMemsetAsync(c->status.p, 0, sizeof(DevStatus), c->stream);
 
     // geometry (GeomKey)
@@ -867,26 +879,79 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
         fprintf(stderr, "Number of points for star 2 (coarse) = %lld\n", (long long)g2c.n);
     }
 
+    // disc, rim and bright-spot elements (set_disc_grid, set_disc_edge,
+    // set_bright_spot_grid with their continua), rebuilt every call
+    int32_t ncomp = 0;
+    if (comps) {
+        std::vector<DiscRing> rings;
+        Fail f{0, ""};
+        if (!comp_setup(m, c->comp, rings, f)) return c->fail(f.code, "%s", f.msg.c_str());
+        ncomp = c->comp.nd + c->comp.ne + c->comp.ns;
+        if ((e = c->elem.ensure(ncomp)) || (e = c->epos.ensure(ncomp)) ||
+            (e = c->drings.ensure(rings.size())))
+            return c->cuda_fail(e, "component elements");
+        if (!rings.empty())
+            cudaMemcpyAsync(c->drings.p, rings.data(), rings.size() * sizeof(DiscRing),
+                            cudaMemcpyHostToDevice, c->stream);
+        c->comp.rings = c->drings.p;
+        StageScope t(c, LCG_STAGE_GRID);
+        launch_components(c->comp, c->elem.p, c->epos.p, c->status.p, c->stream);
+        if ((flags & LCG_FLAG_INFO) && m.add_disc)
+            fprintf(stderr, "Number of points for the disc = %d\n", c->comp.nd);
+    }
+
     // continuum (ContKey) + FlatGrid
+    // (opaque discs bypass the reuse, light_curve_comp.cpp:163)
     const bool cont_hit = c->has_cont && geom_hit && same_continuum(c->key, m) &&
-                          c->cached_mixed_pos == (int)need_pos;
+                          c->cached_mixed_pos == (int)need_pos && !opaque && !c->g1f.disc &&
+                          !c->g2f.disc && !c->g1c.disc && !c->g2c.disc;
     if (!cont_hit) {
         Grid *gl[] = {&c->g1f, &c->g2f, &c->g1c, &c->g2c};
         const int stars[] = {kStar1, kStar2, kStar1, kStar2};
         const bool use[] = {true, true, !c->copy1, !c->copy2};
         for (int k = 0; k < 4; k++) {
+            gl[k]->disc = false;
             if (!use[k]) continue;
             ContParams cp = continuum_params(m, stars[k]);
             {
                 StageScope t(c, LCG_STAGE_CONTINUUM);
                 launch_continuum(cp, gl[k]->dev(), c->stream);
             }
-            if ((rc = flatten(c, *gl[k], need_pos, fast_coef(m, stars[k], c->precision == LCG_PREC_MIXED))))
-                return rc;
+            // (with an opaque disc the grids are flattened below, after the
+            // disc's ranges; first without them when the Ginterp scales need it)
+            if (!opaque || !c->copy1 || !c->copy2)
+                if ((rc = flatten(c, *gl[k], need_pos,
+                                  fast_coef(m, stars[k], c->precision == LCG_PREC_MIXED))))
+                    return rc;
         }
         c->gi = Ginterp{m.phase1, m.phase2, 1., 1., 1., 1.};
         if (!c->copy1 || !c->copy2) {
             if ((rc = ginterp_scales(c, m, rlens1))) return rc;
+        }
+        if (opaque) {
+            // the disc's ranges join the stars' after the Ginterp scales were
+            // taken (light_curve_comp.cpp:279-323, 327-333); rdisc1 defaults
+            // to r1 as given, before any lobe filling
+            double r1g, r2g;
+            get_r1r2(m, r1g, r2g);
+            const DiscGeom dg{sin(kPi / 180. * m.iangle), cos(kPi / 180. * m.iangle),
+                              m.rdisc1 > 0. ? m.rdisc1 : r1g,
+                              m.rdisc2 > 0. ? m.rdisc2 : m.radius_spot, m.beta_disc,
+                              m.height_disc};
+            for (int k = 0; k < 4; k++) {
+                if (!use[k]) continue;
+                Grid &g = *gl[k];
+                if ((e = g.ndx.ensure(g.n)) || (e = g.xr.ensure(kDiscRanges * g.n)))
+                    return c->cuda_fail(e, "disc eclipses");
+                {
+                    StageScope t(c, LCG_STAGE_ECLIPSE);
+                    launch_disc_faces(dg, g.dev(), g.ndx.p, g.xr.p, c->status.p, c->stream);
+                }
+                g.disc = true;
+                if ((rc = flatten(c, g, need_pos,
+                                  fast_coef(m, stars[k], c->precision == LCG_PREC_MIXED))))
+                    return rc;
+            }
         }
         c->cached_mixed_pos = (int)need_pos;
     }
@@ -906,14 +971,14 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
                 c->pef.p, c->ptype.p, nall};
     const double ri = deg2rad(m.iangle);
     const double cosi = cos(ri), sini = sin(ri);
+    PhaseParams pp{};
+    pp.t0 = m.t0; pp.period = m.period; pp.pdot = m.pdot; pp.deltat = m.deltat;
+    pp.slope = m.slope; pp.quad = m.quad; pp.cube = m.cube;
+    pp.middle = (xmin + xmax) / 2.;
+    pp.range = (xmax - xmin) / 2.;
+    pp.cosi = cosi; pp.sini = sini;
+    pp.gi = c->gi;
     {
-        PhaseParams pp{};
-        pp.t0 = m.t0; pp.period = m.period; pp.pdot = m.pdot; pp.deltat = m.deltat;
-        pp.slope = m.slope; pp.quad = m.quad; pp.cube = m.cube;
-        pp.middle = (xmin + xmax) / 2.;
-        pp.range = (xmax - xmin) / 2.;
-        pp.cosi = cosi; pp.sini = sini;
-        pp.gi = c->gi;
         StageScope t(c, LCG_STAGE_PHASES);
         launch_phases(pp, c->data.p, c->off.p, n, ph, c->stream);
         if (diag) {
@@ -940,10 +1005,13 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
         int64_t nent;
         FluxPlan plan;
     };
-    Sweep sw[4] = {{&g1f, kStar1, m.spin1, &c->part1f, nall, {}},
-                   {&g1c, kStar1, m.spin1, &c->part1c, nall, {}},
-                   {&g2f, kStar2, m.spin2, &c->part2f, nent, {}},
-                   {&g2c, kStar2, m.spin2, &c->part2c, nent, {}}};
+    // iscale's components are comp_star1_flat / comp_star2_flat sums, which
+    // take spin 1 in the beaming (comp_light_flat.cpp:538-602)
+    const double spin1 = iscale ? 1.0 : m.spin1, spin2 = iscale ? 1.0 : m.spin2;
+    Sweep sw[4] = {{&g1f, kStar1, spin1, &c->part1f, nall, {}},
+                   {&g1c, kStar1, spin1, &c->part1c, nall, {}},
+                   {&g2f, kStar2, spin2, &c->part2f, nent, {}},
+                   {&g2c, kStar2, spin2, &c->part2c, nent, {}}};
     const bool use_sw[4] = {true, !c->copy1, true, !c->copy2};
     for (int k = 0; k < 4; k++) {
         if (!use_sw[k]) continue;
@@ -957,7 +1025,18 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
         StageScope t(c, LCG_STAGE_FLUX);
         launch_flux(mixed, s.star, kc, s.g->flat(), phk, s.plan, s.part->p, ldp, c->status.p,
                     c->stream);
+        if (s.g->disc)
+            launch_flux_ragged(s.star, kc, s.g->flat(), s.g->dev(), phk, s.plan.chunk,
+                               s.plan.nchunk, s.part->p, ldp, c->stream);
         c->flux_elements += s.g->n * s.nent;
+    }
+    if (comps) {
+        if ((e = c->csum.ensure(3 * (size_t)ldp))) return c->cuda_fail(e, "component sums");
+        PhaseDev phc = ph;
+        phc.nent = nent;
+        StageScope t(c, LCG_STAGE_FLUX);
+        launch_comp_sums(c->elem.p, c->comp.nd, c->comp.ne, ncomp, m.lin_limb_disc,
+                         m.quad_limb_disc, phc, c->csum.p, ldp, c->stream);
     }
 
     // scatter, third light, scale, chi**2
@@ -966,6 +1045,14 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
         sp.copy1 = c->copy1;
         sp.copy2 = c->copy2;
         sp.third = m.third;
+        sp.csum = comps ? c->csum.p : nullptr;
+        sp.ldc = ldp;
+        sp.pp = pp;
+        if (iscale) {
+            if ((e = c->fcomp.ensure(5 * (size_t)n)) || (e = c->iwork.ensure(6 * (size_t)n)))
+                return c->cuda_fail(e, "iscale components");
+            sp.fcomp = c->fcomp.p;
+        }
         if ((e = c->osum.ensure(4 * (size_t)ldp))) return c->cuda_fail(e, "entry sums");
         ReduceParams rp{};
         rp.ldp = ldp;
@@ -978,7 +1065,11 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
         StageScope t(c, LCG_STAGE_REDUCE);
         launch_scatter(sp, rp, ph, c->data.p, c->off.p, n, c->calc.p, c->stream);
         cudaMemcpyAsync(c->sfac.p, sfac, 5 * sizeof(double), cudaMemcpyHostToDevice, c->stream);
-        launch_finalize(flags & 3, c->data.p, n, c->calc.p, c->sfac.p, c->out.p, c->stream);
+        if (iscale)
+            launch_iscale(flags & 3, m.t2 > 0 ? 5 : 4, c->data.p, n, c->fcomp.p, c->iwork.p,
+                          c->calc.p, c->sfac.p, c->out.p, c->stream);
+        else
+            launch_finalize(flags & 3, c->data.p, n, c->calc.p, c->sfac.p, c->out.p, c->stream);
     }
     double hout[4] = {0, 0, 0, 0};
     if (calc)
@@ -1006,6 +1097,13 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
     if ((rc = finish_status(c))) return rc;
     c->key = m;
     c->has_geom = c->has_cont = true;
+    if (diag && m.beam_factor1 != 0. && m.spin1 != 1.0 && !iscale) {
+        // wdwarf is comp_star1_flat at phase 0.5, which beams with spin 1
+        // (light_curve_comp.cpp:504-508); the sweeps above used spin1
+        const bool fine = c->copy1 || gi_type(c->gi, 0.5) == 1;
+        if ((rc = sweep_one(c, m, fine ? g1f : g1c, kStar1, 0.5, cosi, sini, rlens1, wsum)))
+            return rc;
+    }
 
     if (hout[2] != 0.) {
         scalars[LCG_OUT_CHISQ] = hout[0];
@@ -1083,6 +1181,60 @@ lcg_status lcg_star_face_count(lcg_ctx *c, const lcg_model *m, int32_t star, int
     Fail f{0, ""};
     if (!prepare_star(*m, star, fine, s, f)) return c->fail(f.code, "%s", f.msg.c_str());
     *nface = s.nface;
+    return LCG_OK;
+}
+
+lcg_status lcg_components(lcg_ctx *c, const lcg_model *m, int32_t which, int32_t cap,
+                          int32_t *n, double *posn, double *dirn, float *area, float *flux,
+                          int32_t *nr, double *rin, double *rout) {
+    if (!c) return LCG_E_INVALID;
+    c->err.clear();
+    lcg_status rc = check_model(c, m);
+    if (rc) return rc;
+    if (!n || which < 0 || which > 2) return c->fail(LCG_E_INVALID, "bad component request");
+    cudaSetDevice(c->device);
+    std::vector<DiscRing> rings;
+    Fail f{0, ""};
+    lcg_model mm = *m;
+    if (which < 2) mm.add_spot = 0;
+    else mm.add_disc = 0;
+    if ((which < 2 && !m->add_disc) || (which == 2 && !m->add_spot)) {
+        *n = 0;
+        return LCG_OK;
+    }
+    if (!comp_setup(mm, c->comp, rings, f)) return c->fail(f.code, "%s", f.msg.c_str());
+    const int32_t total = c->comp.nd + c->comp.ne + c->comp.ns;
+    const int32_t lo = which == 0 ? 0 : (which == 1 ? c->comp.nd : c->comp.nd + c->comp.ne);
+    const int32_t cnt = which == 0 ? c->comp.nd : (which == 1 ? c->comp.ne : c->comp.ns);
+    *n = cnt;
+    cudaError_t e;
+    if ((e = c->elem.ensure(total)) || (e = c->epos.ensure(total)) ||
+        (e = c->drings.ensure(rings.size())))
+        return c->cuda_fail(e, "component elements");
+    if (!rings.empty())
+        cudaMemcpyAsync(c->drings.p, rings.data(), rings.size() * sizeof(DiscRing),
+                        cudaMemcpyHostToDevice, c->stream);
+    c->comp.rings = c->drings.p;
+    cudaMemsetAsync(c->status.p, 0, sizeof(DevStatus), c->stream);
+    launch_components(c->comp, c->elem.p, c->epos.p, c->status.p, c->stream);
+    if ((rc = finish_status(c))) return rc;
+    if (cnt > cap || !posn || cnt == 0) return LCG_OK;
+    std::vector<ElemRec> el((size_t)cnt);
+    std::vector<double4> pos((size_t)cnt);
+    if ((e = cudaMemcpy(el.data(), c->elem.p + lo, cnt * sizeof(ElemRec), cudaMemcpyDeviceToHost)) ||
+        (e = cudaMemcpy(pos.data(), c->epos.p + lo, cnt * sizeof(double4), cudaMemcpyDeviceToHost)))
+        return c->cuda_fail(e, "component copy");
+    for (int32_t i = 0; i < cnt; i++) {
+        posn[3 * i] = pos[i].x; posn[3 * i + 1] = pos[i].y; posn[3 * i + 2] = pos[i].z;
+        dirn[3 * i] = el[i].dx; dirn[3 * i + 1] = el[i].dy; dirn[3 * i + 2] = el[i].dz;
+        area[i] = (float)pos[i].w;
+        flux[i] = el[i].flux;
+        nr[i] = el[i].nr;
+        for (int k = 0; k < kMaxRanges; k++) {
+            rin[kMaxRanges * i + k] = el[i].r[k].x;
+            rout[kMaxRanges * i + k] = el[i].r[k].y;
+        }
+    }
     return LCG_OK;
 }
 

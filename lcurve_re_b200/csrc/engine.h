@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include "roche.cuh"
+#include "disc.cuh"
 
 namespace lcg {
 
@@ -31,7 +32,13 @@ struct GridDev {
     uint8_t *necl;
     double *ein, *eout;
     int64_t n, ntiled;
+    // ranges an opaque disc adds to each face (light_curve_comp.cpp:288-323):
+    // ndx[i] of them in xr[kDiscRanges i ...]; NULL when there is no opaque disc
+    const uint8_t *ndx;
+    const double2 *xr;
 };
+constexpr int kDiscRanges = 2;   // disc_eclipse gives at most two ranges
+constexpr int kRagRanges = 1 + kDiscRanges;  // the companion's, then the disc's
 
 struct GridParams {
     int32_t star, roche, npole, nrings;
@@ -89,6 +96,13 @@ struct FlatDev {
     // of the run (C includes a margin over FP32 rounding), so a warp can skip
     // a run that faces away at all its phases
     float4 *runb;
+    // faces with two or more eclipse ranges (opaque discs) sit last, in
+    // [*n1, n): their records above are zero (they add nothing to the main
+    // sweeps); ridx is each one's face index in the grid, rr its rn ranges
+    int64_t *n1;
+    int32_t *ridx;
+    double2 *rr;  // kRagRanges per ragged face
+    uint8_t *rn;
 };
 
 // Face records of the fast mixed sweep (no beaming, no lensing, mucrit <= 0):
@@ -125,6 +139,14 @@ struct FluxConsts {
 struct ScatterParams {
     int32_t copy1, copy2;
     double third;
+    // disc / rim / spot: per-entry element sums (3 rows of ldc), added per
+    // point as slfac * (disc + rim + spot) (light_curve_comp.cpp:476-490)
+    const double *csum;
+    int64_t ldc;
+    PhaseParams pp;  // to recompute each point's slfac
+    // iscale: write the per-point components [star 1, disc, rim, spot,
+    // star 2] to fcomp (5 per point) instead of the light curve
+    double *fcomp;
 };
 
 // The four sweeps' chunk partials (1f, 1c, 2f, 2c; NULL when a sweep did not
@@ -277,6 +299,65 @@ void launch_batch_flux(const BatchDev &b, const BatchPhases &ph, const FluxPlan 
 void launch_fma_probe(float *sink, int blocks, int iters, double *gflop, cudaStream_t s);
 void launch_flux64(int star, const FluxConsts &k, const FlatDev &f, const PhaseDev &ph,
                    const FluxPlan &plan, double *part, int64_t ldp, DevStatus *st,
+                   cudaStream_t s);
+// Faces with several eclipse ranges, [*f.n1, f.n): each CTA row continues the
+// partial sums of one face block of blk faces (1024 for the FP64 sweep: the
+// reference's block order; plan.chunk for the mixed sweeps), in face order,
+// after the main sweep has written them.
+void launch_flux_ragged(int star, const FluxConsts &k, const FlatDev &f, const GridDev &g,
+                        const PhaseDev &ph, int64_t blk, int64_t nblk, double *part,
+                        int64_t ldp, cudaStream_t s);
+
+// ---- accretion disc, disc rim and bright spot (components.cu) ----------------
+// One component element: outward normal, flux (brightness x area, rounded to
+// float as the reference's Point::flux) and up to kMaxRanges eclipse ranges in
+// the order the reference pushes them (opaque disc, star 1, star 2).
+constexpr int kMaxRanges = 4;
+struct ElemRec {
+    double dx, dy, dz;
+    float flux;
+    int32_t nr;
+    double2 r[kMaxRanges];
+};
+// One ring of disc elements (set_disc_grid.cpp:79-96)
+struct DiscRing {
+    double rad, h, sinp, cosp, area;
+    int32_t ntheta, off;
+};
+// Everything the element kernel needs, derived on the host per model. The
+// elements are the disc [0, nd), its outer rim [nd, nd + ne) and the spot
+// [nd + ne, nd + ne + ns), each in the reference's vector order.
+struct CompParams {
+    int32_t nd, ne, ns, nrad;
+    const DiscRing *rings;
+    double bright_disc, rdisc2, texp;                    // set_disc_continuum
+    double rad_e, h_e, area_e;                           // set_disc_edge (outer)
+    int32_t nout, ntheta_e;
+    double tedge, t2, absorb_edge, wave;                 // set_edge_continuum
+    double bspot[3], bvec[3], tvec[3];                   // set_bright_spot_grid
+    double bmax, sfac, area_s, bright_s, expon, epow, cfrac, length;
+    int32_t nspot;
+    int32_t opaque, eclipse1, eclipse2, roche1, roche2;  // star_eclipse
+    double q, spin1, spin2, cosi, sini, delta, r1, r2, rref1, pref1, rref2, pref2;
+    DiscGeom dg;
+};
+// Elements into el (and (x, y, z, area) into pos); errors into *st.
+void launch_components(const CompParams &p, ElemRec *el, double4 *pos, DevStatus *st,
+                       cudaStream_t s);
+// The ranges an opaque disc adds to each face of a star grid.
+void launch_disc_faces(const DiscGeom &dg, const GridDev &g, uint8_t *ndx, double2 *xr,
+                       DevStatus *st, cudaStream_t s);
+// Per phase entry, the disc, rim and spot element sums (comp_light.cpp:323-408)
+// into rows 0, 1, 2 of out (row stride ldc).
+void launch_comp_sums(const ElemRec *el, int32_t nd, int32_t ne, int32_t n, double lin,
+                      double quad, const PhaseDev &ph, double *out, int64_t ldc,
+                      cudaStream_t s);
+// iscale: per-component scale factors by least squares (svdfit.cpp:22-80) from
+// fcomp (5 per point; nc = 5 with star 2's column, else 4), or the given sfac
+// when scaling is off; then calc and, when scaled or rdata, chi**2 / wnok into
+// out[0..1] with out[2] = 1. work holds 6 n doubles.
+void launch_iscale(int32_t flags, int32_t nc, const DatumRec *data, int32_t n,
+                   const double *fcomp, double *work, double *calc, double *sfac, double *out,
                    cudaStream_t s);
 
 }  // namespace lcg

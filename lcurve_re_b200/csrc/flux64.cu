@@ -163,6 +163,66 @@ __global__ void __launch_bounds__(kThreads64)
     }
 }
 
+// Several-range faces (the ragged segment of comp_light_flat.cpp:306-316):
+// one thread per (face block, phase entry) continues the block's partial sum
+// over the block's ragged faces in face order, each range tested in order.
+// Element values come from the grid in Point order (the FlatGrid holds the
+// same doubles).
+template <int LT, bool BEAM, bool GLENS, int STAR>
+__global__ void __launch_bounds__(kThreads64)
+    k_flux_ragged(FluxConsts k, FlatDev f, GridDev g, PhaseDev ph, int64_t blk, double *part,
+                  int64_t ldp) {
+    const int64_t b = blockIdx.y;
+    const int64_t n = f.n, n1 = f.n1[0];
+    const int64_t lo = b * blk, hi = (lo + blk < n) ? lo + blk : n;
+    const int64_t c0 = lo > n1 ? lo : n1;
+    const int64_t e = blockIdx.x * (int64_t)kThreads64 + threadIdx.x;
+    if (c0 >= hi || e >= ph.nent) return;
+    const Consts64 L{k.c[0], k.c[1], k.c[2], k.c[3], k.base, k.mucrit,
+                     k.beam, k.spin, k.vfac, k.xcofm, k.rlens1};
+    const double ex = ph.ex[e], ey = ph.ey[e], ez = ph.ez[e], pn = ph.phin[e];
+    double acc = part[b * ldp + e];
+    for (int64_t i = c0; i < hi; i++) {
+        const int64_t r = i - n1;
+        const int32_t fi = f.ridx[r];
+        const int nr = f.rn[r];
+        bool ecl = false;
+        for (int q = 0; q < nr; q++) {
+            const double2 R = f.rr[kRagRanges * r + q];
+            if ((pn >= R.x && pn <= R.y) || pn <= R.y - 1.0) { ecl = true; break; }
+        }
+        if (!ecl)
+            acc += elem<LT, BEAM, GLENS, STAR>(ex, ey, ez, g.nx[fi], g.ny[fi], g.nz[fi], g.px[fi],
+                                               g.py[fi], g.pz[fi], (double)g.flux[fi], L);
+    }
+    part[b * ldp + e] = acc;
+}
+
+template <int LT, bool BEAM, bool GLENS, int STAR>
+void launch_rag_t(const FluxConsts &k, const FlatDev &f, const GridDev &g, const PhaseDev &ph,
+                  int64_t blk, int64_t nblk, double *part, int64_t ldp, cudaStream_t s) {
+    dim3 grid((unsigned)((ph.nent + kThreads64 - 1) / kThreads64), (unsigned)nblk);
+    k_flux_ragged<LT, BEAM, GLENS, STAR><<<grid, kThreads64, 0, s>>>(k, f, g, ph, blk, part, ldp);
+    count_launch();
+}
+
+template <int LT>
+void launch_rag_lt(int star, const FluxConsts &k, const FlatDev &f, const GridDev &g,
+                   const PhaseDev &ph, int64_t blk, int64_t nblk, double *part, int64_t ldp,
+                   cudaStream_t s) {
+    const bool beam = k.beam_on != 0, glens = (star == 1) && k.glens;
+    if (star == 0) {
+        if (beam) launch_rag_t<LT, true, false, 0>(k, f, g, ph, blk, nblk, part, ldp, s);
+        else launch_rag_t<LT, false, false, 0>(k, f, g, ph, blk, nblk, part, ldp, s);
+    } else if (glens) {
+        if (beam) launch_rag_t<LT, true, true, 1>(k, f, g, ph, blk, nblk, part, ldp, s);
+        else launch_rag_t<LT, false, true, 1>(k, f, g, ph, blk, nblk, part, ldp, s);
+    } else {
+        if (beam) launch_rag_t<LT, true, false, 1>(k, f, g, ph, blk, nblk, part, ldp, s);
+        else launch_rag_t<LT, false, false, 1>(k, f, g, ph, blk, nblk, part, ldp, s);
+    }
+}
+
 template <int PPT, int LT, bool BEAM, bool GLENS, int STAR>
 void launch_t(const FluxConsts &k, const FlatDev &f, const PhaseDev &ph, const FluxPlan &plan,
               double *part, int64_t ldp, DevStatus *st, cudaStream_t s) {
@@ -199,6 +259,14 @@ void launch_ppt(int star, const FluxConsts &k, const FlatDev &f, const PhaseDev 
 }
 
 }  // namespace
+
+void launch_flux_ragged(int star, const FluxConsts &k, const FlatDev &f, const GridDev &g,
+                        const PhaseDev &ph, int64_t blk, int64_t nblk, double *part,
+                        int64_t ldp, cudaStream_t s) {
+    if (ph.nent <= 0 || nblk <= 0 || !f.n1) return;
+    if (k.ltype == 1) launch_rag_lt<1>(star, k, f, g, ph, blk, nblk, part, ldp, s);
+    else launch_rag_lt<0>(star, k, f, g, ph, blk, nblk, part, ldp, s);
+}
 
 void launch_flux64(int star, const FluxConsts &k, const FlatDev &f, const PhaseDev &ph,
                    const FluxPlan &plan, double *part, int64_t ldp, DevStatus *st,

@@ -296,11 +296,25 @@ __global__ void k_continuum(ContParams p, GridDev g) {
 
 constexpr int kFlatBlock = 1024;
 
+// Eclipse class of face i for the FlatGrid partition (comp_light_flat.cpp:26-65):
+// 0 never eclipsed, 1 one range, 2 several (an opaque disc's ranges added to
+// the companion's).
+__device__ __forceinline__ int flat_class(const GridDev &g, int64_t i) {
+    const int k = g.necl[i] + (g.ndx ? g.ndx[i] : 0);
+    return k < 2 ? k : 2;
+}
+
+// Per 1024-face block: the one-range count in blockcnt[b], the several-range
+// count in blockcnt[nb + b].
 __global__ void k_flat_count(GridDev g, int32_t *blockcnt) {
     const int64_t i = blockIdx.x * (int64_t)kFlatBlock + threadIdx.x;
-    const int flag = (i < g.n) && g.necl[i] == 1;
-    const int c = __syncthreads_count(flag);
-    if (threadIdx.x == 0) blockcnt[blockIdx.x] = c;
+    const int cls = i < g.n ? flat_class(g, i) : 0;
+    const int c1 = __syncthreads_count(cls == 1);
+    const int c2 = g.ndx ? __syncthreads_count(cls == 2) : 0;
+    if (threadIdx.x == 0) {
+        blockcnt[blockIdx.x] = c1;
+        blockcnt[gridDim.x + blockIdx.x] = c2;
+    }
 }
 
 // Single block: exclusive scan of the per-block eclipse counts; n0 = faces
@@ -331,8 +345,17 @@ __device__ __forceinline__ void scan_blocks(int32_t *blockcnt, int32_t nb, int64
     __syncthreads();
 }
 
+// Both counts scanned: n0 = faces never eclipsed, n1 = n0 + one-range faces
+// (n0[0] and n0[1]).
 __global__ void k_flat_scan(int32_t *blockcnt, int32_t nb, int64_t n, int64_t *n0) {
-    scan_blocks(blockcnt, nb, n, n0);
+    __shared__ int64_t c2;
+    int64_t t2 = 0;
+    scan_blocks(blockcnt + nb, nb, n, n0);  // n0[0] = n - (several-range faces)
+    if (threadIdx.x == 0) c2 = n - n0[0];
+    __syncthreads();
+    t2 = c2;
+    scan_blocks(blockcnt, nb, n - t2, n0);  // n0[0] = n - several - one-range
+    if (threadIdx.x == 0) n0[1] = n - t2;
 }
 
 __device__ __forceinline__ uint32_t phase_fx(double ph) {
@@ -363,38 +386,78 @@ __device__ __forceinline__ void fast_record(float *fp, int64_t dest, GridDev g, 
     r[14] = (float)(fl * fc.p[4]);
 }
 
+// Stable three-way partition [never | one range | several]. Several-range
+// faces get all-zero records (they add exact zeros to the main sweeps) and
+// their face index and ranges in FlatGrid order; k_flux_ragged adds them.
 __global__ void k_flat_scatter(GridDev g, FlatDev f, const int32_t *__restrict__ blockoff,
                                int mixed, int need_pos, FastCoef fc) {
-    __shared__ int32_t warp_tot[32];
+    __shared__ int32_t warp_tot[2][32];
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
     const int64_t i = blockIdx.x * (int64_t)kFlatBlock + t;
     const bool in = i < g.n;
-    const int flag = in && g.necl[i] == 1;
-    const unsigned m = __ballot_sync(0xffffffffu, flag);
-    if (lane == 0) warp_tot[w] = __popc(m);
+    const int cls = in ? flat_class(g, i) : 0;
+    const unsigned m1 = __ballot_sync(0xffffffffu, cls == 1);
+    const unsigned m2 = __ballot_sync(0xffffffffu, cls == 2);
+    if (lane == 0) {
+        warp_tot[0][w] = __popc(m1);
+        warp_tot[1][w] = __popc(m2);
+    }
     __syncthreads();
-    int before = 0;
-    for (int k = 0; k < w; k++) before += warp_tot[k];
-    const int rank = before + __popc(m & ((1u << lane) - 1u));
+    int b1 = 0, b2 = 0;
+    for (int k = 0; k < w; k++) {
+        b1 += warp_tot[0][k];
+        b2 += warp_tot[1][k];
+    }
+    const unsigned below = (1u << lane) - 1u;
+    const int rank1 = b1 + __popc(m1 & below), rank2 = b2 + __popc(m2 & below);
     if (!in) return;
-    const int64_t n0 = *f.n0;
-    const int64_t boff = blockoff[blockIdx.x];
-    const int64_t dest = flag ? n0 + boff + rank
-                              : blockIdx.x * (int64_t)kFlatBlock - boff + (t - rank);
+    const int64_t n0 = f.n0[0], n1 = f.n0[1];
+    const int64_t boff1 = blockoff[blockIdx.x], boff2 = blockoff[gridDim.x + blockIdx.x];
+    const int64_t dest = cls == 1   ? n0 + boff1 + rank1
+                         : cls == 2 ? n1 + boff2 + rank2
+                                    : blockIdx.x * (int64_t)kFlatBlock - boff1 - boff2 +
+                                          (t - rank1 - rank2);
+    // a one-range face's range: the companion's, else the disc's first
+    double ein = 0., eout = 0.;
+    if (cls == 1) {
+        if (g.necl[i]) { ein = g.ein[i]; eout = g.eout[i]; }
+        else { ein = g.xr[kDiscRanges * i].x; eout = g.xr[kDiscRanges * i].y; }
+    }
+    const bool live = cls < 2;
     if (mixed) {
         if (fc.on) {
-            fast_record(f.fp, dest, g, i, fc);
+            if (live) {
+                fast_record(f.fp, dest, g, i, fc);
+            } else {
+                float *r = f.fp + 16 * (dest >> 1) + (dest & 1);
+                for (int q = 0; q < 16; q += 2) r[q] = 0.f;
+            }
         } else {
-            f.geo[dest] = make_float4((float)g.nx[i], (float)g.ny[i], (float)g.nz[i], g.flux[i]);
+            f.geo[dest] = live ? make_float4((float)g.nx[i], (float)g.ny[i], (float)g.nz[i],
+                                             g.flux[i])
+                               : make_float4(0.f, 0.f, 0.f, 0.f);
         }
-        f.ecl[dest] = flag ? ecl_fx(g.ein[i], g.eout[i]) : make_uint2(0u, 0u);
-        if (need_pos) f.pos[dest] = make_float4((float)g.px[i], (float)g.py[i], (float)g.pz[i], 0.f);
+        f.ecl[dest] = cls == 1 ? ecl_fx(ein, eout) : make_uint2(0u, 0u);
+        if (need_pos)
+            f.pos[dest] = live ? make_float4((float)g.px[i], (float)g.py[i], (float)g.pz[i], 0.f)
+                               : make_float4(0.f, 0.f, 0.f, 0.f);
     } else {
-        f.dx[dest] = g.nx[i]; f.dy[dest] = g.ny[i]; f.dz[dest] = g.nz[i];
-        f.px[dest] = g.px[i]; f.py[dest] = g.py[i]; f.pz[dest] = g.pz[i];
-        f.flux[dest] = (double)g.flux[i];
-        f.in1[dest] = flag ? g.ein[i] : 0.;
-        f.out1[dest] = flag ? g.eout[i] : 0.;
+        const double z = 0.;
+        f.dx[dest] = live ? g.nx[i] : z; f.dy[dest] = live ? g.ny[i] : z;
+        f.dz[dest] = live ? g.nz[i] : z;
+        f.px[dest] = live ? g.px[i] : z; f.py[dest] = live ? g.py[i] : z;
+        f.pz[dest] = live ? g.pz[i] : z;
+        f.flux[dest] = live ? (double)g.flux[i] : z;
+        f.in1[dest] = ein;
+        f.out1[dest] = eout;
+    }
+    if (cls == 2) {
+        const int64_t r = dest - n1;
+        int q = 0;
+        if (g.necl[i]) f.rr[kRagRanges * r + q++] = make_double2(g.ein[i], g.eout[i]);
+        for (int k = 0; k < g.ndx[i]; k++) f.rr[kRagRanges * r + q++] = g.xr[kDiscRanges * i + k];
+        f.rn[r] = (uint8_t)q;
+        f.ridx[r] = (int32_t)i;
     }
 }
 
@@ -490,11 +553,47 @@ __global__ void k_scatter(ScatterParams p, const double *__restrict__ o1f,
     if (!p.copy1)
         for (int64_t e = e0; e < e1; e++)
             if (ph.type[e] != 1) c += ph.w1[e] * o1c[e];
+    double c2 = 0.;
+    double *acc = p.fcomp ? &c2 : &c;  // iscale keeps the stars apart
     for (int64_t e = e0; e < e1; e++)
-        if (p.copy2 || ph.type[e] == 3) c += ph.w2[e] * o2f[e];
+        if (p.copy2 || ph.type[e] == 3) *acc += ph.w2[e] * o2f[e];
     if (!p.copy2)
         for (int64_t e = e0; e < e1; e++)
-            if (ph.type[e] != 3) c += ph.w2[e] * o2c[e];
+            if (ph.type[e] != 3) *acc += ph.w2[e] * o2c[e];
+    if (p.csum || p.fcomp) {
+        // comp_disc / comp_edge / comp_spot of the point: sub-exposure sums
+        // weighted and merged in order, over max(1, ndiv - 1)
+        // (comp_light.cpp:323-408, light_curve_comp.cpp:476-490, 378-414)
+        const DatumRec d = data[np];
+        double phase, slfac;
+        point_phase(p.pp, d, phase, slfac);
+        const int ndiv = d.ndiv;
+        double cd = 0.0, ce = 0.0, cs = 0.0;
+        if (p.csum) {
+            for (int nd = 0; nd < ndiv; nd++) {
+                const int64_t e = e0 + nd;
+                const double wgt = ndiv == 1 ? 1.0 : ((nd == 0 || nd == ndiv - 1) ? 0.5 : 1.0);
+                cd += wgt * p.csum[e];
+                ce += wgt * p.csum[p.ldc + e];
+                cs += wgt * p.csum[2 * p.ldc + e];
+            }
+            const int norm = (ndiv - 1 > 1) ? ndiv - 1 : 1;
+            cd /= norm;
+            ce /= norm;
+            cs /= norm;
+        }
+        if (p.fcomp) {
+            double *f = p.fcomp + 5 * (int64_t)np;
+            f[0] = c;
+            f[1] = slfac * cd;
+            f[2] = slfac * ce;
+            f[3] = slfac * cs;
+            f[4] = c2;
+            calc[np] = 0.;
+            return;
+        }
+        c += slfac * (cd + ce + cs);
+    }
     calc[np] = c + p.third;
 }
 
@@ -1056,7 +1155,7 @@ void launch_flatten(GridDev g, FlatDev f, int32_t *blockcnt, int mixed, int need
     (void)st;
     const unsigned nb = nblocks(g.n, kFlatBlock);
     if (nb == 0) {
-        cudaMemsetAsync(f.n0, 0, sizeof(int64_t), s);
+        cudaMemsetAsync(f.n0, 0, 2 * sizeof(int64_t), s);
         return;
     }
     if (mixed && fc.on && f.npad > g.n) {

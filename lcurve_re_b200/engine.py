@@ -209,6 +209,26 @@ class Engine:
             _dptr(g["ecl_out"])))
         return g
 
+    def components(self, model, which):
+        """One component grid with its continuum (0 the disc, 1 its outer rim,
+        2 the bright spot; set_disc_grid / set_disc_edge / set_bright_spot_grid):
+        a dict of numpy arrays, rin / rout holding 4 ranges per element."""
+        m = _as_model(model)
+        n = C.c_int32(0)
+        I = C.POINTER(C.c_int32)
+        self._check(self.lib.lcg_components(self.ctx, C.byref(m), which, 0, C.byref(n), None, None,
+                                            None, None, None, None, None))
+        k = n.value
+        g = {"posn": np.zeros((k, 3)), "dirn": np.zeros((k, 3)), "area": np.zeros(k, np.float32),
+             "flux": np.zeros(k, np.float32), "nr": np.zeros(k, np.int32),
+             "rin": np.zeros((k, 4)), "rout": np.zeros((k, 4))}
+        fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+        self._check(self.lib.lcg_components(
+            self.ctx, C.byref(m), which, k, C.byref(n), _dptr(g["posn"]), _dptr(g["dirn"]),
+            fp(g["area"]), fp(g["flux"]), g["nr"].ctypes.data_as(I), _dptr(g["rin"]),
+            _dptr(g["rout"])))
+        return g
+
     def sum_star_multi(self, star, flat, phases, ldc, ltype, mucrit=0.0, beam=0.0, spin=1.0,
                        vfac=0.0, xcofm=0.0, glens1=False, rlens1=0.0):
         """flat_sum_star{1,2}_multi over a FlatGrid dict (dx,dy,dz,px,py,pz,flux,

@@ -101,6 +101,10 @@ VARY_ORDER = ["q", "iangle", "r1", "r2", "spin1", "spin2", "t1", "t2",
               "velocity_scale", "beam_factor1", "beam_factor2", "t0", "period", "pdot",
               "deltat", "gravity_dark1", "gravity_dark2", "absorb", "slope", "quad", "cube",
               "third"]
+DISC_VARY = ["rdisc1", "rdisc2", "height_disc", "beta_disc", "temp_disc", "texp_disc",
+             "lin_limb_disc", "quad_limb_disc", "temp_edge", "absorb_edge"]
+SPOT_VARY = ["radius_spot", "length_spot", "height_spot", "expon_spot", "epow_spot",
+             "angle_spot", "yaw_spot", "temp_spot", "tilt_spot", "cfrac_spot"]
 
 
 class Model:
@@ -172,12 +176,21 @@ class Model:
         return copy.deepcopy(self)
 
     def vary_names(self):
-        """Names of the varying star parameters in set_param order."""
+        """Names of the varying parameters in set_param order (the star
+        part, the disc and bright-spot parameters when those components are
+        on, then defined star-spot parameters, model.cpp:383-457)."""
         out = []
         for n in VARY_ORDER:
             if n in ("r1", "r2") and not self.c["use_radii"]:
                 n = "cphi3" if n == "r1" else "cphi4"
             if self.p[n].vary:
+                out.append(n)
+        if self.c["add_disc"]:
+            out += [n for n in DISC_VARY if self.p[n].vary]
+        if self.c["add_spot"]:
+            out += [n for n in SPOT_VARY if self.p[n].vary]
+        for n in sum(SPOT_GROUPS, []) + UESP:
+            if self.p[n].defined and self.p[n].vary:
                 out.append(n)
         return out
 
@@ -215,6 +228,9 @@ class Model:
                   "iscale"):
             setattr(m, n, int(self.c[n]))
         m.limb1, m.limb2 = self.c["limb1"], self.c["limb2"]
+        for n in abi.DISC_SPOT:
+            setattr(m, n, self.p[n].value)
+        m.nrad, m.nspot = self.c["nrad"], self.c["nspot"]
         return m
 
     def geometry_key(self):

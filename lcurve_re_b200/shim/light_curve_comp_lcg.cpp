@@ -75,6 +75,15 @@ lcg_model to_lcg(const Lcurve::Model &m) {
     c.limb2 = m.limb2 == Lcurve::LDC::CLARET ? LCG_LIMB_CLARET : LCG_LIMB_POLY;
     c.mirror = m.mirror; c.add_disc = m.add_disc; c.opaque = m.opaque;
     c.add_spot = m.add_spot; c.iscale = m.iscale;
+    c.rdisc1 = m.rdisc1; c.rdisc2 = m.rdisc2; c.height_disc = m.height_disc;
+    c.beta_disc = m.beta_disc; c.temp_disc = m.temp_disc; c.texp_disc = m.texp_disc;
+    c.lin_limb_disc = m.lin_limb_disc; c.quad_limb_disc = m.quad_limb_disc;
+    c.temp_edge = m.temp_edge; c.absorb_edge = m.absorb_edge;
+    c.radius_spot = m.radius_spot; c.length_spot = m.length_spot;
+    c.height_spot = m.height_spot; c.expon_spot = m.expon_spot; c.epow_spot = m.epow_spot;
+    c.angle_spot = m.angle_spot; c.yaw_spot = m.yaw_spot; c.temp_spot = m.temp_spot;
+    c.tilt_spot = m.tilt_spot; c.cfrac_spot = m.cfrac_spot;
+    c.nrad = m.nrad; c.nspot = m.nspot;
     return c;
 }
 

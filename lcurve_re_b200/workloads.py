@@ -10,6 +10,8 @@ Gaussian noise drawn from a seeded numpy Generator.
   mcmc_batch     256 models around wd_dm_small, nlat2f in 60..400, 2000 points
   tiny_star      r1 in {0.002, 0.005, 0.01}, nlat 400/200, 10000 points near eclipse
   surrogate_box  the prior box of the surrogate training set
+  cv_disc        cataclysmic variable: white dwarf, Roche-filling donor, flared
+                 accretion disc with its rim, and the bright spot
 """
 import numpy as np
 
@@ -60,7 +62,8 @@ def model(**over):
         if k in ("nlat1f", "nlat2f", "nlat1c", "nlat2c", "nlatfill", "nlngfill", "npole",
                  "roche1", "roche2", "eclipse1", "eclipse2", "glens1", "use_radii", "mirror",
                  "gdark_bolom1", "gdark_bolom2", "delta_phase", "phase1", "phase2", "wavelength",
-                 "tperiod", "mucrit1", "mucrit2", "llo", "lhi", "lfudge"):
+                 "tperiod", "mucrit1", "mucrit2", "llo", "lhi", "lfudge", "add_disc", "opaque",
+                 "add_spot", "iscale", "nrad", "nspot"):
             p[k] = str(v)
         elif k in ("limb1", "limb2"):
             p[k] = v
@@ -118,6 +121,26 @@ def mcmc_batch(nmodels=256, seed=2024):
                          t2=3200.0 * (1 + 0.03 * rng.standard_normal()),
                          nlat1f=nl2 // 2, nlat2f=nl2))
     return out, data(2000)
+
+
+CV_DISC = dict(q=0.15, iangle=84.0, r1=0.012, r2=0.25, t1=15000.0, t2=3000.0,
+               add_disc=1, rdisc1=0.03, rdisc2=0.3, height_disc=0.02, beta_disc=1.3,
+               temp_disc=8000.0, texp_disc=-0.8, lin_limb_disc=0.3, quad_limb_disc=0.1,
+               temp_edge=6000.0, absorb_edge=0.5, nrad=40, opaque=1,
+               add_spot=1, radius_spot=0.3, length_spot=0.02, height_spot=0.01,
+               expon_spot=2.0, epow_spot=1.0, angle_spot=140.0, yaw_spot=10.0,
+               temp_spot=12000.0, tilt_spot=60.0, cfrac_spot=0.2, nspot=50)
+
+
+def cv_disc(**over):
+    """A cataclysmic variable: q=0.15, i=84 deg, white dwarf r1=0.012,
+    donor r2=0.25, flared opaque disc from 0.03 to 0.3 (height 0.02 r^1.3,
+    T 8000 K r^-0.8, 40 radii) with its outer rim, and a 50-element bright
+    spot where the stream meets r=0.3. Keyword arguments override any of
+    these or the detached binary's parameters."""
+    kw = dict(CV_DISC)
+    kw.update(over)
+    return model(**kw)
 
 
 def elements(nface1, nface2, nent):

@@ -1437,15 +1437,17 @@ static inline int ecl_range(double phin, double in, double out) {
     return (phin >= in && phin <= out) || phin <= out - 1.0;
 }
 
-int lco_sum_star_multi(int star, int64_t n, int64_t n0, const double *dx,
+/* The blocked sweep over [never | one range | ragged] faces: faces [n1, n)
+ * have ranges moff[i - n1] .. moff[i - n1 + 1] of rmin / rmout. */
+static int sum_multi_r(int star, int64_t n, int64_t n0, int64_t n1, const double *dx,
                        const double *dy, const double *dz, const double *px,
                        const double *py, const double *pz, const double *flux,
-                       const double *in1, const double *out1, int32_t nent,
+                       const double *in1, const double *out1, const int64_t *moff,
+                       const double *rmin, const double *rmout, int32_t nent,
                        const double *ex, const double *ey, const double *ez,
                        const double *phin, const double *ldc, int32_t ltype,
                        double mucrit, double beam, double spin, double vfac,
-                       double xcofm, int32_t glens1, double rlens1,
-                       double *out) {
+                       double xcofm, int32_t glens1, double rlens1, double *out) {
     sweep g;
     g.dx = dx; g.dy = dy; g.dz = dz; g.px = px; g.py = py; g.pz = pz; g.flux = flux;
     g.ltype = ltype; g.star = star; g.glens = (star == LCG_STAR2) && glens1;
@@ -1467,15 +1469,25 @@ int lco_sum_star_multi(int star, int64_t n, int64_t n0, const double *dx,
         const int64_t hi = (n < lo + FACE_BLOCK) ? n : lo + FACE_BLOCK;
         const int64_t a1 = hi < n0 ? hi : n0;
         const int64_t b0 = lo > n0 ? lo : n0;
+        const int64_t b1 = hi < n1 ? hi : n1;
+        const int64_t c0 = lo > n1 ? lo : n1;
         for (int k = 0; k < nent; k++) brow[k] = 0.0;
         for (int64_t i = lo; i < a1; i++)
             for (int k = 0; k < nent; k++)
                 brow[k] += elem(&g, i, ex[k], ey[k], ez[k]);
-        for (int64_t i = b0; i < hi; i++) {
+        for (int64_t i = b0; i < b1; i++) {
             const double ein = in1[i - n0], eout = out1[i - n0];
             for (int k = 0; k < nent; k++) {
                 double v = elem(&g, i, ex[k], ey[k], ez[k]);
                 brow[k] += ecl_range(phin[k], ein, eout) ? 0.0 : v;
+            }
+        }
+        for (int64_t i = c0; i < hi; i++) {
+            for (int k = 0; k < nent; k++) {
+                int ecl = 0;
+                for (int64_t j = moff[i - n1]; j < moff[i - n1 + 1]; j++)
+                    if (ecl_range(phin[k], rmin[j], rmout[j])) { ecl = 1; break; }
+                if (!ecl) brow[k] += elem(&g, i, ex[k], ey[k], ez[k]);
             }
         }
     }
@@ -1485,6 +1497,21 @@ int lco_sum_star_multi(int star, int64_t n, int64_t n0, const double *dx,
     }
     free(blk);
     return LCG_OK;
+}
+
+int lco_sum_star_multi(int star, int64_t n, int64_t n0, const double *dx,
+                       const double *dy, const double *dz, const double *px,
+                       const double *py, const double *pz, const double *flux,
+                       const double *in1, const double *out1, int32_t nent,
+                       const double *ex, const double *ey, const double *ez,
+                       const double *phin, const double *ldc, int32_t ltype,
+                       double mucrit, double beam, double spin, double vfac,
+                       double xcofm, int32_t glens1, double rlens1,
+                       double *out) {
+    const int64_t moff0 = 0;
+    return sum_multi_r(star, n, n0, n, dx, dy, dz, px, py, pz, flux, in1, out1, &moff0, NULL,
+                       NULL, nent, ex, ey, ez, phin, ldc, ltype, mucrit, beam, spin, vfac,
+                       xcofm, glens1, rlens1, out);
 }
 
 /* ---- Ginterp (lcurve.h:92-148) ------------------------------------------ */
@@ -1522,16 +1549,23 @@ typedef struct {
     double *posn, *dirn, *ein, *eout;
     float *area, *gravity, *flux;
     int32_t *necl;
+    /* ranges appended by an opaque disc (light_curve_comp.cpp:288-323) */
+    int32_t *ndx;
+    double *xin, *xout;  /* LCO_DISC_R per face */
     /* FlatGrid */
     double *dx, *dy, *dz, *px, *py, *pz, *ff, *in1, *out1;
     int64_t n0, n1;
+    int64_t *moff;       /* ragged faces [n1, n): ranges moff[k] .. moff[k + 1] */
+    double *rmin, *rmout;
 } sgrid;
+#define LCO_DISC_R 2
 
 static void sgrid_free(sgrid *g) {
     free(g->posn); free(g->dirn); free(g->ein); free(g->eout);
     free(g->area); free(g->gravity); free(g->flux); free(g->necl);
     free(g->dx); free(g->dy); free(g->dz); free(g->px); free(g->py); free(g->pz);
     free(g->ff); free(g->in1); free(g->out1);
+    free(g->ndx); free(g->xin); free(g->xout); free(g->moff); free(g->rmin); free(g->rmout);
     memset(g, 0, sizeof(*g));
 }
 
@@ -1566,9 +1600,42 @@ static void sgrid_flatten(sgrid *g) {
     g->ff = (double *)malloc(N * sizeof(double));
     g->in1 = (double *)malloc(N * sizeof(double));
     g->out1 = (double *)malloc(N * sizeof(double));
-    lco_flatten(g->n, g->posn, g->dirn, g->flux, g->necl, g->ein, g->eout, g->dx,
-                g->dy, g->dz, g->px, g->py, g->pz, g->ff, g->in1, g->out1, &g->n0,
-                &g->n1);
+    g->moff = (int64_t *)calloc(N + 1, sizeof(int64_t));
+    g->rmin = (double *)malloc((1 + LCO_DISC_R) * N * sizeof(double));
+    g->rmout = (double *)malloc((1 + LCO_DISC_R) * N * sizeof(double));
+    /* FlatGrid::build (comp_light_flat.cpp:26-65): a face's ranges are its
+       Roche eclipse, if any, then the disc's */
+    int64_t c0 = 0, c1 = 0;
+    for (int j = 0; j < g->n; j++) {
+        int k = g->necl[j] + (g->ndx ? g->ndx[j] : 0);
+        c0 += (k == 0);
+        c1 += (k == 1);
+    }
+    g->n0 = c0;
+    g->n1 = c0 + c1;
+    int64_t i0 = 0, i1 = g->n0, i2 = g->n1, nr = 0;
+    g->moff[0] = 0;
+    for (int j = 0; j < g->n; j++) {
+        const int nd = g->ndx ? g->ndx[j] : 0, k = g->necl[j] + nd;
+        int64_t i = (k == 0) ? i0++ : (k == 1 ? i1++ : i2++);
+        g->dx[i] = g->dirn[3 * j]; g->dy[i] = g->dirn[3 * j + 1]; g->dz[i] = g->dirn[3 * j + 2];
+        g->px[i] = g->posn[3 * j]; g->py[i] = g->posn[3 * j + 1]; g->pz[i] = g->posn[3 * j + 2];
+        g->ff[i] = g->flux[j];
+        double rin[1 + LCO_DISC_R], rout[1 + LCO_DISC_R];
+        int q = 0;
+        if (g->necl[j]) { rin[q] = g->ein[j]; rout[q++] = g->eout[j]; }
+        for (int r = 0; r < nd; r++) {
+            rin[q] = g->xin[LCO_DISC_R * j + r];
+            rout[q++] = g->xout[LCO_DISC_R * j + r];
+        }
+        if (k == 1) {
+            g->in1[i - g->n0] = rin[0];
+            g->out1[i - g->n0] = rout[0];
+        } else if (k >= 2) {
+            for (int r = 0; r < q; r++) { g->rmin[nr] = rin[r]; g->rmout[nr++] = rout[r]; }
+            g->moff[i - g->n1 + 1] = nr;
+        }
+    }
 }
 
 /* LDC::imu (lcurve.h:216-231) */
@@ -1728,9 +1795,9 @@ int64_t lco_phase_batch(const lcg_model *m, const lcg_datum *data, int32_t n,
 static double sweep_flat(const lcg_model *m, int star, const sgrid *g,
                          const pbatch *pb, double *out, double spin, double vfac,
                          double xcofm, double rlens1) {
-    return (double)lco_sum_star_multi(
-        star, g->n, g->n0, g->dx, g->dy, g->dz, g->px, g->py, g->pz, g->ff, g->in1,
-        g->out1, (int32_t)pb->n, pb->ex, pb->ey, pb->ez, pb->phin,
+    return (double)sum_multi_r(
+        star, g->n, g->n0, g->n1, g->dx, g->dy, g->dz, g->px, g->py, g->pz, g->ff, g->in1,
+        g->out1, g->moff, g->rmin, g->rmout, (int32_t)pb->n, pb->ex, pb->ey, pb->ez, pb->phin,
         star == LCG_STAR1 ? m->ldc1 : m->ldc2, star == LCG_STAR1 ? m->limb1 : m->limb2,
         star == LCG_STAR1 ? m->mucrit1 : m->mucrit2,
         star == LCG_STAR1 ? m->beam_factor1 : m->beam_factor2, spin, vfac, xcofm,
@@ -1748,6 +1815,41 @@ static double flat_sum_one(const lcg_model *m, int star, const sgrid *g, v3 eart
     sweep_flat(m, star, g, &pb, &out, 1.0, vfac, xcofm, rlens1);
     pb_free(&pb);
     return out;
+}
+
+/* comp_star1_flat / comp_star2_flat (comp_light_flat.cpp:538-602): the
+ * sub-exposure sums of one star, Ginterp-scaled, spin 1 in the beaming. */
+static double comp_star_flat(const lcg_model *m, int star, double phase, double expose,
+                             int ndiv, const ginterp *gi, const sgrid *gf, const sgrid *gc,
+                             double vfac, double xcofm, double rlens1) {
+    const double ri = deg2rad(m->iangle);
+    const double cosi = cos(ri), sini = sin(ri);
+    double sum = 0.0;
+    for (int nd = 0; nd < ndiv; ++nd) {
+        double phi, wgt;
+        if (ndiv == 1) { phi = phase; wgt = 1.0; }
+        else {
+            phi = phase + expose * (nd - (ndiv - 1) / 2.0) / (ndiv - 1);
+            wgt = (nd == 0 || nd == ndiv - 1) ? 0.5 : 1.0;
+        }
+        v3 earth = set_earth(cosi, sini, phi);
+        double phin = phi - floor(phi);
+        const sgrid *g = star == LCG_STAR1 ? ((gi_type(gi, phi) == 1) ? gf : gc)
+                                           : ((gi_type(gi, phi) == 3) ? gf : gc);
+        sum += wgt * (star == LCG_STAR1 ? gi_scale1(gi, phi) : gi_scale2(gi, phi)) *
+               flat_sum_one(m, star, g, earth, phin, vfac, xcofm, rlens1);
+    }
+    return sum / ((ndiv - 1 > 1) ? ndiv - 1 : 1);
+}
+
+/* The iscale fit from the components (light_curve_comp.cpp:532-556). */
+static void iscale_calc(const lcg_model *m, int32_t n, const double *fcomp,
+                        const double *sfac, double *calc) {
+    for (int np = 0; np < n; np++) {
+        const double *f = fcomp + 5 * np;
+        calc[np] = sfac[0] * f[0] + sfac[1] * f[1] + sfac[2] * f[2] + sfac[3] * f[3];
+        if (m->t2 > 0.) calc[np] += sfac[4] * f[4];
+    }
 }
 
 /* comp_gravity1/2 (comp_gravity.cpp:20-155) and comp_radius1/2
@@ -1825,6 +1927,688 @@ static double comp_radius(int star, const sgrid *g) {
 }
 
 /* ---- the whole path (light_curve_comp.cpp:119-599) ---------------------- */
+/* ---- accretion disc, disc edge and bright spot --------------------------
+ * set_disc_grid.cpp:27-127 (disc), :144-264 (edge), set_bright_spot_grid.cpp
+ * :27-100 (spot), set_disc_continuum.cpp:19-88, disc_eclipse.cpp:38-366,
+ * star_eclipse.cpp:15-26. Elements are kept in the reference's vector order;
+ * each carries up to LCO_MAXR eclipse ranges in the order they were pushed. */
+#define LCO_MAXR 4
+
+typedef struct {
+    int n;
+    double *posn, *dirn;  /* 3 per element */
+    float *area, *flux;
+    int32_t *nr;          /* eclipse ranges per element */
+    double *rin, *rout;   /* LCO_MAXR per element */
+} elist;
+
+static void el_free(elist *d) {
+    free(d->posn); free(d->dirn); free(d->area); free(d->flux);
+    free(d->nr); free(d->rin); free(d->rout);
+    memset(d, 0, sizeof(*d));
+}
+
+static void el_alloc(elist *d, int n) {
+    memset(d, 0, sizeof(*d));
+    size_t N = (size_t)(n > 0 ? n : 1);
+    d->n = n;
+    d->posn = (double *)calloc(3 * N, sizeof(double));
+    d->dirn = (double *)calloc(3 * N, sizeof(double));
+    d->area = (float *)calloc(N, sizeof(float));
+    d->flux = (float *)calloc(N, sizeof(float));
+    d->nr = (int32_t *)calloc(N, sizeof(int32_t));
+    d->rin = (double *)calloc(LCO_MAXR * N, sizeof(double));
+    d->rout = (double *)calloc(LCO_MAXR * N, sizeof(double));
+}
+
+/* Appends one range to a list of at most LCO_MAXR. */
+static void push_range(int32_t *nr, double *rin, double *rout, double in, double out) {
+    if (*nr < LCO_MAXR) {
+        rin[*nr] = in;
+        rout[*nr] = out;
+    }
+    (*nr)++;
+}
+
+enum { CIRC_ABOVE, CIRC_INSIDE, CIRC_OUTSIDE, CIRC_SEPARATE, CIRC_CROSSING };
+
+/* cut_phase (disc_eclipse.cpp:349-366) */
+static double cut_phase(double rxy, double rcone, double radius, oerr *e) {
+    if (rxy + rcone <= radius) { seterr(e, LCG_E_ROCHE, "rxy + rcone <= radius"); return 0.; }
+    if (rxy >= radius + rcone) { seterr(e, LCG_E_ROCHE, "rxy >= radius + rcone"); return 0.; }
+    if (rcone >= radius + rxy) { seterr(e, LCG_E_ROCHE, "rcone >= radius + rxy"); return 0.; }
+    return acos((sqr(rxy) + sqr(rcone) - sqr(radius)) / (2. * rcone * rxy)) / TWOPI_;
+}
+
+/* circle_eclipse (disc_eclipse.cpp:316-340) */
+static int circle_eclipse(double rxy, double z, double zcirc, double radius, double tani,
+                          double *phase, oerr *e) {
+    if (z >= zcirc) return CIRC_ABOVE;
+    const double RCONE = tani * (zcirc - z);
+    if (RCONE >= rxy + radius) return CIRC_OUTSIDE;
+    if (rxy >= RCONE + radius) return CIRC_SEPARATE;
+    if (rxy + RCONE <= radius) return CIRC_INSIDE;
+    *phase = cut_phase(rxy, RCONE, radius, e);
+    return CIRC_CROSSING;
+}
+
+/* Roche::disc_eclipse (disc_eclipse.cpp:38-301): the phase ranges over which
+ * the flared disc hides point r; 0, 1 or 2 ranges appended. */
+static void disc_eclipse(double iangle, double rdisc1, double rdisc2, double beta,
+                         double height, v3 r, int32_t *nr, double *rin, double *rout,
+                         oerr *e) {
+    if (beta < 1) { seterr(e, LCG_E_ROCHE, "Roche::disc_eclipse: beta must be >= 1"); return; }
+    const double sini = sin(PI_ / 180. * iangle);
+    const double cosi = cos(PI_ / 180. * iangle);
+    const double HOUT = height * pow(rdisc2, beta);
+    if (r.z >= HOUT) return;
+    if (cosi == 0.) {
+        if (fabs(r.z) < HOUT) {
+            double rxy = sqrt(sqr(r.x) + sqr(r.y));
+            if (rxy <= rdisc2) {
+                push_range(nr, rin, rout, 0., 1.);
+            } else {
+                double subtend = asin(rdisc2 / rxy) / TWOPI_;
+                double pcen = atan2(r.y, -r.x) / TWOPI_;
+                double ingress = pcen - subtend;
+                ingress = ingress - floor(ingress);
+                double egress = ingress + 2. * subtend;
+                push_range(nr, rin, rout, ingress, egress);
+            }
+        }
+        return;
+    }
+    const double RXY = sqrt(sqr(r.x) + sqr(r.y));
+    if (rdisc1 < RXY && RXY < rdisc2 && fabs(r.z) < height * pow(RXY, beta)) {
+        push_range(nr, rin, rout, 0., 1.1);
+        return;
+    }
+    const double TANI = sini / cosi;
+    int result;
+    double phase = 0., ingress, egress;
+    if (RXY < rdisc2 && r.z >= height * pow(dmax(rdisc1, RXY), beta)) {
+        result = circle_eclipse(RXY, r.z, HOUT, rdisc2, TANI, &phase, e);
+        if (e->st) return;
+        if (result == CIRC_OUTSIDE) {
+            push_range(nr, rin, rout, 0., 1.1);
+        } else if (result == CIRC_CROSSING) {
+            double phi0 = atan2(r.y, -r.x) / TWOPI_;
+            ingress = phi0 + phase;
+            ingress -= floor(ingress);
+            egress = ingress + 1 - 2. * phase;
+            push_range(nr, rin, rout, ingress, egress);
+        }
+        return;
+    }
+    const double RCONE_LO = dmax(0., TANI * (-HOUT - r.z));
+    if (RCONE_LO >= RXY + rdisc2) return;
+    const double RCONE_HI = TANI * (HOUT - r.z);
+    if (RXY >= RCONE_HI + rdisc2) return;
+    double eclipse_phase = 0;
+    if (RXY + RCONE_LO <= rdisc2) {
+        eclipse_phase = 0.5;
+    } else if (RXY <= rdisc2) {
+        eclipse_phase = cut_phase(RXY, RCONE_LO, rdisc2, e);
+    } else {
+        if (sqr(RCONE_HI) + sqr(rdisc2) >= sqr(RXY) && sqr(RCONE_LO) + sqr(rdisc2) <= sqr(RXY)) {
+            eclipse_phase = asin(rdisc2 / RXY) / TWOPI_;
+        } else if (sqr(RCONE_HI) + sqr(rdisc2) < sqr(RXY)) {
+            eclipse_phase = cut_phase(RXY, RCONE_HI, rdisc2, e);
+        } else {
+            eclipse_phase = cut_phase(RXY, RCONE_LO, rdisc2, e);
+        }
+    }
+    if (e->st) return;
+    const double HIN = height * pow(rdisc1, beta);
+    double appear_phase = -1;
+    /* the LOSC passes the rims in turn; the first sets appear_phase, the
+       rest can only lower it or rule out a view through the hole */
+    double zc[4], rc[4];
+    int nc = 0;
+    if (r.z < -HOUT) {
+        zc[0] = -HOUT; rc[0] = rdisc2; zc[1] = -HIN; rc[1] = rdisc1;
+        zc[2] = HIN; rc[2] = rdisc1; zc[3] = HOUT; rc[3] = rdisc2; nc = 4;
+    } else if (RXY < rdisc1) {
+        if (r.z < -HIN) {
+            zc[0] = -HIN; rc[0] = rdisc1; zc[1] = HIN; rc[1] = rdisc1;
+            zc[2] = HOUT; rc[2] = rdisc2; nc = 3;
+        } else if (r.z < HIN) {
+            zc[0] = HIN; rc[0] = rdisc1; zc[1] = HOUT; rc[1] = rdisc2; nc = 2;
+        }
+    }
+    for (int k = 0; k < nc; k++) {
+        if (k > 0 && !(appear_phase > 0)) break;
+        result = circle_eclipse(RXY, r.z, zc[k], rc[k], TANI, &phase, e);
+        if (e->st) return;
+        if (k == 0) {
+            if (result == CIRC_INSIDE) appear_phase = 0.5;
+            else if (result == CIRC_CROSSING) appear_phase = phase;
+        } else if (result == CIRC_CROSSING) {
+            appear_phase = dmin(appear_phase, phase);
+        } else if (result != CIRC_INSIDE) {
+            appear_phase = -1.;
+        }
+    }
+    double phi0 = atan2(r.y, -r.x) / TWOPI_;
+    if (appear_phase <= 0) {
+        ingress = phi0 - eclipse_phase;
+        ingress -= floor(ingress);
+        egress = ingress + 2. * eclipse_phase;
+        push_range(nr, rin, rout, ingress, egress);
+    } else if (appear_phase < eclipse_phase) {
+        ingress = phi0 - eclipse_phase;
+        ingress -= floor(ingress);
+        egress = ingress + (eclipse_phase - appear_phase);
+        push_range(nr, rin, rout, ingress, egress);
+        ingress = phi0 + appear_phase;
+        ingress -= floor(ingress);
+        egress = ingress + (eclipse_phase - appear_phase);
+        push_range(nr, rin, rout, ingress, egress);
+    }
+}
+
+/* Lcurve::star_eclipse (star_eclipse.cpp:15-26): eclipse of point posn by
+ * star `star` (Roche-distorted with reference sphere rref/pref, or a sphere
+ * of radius r); one range appended when eclipsed. */
+static void star_eclipse(double q, double r, double spin, double iangle, v3 posn,
+                         double delta, int roche, int star, double rref, double pref,
+                         int32_t *nr, double *rin, double *rout, oerr *e) {
+    double ri = deg2rad(iangle);
+    const double cosi = cos(ri), sini = sin(ri);
+    double ingress = 0., egress = 0., lam1, lam2;
+    v3 cofm = (star == LCG_STAR1) ? mk3(0., 0., 0.) : mk3(1., 0., 0.);
+    int ecl = roche ? ingress_egress(q, star, spin, iangle, delta, posn, &ingress, &egress,
+                                     rref, pref, e)
+                    : sphere_eclipse_ph(cosi, sini, posn, cofm, r, &ingress, &egress, &lam1,
+                                        &lam2);
+    if (e->st) return;
+    if (ecl) push_range(nr, rin, rout, ingress, egress);
+}
+
+/* What set_disc_grid / set_disc_edge / set_bright_spot_grid derive from the
+ * model before making elements (set_disc_grid.cpp:31-66). */
+typedef struct {
+    double r1, r2, rl1, rl2, rdisc1, rdisc2;
+    double rref1, pref1, rref2, pref2, ffac1, ffac2;
+} comp_setup;
+
+static int comp_prepare(const lcg_model *m, const char *who, comp_setup *s, oerr *e) {
+    get_r1r2(m, &s->r1, &s->r2);
+    s->rl1 = xl11(m->q, m->spin1, e);
+    if (e->st) return e->st;
+    if (s->r1 < 0) s->r1 = s->rl1;
+    else if (s->r1 > s->rl1)
+        return seterr(e, LCG_E_LOBE, "%s: the primary star is larger than its Roche lobe!", who);
+    s->rl2 = 1. - xl12(m->q, m->spin2, e);
+    if (e->st) return e->st;
+    if (s->r2 < 0) s->r2 = s->rl2;
+    else if (s->r2 > s->rl2)
+        return seterr(e, LCG_E_LOBE, "%s: the secondary star is larger than its Roche lobe!", who);
+    s->rdisc1 = m->rdisc1 > 0. ? m->rdisc1 : s->r1;
+    s->rdisc2 = m->rdisc2 > 0. ? m->rdisc2 : m->radius_spot;
+    s->ffac1 = s->r1 / s->rl1;
+    ref_sphere(m->q, LCG_STAR1, m->spin1, s->ffac1, &s->rref1, &s->pref1, e);
+    s->ffac2 = s->r2 / s->rl2;
+    ref_sphere(m->q, LCG_STAR2, m->spin2, s->ffac2, &s->rref2, &s->pref2, e);
+    return e->st;
+}
+
+/* The eclipses every component element gets: the opaque disc, then star 1,
+ * then star 2. trap1: a Roche_Error from star 1's eclipse becomes a range
+ * (0, 1) (the edge's upper rim, set_disc_grid.cpp:222-231). */
+static void element_eclipses(const lcg_model *m, const comp_setup *s, v3 posn, int opaque,
+                             int trap1, int32_t *nr, double *rin, double *rout, oerr *e) {
+    *nr = 0;
+    if (opaque)
+        disc_eclipse(m->iangle, s->rdisc1, s->rdisc2, m->beta_disc, m->height_disc, posn, nr,
+                     rin, rout, e);
+    if (e->st) return;
+    if (m->eclipse1) {
+        star_eclipse(m->q, s->r1, m->spin1, m->iangle, posn, m->delta_phase, m->roche1,
+                     LCG_STAR1, s->rref1, s->pref1, nr, rin, rout, e);
+        if (e->st && trap1 && e->st == LCG_E_ROCHE) {
+            e->st = 0;
+            e->msg[0] = 0;
+            push_range(nr, rin, rout, 0., 1.);
+        }
+        if (e->st) return;
+    }
+    if (m->eclipse2)
+        star_eclipse(m->q, s->r2, m->spin2, m->iangle, posn, m->delta_phase, m->roche2,
+                     LCG_STAR2, s->rref2, s->pref2, nr, rin, rout, e);
+}
+
+static void el_set(elist *d, int i, v3 posn, v3 dirn, double area) {
+    d->posn[3 * i] = posn.x; d->posn[3 * i + 1] = posn.y; d->posn[3 * i + 2] = posn.z;
+    d->dirn[3 * i] = dirn.x; d->dirn[3 * i + 1] = dirn.y; d->dirn[3 * i + 2] = dirn.z;
+    d->area[i] = (float)area;
+}
+
+/* Lcurve::set_disc_grid (set_disc_grid.cpp:27-127) */
+static int disc_grid(const lcg_model *m, elist *d, oerr *e) {
+    const double EFAC = 1.0000001;
+    comp_setup s;
+    if (comp_prepare(m, "set_disc_grid", &s, e)) return e->st;
+    int nface = 0, ntheta = 0;
+    double drad = (s.rdisc2 - s.rdisc1) / m->nrad, drrad = s.rdisc2 / m->nrad;
+    for (int i = 0; i < m->nrad; i++) {
+        ntheta = (int)ceil(TWOPI_ * (s.rdisc1 + (s.rdisc2 - s.rdisc1) * (i + 0.5) / m->nrad) / drrad);
+        ntheta = ntheta > 8 ? ntheta : 8;
+        nface += ntheta;
+    }
+    el_alloc(d, nface);
+    nface = 0;
+    for (int i = 0; i < m->nrad; i++) {
+        double rad = s.rdisc1 + (s.rdisc2 - s.rdisc1) * (i + 0.5) / m->nrad;
+        ntheta = (int)ceil(TWOPI_ * rad / drrad);
+        ntheta = ntheta > 8 ? ntheta : 8;
+        double h = EFAC * m->height_disc * pow(rad, m->beta_disc);
+        double tanp = m->beta_disc * h / rad;
+        double cosp = 1. / sqrt(1 + sqr(tanp));
+        double sinp = tanp * cosp;
+        double area = TWOPI_ / ntheta * rad * drad;
+        for (int j = 0; j < ntheta; j++, nface++) {
+            double theta = TWOPI_ * j / ntheta;
+            double sint = sin(theta), cost = cos(theta);
+            v3 posn = mk3(rad * cost, rad * sint, h);
+            v3 dirn = mk3(-cost * sinp, -sint * sinp, cosp);
+            element_eclipses(m, &s, posn, m->opaque, 0, d->nr + nface, d->rin + LCO_MAXR * nface,
+                             d->rout + LCO_MAXR * nface, e);
+            if (e->st) return e->st;
+            el_set(d, nface, posn, dirn, area);
+        }
+    }
+    return LCG_OK;
+}
+
+/* Lcurve::set_disc_edge with outer = true, visual = false
+ * (set_disc_grid.cpp:144-264) */
+static int disc_edge(const lcg_model *m, elist *d, oerr *e) {
+    const double EFAC = 1.0000001;
+    comp_setup s;
+    if (comp_prepare(m, "set_disc_grid", &s, e)) return e->st;
+    const double size = s.rdisc2 / m->nrad;
+    const double RAD = s.rdisc2;
+    const double H = m->height_disc * pow(RAD, m->beta_disc);
+    const int NOUT = (int)(2 * H / size) + 2;
+    const int NTHETA = (int)ceil(TWOPI_ * RAD / size) > 8 ? (int)ceil(TWOPI_ * RAD / size) : 8;
+    el_alloc(d, NTHETA * NOUT);
+    double area = TWOPI_ / NTHETA * RAD * 2 * H / (NOUT - 1);
+    int nface = 0;
+    for (int i = 0; i < NTHETA; i++) {
+        double theta = TWOPI_ * i / NTHETA;
+        double sint = sin(theta), cost = cos(theta);
+        v3 posn = mk3(EFAC * RAD * cost, EFAC * RAD * sint, EFAC * H);
+        v3 dirn = mk3(cost, sint, 0);
+        element_eclipses(m, &s, posn, m->opaque, 1, d->nr + nface, d->rin + LCO_MAXR * nface,
+                         d->rout + LCO_MAXR * nface, e);
+        if (e->st) return e->st;
+        el_set(d, nface++, posn, dirn, area / 2.);
+        for (int j = 0; j < NOUT - 1; j++) {
+            posn = mk3(EFAC * RAD * cost, EFAC * RAD * sint, -H + 2 * H * j / (NOUT - 1));
+            dirn = mk3(cost, sint, 0);
+            element_eclipses(m, &s, posn, m->opaque, 0, d->nr + nface,
+                             d->rin + LCO_MAXR * nface, d->rout + LCO_MAXR * nface, e);
+            if (e->st) return e->st;
+            el_set(d, nface++, posn, dirn, area);
+        }
+    }
+    return LCG_OK;
+}
+
+/* set_disc_continuum (set_disc_continuum.cpp:19-31) */
+static void disc_continuum(double rdisc, double tdisc, double texp, double wave, elist *d) {
+    const double BRIGHT = planck(wave, tdisc);
+    for (int i = 0; i < d->n; i++) {
+        double r = len3(mk3(d->posn[3 * i], d->posn[3 * i + 1], d->posn[3 * i + 2]));
+        d->flux[i] = (float)(BRIGHT * pow(r / rdisc, texp) * d->area[i]);
+    }
+}
+
+/* set_edge_continuum (set_disc_continuum.cpp:48-88) */
+static void edge_continuum(double tedge, double r2, double t2, double absorb, double wave,
+                           elist *d) {
+    const v3 cofm2 = mk3(1., 0., 0.);
+    for (int i = 0; i < d->n; i++) {
+        v3 p = mk3(d->posn[3 * i], d->posn[3 * i + 1], d->posn[3 * i + 2]);
+        v3 n = mk3(d->dirn[3 * i], d->dirn[3 * i + 1], d->dirn[3 * i + 2]);
+        v3 vec = sub3(cofm2, p);
+        double r = len3(vec);
+        double mu = dot3(n, vec) / r, geom, temp;
+        if (mu >= r2) {
+            geom = sqr(r2 / r) * mu;
+            temp = pow(pow(tedge, 4) + absorb * pow(t2, 4) * geom, 0.25);
+        } else if (mu > -r2) {
+            double x0 = -mu / r2;
+            geom = sqr(r2 / r) * r2 *
+                   (sqrt(1. - x0 * x0) * (2 + x0 * x0) / 3 - x0 * (PI_ / 2 - asin(x0))) / PI_;
+            temp = pow(pow(tedge, 4) + absorb * pow(t2, 4) * geom, 0.25);
+        } else {
+            temp = tedge;
+        }
+        d->flux[i] = (float)(d->area[i] * planck(wave, temp));
+    }
+}
+
+/* ---- gas stream to the bright spot --------------------------------------
+ * Roche::strinit (strining.cpp:14-33) starts a particle just inside L1 with
+ * the Lubow & Shu velocity; the reference then integrates the restricted
+ * three-body motion (rocacc.cpp) with a Bulirsch-Stoer stepper until the
+ * stream reaches radius_spot (stradv.cpp:27-80, accuracy 1e-10 in radius).
+ * Here the same motion is integrated with the Dormand-Prince 5(4) pair
+ * (Dormand & Prince 1980, J. Comp. Appl. Math. 6, 19) under a much tighter
+ * tolerance, and the crossing is bisected in time to the same radius
+ * accuracy, so the spot lands on the stream within the reference's own
+ * integration error (the reference's stepper keeps its step size in a
+ * static between calls, so its result depends on call history). */
+static void rocacc(double q, const double *y, double *dy) {
+    double f1 = 1.0 / (1.0 + q), f2 = f1 * q;
+    double yzsq = sqr(y[1]) + sqr(y[2]);
+    double r1sq = sqr(y[0]) + yzsq, r2sq = sqr(y[0] - 1.0) + yzsq;
+    double fm1 = f1 / (r1sq * sqrt(r1sq)), fm2 = f2 / (r2sq * sqrt(r2sq)), fm3 = fm1 + fm2;
+    dy[0] = y[3]; dy[1] = y[4]; dy[2] = y[5];
+    dy[3] = -fm3 * y[0] + fm2 + 2.0 * y[4] + y[0] - f2;
+    dy[4] = -fm3 * y[1] - 2.0 * y[3] + y[1];
+    dy[5] = -fm3 * y[2];
+}
+
+/* One Dormand-Prince step of size h from y; returns the error norm. */
+static double dp_step(double q, const double *y, double h, double *yo) {
+    static const double a21 = 1. / 5, a31 = 3. / 40, a32 = 9. / 40, a41 = 44. / 45,
+                        a42 = -56. / 15, a43 = 32. / 9, a51 = 19372. / 6561,
+                        a52 = -25360. / 2187, a53 = 64448. / 6561, a54 = -212. / 729,
+                        a61 = 9017. / 3168, a62 = -355. / 33, a63 = 46732. / 5247,
+                        a64 = 49. / 176, a65 = -5103. / 18656, b1 = 35. / 384,
+                        b3 = 500. / 1113, b4 = 125. / 192, b5 = -2187. / 6784, b6 = 11. / 84,
+                        e1 = 71. / 57600, e3 = -71. / 16695, e4 = 71. / 1920,
+                        e5 = -17253. / 339200, e6 = 22. / 525, e7 = -1. / 40;
+    double k1[6], k2[6], k3[6], k4[6], k5[6], k6[6], k7[6], t[6];
+    int i;
+    rocacc(q, y, k1);
+    for (i = 0; i < 6; i++) t[i] = y[i] + h * (a21 * k1[i]);
+    rocacc(q, t, k2);
+    for (i = 0; i < 6; i++) t[i] = y[i] + h * (a31 * k1[i] + a32 * k2[i]);
+    rocacc(q, t, k3);
+    for (i = 0; i < 6; i++) t[i] = y[i] + h * (a41 * k1[i] + a42 * k2[i] + a43 * k3[i]);
+    rocacc(q, t, k4);
+    for (i = 0; i < 6; i++)
+        t[i] = y[i] + h * (a51 * k1[i] + a52 * k2[i] + a53 * k3[i] + a54 * k4[i]);
+    rocacc(q, t, k5);
+    for (i = 0; i < 6; i++)
+        t[i] = y[i] + h * (a61 * k1[i] + a62 * k2[i] + a63 * k3[i] + a64 * k4[i] + a65 * k5[i]);
+    rocacc(q, t, k6);
+    for (i = 0; i < 6; i++)
+        yo[i] = y[i] + h * (b1 * k1[i] + b3 * k3[i] + b4 * k4[i] + b5 * k5[i] + b6 * k6[i]);
+    rocacc(q, yo, k7);
+    double err = 0.;
+    for (i = 0; i < 6; i++) {
+        double ei = h * (e1 * k1[i] + e3 * k3[i] + e4 * k4[i] + e5 * k5[i] + e6 * k6[i] +
+                         e7 * k7[i]);
+        double sc = 1e-14 + 1e-13 * fmax(fabs(y[i]), fabs(yo[i]));
+        err = fmax(err, fabs(ei) / sc);
+    }
+    return err;
+}
+
+/* The stream position where it first reaches radius rad from star 1. */
+static int stream_to_radius(double q, double rad, v3 *pos, oerr *e) {
+    const double SMALL = 1.e-5, ACC = 1.e-10, SMAX = 1.e-3, TMAX = 10.;
+    double rl1 = xl1(q, e);
+    if (e->st) return e->st;
+    double mu = q / (1.0 + q);
+    double a = (1.0 - mu) / pow(rl1, 3) + mu / pow((1. - rl1), 3);
+    double lambda1 = sqrt(((a - 2.0) + sqrt(a * (9.0 * a - 8.0))) / 2.0);
+    double m1 = (lambda1 * lambda1 - 2.0 * a - 1.0) / 2.0 / lambda1;
+    double y[6] = {rl1 - SMALL, -m1 * SMALL, 0., -lambda1 * SMALL, -lambda1 * m1 * SMALL, 0.};
+    double yo[6], ylo[6], h = 1e-4, t = 0.;
+    const double rinit = sqrt(sqr(y[0]) + sqr(y[1]) + sqr(y[2]));
+    double rnow = rinit;
+    int guard = 0;
+    while ((rinit > rad && rnow > rad) || (rinit < rad && rnow < rad)) {
+        if (++guard > 1000000 || t > TMAX)
+            return seterr(e, LCG_E_ROCHE, "Roche::stradv: taken too long without crossing radius");
+        h = fmin(h, SMAX);
+        double err = dp_step(q, y, h, yo);
+        if (err > 1.) {
+            h *= fmax(0.2, 0.9 * pow(err, -0.2));
+            continue;
+        }
+        memcpy(ylo, y, sizeof y);
+        memcpy(y, yo, sizeof y);
+        t += h;
+        rnow = sqrt(sqr(y[0]) + sqr(y[1]) + sqr(y[2]));
+        double hstep = h;
+        h *= err > 0. ? fmin(5., 0.9 * pow(err, -0.2)) : 5.;
+        if (!((rinit > rad && rnow > rad) || (rinit < rad && rnow < rad))) {
+            /* bisect the last step in time until the radius is pinned */
+            double lo = 0., hi = hstep;
+            double rlo = sqrt(sqr(ylo[0]) + sqr(ylo[1]) + sqr(ylo[2])), rhi = rnow;
+            int g2 = 0;
+            while (fabs(rhi - rlo) > ACC && ++g2 < 200) {
+                double tt = (lo + hi) / 2.;
+                dp_step(q, ylo, tt, y);
+                rnow = sqrt(sqr(y[0]) + sqr(y[1]) + sqr(y[2]));
+                if ((rhi > rad && rnow > rad) || (rhi < rad && rnow < rad)) {
+                    rhi = rnow;
+                    hi = tt;
+                } else {
+                    rlo = rnow;
+                    lo = tt;
+                }
+            }
+            break;
+        }
+    }
+    *pos = mk3(y[0], y[1], y[2]);
+    return LCG_OK;
+}
+
+/* Lcurve::set_bright_spot_grid (set_bright_spot_grid.cpp:27-100) */
+static int spot_grid(const lcg_model *m, elist *d, oerr *e) {
+    comp_setup s;
+    if (comp_prepare(m, "set_bright_spot_grid", &s, e)) return e->st;
+    v3 bspot = {0., 0., 0.};
+    if (stream_to_radius(m->q, m->radius_spot, &bspot, e)) return e->st;
+    double theta = atan2(bspot.y, bspot.x) + TWOPI_ / 4. + deg2rad(m->angle_spot);
+    double alpha = deg2rad(m->yaw_spot);
+    double tilt = deg2rad(m->tilt_spot);
+    v3 bvec = mk3(cos(theta), sin(theta), 0);
+    v3 pvec = mk3(0, 0, 1);
+    v3 tvec = mk3(sin(tilt) * sin(theta + alpha), -sin(tilt) * cos(theta + alpha), cos(tilt));
+    const double BMAX = pow(m->expon_spot / m->epow_spot, 1. / m->epow_spot);
+    const double SFAC = 20. + BMAX;
+    const int ns = m->nspot;
+    el_alloc(d, 2 * ns);
+    const double AREA = SFAC * m->length_spot * m->height_spot / (ns - 1);
+    const double BRIGHT = planck(m->wavelength, m->temp_spot);
+    for (int i = 0; i < ns; i++) {
+        double dist = SFAC * i / (ns - 1);
+        v3 posn = add3(bspot, scl3(m->length_spot * (dist - BMAX), bvec));
+        int32_t nr = 0;
+        double rin[LCO_MAXR], rout[LCO_MAXR];
+        element_eclipses(m, &s, posn, 0, 0, &nr, rin, rout, e);
+        if (e->st) return e->st;
+        double bright = BRIGHT * pow(dist / BMAX, m->expon_spot) *
+                        exp(m->expon_spot / m->epow_spot - pow(dist, m->epow_spot));
+        el_set(d, i, posn, tvec, AREA);
+        el_set(d, ns + i, posn, pvec, AREA);
+        d->flux[i] = (float)(bright * (1 - m->cfrac_spot) * d->area[i]);
+        d->flux[ns + i] = (float)(bright * m->cfrac_spot * d->area[i]);
+        for (int k = 0; k < 2; k++) {
+            int j = k ? ns + i : i;
+            d->nr[j] = nr;
+            memcpy(d->rin + LCO_MAXR * j, rin, sizeof rin);
+            memcpy(d->rout + LCO_MAXR * j, rout, sizeof rout);
+        }
+    }
+    return LCG_OK;
+}
+
+/* Point::visible (lcurve.h:81-89) over an element's ranges. */
+static inline int el_visible(const elist *d, int i, double phase) {
+    double phi = phase - floor(phase);
+    for (int k = 0; k < d->nr[i]; k++) {
+        double in = d->rin[LCO_MAXR * i + k], out = d->rout[LCO_MAXR * i + k];
+        if ((phi >= in && phi <= out) || phi <= out - 1.0) return 0;
+    }
+    return 1;
+}
+
+/* comp_disc / comp_edge / comp_spot (comp_light.cpp:323-408): per
+ * sub-exposure a serial sum over the elements in vector order, weighted and
+ * merged in order. spot selects spot_elem (mu flux) over disc_elem (linear +
+ * quadratic limb darkening). */
+static double comp_elements(const lcg_model *m, const elist *d, int spot, double phase,
+                            double expose, int ndiv) {
+    double sum = 0.0;
+    for (int nd = 0; nd < ndiv; ++nd) {
+        double phi, wgt;
+        if (ndiv == 1) { phi = phase; wgt = 1.0; }
+        else {
+            phi = phase + expose * (nd - (ndiv - 1) / 2.0) / (ndiv - 1);
+            wgt = (nd == 0 || nd == ndiv - 1) ? 0.5 : 1.0;
+        }
+        double ri = deg2rad(m->iangle);
+        double cosi = cos(ri), sini = sin(ri);
+        v3 earth = set_earth(cosi, sini, phi);
+        double s = 0.0;
+        for (int i = 0; i < d->n; i++) {
+            double v = 0.0;
+            if (el_visible(d, i, phi)) {
+                double mu = dot3(earth, mk3(d->dirn[3 * i], d->dirn[3 * i + 1], d->dirn[3 * i + 2]));
+                if (spot) {
+                    v = (mu > 0.0) ? mu * d->flux[i] : 0.0;
+                } else if (mu > 0.0) {
+                    double om = 1.0 - mu;
+                    v = mu * d->flux[i] * (1.0 - om * (m->lin_limb_disc + m->quad_limb_disc * om));
+                }
+            }
+            s += v;
+        }
+        sum += wgt * s;
+    }
+    return sum / ((ndiv - 1 > 1) ? ndiv - 1 : 1);
+}
+
+/* ---- iscale: Subs::svdfit (svdfit.cpp:22-80) ----------------------------
+ * Least squares for the component scale factors: rows with sigma z > 0,
+ * weighted by 1/z; singular values below 1e-5 of the largest are dropped.
+ * The decomposition is a one-sided Jacobi SVD (Hestenes 1958) of the
+ * weighted design matrix: the reference's svdcmp is a different SVD
+ * algorithm, so the factors agree to rounding, not bit for bit. */
+static void svd_solve(int nrow, int nc, double *A, const double *b, double *x) {
+    double V[25], w[5];
+    for (int i = 0; i < nc * nc; i++) V[i] = 0.;
+    for (int i = 0; i < nc; i++) V[i * nc + i] = 1.;
+    for (int sweep = 0; sweep < 60; sweep++) {
+        int rotated = 0;
+        for (int p = 0; p < nc - 1; p++)
+            for (int q = p + 1; q < nc; q++) {
+                double al = 0., be = 0., ga = 0.;
+                for (int i = 0; i < nrow; i++) {
+                    al += A[i * nc + p] * A[i * nc + p];
+                    be += A[i * nc + q] * A[i * nc + q];
+                    ga += A[i * nc + p] * A[i * nc + q];
+                }
+                if (ga == 0. || fabs(ga) <= 1e-15 * sqrt(al * be)) continue;
+                rotated = 1;
+                double zeta = (be - al) / (2. * ga);
+                double t = (zeta >= 0. ? 1. : -1.) / (fabs(zeta) + sqrt(1. + zeta * zeta));
+                double c = 1. / sqrt(1. + t * t), sn = c * t;
+                for (int i = 0; i < nrow; i++) {
+                    double ap = A[i * nc + p], aq = A[i * nc + q];
+                    A[i * nc + p] = c * ap - sn * aq;
+                    A[i * nc + q] = sn * ap + c * aq;
+                }
+                for (int i = 0; i < nc; i++) {
+                    double vp = V[i * nc + p], vq = V[i * nc + q];
+                    V[i * nc + p] = c * vp - sn * vq;
+                    V[i * nc + q] = sn * vp + c * vq;
+                }
+            }
+        if (!rotated) break;
+    }
+    double wmax = 0.;
+    for (int j = 0; j < nc; j++) {
+        double s = 0.;
+        for (int i = 0; i < nrow; i++) s += A[i * nc + j] * A[i * nc + j];
+        w[j] = sqrt(s);
+        wmax = fmax(wmax, w[j]);
+    }
+    for (int j = 0; j < nc; j++) x[j] = 0.;
+    for (int j = 0; j < nc; j++) {
+        if (!(w[j] >= 1e-5 * wmax) || w[j] == 0.) continue;
+        double ub = 0.;
+        for (int i = 0; i < nrow; i++) ub += A[i * nc + j] * b[i];
+        ub /= w[j] * w[j];  /* (u_j . b) / w_j with u_j = column j / w_j */
+        for (int k = 0; k < nc; k++) x[k] += V[k * nc + j] * ub;
+    }
+}
+
+/* sfac[0..nc-1] from the per-point components fcomp[n][5] (svdfit.cpp:22-80,
+ * light_curve_comp.cpp:511-530). */
+static void iscale_fit(const lcg_datum *data, int32_t n, const double *fcomp, int nc,
+                       double *sfac) {
+    int nrow = 0;
+    for (int i = 0; i < n; i++) {
+        double z = data[i].weight <= 0. ? -1. : data[i].ferr / sqrt(data[i].weight);
+        if (z > 0) nrow++;
+    }
+    double *A = (double *)malloc(sizeof(double) * (size_t)(nrow > 0 ? nrow : 1) * nc);
+    double *b = (double *)malloc(sizeof(double) * (size_t)(nrow > 0 ? nrow : 1));
+    int k = 0;
+    for (int i = 0; i < n; i++) {
+        double z = data[i].weight <= 0. ? -1. : data[i].ferr / sqrt(data[i].weight);
+        if (!(z > 0)) continue;
+        double invsig = 1. / z;
+        for (int j = 0; j < nc; j++) A[k * nc + j] = invsig * fcomp[5 * i + j];
+        b[k++] = invsig * data[i].flux;
+    }
+    svd_solve(nrow, nc, A, b, sfac);
+    free(A);
+    free(b);
+}
+
+int lco_components(const lcg_model *m, int32_t which, int32_t cap, int32_t maxr,
+                   int32_t *nout, double *posn, double *dirn, float *area, float *flux,
+                   int32_t *nr, double *rin, double *rout, char *err, int errlen) {
+    oerr e = {0, ""};
+    elist d;
+    memset(&d, 0, sizeof(d));
+    double r1, r2;
+    get_r1r2(m, &r1, &r2);
+    const double rl2 = 1. - xl12(m->q, m->spin2, &e);
+    if (r2 < 0) r2 = rl2;
+    const double rdisc2 = m->rdisc2 > 0. ? m->rdisc2 : m->radius_spot;
+    if (!e.st) {
+        if (which == 0 && !disc_grid(m, &d, &e))
+            disc_continuum(rdisc2, m->temp_disc, m->texp_disc, m->wavelength, &d);
+        else if (which == 1 && !disc_edge(m, &d, &e))
+            edge_continuum(m->temp_edge, r2, fabs(m->t2), m->absorb_edge, m->wavelength, &d);
+        else if (which == 2)
+            spot_grid(m, &d, &e);
+    }
+    if (!e.st) {
+        *nout = d.n;
+        if (d.n <= cap && posn) {
+            memcpy(posn, d.posn, 3 * sizeof(double) * (size_t)d.n);
+            memcpy(dirn, d.dirn, 3 * sizeof(double) * (size_t)d.n);
+            memcpy(area, d.area, sizeof(float) * (size_t)d.n);
+            memcpy(flux, d.flux, sizeof(float) * (size_t)d.n);
+            for (int i = 0; i < d.n; i++) {
+                nr[i] = d.nr[i];
+                for (int k = 0; k < maxr && k < d.nr[i] && k < LCO_MAXR; k++) {
+                    rin[maxr * i + k] = d.rin[LCO_MAXR * i + k];
+                    rout[maxr * i + k] = d.rout[LCO_MAXR * i + k];
+                }
+            }
+        }
+    }
+    el_free(&d);
+    copyerr(&e, err, errlen);
+    return e.st;
+}
+
 int lco_light_curve(const lcg_model *m, const lcg_datum *data, int32_t n,
                     int32_t flags, double *sfac, double *calc, double *scalars,
                     char *err, int errlen) {
@@ -1833,14 +2617,12 @@ int lco_light_curve(const lcg_model *m, const lcg_datum *data, int32_t n,
     memset(&s1f, 0, sizeof(s1f)); memset(&s2f, 0, sizeof(s2f));
     memset(&s1c, 0, sizeof(s1c)); memset(&s2c, 0, sizeof(s2c));
     pbatch pb1f = {0}, pb1c = {0}, pb2f = {0}, pb2c = {0};
-    double *phases = NULL, *slfacs = NULL;
+    double *phases = NULL, *slfacs = NULL, *fcomp = NULL;
     double *o1f = NULL, *o1c = NULL, *o2f = NULL, *o2c = NULL;
+    elist disc, edge, spot;
+    memset(&disc, 0, sizeof(disc)); memset(&edge, 0, sizeof(edge)); memset(&spot, 0, sizeof(spot));
 
     if (n < 1) { seterr(&e, LCG_E_INVALID, "light_curve_comp: no data points"); goto done; }
-    if (m->add_disc || m->add_spot || m->iscale) {
-        seterr(&e, LCG_E_UNSUPPORTED, "disc, bright spot and iscale models are not supported");
-        goto done;
-    }
     if (m->q <= 0.) { seterr(&e, LCG_E_INVALID, "Roche::xl12(double, double): q = %f <= 0.", m->q); goto done; }
 
     double r1, r2;
@@ -1898,6 +2680,35 @@ int lco_light_curve(const lcg_model *m, const lcg_datum *data, int32_t n,
         fc = comp_star_point(m, LCG_STAR2, 0.9999999999 * m->phase2, &gi, &s2f, g2c, rlens1);
         gi.scale22 = ff / fc;
     }
+    /* disc, edge, opaque-disc eclipses of the stars, bright spot
+       (light_curve_comp.cpp:272-333) */
+    if (m->add_disc) {
+        if (disc_grid(m, &disc, &e)) goto done;
+        if (disc_edge(m, &edge, &e)) goto done;
+        double rdisc1 = m->rdisc1 > 0. ? m->rdisc1 : r1;
+        double rdisc2 = m->rdisc2 > 0. ? m->rdisc2 : m->radius_spot;
+        if (m->opaque) {
+            sgrid *gs[4] = {&s1f, copy1 ? NULL : &s1c, &s2f, copy2 ? NULL : &s2c};
+            for (int k = 0; k < 4; k++) {
+                sgrid *g = gs[k];
+                if (!g) continue;
+                size_t N = (size_t)(g->n > 0 ? g->n : 1);
+                g->ndx = (int32_t *)calloc(N, sizeof(int32_t));
+                g->xin = (double *)calloc(LCO_DISC_R * N, sizeof(double));
+                g->xout = (double *)calloc(LCO_DISC_R * N, sizeof(double));
+                for (int i = 0; i < g->n; i++) {
+                    disc_eclipse(m->iangle, rdisc1, rdisc2, m->beta_disc, m->height_disc,
+                                 mk3(g->posn[3 * i], g->posn[3 * i + 1], g->posn[3 * i + 2]),
+                                 g->ndx + i, g->xin + LCO_DISC_R * i, g->xout + LCO_DISC_R * i,
+                                 &e);
+                    if (e.st) goto done;
+                }
+            }
+        }
+        disc_continuum(rdisc2, m->temp_disc, m->texp_disc, m->wavelength, &disc);
+        edge_continuum(m->temp_edge, r2, fabs(m->t2), m->absorb_edge, m->wavelength, &edge);
+    }
+    if (m->add_spot && spot_grid(m, &spot, &e)) goto done;
     sgrid_flatten(&s1f);
     sgrid_flatten(&s2f);
     if (!copy1) sgrid_flatten(&s1c);
@@ -1912,7 +2723,25 @@ int lco_light_curve(const lcg_model *m, const lcg_datum *data, int32_t n,
         float vs = (float)m->velocity_scale;
         const double XCOFM = m->q / (1.0 + m->q);
         const double VFAC = vs / (C_LIGHT / 1.e3);
-        for (int np = 0; np < n; np++) {
+        if (m->iscale) {
+            /* per-point components (light_curve_comp.cpp:378-414) */
+            fcomp = (double *)calloc(5 * (size_t)n, sizeof(double));
+            for (int np = 0; np < n; np++) {
+                double phase = phases[np], slfac = slfacs[np];
+                double expose = data[np].expose / m->period;
+                const int ndiv = data[np].ndiv;
+                double *f = fcomp + 5 * np;
+                f[0] = slfac * comp_star_flat(m, LCG_STAR1, phase, expose, ndiv, &gi, &s1f, g1c,
+                                              VFAC, XCOFM, rlens1);
+                f[1] = slfac * comp_elements(m, &disc, 0, phase, expose, ndiv);
+                f[2] = slfac * comp_elements(m, &edge, 0, phase, expose, ndiv);
+                f[3] = slfac * comp_elements(m, &spot, 1, phase, expose, ndiv);
+                if (m->t2 > 0)
+                    f[4] = slfac * comp_star_flat(m, LCG_STAR2, phase, expose, ndiv, &gi, &s2f,
+                                                  g2c, VFAC, XCOFM, rlens1);
+            }
+        }
+        for (int np = 0; !m->iscale && np < n; np++) {
             double phase = phases[np], slfac = slfacs[np];
             double expose = data[np].expose / m->period;
             int ndiv = data[np].ndiv;
@@ -1934,6 +2763,7 @@ int lco_light_curve(const lcg_model *m, const lcg_datum *data, int32_t n,
                 pb_push(b2, earth.x, earth.y, earth.z, phin, w2, np);
             }
         }
+        for (int np = 0; np < n; np++) calc[np] = 0.;
         o1f = (double *)calloc((size_t)pb1f.n + 1, sizeof(double));
         o1c = (double *)calloc((size_t)pb1c.n + 1, sizeof(double));
         o2f = (double *)calloc((size_t)pb2f.n + 1, sizeof(double));
@@ -1942,12 +2772,21 @@ int lco_light_curve(const lcg_model *m, const lcg_datum *data, int32_t n,
         if (pb1c.n) sweep_flat(m, LCG_STAR1, g1c, &pb1c, o1c, m->spin1, VFAC, XCOFM, rlens1);
         if (pb2f.n) sweep_flat(m, LCG_STAR2, &s2f, &pb2f, o2f, m->spin2, VFAC, XCOFM, rlens1);
         if (pb2c.n) sweep_flat(m, LCG_STAR2, g2c, &pb2c, o2c, m->spin2, VFAC, XCOFM, rlens1);
-        for (int np = 0; np < n; np++) calc[np] = 0.;
         for (int64_t k = 0; k < pb1f.n; k++) calc[pb1f.idx[k]] += pb1f.w[k] * o1f[k];
         for (int64_t k = 0; k < pb1c.n; k++) calc[pb1c.idx[k]] += pb1c.w[k] * o1c[k];
         for (int64_t k = 0; k < pb2f.n; k++) calc[pb2f.idx[k]] += pb2f.w[k] * o2f[k];
         for (int64_t k = 0; k < pb2c.n; k++) calc[pb2c.idx[k]] += pb2c.w[k] * o2c[k];
-        for (int np = 0; np < n; np++) calc[np] += m->third;
+        if (!m->iscale && (disc.n || edge.n || spot.n)) {
+            for (int np = 0; np < n; np++) {
+                double expose = data[np].expose / m->period;
+                const int ndiv = data[np].ndiv;
+                calc[np] += slfacs[np] * (comp_elements(m, &disc, 0, phases[np], expose, ndiv) +
+                                          comp_elements(m, &edge, 0, phases[np], expose, ndiv) +
+                                          comp_elements(m, &spot, 1, phases[np], expose, ndiv));
+            }
+        }
+        if (!m->iscale)
+            for (int np = 0; np < n; np++) calc[np] += m->third;
 
         const int diagnostics = (flags & LCG_FLAG_DIAGNOSTICS) != 0;
         double wdwarf = 0.0;
@@ -1959,7 +2798,22 @@ int lco_light_curve(const lcg_model *m, const lcg_datum *data, int32_t n,
                      flat_sum_one(m, LCG_STAR1, g, earth, phi - floor(phi), VFAC, XCOFM, rlens1);
             wdwarf = wdwarf / 1;
         }
-        if (flags & LCG_FLAG_SCALE) {
+        const int nc = m->t2 > 0 ? 5 : 4;
+        if ((flags & LCG_FLAG_SCALE) && m->iscale) {
+            iscale_fit(data, n, fcomp, nc, sfac);
+            wdwarf *= sfac[0];
+            if (m->t2 <= 0.) sfac[4] = 0.;
+            iscale_calc(m, n, fcomp, sfac, calc);
+            double wnok = 0., chisq = 0.;
+            for (int i = 0; i < n; i++) {
+                if (data[i].weight > 0.) {
+                    wnok += data[i].weight;
+                    chisq += data[i].weight * sqr((data[i].flux - calc[i]) / data[i].ferr);
+                }
+            }
+            scalars[LCG_OUT_CHISQ] = chisq;
+            scalars[LCG_OUT_WNOK] = wnok;
+        } else if (flags & LCG_FLAG_SCALE) {
             /* re_scale (re_scale.cpp:16-42) */
             double wgt, sdy = 0., syy = 0., wnok = 0., chisq = 0.;
             for (int i = 0; i < n; i++) {
@@ -1988,7 +2842,9 @@ int lco_light_curve(const lcg_model *m, const lcg_datum *data, int32_t n,
             scalars[LCG_OUT_WNOK] = wnok;
         } else {
             wdwarf *= sfac[0];
-            for (int np = 0; np < n; np++) calc[np] *= sfac[0];
+            if (m->iscale) iscale_calc(m, n, fcomp, sfac, calc);
+            else
+                for (int np = 0; np < n; np++) calc[np] *= sfac[0];
             if (flags & LCG_FLAG_RDATA) {
                 double wnok = 0., chisq = 0.;
                 for (int i = 0; i < n; i++) {
@@ -2016,8 +2872,9 @@ int lco_light_curve(const lcg_model *m, const lcg_datum *data, int32_t n,
 done:
     sgrid_free(&s1f); sgrid_free(&s2f); sgrid_free(&s1c); sgrid_free(&s2c);
     pb_free(&pb1f); pb_free(&pb1c); pb_free(&pb2f); pb_free(&pb2c);
-    free(phases); free(slfacs);
+    free(phases); free(slfacs); free(fcomp);
     free(o1f); free(o1c); free(o2f); free(o2c);
+    el_free(&disc); el_free(&edge); el_free(&spot);
     copyerr(&e, err, errlen);
     return e.st;
 }

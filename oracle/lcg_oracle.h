@@ -61,6 +61,16 @@ int64_t lco_phase_batch(const lcg_model *m, const lcg_datum *data, int32_t n,
                         double *ex, double *ey, double *ez, double *phin,
                         double *w1, double *w2, int32_t *idx);
 
+/* One component grid as light_curve_comp builds it: which = 0 the disc
+ * (set_disc_grid.cpp:27-127 + set_disc_continuum), 1 its outer edge
+ * (set_disc_grid.cpp:144-264 + set_edge_continuum), 2 the bright spot
+ * (set_bright_spot_grid.cpp:27-100). *nout gets the element count; the
+ * arrays (3 per element for posn/dirn, maxr per element for rin/rout) are
+ * filled when it is <= cap. nr holds each element's number of ranges. */
+int lco_components(const lcg_model *m, int32_t which, int32_t cap, int32_t maxr,
+                   int32_t *nout, double *posn, double *dirn, float *area, float *flux,
+                   int32_t *nr, double *rin, double *rout, char *err, int errlen);
+
 /* The whole path: Lcurve::light_curve_comp (light_curve_comp.cpp:119-599). */
 int lco_light_curve(const lcg_model *m, const lcg_datum *data, int32_t n,
                     int32_t flags, double *sfac, double *calc,

@@ -10,6 +10,9 @@
 //   Lcurve::set_star_grid         (src/lcurve_base/lcurve.h:528)
 //   Lcurve::set_star_continuum    (src/lcurve_base/lcurve.h:550)
 //   Lcurve::flat_sum_star1_multi / flat_sum_star2_multi (lcurve.h:299-307)
+//   Lcurve::set_disc_grid, set_disc_edge, set_bright_spot_grid,
+//   set_disc_continuum, set_edge_continuum (lcurve.h:539-561)
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <exception>
@@ -54,7 +57,12 @@ Lcurve::Model to_model(const lcg_model &m) {
                           "absorb_edge", "radius_spot", "length_spot", "height_spot",
                           "expon_spot", "epow_spot", "angle_spot", "yaw_spot",
                           "temp_spot", "tilt_spot", "cfrac_spot"};
-    for (const char *k : disc) p[k] = pp(0.);
+    const double dv[] = {m.rdisc1, m.rdisc2, m.height_disc, m.beta_disc, m.temp_disc,
+                         m.texp_disc, m.lin_limb_disc, m.quad_limb_disc, m.temp_edge,
+                         m.absorb_edge, m.radius_spot, m.length_spot, m.height_spot,
+                         m.expon_spot, m.epow_spot, m.angle_spot, m.yaw_spot, m.temp_spot,
+                         m.tilt_spot, m.cfrac_spot};
+    for (int k = 0; k < 20; k++) p[disc[k]] = pp(dv[k]);
     const char *spots[5] = {"stsp11", "stsp12", "stsp13", "stsp21", "stsp22"};
     const char *fields[4] = {"_long", "_lat", "_fwhm", "_tcen"};
     for (int s = 0; s < 5; s++)
@@ -83,9 +91,9 @@ Lcurve::Model to_model(const lcg_model &m) {
     p["limb1"] = m.limb1 == LCG_LIMB_CLARET ? "Claret" : "Poly";
     p["limb2"] = m.limb2 == LCG_LIMB_CLARET ? "Claret" : "Poly";
     p["mirror"] = m.mirror ? "1" : "0";
-    p["add_disc"] = m.add_disc ? "1" : "0"; p["nrad"] = "40";
+    p["add_disc"] = m.add_disc ? "1" : "0"; p["nrad"] = std::to_string(m.nrad);
     p["opaque"] = m.opaque ? "1" : "0";
-    p["add_spot"] = m.add_spot ? "1" : "0"; p["nspot"] = "0";
+    p["add_spot"] = m.add_spot ? "1" : "0"; p["nspot"] = std::to_string(m.nspot);
     p["iscale"] = m.iscale ? "1" : "0";
     nlohmann::json cfg;
     cfg["model_parameters"] = p;
@@ -191,6 +199,53 @@ int lcref_star_grid(const lcg_model *m, int32_t star, int32_t fine, int32_t cap,
             necl[i] = (int32_t)p.eclipse.size();
             ein[i] = p.eclipse.empty() ? 0. : p.eclipse[0].first;
             eout[i] = p.eclipse.empty() ? 0. : p.eclipse[0].second;
+        }
+        return 0;
+    } catch (const Lcurve::Lcurve_Error &ex) {
+        return fail(ex, err, errlen, LCG_E_LOBE);
+    } catch (const Roche::Roche_Error &ex) {
+        return fail(ex, err, errlen, LCG_E_ROCHE);
+    } catch (const std::exception &ex) {
+        return fail(ex, err, errlen, LCG_E_INVALID);
+    }
+}
+
+// One component grid as light_curve_comp builds it (light_curve_comp.cpp:272-333):
+// which = 0 the disc, 1 its outer edge (continua applied), 2 the bright spot.
+// Up to maxr eclipse ranges per element are returned (nr holds the full count).
+int lcref_components(const lcg_model *m, int32_t which, int32_t cap, int32_t maxr,
+                     int32_t *nout, double *posn, double *dirn, float *area, float *flux,
+                     int32_t *nr, double *rin, double *rout, char *err, int errlen) {
+    try {
+        Lcurve::Model mdl = to_model(*m);
+        std::vector<Lcurve::Point> g;
+        double r1, r2;
+        mdl.get_r1r2(r1, r2);
+        const double rl2 = 1. - Roche::xl12(mdl.q, mdl.spin2);
+        if (r2 < 0) r2 = rl2;
+        const double rdisc2 = mdl.rdisc2 > 0. ? mdl.rdisc2 : mdl.radius_spot;
+        if (which == 0) {
+            Lcurve::set_disc_grid(mdl, g);
+            Lcurve::set_disc_continuum(rdisc2, mdl.temp_disc, mdl.texp_disc, mdl.wavelength, g);
+        } else if (which == 1) {
+            Lcurve::set_disc_edge(mdl, true, g, false);
+            Lcurve::set_edge_continuum(mdl.temp_edge, r2, std::fabs(mdl.t2), mdl.absorb_edge,
+                                       mdl.wavelength, g);
+        } else {
+            Lcurve::set_bright_spot_grid(mdl, g);
+        }
+        *nout = (int32_t)g.size();
+        if ((int32_t)g.size() > cap || !posn) return 0;
+        for (size_t i = 0; i < g.size(); i++) {
+            const Lcurve::Point &p = g[i];
+            posn[3 * i] = p.posn.x(); posn[3 * i + 1] = p.posn.y(); posn[3 * i + 2] = p.posn.z();
+            dirn[3 * i] = p.dirn.x(); dirn[3 * i + 1] = p.dirn.y(); dirn[3 * i + 2] = p.dirn.z();
+            area[i] = p.area; flux[i] = p.flux;
+            nr[i] = (int32_t)p.eclipse.size();
+            for (int k = 0; k < maxr && k < (int)p.eclipse.size(); k++) {
+                rin[maxr * i + k] = p.eclipse[k].first;
+                rout[maxr * i + k] = p.eclipse[k].second;
+            }
         }
         return 0;
     } catch (const Lcurve::Lcurve_Error &ex) {

@@ -58,6 +58,27 @@ def small_cases():
     return cases
 
 
+def disc_cases():
+    """Cataclysmic-variable components (set_disc_grid.cpp, set_bright_spot_grid.cpp,
+    disc_eclipse.cpp, light_curve_comp.cpp:272-333, 378-414, 511-556): disc and
+    rim with and without an opaque disc, the bright spot, iscale fits (with and
+    without the donor's column), spherical stars, sub-exposures."""
+    small = dict(nlat1f=16, nlat2f=24, nrad=16, nspot=20)
+    cases = [
+        ("disc_rim", W.cv_disc(opaque=0, add_spot=0, **small), _d(150)),
+        ("disc_opaque", W.cv_disc(add_spot=0, **small), _d(150)),
+        ("disc_spot", W.cv_disc(**small), _d(150)),
+        ("spot_only", W.cv_disc(add_disc=0, **small), _d(150)),
+        ("iscale", W.cv_disc(iscale=1, **small), _d(150)),
+        ("iscale_no_donor", W.cv_disc(iscale=1, t2=-3000.0, **small), _d(150)),
+        ("disc_spheres", W.cv_disc(roche1=0, roche2=0, **small), _d(150)),
+        ("disc_ndiv", W.cv_disc(**small), _d(60, ndiv=5, expose=0.01)),
+    ]
+    for _, m, d in cases:
+        d["flux"] = 1.0 + 0.01 * np.sin(np.arange(len(d)))
+    return cases
+
+
 def glens_case():
     # lensing needs a spherical star 1 (Model ctor rule, model.cpp:331-332)
     return ("lensing", W.model(nlat1f=20, nlat2f=40, roche1=0, glens1=1, eclipse2=0,

@@ -86,6 +86,29 @@ class _Lib:
         st = fn(C.byref(m), d.ctypes.data, n, flags, max_pts, _d(sf), _d(calc), _d(sc), err, 512)
         return st, err.value.decode(), calc, sf, sc
 
+    def components(self, model, which, maxr=4):
+        """One component grid (0 disc, 1 disc edge, 2 bright spot) with its
+        continuum: (status, message, dict of per-element arrays)."""
+        m = model.to_c() if hasattr(model, "to_c") else model
+        fn = getattr(self.lib, self.prefix + "components")
+        fn.restype = C.c_int
+        fn.argtypes = [M, C.c_int32, C.c_int32, C.c_int32, I32, D, D, F, F, I32, D, D,
+                       C.c_char_p, C.c_int]
+        err = C.create_string_buffer(512)
+        n = C.c_int32(0)
+        st = fn(C.byref(m), which, 0, maxr, C.byref(n), None, None, None, None, None, None,
+                None, err, 512)
+        if st:
+            return st, err.value.decode(), None
+        k = n.value
+        g = dict(posn=np.zeros((k, 3)), dirn=np.zeros((k, 3)), area=np.zeros(k, np.float32),
+                 flux=np.zeros(k, np.float32), nr=np.zeros(k, np.int32),
+                 rin=np.zeros((k, maxr)), rout=np.zeros((k, maxr)))
+        st = fn(C.byref(m), which, k, maxr, C.byref(n), _d(g["posn"]), _d(g["dirn"]),
+                g["area"].ctypes.data_as(F), g["flux"].ctypes.data_as(F),
+                g["nr"].ctypes.data_as(I32), _d(g["rin"]), _d(g["rout"]), err, 512)
+        return st, err.value.decode(), g
+
     def sum_star_multi(self, star, flat, phases, ldc, ltype, mucrit=0.0, beam=0.0, spin=1.0,
                        vfac=0.0, xcofm=0.0, glens1=False, rlens1=0.0):
         cols = [np.ascontiguousarray(flat[k], dtype=np.float64)

@@ -175,11 +175,10 @@ def test_cache_reuse(engine_mixed):
 def test_errors(engine_mixed):
     with pytest.raises(LcurveError, match="larger than its Roche lobe"):
         engine_mixed.light_curve_comp(W.model(nlat1f=8, nlat2f=8, r2=0.5), W.data(10))
-    m = W.model(nlat1f=8, nlat2f=8)
-    m["add_disc"] = True
+    m = W.cv_disc(nlat1f=8, nlat2f=8, nrad=0)
     with pytest.raises(LcurveError) as ei:
         engine_mixed.light_curve_comp(m, W.data(10))
-    assert ei.value.status == 5
+    assert ei.value.status == 1  # a disc needs nrad >= 1
     # a failure leaves the context usable
     calc = engine_mixed.light_curve_comp(W.model(nlat1f=8, nlat2f=8), W.data(10))[0]
     assert np.all(np.isfinite(calc))
