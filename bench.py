@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", default="wd_dm_large",
                     choices=("wd_dm_large", "wd_dm_small", "tiny_star", "mcmc_batch",
-                             "surrogate_da"))
+                             "surrogate_da", "cv_disc"))
     ap.add_argument("--batch-models", type=int, default=256,
                     help="models per step of mcmc_batch (256 is the benchmark)")
     ap.add_argument("--train-curves", type=int, default=200000)
@@ -66,6 +66,9 @@ def parse():
     ap.add_argument("--precision", choices=("mixed", "fp64"), default="mixed")
     ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--eclipse-warp", type=int, default=0,
+                    help="Roche eclipse candidates up to which one warp bisects each face "
+                         "(0 automatic, -1 never)")
     return ap.parse_args()
 
 
@@ -77,6 +80,11 @@ def workload(name):
     elif name == "wd_dm_small":
         m, d = W.wd_dm_small()
         desc = "wd_dm_small: WD+dM q=0.25 i=86 r1=0.015 r2=0.20, nlat 40/80, 500 pts"
+    elif name == "cv_disc":
+        m = W.cv_disc(nlat1f=100, nlat2f=200, nrad=60, nspot=100)
+        d = W.data(2000)
+        desc = ("cv_disc: WD + Roche-filling donor q=0.15 i=84, opaque flared disc 0.03-0.3 "
+                "(nrad 60) with its rim, bright spot (nspot 100), nlat 100/200, 2000 pts")
     else:
         m, d = W.tiny_star()
         desc = "tiny_star: r1=0.005 q=0.2 i=87, nlat 400/200, 10000 pts in +-0.03"
@@ -145,9 +153,15 @@ class RefTimer:
     Bounded sample: one light curve costs t_grid + frac * t_sample, where
     t_grid is a cold call on 1 point (the geometry perturbed by 1e-13 so the
     reference's grid cache misses: grids, eclipses, continuum, FlatGrids) and
-    t_sample a warm call (cache hit) on 1/frac of the points."""
+    t_sample a warm call (cache hit) on 1/frac of the points. A model with an
+    opaque disc bypasses the reference's cache (light_curve_comp.cpp:163) and
+    rebuilds its disc every call, so each timed call is a whole light curve
+    (frac 1, no separate grid term)."""
 
     def __init__(self, model, data, frac=50):
+        self.full = bool(model["add_disc"] or model["add_spot"])
+        if self.full:
+            frac = 1
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         import oracle_lib as OL
         self.kind = "reference"
@@ -169,6 +183,9 @@ class RefTimer:
             raise RuntimeError(err)
 
     def cold_grid(self, reps=3):
+        if self.full:
+            self.t_grid = 0.0
+            return 0.0
         ts = []
         for _ in range(reps):
             self.k += 1
@@ -187,6 +204,9 @@ class RefTimer:
         return time.perf_counter() - t
 
     def describe(self, reps, t_curve):
+        if self.full:
+            return ("whole light curves (%d points; grids, disc, rim and spot rebuilt each call); "
+                    "%d calls; one light curve = %.3f s" % (self.n, reps, t_curve))
         return ("every %dth point (%d of %d) per timed call (warm grids), x%.0f, plus a cold 1-point call for "
                 "grids+eclipses+continuum (%.3f s); %d calls; one light curve = %.3f s"
                 % (round(self.frac), self.ns, self.n, self.frac, self.t_grid, reps, t_curve))
@@ -242,7 +262,7 @@ def run_ours(args):
     from lcurve_re_b200.engine import Engine
 
     model, data, desc = workload(args.workload)
-    eng = Engine(device=local, precision=args.precision)
+    eng = Engine(device=local, precision=args.precision, eclipse_warp=args.eclipse_warp)
     lib, ctx = eng.lib, eng.ctx
     # synthetic noisy data from the model itself (seeded per rank)
     calc0 = eng.light_curve_comp(model, data, scale=False, rdata=False, diagnostics=False)[0]

@@ -6,9 +6,10 @@
 // and star_eclipse (star_eclipse.cpp:15-26) with one thread per element: the
 // per-ring and per-model scalars come from the host, the trigonometry, the
 // continuum and the eclipse solves run on the device. Element sums per phase
-// entry follow comp_disc / comp_edge / comp_spot (comp_light.cpp:323-408): a
-// serial sum over the elements in vector order, so with the same elements and
-// phases the result is the reference's. Compiled with --fmad=false.
+// entry follow comp_disc / comp_edge / comp_spot (comp_light.cpp:323-408) with
+// the elements in vector order, summed in chunks of 256 whose partial sums
+// are added in order (the reference's single serial sum, regrouped: equal to
+// rounding). Compiled with --fmad=false.
 #include "context.h"
 #include "eclipse.cuh"
 
@@ -30,6 +31,9 @@ __device__ __forceinline__ int elem_tag(int i) { return -1 - i; }
 // spot gets none, set_bright_spot_grid.cpp:80-81), then star 1's, then star
 // 2's (set_disc_grid.cpp:99-113). trap1: a Roche_Error from star 1 becomes
 // the range (0, 1), as for the rim's upper elements (set_disc_grid.cpp:222-231).
+// One thread solves all of an element's eclipses: nearly every disc element is
+// a Roche candidate of the donor, and a warp per candidate (as for star grids
+// with few candidates) measured slower here.
 __device__ void elem_eclipses(const CompParams &p, V3 posn, bool opaque, bool trap1, ElemRec &r,
                               DevStatus *st, int idx) {
     r.nr = 0;  // an element whose eclipse failed is left with none
@@ -169,23 +173,25 @@ __global__ void k_disc_faces(DiscGeom dg, GridDev g, uint8_t *ndx, double2 *xr, 
         xr[kDiscRanges * i + k] = k < nr ? make_double2(rin[k], rout[k]) : make_double2(0., 0.);
 }
 
-// One thread per phase entry; elements staged through shared memory in tiles
-// (every thread reads the same element: a broadcast).
-constexpr int kTile = 64;
+// One CTA per (tile of phase entries, chunk of kElemChunk elements): each
+// thread sums the chunk's elements in order for its entry (the chunk staged in
+// shared memory, every thread reading the same element: a broadcast) and
+// writes three partial sums; k_comp_reduce adds the chunks in order.
+constexpr int kElemChunk = 256;
 
 __global__ void __launch_bounds__(kThreadsC) k_comp_sums(const ElemRec *__restrict__ el,
                                                          int32_t nd, int32_t ne, int32_t n,
                                                          double lin, double quad, PhaseDev ph,
-                                                         double *out, int64_t ldc) {
-    __shared__ ElemRec tile[kTile];
+                                                         double *part, int64_t ldc) {
+    __shared__ ElemRec tile[kElemChunk];
     const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const bool ok = e < ph.nent;
     const double ex = ok ? ph.ex[e] : 0., ey = ok ? ph.ey[e] : 0., ez = ok ? ph.ez[e] : 0.;
     const double phi = ok ? ph.phin[e] : 0.;
     double s[3] = {0.0, 0.0, 0.0};
-    for (int base = 0; base < n; base += kTile) {
-        const int m = (n - base < kTile) ? n - base : kTile;
-        __syncthreads();
+    {
+        const int base = blockIdx.y * kElemChunk;
+        const int m = (n - base < kElemChunk) ? n - base : kElemChunk;
         for (int t = threadIdx.x; t < m; t += blockDim.x) tile[t] = el[base + t];
         __syncthreads();
         for (int t = 0; t < m; t++) {
@@ -213,10 +219,27 @@ __global__ void __launch_bounds__(kThreadsC) k_comp_sums(const ElemRec *__restri
         }
     }
     if (ok) {
-        out[e] = s[0];
-        out[ldc + e] = s[1];
-        out[2 * ldc + e] = s[2];
+        double *row = part + 3 * (int64_t)blockIdx.y * ldc;
+        row[e] = s[0];
+        row[ldc + e] = s[1];
+        row[2 * ldc + e] = s[2];
     }
+}
+
+__global__ void k_comp_reduce(const double *__restrict__ part, int nchunk, int64_t nent,
+                              double *out, int64_t ldc) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= nent) return;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+    for (int c = 0; c < nchunk; c++) {
+        const double *row = part + 3 * (int64_t)c * ldc;
+        s0 += row[e];
+        s1 += row[ldc + e];
+        s2 += row[2 * ldc + e];
+    }
+    out[e] = s0;
+    out[ldc + e] = s1;
+    out[2 * ldc + e] = s2;
 }
 
 // ---- iscale -------------------------------------------------------------------
@@ -385,12 +408,23 @@ void launch_disc_faces(const DiscGeom &dg, const GridDev &g, uint8_t *ndx, doubl
     count_launch();
 }
 
+int64_t comp_sums_scratch(int32_t n, int64_t ldc) {
+    return 3 * (int64_t)((n + kElemChunk - 1) / kElemChunk) * ldc;
+}
+
 void launch_comp_sums(const ElemRec *el, int32_t nd, int32_t ne, int32_t n, double lin,
-                      double quad, const PhaseDev &ph, double *out, int64_t ldc,
+                      double quad, const PhaseDev &ph, double *part, double *out, int64_t ldc,
                       cudaStream_t s) {
     if (ph.nent <= 0) return;
-    k_comp_sums<<<nblk(ph.nent, kThreadsC), kThreadsC, 0, s>>>(el, nd, ne, n, lin, quad, ph, out,
-                                                               ldc);
+    const int nchunk = (n + kElemChunk - 1) / kElemChunk;
+    if (nchunk == 0) {
+        cudaMemsetAsync(out, 0, 3 * ldc * sizeof(double), s);
+        return;
+    }
+    k_comp_sums<<<dim3(nblk(ph.nent, kThreadsC), nchunk), kThreadsC, 0, s>>>(el, nd, ne, n, lin,
+                                                                             quad, ph, part, ldc);
+    count_launch();
+    k_comp_reduce<<<nblk(ph.nent, 256), 256, 0, s>>>(part, nchunk, ph.nent, out, ldc);
     count_launch();
 }
 

@@ -173,6 +173,10 @@ struct lcg_ctx {
     DBuf<lcg::DiscRing> drings;
     DBuf<double> csum, fcomp, iwork;
     lcg::CompParams comp{};
+    // second stream: the component elements (latency-bound eclipse solves)
+    // run beside the star grids; created on first use
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     std::vector<int64_t> h_off;
     std::vector<double> h_diag;
     // resident light-curve points (lcg_set_data)

@@ -688,8 +688,16 @@ void lcg_destroy(lcg_ctx *c) {
     c->status.release(); c->queue.release(); c->counters.release(); c->blockcnt.release();
     c->data.release(); c->off.release(); c->pef.release(); c->ptype.release();
     c->fdata.release(); c->fidx.release(); c->fcalc.release(); c->fout.release();
+    c->elem.release(); c->epos.release(); c->drings.release(); c->csum.release();
+    c->fcomp.release(); c->iwork.release();
     batch_release(c->batch);
     c->batch = nullptr;
+    if (c->side) {
+        cudaStreamSynchronize(c->side);
+        cudaStreamDestroy(c->side);
+        cudaEventDestroy(c->ev_fork);
+        cudaEventDestroy(c->ev_join);
+    }
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -880,9 +888,15 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
     }
 
     // disc, rim and bright-spot elements (set_disc_grid, set_disc_edge,
-    // set_bright_spot_grid with their continua), rebuilt every call
+    // set_bright_spot_grid with their continua), rebuilt every call on the
+    // side stream, beside the star grids; joined before the component sums
     int32_t ncomp = 0;
     if (comps) {
+        if (!c->side &&
+            ((e = cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking)) ||
+             (e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming)) ||
+             (e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming))))
+            return c->cuda_fail(e, "side stream");
         std::vector<DiscRing> rings;
         Fail f{0, ""};
         if (!comp_setup(m, c->comp, rings, f)) return c->fail(f.code, "%s", f.msg.c_str());
@@ -890,12 +904,14 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
         if ((e = c->elem.ensure(ncomp)) || (e = c->epos.ensure(ncomp)) ||
             (e = c->drings.ensure(rings.size())))
             return c->cuda_fail(e, "component elements");
+        cudaEventRecord(c->ev_fork, c->stream);  // after the status reset
+        cudaStreamWaitEvent(c->side, c->ev_fork, 0);
         if (!rings.empty())
             cudaMemcpyAsync(c->drings.p, rings.data(), rings.size() * sizeof(DiscRing),
-                            cudaMemcpyHostToDevice, c->stream);
+                            cudaMemcpyHostToDevice, c->side);
         c->comp.rings = c->drings.p;
-        StageScope t(c, LCG_STAGE_GRID);
-        launch_components(c->comp, c->elem.p, c->epos.p, c->status.p, c->stream);
+        launch_components(c->comp, c->elem.p, c->epos.p, c->status.p, c->side);
+        cudaEventRecord(c->ev_join, c->side);
         if ((flags & LCG_FLAG_INFO) && m.add_disc)
             fprintf(stderr, "Number of points for the disc = %d\n", c->comp.nd);
     }
@@ -1031,12 +1047,14 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
         c->flux_elements += s.g->n * s.nent;
     }
     if (comps) {
-        if ((e = c->csum.ensure(3 * (size_t)ldp))) return c->cuda_fail(e, "component sums");
+        if ((e = c->csum.ensure(3 * (size_t)ldp + (size_t)comp_sums_scratch(ncomp, ldp))))
+            return c->cuda_fail(e, "component sums");
         PhaseDev phc = ph;
         phc.nent = nent;
+        cudaStreamWaitEvent(c->stream, c->ev_join, 0);
         StageScope t(c, LCG_STAGE_FLUX);
         launch_comp_sums(c->elem.p, c->comp.nd, c->comp.ne, ncomp, m.lin_limb_disc,
-                         m.quad_limb_disc, phc, c->csum.p, ldp, c->stream);
+                         m.quad_limb_disc, phc, c->csum.p + 3 * ldp, c->csum.p, ldp, c->stream);
     }
 
     // scatter, third light, scale, chi**2

@@ -348,9 +348,11 @@ void launch_components(const CompParams &p, ElemRec *el, double4 *pos, DevStatus
 void launch_disc_faces(const DiscGeom &dg, const GridDev &g, uint8_t *ndx, double2 *xr,
                        DevStatus *st, cudaStream_t s);
 // Per phase entry, the disc, rim and spot element sums (comp_light.cpp:323-408)
-// into rows 0, 1, 2 of out (row stride ldc).
+// into rows 0, 1, 2 of out (row stride ldc); part holds comp_sums_scratch
+// doubles (per-chunk partial sums, added in chunk order).
+int64_t comp_sums_scratch(int32_t n, int64_t ldc);
 void launch_comp_sums(const ElemRec *el, int32_t nd, int32_t ne, int32_t n, double lin,
-                      double quad, const PhaseDev &ph, double *out, int64_t ldc,
+                      double quad, const PhaseDev &ph, double *part, double *out, int64_t ldc,
                       cudaStream_t s);
 // iscale: per-component scale factors by least squares (svdfit.cpp:22-80) from
 // fcomp (5 per point; nc = 5 with star 2's column, else 4), or the given sfac
