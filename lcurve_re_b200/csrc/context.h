@@ -57,6 +57,7 @@ struct Grid {
     DBuf<float> area, grav, flux;
     DBuf<uint8_t> necl;
     DBuf<RingRec> rings;
+    DBuf<int32_t> queue, counters;  // eclipse candidates of this grid
     // flat
     DBuf<int64_t> n0;
     DBuf<float4> geo, pos;
@@ -122,6 +123,7 @@ struct Grid {
                              &fdz, &fpx, &fpy, &fpz, &fflux, &fin, &fout};
         for (auto *b : d) b->release();
         area.release(); grav.release(); flux.release(); necl.release(); rings.release();
+        queue.release(); counters.release();
         n0.release(); geo.release(); pos.release(); ecl.release(); fp.release();
         runb.release(); ndx.release(); rn.release(); xr.release(); rr.release(); ridx.release();
         disc = false;
@@ -173,10 +175,11 @@ struct lcg_ctx {
     DBuf<lcg::DiscRing> drings;
     DBuf<double> csum, fcomp, iwork;
     lcg::CompParams comp{};
-    // second stream: the component elements (latency-bound eclipse solves)
-    // run beside the star grids; created on first use
-    cudaStream_t side = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    // side streams: star 2's grids (side[0]) and the component elements
+    // (side[1]) run beside star 1's; their eclipse solves are latency-bound,
+    // so they overlap well. Created by the first call.
+    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
     std::vector<int64_t> h_off;
     std::vector<double> h_diag;
     // resident light-curve points (lcg_set_data)

@@ -406,8 +406,10 @@ FluxConsts flux_consts(const lcg_model &m, int star, double spin, double rlens1)
     return k;
 }
 
-// Grid + eclipse (+ nothing else): the geometry stage of one star grid.
-lcg_status build_geometry(lcg_ctx *c, const lcg_model &m, int star, int fine, Grid &g) {
+// Grid + eclipse (+ nothing else): the geometry stage of one star grid, on
+// stream st (the grid's own candidate queue, so two grids can build at once).
+lcg_status build_geometry(lcg_ctx *c, const lcg_model &m, int star, int fine, Grid &g,
+                          cudaStream_t st) {
     Fail f{0, ""};
     if (!prepare_star(m, star, fine, g.setup, f)) return c->fail(f.code, "%s", f.msg.c_str());
     const StarSetup &s = g.setup;
@@ -416,7 +418,7 @@ lcg_status build_geometry(lcg_ctx *c, const lcg_model &m, int star, int fine, Gr
     g.ntiled = s.ntiled;
     if ((e = g.rings.ensure(s.rings.size())) != cudaSuccess) return c->cuda_fail(e, "rings");
     cudaMemcpyAsync(g.rings.p, s.rings.data(), s.rings.size() * sizeof(RingRec),
-                    cudaMemcpyHostToDevice, c->stream);
+                    cudaMemcpyHostToDevice, st);
     GridParams gp{};
     gp.star = star;
     gp.roche = star == kStar1 ? m.roche1 : m.roche2;
@@ -432,9 +434,10 @@ lcg_status build_geometry(lcg_ctx *c, const lcg_model &m, int star, int fine, Gr
     gp.rad_sphere = star == kStar1 ? s.r1 : s.r2;
     {
         StageScope t(c, LCG_STAGE_GRID);
-        launch_grid(gp, g.rings.p, g.dev(), c->status.p, c->stream);
+        launch_grid(gp, g.rings.p, g.dev(), c->status.p, st);
     }
-    if ((e = c->queue.ensure(s.nface)) != cudaSuccess) return c->cuda_fail(e, "queue");
+    if ((e = g.queue.ensure(s.nface)) || (e = g.counters.ensure(2)))
+        return c->cuda_fail(e, "queue");
     EclParams ep{};
     ep.comp_star = star == kStar1 ? kStar2 : kStar1;
     ep.comp_roche = star == kStar1 ? m.roche2 : m.roche1;
@@ -449,8 +452,8 @@ lcg_status build_geometry(lcg_ctx *c, const lcg_model &m, int star, int fine, Gr
     ep.delta = m.delta_phase;
     {
         StageScope t(c, LCG_STAGE_ECLIPSE);
-        launch_eclipse(ep, s.eclipse, g.dev(), c->queue.p, c->counters.p, c->status.p, c->nsm,
-                       c->eclipse_warp, c->stream);
+        launch_eclipse(ep, s.eclipse, g.dev(), g.queue.p, g.counters.p, c->status.p, c->nsm,
+                       c->eclipse_warp, st);
     }
     return LCG_OK;
 }
@@ -657,6 +660,11 @@ lcg_status lcg_create(lcg_ctx **out, const lcg_options *opt) {
     c->eclipse_warp = o.eclipse_warp;
     c->nsm = prop.multiProcessorCount;
     if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&c->side[0], cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&c->side[1], cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&c->ev_join[0], cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&c->ev_join[1], cudaEventDisableTiming)) != cudaSuccess ||
         (e = c->status.ensure(1)) != cudaSuccess || (e = c->counters.ensure(2)) != cudaSuccess ||
         (e = c->sfac.ensure(8)) != cudaSuccess || (e = c->out.ensure(4)) != cudaSuccess) {
         g_create_error = cudaGetErrorString(e);
@@ -692,12 +700,13 @@ void lcg_destroy(lcg_ctx *c) {
     c->fcomp.release(); c->iwork.release();
     batch_release(c->batch);
     c->batch = nullptr;
-    if (c->side) {
-        cudaStreamSynchronize(c->side);
-        cudaStreamDestroy(c->side);
-        cudaEventDestroy(c->ev_fork);
-        cudaEventDestroy(c->ev_join);
-    }
+    for (int k = 0; k < 2; k++)
+        if (c->side[k]) {
+            cudaStreamSynchronize(c->side[k]);
+            cudaStreamDestroy(c->side[k]);
+            cudaEventDestroy(c->ev_join[k]);
+        }
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -864,18 +873,23 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
     const bool opaque = m.add_disc && m.opaque;
     const bool iscale = m.iscale != 0;
     cudaMemsetAsync(c->status.p, 0, sizeof(DevStatus), c->stream);
+    cudaEventRecord(c->ev_fork, c->stream);  // side-stream work starts here
 
     // geometry (GeomKey)
     const bool geom_hit = c->has_geom && !(flags & LCG_FLAG_NO_CACHE) && same_geometry(c->key, m);
     if (!geom_hit) {
         c->has_geom = c->has_cont = false;
-        if ((rc = build_geometry(c, m, kStar1, 1, c->g1f))) return rc;
-        if ((rc = build_geometry(c, m, kStar2, 1, c->g2f))) return rc;
+        // star 2's grids on side[0], beside star 1's (joined before the continuum)
+        cudaStreamWaitEvent(c->side[0], c->ev_fork, 0);
+        if ((rc = build_geometry(c, m, kStar1, 1, c->g1f, c->stream))) return rc;
+        if ((rc = build_geometry(c, m, kStar2, 1, c->g2f, c->side[0]))) return rc;
         c->copy1 = (m.nlat1f == m.nlat1c);
         c->copy2 = (m.nlat2f == m.nlat2c) &&
                    (!m.npole || r1 >= r2 || (m.nlatfill == 0 && m.nlngfill == 0));
-        if (!c->copy1 && (rc = build_geometry(c, m, kStar1, 0, c->g1c))) return rc;
-        if (!c->copy2 && (rc = build_geometry(c, m, kStar2, 0, c->g2c))) return rc;
+        if (!c->copy1 && (rc = build_geometry(c, m, kStar1, 0, c->g1c, c->stream))) return rc;
+        if (!c->copy2 && (rc = build_geometry(c, m, kStar2, 0, c->g2c, c->side[0]))) return rc;
+        cudaEventRecord(c->ev_join[0], c->side[0]);
+        cudaStreamWaitEvent(c->stream, c->ev_join[0], 0);
     }
     Grid &g1f = c->g1f, &g2f = c->g2f;
     Grid &g1c = c->copy1 ? c->g1f : c->g1c;
@@ -892,11 +906,7 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
     // side stream, beside the star grids; joined before the component sums
     int32_t ncomp = 0;
     if (comps) {
-        if (!c->side &&
-            ((e = cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking)) ||
-             (e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming)) ||
-             (e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming))))
-            return c->cuda_fail(e, "side stream");
+
         std::vector<DiscRing> rings;
         Fail f{0, ""};
         if (!comp_setup(m, c->comp, rings, f)) return c->fail(f.code, "%s", f.msg.c_str());
@@ -904,14 +914,13 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
         if ((e = c->elem.ensure(ncomp)) || (e = c->epos.ensure(ncomp)) ||
             (e = c->drings.ensure(rings.size())))
             return c->cuda_fail(e, "component elements");
-        cudaEventRecord(c->ev_fork, c->stream);  // after the status reset
-        cudaStreamWaitEvent(c->side, c->ev_fork, 0);
+        cudaStreamWaitEvent(c->side[1], c->ev_fork, 0);
         if (!rings.empty())
             cudaMemcpyAsync(c->drings.p, rings.data(), rings.size() * sizeof(DiscRing),
-                            cudaMemcpyHostToDevice, c->side);
+                            cudaMemcpyHostToDevice, c->side[1]);
         c->comp.rings = c->drings.p;
-        launch_components(c->comp, c->elem.p, c->epos.p, c->status.p, c->side);
-        cudaEventRecord(c->ev_join, c->side);
+        launch_components(c->comp, c->elem.p, c->epos.p, c->status.p, c->side[1]);
+        cudaEventRecord(c->ev_join[1], c->side[1]);
         if ((flags & LCG_FLAG_INFO) && m.add_disc)
             fprintf(stderr, "Number of points for the disc = %d\n", c->comp.nd);
     }
@@ -1051,7 +1060,7 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
             return c->cuda_fail(e, "component sums");
         PhaseDev phc = ph;
         phc.nent = nent;
-        cudaStreamWaitEvent(c->stream, c->ev_join, 0);
+        cudaStreamWaitEvent(c->stream, c->ev_join[1], 0);
         StageScope t(c, LCG_STAGE_FLUX);
         launch_comp_sums(c->elem.p, c->comp.nd, c->comp.ne, ncomp, m.lin_limb_disc,
                          m.quad_limb_disc, phc, c->csum.p + 3 * ldp, c->csum.p, ldp, c->stream);
@@ -1267,7 +1276,7 @@ lcg_status lcg_star_grid(lcg_ctx *c, const lcg_model *m, int32_t star, int32_t f
     cudaMemsetAsync(c->status.p, 0, sizeof(DevStatus), c->stream);
     c->has_geom = c->has_cont = false;  // this call reuses the cache's grid slot
     Grid &g = star == kStar1 ? c->g1c : c->g2c;
-    if ((rc = build_geometry(c, *m, star, fine, g))) return rc;
+    if ((rc = build_geometry(c, *m, star, fine, g, c->stream))) return rc;
     if (g.n != nface)
         return c->fail(LCG_E_INVALID, "nface = %d but the grid has %lld faces", nface,
                        (long long)g.n);
