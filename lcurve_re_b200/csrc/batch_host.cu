@@ -100,6 +100,8 @@ struct BatchState {
     DBuf<int32_t> blockcnt, queue, counters;
     DBuf<DevStatus> st;
     DBuf<float4> ef, runb;
+    DBuf<double4> es;
+    DBuf<uint8_t> ehit;
     DBuf<double> w1, w2, part, osum, calc, sfac, out;
     // results (pinned): calc, sfac, out, status
     unsigned char *h_res = nullptr;
@@ -128,7 +130,7 @@ struct BatchState {
         for (auto *b : d) b->release();
         area.release(); grav.release(); flux.release(); fp.release(); necl.release();
         ecl.release(); n0.release(); blockcnt.release(); queue.release(); counters.release();
-        st.release(); ef.release(); runb.release(); rings.release(); d_tab.release();
+        st.release(); ef.release(); runb.release(); rings.release(); es.release(); ehit.release(); d_tab.release();
         rows.release(); gathered.release();
         if (h_rows) cudaFreeHost(h_rows);
         h_rows = nullptr;
@@ -157,6 +159,8 @@ struct BatchState {
         b.blockcnt = blockcnt.p;
         b.queue = queue.p;
         b.counters = counters.p;
+        b.es = es.p;
+        b.ehit = ehit.p;
         b.st = st.p;
         b.counts = reinterpret_cast<const int32_t *>(d + o_counts);
         b.geo_slot = reinterpret_cast<const int32_t *>(d + o_geo_slot);
@@ -307,7 +311,8 @@ lcg_status relayout(lcg_ctx *c, BatchState &B, const lcg_model *models, int32_t 
         (e = B.fp.ensure(8 * (size_t)B.nflat)) || (e = B.ecl.ensure((size_t)B.nflat)) ||
         (e = B.runb.ensure((size_t)B.nflat / 64)) ||
         (e = B.n0.ensure(ns)) || (e = B.blockcnt.ensure((size_t)B.nblk)) ||
-        (e = B.counters.ensure(2)) || (e = B.st.ensure(nm)) ||
+        (e = B.counters.ensure(4)) || (e = B.st.ensure(nm)) ||
+        (e = B.es.ensure(nf)) || (e = B.ehit.ensure(nf)) ||
         (e = B.ef.ensure(nm * (size_t)B.ldp)) || (e = B.w1.ensure(nm * (size_t)B.ldp)) ||
         (e = B.w2.ensure(nm * (size_t)B.ldp)) ||
         (e = B.part.ensure((size_t)std::max<int64_t>(B.plan.nchunk, 1) * (size_t)B.ldp)) ||

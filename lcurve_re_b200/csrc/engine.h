@@ -198,7 +198,11 @@ struct BatchDev {
     float4 *runb;  // FlatDev::runb per slot, from flat0 / 64
     uint2 *ecl;
     int64_t *n0;  // per slot
-    int32_t *blockcnt, *queue, *counters;
+    int32_t *blockcnt, *queue, *counters;  // counters: 4 work counters
+    // eclipse candidates between the two passes of the thread mode: per queue
+    // entry (phase of the potential minimum, phi1, phi2, ACC) and a hit flag
+    double4 *es;
+    uint8_t *ehit;
     DevStatus *st;  // per model
     // work lists: counts[0] geometry slots, counts[1] continuum slots; each
     // list has its slots and prefix sums (count + 1 entries) of its units
@@ -231,9 +235,11 @@ struct BatchPhases {
 // ---- launchers (geometry.cu) ------------------------------------------------
 void launch_grid(const GridParams &p, const RingRec *rings, GridDev g, DevStatus *st,
                  cudaStream_t s);
+// queue: one int per face; counters: 4 work counters; es / ehit: per-candidate
+// state between the thread mode's two passes (one per face).
 void launch_eclipse(const EclParams &p, int32_t eclipse_on, GridDev g, int32_t *queue,
-                    int32_t *counters, DevStatus *st, int nsm, int32_t warp_mode,
-                    cudaStream_t s);
+                    int32_t *counters, double4 *es, uint8_t *ehit, DevStatus *st, int nsm,
+                    int32_t warp_mode, cudaStream_t s);
 void launch_continuum(const ContParams &p, GridDev g, cudaStream_t s);
 void launch_flatten(GridDev g, FlatDev f, int32_t *blockcnt, int mixed, int need_pos,
                     const FastCoef &fc, DevStatus *st, cudaStream_t s);

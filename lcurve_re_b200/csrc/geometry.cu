@@ -152,10 +152,11 @@ __global__ void k_ecl_pre(EclParams p, int32_t eclipse_on, GridDev g, int32_t *q
 
 // Ingress/egress of the queued candidates. Up to warp_max candidates, one
 // warp bisects each face (ingress_egress_warp): few candidates leave most of
-// the GPU idle otherwise. Beyond that, one thread per face, each warp taking
-// 32 consecutive candidates at a time so that neighbouring faces (similar
-// iteration counts) run in lockstep. The count is read on the device, so the
-// choice needs no host round trip.
+// the GPU idle otherwise. Beyond that, k_ecl_potmin and k_ecl_bisect take
+// over (one thread per candidate, each warp taking 32 consecutive candidates
+// at a time so that neighbouring faces, with similar iteration counts, run in
+// lockstep) and this kernel returns at once. The count is read on the device,
+// so the choice needs no host round trip.
 __global__ void __launch_bounds__(128, 4) k_ecl_roche(EclParams p, GridDev g,
                                                    const int32_t *__restrict__ queue,
                                                    int32_t *counters, DevStatus *st,
@@ -188,24 +189,94 @@ __global__ void __launch_bounds__(128, 4) k_ecl_roche(EclParams p, GridDev g,
         }
         return;
     }
+}
+
+// Thread mode (more candidates than warp_max), in two passes with a small code
+// footprint each, as for the batch (k_ecl_potmin_b / k_ecl_bisect_b): the
+// sphere test and pot_min per candidate, then ingress and egress on the two
+// lanes of a pair. es / ehit hold each candidate's state between the passes.
+__global__ void __launch_bounds__(128, 4) k_ecl_potmin(EclParams p, GridDev g,
+                                                    const int32_t *__restrict__ queue,
+                                                    int32_t *counters, double4 *es, uint8_t *ehit,
+                                                    DevStatus *st, int32_t warp_max) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int total = counters[0];
+    if (total <= warp_max) return;
+    const V3 cofm = p.comp_star == kStar1 ? v3(0., 0., 0.) : v3(1., 0., 0.);
     for (;;) {
         int base = 0;
-        if (lane == 0) base = atomicAdd(&counters[1], 32);
+        if (lane == 0) base = atomicAdd(&counters[2], 32);
         base = __shfl_sync(full, base, 0);
         if (base >= total) break;
         const int k = base + lane;
-        if (k < total) {
-            const int32_t i = queue[k];
-            const V3 pos = v3(g.px[i], g.py[i], g.pz[i]);
-            double ing = 0., egr = 0.;
+        if (k >= total) continue;
+        const int32_t i = queue[k];
+        const V3 pos = v3(g.px[i], g.py[i], g.pz[i]);
+        double phi1, phi2, lam1, lam2, phi = 0., lam = 0.;
+        uint8_t hit = 0;
+        if (sphere_eclipse_ph(p.cosi, p.sini, pos, cofm, p.comp_rref, phi1, phi2, lam1, lam2)) {
+            const double ACC = 2. * sqrt(2. * kTwoPi * (lam2 - lam1) * p.delta);
             int s = 0;
-            bool ecl = ingress_egress(p.comp_star, p.q, p.comp_spin, p.cosi, p.sini, p.delta, pos,
-                                      p.comp_rref, p.comp_pref, ing, egr, s);
+            hit = pot_min(p.comp_star, p.q, p.comp_spin, p.cosi, p.sini, pos, phi1, phi2, lam1,
+                          lam2, p.comp_rref, p.comp_pref, ACC, phi, lam, s);
             if (s) {
                 set_status(st, s, i);
-            } else if (ecl) {
+                hit = 0;
+            }
+            es[k] = make_double4(phi, phi1, phi2, ACC);
+        }
+        ehit[k] = hit;
+    }
+}
+
+__global__ void __launch_bounds__(128, 4) k_ecl_bisect(EclParams p, GridDev g,
+                                                    const int32_t *__restrict__ queue,
+                                                    int32_t *counters, const double4 *es,
+                                                    const uint8_t *ehit, DevStatus *st,
+                                                    int32_t warp_max) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const unsigned pair = 3u << (lane & ~1);
+    const int total = counters[0];
+    if (total <= warp_max) return;
+    const int64_t n2 = 2 * (int64_t)total;
+    for (;;) {
+        int64_t base = 0;
+        if (lane == 0) base = atomicAdd(&counters[3], 32);
+        base = __shfl_sync(full, base, 0);
+        if (base >= n2) break;
+        const int64_t u = base + lane;
+        if (u >= n2) continue;
+        const int k = (int)(u >> 1), side = (int)(u & 1);
+        if (!ehit[k]) continue;  // both lanes of a pair
+        const int32_t i = queue[k];
+        const double4 E = es[k];
+        const V3 pos = v3(g.px[i], g.py[i], g.pz[i]);
+        double pin = E.x, pout = side ? E.z : E.y, pmid;
+        int s = 0, guard = 0;
+        while (fabs(pin - pout) > p.delta) {
+            if (++guard > 400) { s = kEclNoConverge; break; }
+            pmid = (pin + pout) / 2.;
+            if (fblink(p.comp_star, p.q, p.comp_spin, E.w, set_earth(p.cosi, p.sini, pmid), pos,
+                       p.comp_rref, p.comp_pref, s))
+                pin = pmid;
+            else
+                pout = pmid;
+            if (s) break;
+        }
+        double v = (pin + pout) / 2.;
+        v = v - floor(v);
+        const double other = __shfl_xor_sync(pair, v, 1);
+        const int os = __shfl_xor_sync(pair, s, 1);
+        if (side == 0) {
+            if (s || os) {
+                set_status(st, s ? s : os, i);
+            } else {
+                double egr = other;
+                if (egr < v) egr++;
                 g.necl[i] = 1;
-                g.ein[i] = ing;
+                g.ein[i] = v;
                 g.eout[i] = egr;
             }
         }
@@ -892,6 +963,9 @@ __global__ void k_ecl_pre_b(BatchDev b) {
 
 // k_ecl_roche over the batch queue: each candidate finds its slot by its
 // face index.
+// Warp mode of the batched eclipse (few candidates): one warp per candidate.
+// With more candidates than warp_max, k_ecl_potmin_b and k_ecl_bisect_b do
+// the work and this kernel returns at once (the choice is made on the device).
 __global__ void __launch_bounds__(128, 4) k_ecl_roche_b(BatchDev b, int32_t warp_max) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -924,26 +998,95 @@ __global__ void __launch_bounds__(128, 4) k_ecl_roche_b(BatchDev b, int32_t warp
         }
         return;
     }
+}
+
+// Thread mode of the batched eclipse, in two passes whose code is small enough
+// to stay in the instruction cache (the fused solve stalled on instruction
+// fetch): the sphere test and pot_min per candidate, then the ingress and
+// egress bisections (ingress_egress.cpp:61-86) on the two lanes of a pair.
+// Warps take consecutive candidates (similar iteration counts run together).
+// Same arithmetic and decisions as ingress_egress: identical results.
+__global__ void __launch_bounds__(128, 4) k_ecl_potmin_b(BatchDev b, int32_t warp_max) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int total = b.counters[0];
+    if (total <= warp_max) return;
+    const GridDev g = b.g;
     for (;;) {
         int base = 0;
-        if (lane == 0) base = atomicAdd(&b.counters[1], 32);
+        if (lane == 0) base = atomicAdd(&b.counters[2], 32);
         base = __shfl_sync(full, base, 0);
         if (base >= total) break;
         const int k = base + lane;
-        if (k < total) {
-            const int32_t i = b.queue[k];
-            const SlotDev &S = b.slots[find_seg(b.face0, b.nslots, i)];
-            const EclParams &p = S.ep;
-            const V3 pos = v3(g.px[i], g.py[i], g.pz[i]);
-            double ing = 0., egr = 0.;
+        if (k >= total) continue;
+        const int32_t i = b.queue[k];
+        const SlotDev &S = b.slots[find_seg(b.face0, b.nslots, i)];
+        const EclParams &p = S.ep;
+        const V3 pos = v3(g.px[i], g.py[i], g.pz[i]);
+        const V3 cofm = p.comp_star == kStar1 ? v3(0., 0., 0.) : v3(1., 0., 0.);
+        double phi1, phi2, lam1, lam2, phi = 0., lam = 0.;
+        uint8_t hit = 0;
+        if (sphere_eclipse_ph(p.cosi, p.sini, pos, cofm, p.comp_rref, phi1, phi2, lam1, lam2)) {
+            const double ACC = 2. * sqrt(2. * kTwoPi * (lam2 - lam1) * p.delta);
             int s = 0;
-            const bool ecl = ingress_egress(p.comp_star, p.q, p.comp_spin, p.cosi, p.sini,
-                                            p.delta, pos, p.comp_rref, p.comp_pref, ing, egr, s);
+            hit = pot_min(p.comp_star, p.q, p.comp_spin, p.cosi, p.sini, pos, phi1, phi2, lam1,
+                          lam2, p.comp_rref, p.comp_pref, ACC, phi, lam, s);
             if (s) {
                 set_status(b.st + S.model, s, i - S.face0);
-            } else if (ecl) {
+                hit = 0;
+            }
+            b.es[k] = make_double4(phi, phi1, phi2, ACC);
+        }
+        b.ehit[k] = hit;
+    }
+}
+
+__global__ void __launch_bounds__(128, 4) k_ecl_bisect_b(BatchDev b, int32_t warp_max) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const unsigned pair = 3u << (lane & ~1);
+    const int total = b.counters[0];
+    if (total <= warp_max) return;
+    const GridDev g = b.g;
+    const int64_t n2 = 2 * (int64_t)total;
+    for (;;) {
+        int64_t base = 0;
+        if (lane == 0) base = atomicAdd(&b.counters[3], 32);
+        base = __shfl_sync(full, base, 0);
+        if (base >= n2) break;
+        const int64_t u = base + lane;  // both lanes of a pair agree on u < n2
+        if (u >= n2) continue;
+        const int k = (int)(u >> 1), side = (int)(u & 1);
+        if (!b.ehit[k]) continue;  // so do both lanes of a pair here
+        const int32_t i = b.queue[k];
+        const SlotDev &S = b.slots[find_seg(b.face0, b.nslots, i)];
+        const EclParams &p = S.ep;
+        const double4 E = b.es[k];
+        const V3 pos = v3(g.px[i], g.py[i], g.pz[i]);
+        double pin = E.x, pout = side ? E.z : E.y, pmid;
+        int s = 0, guard = 0;
+        while (fabs(pin - pout) > p.delta) {
+            if (++guard > 400) { s = kEclNoConverge; break; }
+            pmid = (pin + pout) / 2.;
+            if (fblink(p.comp_star, p.q, p.comp_spin, E.w, set_earth(p.cosi, p.sini, pmid), pos,
+                       p.comp_rref, p.comp_pref, s))
+                pin = pmid;
+            else
+                pout = pmid;
+            if (s) break;
+        }
+        double v = (pin + pout) / 2.;
+        v = v - floor(v);
+        const double other = __shfl_xor_sync(pair, v, 1);
+        const int os = __shfl_xor_sync(pair, s, 1);
+        if (side == 0) {
+            if (s || os) {
+                set_status(b.st + S.model, s ? s : os, i - S.face0);
+            } else {
+                double egr = other;
+                if (egr < v) egr++;
                 g.necl[i] = 1;
-                g.ein[i] = ing;
+                g.ein[i] = v;
                 g.eout[i] = egr;
             }
         }
@@ -1126,10 +1269,10 @@ void launch_grid(const GridParams &p, const RingRec *rings, GridDev g, DevStatus
 }
 
 void launch_eclipse(const EclParams &p, int32_t eclipse_on, GridDev g, int32_t *queue,
-                    int32_t *counters, DevStatus *st, int nsm, int32_t warp_mode,
-                    cudaStream_t s) {
+                    int32_t *counters, double4 *es, uint8_t *ehit, DevStatus *st, int nsm,
+                    int32_t warp_mode, cudaStream_t s) {
     if (g.n <= 0) return;
-    cudaMemsetAsync(counters, 0, 2 * sizeof(int32_t), s);
+    cudaMemsetAsync(counters, 0, 4 * sizeof(int32_t), s);
     k_ecl_pre<<<nblocks(g.n, 256), 256, 0, s>>>(p, eclipse_on, g, queue, counters);
     count_launch();
     if (eclipse_on && p.comp_roche) {
@@ -1140,6 +1283,10 @@ void launch_eclipse(const EclParams &p, int32_t eclipse_on, GridDev g, int32_t *
         const int32_t warps = (int32_t)nb * 4;
         const int32_t warp_max = warp_mode < 0 ? -1 : warp_mode > 0 ? warp_mode : 2 * warps;
         k_ecl_roche<<<nb, 128, 0, s>>>(p, g, queue, counters, st, warp_max);
+        count_launch();
+        k_ecl_potmin<<<nb, 128, 0, s>>>(p, g, queue, counters, es, ehit, st, warp_max);
+        count_launch();
+        k_ecl_bisect<<<nb, 128, 0, s>>>(p, g, queue, counters, es, ehit, st, warp_max);
         count_launch();
     }
 }
@@ -1244,12 +1391,16 @@ void launch_batch_grid(const BatchDev &b, int nsm, cudaStream_t s) {
 }
 
 void launch_batch_eclipse(const BatchDev &b, int nsm, int32_t warp_mode, cudaStream_t s) {
-    cudaMemsetAsync(b.counters, 0, 2 * sizeof(int32_t), s);
+    cudaMemsetAsync(b.counters, 0, 4 * sizeof(int32_t), s);
     k_ecl_pre_b<<<nsm * 4, 256, 0, s>>>(b);
     count_launch();
     const int32_t warps = nsm * 16;
     const int32_t warp_max = warp_mode < 0 ? -1 : warp_mode > 0 ? warp_mode : 2 * warps;
     k_ecl_roche_b<<<nsm * 4, 128, 0, s>>>(b, warp_max);
+    count_launch();
+    k_ecl_potmin_b<<<nsm * 4, 128, 0, s>>>(b, warp_max);
+    count_launch();
+    k_ecl_bisect_b<<<nsm * 4, 128, 0, s>>>(b, warp_max);
     count_launch();
 }
 

@@ -220,3 +220,18 @@ def test_batch_curves_returns_the_rows_of_the_last_call(data):
             e.batch_curves([5])
     finally:
         e.close()
+
+
+def test_batch_eclipse_modes_are_bit_identical(data):
+    """The batched eclipse's warp mode (one warp per candidate) and thread mode
+    (pot_min per candidate, then the two bisections on a lane pair) give the
+    same light curves bit for bit: the same midpoints and decisions."""
+    ms = _models(k=12, seed=21, lo=24, hi=64)
+    out = []
+    for mode in (1 << 30, -1):
+        with Engine(precision="mixed", eclipse_warp=mode) as e:
+            calc, chisq, wnok, sf, st = e.light_curve_batch(ms, data)
+            assert np.all(st == 0), st
+            out.append((calc.copy(), chisq.copy()))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
