@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(128, 4) k_ecl_potmin(EclParams p, GridDev g,
     }
 }
 
-__global__ void __launch_bounds__(128, 4) k_ecl_bisect(EclParams p, GridDev g,
+__global__ void __launch_bounds__(128, 6) k_ecl_bisect(EclParams p, GridDev g,
                                                     const int32_t *__restrict__ queue,
                                                     int32_t *counters, const double4 *es,
                                                     const uint8_t *ehit, DevStatus *st,
@@ -1041,7 +1041,9 @@ __global__ void __launch_bounds__(128, 4) k_ecl_potmin_b(BatchDev b, int32_t war
     }
 }
 
-__global__ void __launch_bounds__(128, 4) k_ecl_bisect_b(BatchDev b, int32_t warp_max) {
+// 6 blocks of 4 warps per SM (a sweep of 4, 5, 6 and 8 on B200 chose 6: more
+// warps hide the FP64 latency, fewer registers spill more)
+__global__ void __launch_bounds__(128, 6) k_ecl_bisect_b(BatchDev b, int32_t warp_max) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const unsigned pair = 3u << (lane & ~1);
@@ -1286,7 +1288,8 @@ void launch_eclipse(const EclParams &p, int32_t eclipse_on, GridDev g, int32_t *
         count_launch();
         k_ecl_potmin<<<nb, 128, 0, s>>>(p, g, queue, counters, es, ehit, st, warp_max);
         count_launch();
-        k_ecl_bisect<<<nb, 128, 0, s>>>(p, g, queue, counters, es, ehit, st, warp_max);
+        const unsigned nb6 = need < (unsigned)nsm * 6u ? need : (unsigned)nsm * 6u;
+        k_ecl_bisect<<<nb6, 128, 0, s>>>(p, g, queue, counters, es, ehit, st, warp_max);
         count_launch();
     }
 }
@@ -1400,7 +1403,7 @@ void launch_batch_eclipse(const BatchDev &b, int nsm, int32_t warp_mode, cudaStr
     count_launch();
     k_ecl_potmin_b<<<nsm * 4, 128, 0, s>>>(b, warp_max);
     count_launch();
-    k_ecl_bisect_b<<<nsm * 4, 128, 0, s>>>(b, warp_max);
+    k_ecl_bisect_b<<<nsm * 6, 128, 0, s>>>(b, warp_max);
     count_launch();
 }
 
