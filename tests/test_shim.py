@@ -61,3 +61,19 @@ def test_shim_raises_the_reference_error(reference):
     st, err, *_ = _shimmed().light_curve(m, W.data(20))
     st_r, err_r, *_ = reference.light_curve(m, W.data(20))
     assert st == st_r != 0 and err == err_r
+
+
+@needs_shim
+@pytest.mark.gpu
+def test_shim_evaluates_disc_models(oracle):
+    """A cataclysmic variable (opaque disc, rim, bright spot) and an iscale fit
+    through the reference's own Model parsing and the shim."""
+    from cases import disc_cases
+    shim = _shimmed()
+    for name, m, d in disc_cases()[2:5]:
+        st, err, calc, sf, sc = shim.light_curve(m, d)
+        assert st == 0, (name, err)
+        so, erro, co, sfo, sco = oracle.light_curve(m, d)
+        assert so == 0, erro
+        rel = np.max(np.abs(calc - co) / np.maximum(np.abs(co), 1e-300))
+        assert rel <= 1e-5, (name, rel)
