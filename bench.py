@@ -59,8 +59,8 @@ def parse():
     ap.add_argument("--mcmc-steps", type=int, default=2000)
     ap.add_argument("--burn", type=int, default=400)
     ap.add_argument("--ncoef", type=int, default=64)
-    ap.add_argument("--local-curves", type=int, default=65536)
-    ap.add_argument("--refine-epochs", type=int, default=300)
+    ap.add_argument("--local-curves", type=int, default=131072)
+    ap.add_argument("--refine-epochs", type=int, default=600)
     ap.add_argument("--da-scale", type=float, default=2.6)
     ap.add_argument("--local-widen", type=float, default=2.0)
     ap.add_argument("--precision", choices=("mixed", "fp64"), default="mixed")
@@ -658,7 +658,8 @@ def run_surrogate(args):
     from lcurve_re_b200 import surrogate as S
     from lcurve_re_b200 import workloads as W
     from lcurve_re_b200.engine import Engine
-    from lcurve_re_b200.sampler import ExactChi2, delayed_acceptance, ess_total, metropolis
+    from lcurve_re_b200.sampler import (ExactChi2, delayed_acceptance, ess_between_chains,
+                                        ess_total, metropolis)
 
     eng = Engine(device=local, precision="mixed")
     clocks = Clocks(local)
@@ -765,10 +766,12 @@ def run_surrogate(args):
                    "ess": "Geyer initial positive sequence, min over parameters of the sum "
                           "over chains (new_scripts/mcmc_solver.cpp:80-115)"},
         "plain": {"ess": ess_p, "ess_per_s": ess_p / wall_p, "wall_s": wall_p,
-                  "acceptance": accp, "exact_evals": n_plain},
+                  "acceptance": accp, "exact_evals": n_plain,
+                  "ess_between_chains": ess_between_chains(chp)[0]},
         "delayed_acceptance": {"surrogate": "refined around the burn-in posterior",
                                "ess": ess_d, "ess_per_s": ess_d / wall_d, "wall_s": wall_d,
-                               "acceptance": accd, "exact_evals": exact2.evals, **st},
+                               "acceptance": accd, "exact_evals": exact2.evals,
+                               "ess_between_chains": ess_between_chains(chd)[0], **st},
         "delayed_acceptance_global": {"surrogate": "prior box only",
                                       "ess": ess_g, "ess_per_s": ess_g / wall_g,
                                       "wall_s": wall_g, "acceptance": accg,
@@ -776,6 +779,8 @@ def run_surrogate(args):
                                       "posterior_mean_shift_sigma_max": float(shift_g.max()),
                                       **stg},
         "ess_per_s_ratio": (ess_d / wall_d) / (ess_p / wall_p),
+        "ess_per_s_ratio_between_chains": (ess_between_chains(chd)[0] / wall_d) /
+                                          (ess_between_chains(chp)[0] / wall_p),
         "posterior_mean_shift_sigma_max": float(shift.max()),
         "surrogate": {"train_curves": args.train_curves, "curve_generation_s": t_gen,
                       "curves_per_s": args.train_curves / t_gen, "fit_s": t_fit,

@@ -244,6 +244,12 @@ lcg_status lcg_light_curve_batch_resident(lcg_ctx *ctx, const lcg_model *models,
  * unchanged hold their earlier curves. */
 lcg_status lcg_batch_curves(lcg_ctx *ctx, const int32_t *rows, int32_t count, double *out);
 
+/* The same rows gathered into device memory dst [count x n] (on ctx's
+ * device), for a caller that keeps them there; returns when they are
+ * written. rows = NULL with count = the batch's model count copies every row. */
+lcg_status lcg_batch_curves_device(lcg_ctx *ctx, const int32_t *rows, int32_t count,
+                                   double *dst);
+
 /* ---- stage-level seams, for parity tests and integrations -------------- */
 
 /* Number of faces of one star grid (Lcurve::numface, numface.cpp:14-52, and

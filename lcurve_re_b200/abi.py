@@ -116,6 +116,7 @@ PROTOTYPES = {
     "lcg_measure_fp32_peak": (C.c_int, [P, D]),
     "lcg_set_data": (C.c_int, [P, P, C.c_int32]),
     "lcg_batch_curves": (C.c_int, [P, I32, C.c_int32, D]),
+    "lcg_batch_curves_device": (C.c_int, [P, I32, C.c_int32, C.c_void_p]),
     "lcg_light_curve_fast": (C.c_int, [P, C.POINTER(LcgModel), P, C.c_int32, C.c_int32,
                                        C.c_int32, D, D, D]),
     "lcg_mlp_gemm": (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, P, P, P, P, P,

@@ -615,9 +615,11 @@ extern "C" lcg_status lcg_light_curve_batch_resident(lcg_ctx *c, const lcg_model
                 if (calc) memset(calc + (size_t)m * n, 0, (size_t)n * sizeof(double));
                 continue;
             }
-            B.key[m] = models[m];
-            B.key_ok[m] = 1;
-            B.key_sfac0[m] = sfac[5 * (size_t)m];
+            if (!reuse[m]) {  // a reused model equals its key already
+                B.key[m] = models[m];
+                B.key_ok[m] = 1;
+                B.key_sfac0[m] = sfac[5 * (size_t)m];
+            }
             if (calc) memcpy(calc + (size_t)m * n, hc + (size_t)m * n, (size_t)n * sizeof(double));
             for (int k = 0; k < 5; k++) sfac[5 * (size_t)m + k] = hs[5 * (size_t)m + k];
             if (ho[3 * m + 2] != 0.) {
@@ -650,9 +652,7 @@ extern "C" lcg_status lcg_light_curve_batch_resident(lcg_ctx *c, const lcg_model
     return LCG_OK;
 }
 
-extern "C" lcg_status lcg_batch_curves(lcg_ctx *c, const int32_t *rows, int32_t count,
-                                       double *out) {
-    if (!c) return LCG_E_INVALID;
+static lcg_status check_rows(lcg_ctx *c, const int32_t *rows, int32_t count, const void *out) {
     c->err.clear();
     if (!rows || !out || count < 0) return c->fail(LCG_E_INVALID, "null argument");
     BatchState *B = c->batch;
@@ -660,7 +660,44 @@ extern "C" lcg_status lcg_batch_curves(lcg_ctx *c, const int32_t *rows, int32_t 
     for (int32_t i = 0; i < count; i++)
         if (rows[i] < 0 || rows[i] >= B->nmodels)
             return c->fail(LCG_E_INVALID, "row %d outside the batch of %d", rows[i], B->nmodels);
-    if (count == 0) return LCG_OK;
+    return LCG_OK;
+}
+
+extern "C" lcg_status lcg_batch_curves_device(lcg_ctx *c, const int32_t *rows, int32_t count,
+                                              double *dst) {
+    if (!c) return LCG_E_INVALID;
+    cudaError_t e;
+    if (!rows) {  // every row: one device copy of the curve matrix
+        c->err.clear();
+        BatchState *B = c->batch;
+        if (!dst) return c->fail(LCG_E_INVALID, "null argument");
+        if (!B || B->nmodels <= 0) return c->fail(LCG_E_INVALID, "no batch has run on this context");
+        if (count != B->nmodels)
+            return c->fail(LCG_E_INVALID, "count %d is not the batch's %d models", count, B->nmodels);
+        cudaSetDevice(c->device);
+        cudaMemcpyAsync(dst, B->calc.p, (size_t)count * B->n * sizeof(double),
+                        cudaMemcpyDeviceToDevice, c->stream);
+        if ((e = cudaStreamSynchronize(c->stream))) return c->cuda_fail(e, "curve rows");
+        return LCG_OK;
+    }
+    lcg_status rc = check_rows(c, rows, count, dst);
+    if (rc || count == 0) return rc;
+    cudaSetDevice(c->device);
+    BatchState *B = c->batch;
+    if ((e = B->rows.ensure((size_t)count))) return c->cuda_fail(e, "curve rows");
+    cudaMemcpyAsync(B->rows.p, rows, (size_t)count * sizeof(int32_t), cudaMemcpyHostToDevice,
+                    c->stream);
+    launch_gather_rows(B->calc.p, B->n, B->rows.p, count, dst, c->stream);
+    if ((e = cudaStreamSynchronize(c->stream))) return c->cuda_fail(e, "curve rows");
+    return LCG_OK;
+}
+
+extern "C" lcg_status lcg_batch_curves(lcg_ctx *c, const int32_t *rows, int32_t count,
+                                       double *out) {
+    if (!c) return LCG_E_INVALID;
+    lcg_status rc = check_rows(c, rows, count, out);
+    if (rc || count == 0) return rc;
+    BatchState *B = c->batch;
     cudaSetDevice(c->device);
     const size_t n = (size_t)B->n, bytes = (size_t)count * n * sizeof(double);
     cudaError_t e;

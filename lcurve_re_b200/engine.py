@@ -178,6 +178,20 @@ class Engine:
             _dptr(wnok), status.ctypes.data_as(C.POINTER(C.c_int32))))
         return out, chisq, wnok, sf.reshape(nm, 5), status
 
+    def batch_curves_device(self, rows, out):
+        """The same rows written into a contiguous float64 device tensor out
+        [len(rows) x n] on the engine's device; rows None: every model's
+        row (out [nmodels x n])."""
+        if rows is None:
+            self._check(self.lib.lcg_batch_curves_device(self.ctx, None, out.shape[0],
+                                                         C.c_void_p(out.data_ptr())))
+            return out
+        r = np.ascontiguousarray(rows, dtype=np.int32)
+        self._check(self.lib.lcg_batch_curves_device(
+            self.ctx, r.ctypes.data_as(C.POINTER(C.c_int32)), r.shape[0],
+            C.c_void_p(out.data_ptr())))
+        return out
+
     def batch_curves(self, rows):
         """Light curves of the given model indices from the last batch call."""
         r = np.ascontiguousarray(rows, dtype=np.int32)

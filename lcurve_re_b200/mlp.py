@@ -86,23 +86,26 @@ class MLP:
     # -- forward / backward ----------------------------------------------------
     def forward(self, x, train=False):
         """x: [n, nin] FP32 device tensor (n <= batch). Returns the [n, nout]
-        FP32 outputs (a view of an internal buffer)."""
+        FP32 outputs (a view of an internal buffer). Training runs the whole
+        batch; inference only the first n rows rounded up to the 128-row
+        tile of the GEMMs."""
         n = x.shape[0]
         if n > self.B:
             raise ValueError("batch larger than the network's buffers")
         B, w = self.B, self.width
+        m = B if train else min(B, max(128, (n + 127) // 128 * 128))
         self.x[:n].copy_(x)
-        if n < B:
-            self.x[n:].zero_()
+        if n < m:
+            self.x[n:m].zero_()
         st = self.lib.lcg_mlp_input(self._stream(), _p(self.x), self.nin, _p(self.W[0]),
-                                    _p(self.b[0]), B, w, n, _p(self.Z[0]), _p(self.Y[0]),
+                                    _p(self.b[0]), m, w, n, _p(self.Z[0]), _p(self.Y[0]),
                                     _p(self.Yt[0]) if train else None, B)
         self._ok(st, "lcg_mlp_input")
         for l in range(1, self.depth):
-            self._gemm(EPI_GELU, B, w, w, self.Y[l - 1], self.Wb[l], bias=self.b[l], z=self.Z[l],
-                       y=self.Y[l], yt=self.Yt[l] if train else None, mvalid=B, ldt=B)
+            self._gemm(EPI_GELU, m, w, w, self.Y[l - 1], self.Wb[l], bias=self.b[l], z=self.Z[l],
+                       y=self.Y[l], yt=self.Yt[l] if train else None, mvalid=m, ldt=B)
         L = self.depth
-        self._gemm(EPI_LINEAR, B, self.nout, w, self.Y[L - 1], self.Wb[L], bias=self.b[L],
+        self._gemm(EPI_LINEAR, m, self.nout, w, self.Y[L - 1], self.Wb[L], bias=self.b[L],
                    out=self.out, mvalid=n)
         return self.out[:n]
 

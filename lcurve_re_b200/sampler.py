@@ -63,6 +63,18 @@ def ess_total(chain):
     return float(per.sum(axis=1).min()), per.sum(axis=1)
 
 
+def ess_between_chains(chain):
+    """A cross-check of ess_total that needs no autocorrelation estimate: with
+    chains started from the stationary distribution, the variance of a
+    chain's mean is sigma**2 / ESS_chain, so ESS = chains x sigma**2 /
+    var(chain means), the minimum over parameters."""
+    steps, nc, npar = chain.shape
+    var_all = chain.reshape(-1, npar).var(axis=0)
+    var_means = chain.mean(axis=0).var(axis=0, ddof=1)
+    per = nc * var_all / np.maximum(var_means, 1e-300)
+    return float(per.min()), per
+
+
 class ExactChi2:
     """chi**2 of the resident data for each row of theta, from the batched
     engine (scale fitted, as re_scale does). Failed models get +inf."""
@@ -96,6 +108,17 @@ class ExactChi2:
         """The last call's light curves (scaled) of the given chains."""
         return self.engine.batch_curves(rows)
 
+    def curves_device(self, rows, device="cuda"):
+        """The same rows as a float64 device tensor, gathered on the device."""
+        import torch
+        out = torch.empty((len(rows), self.engine._n), dtype=torch.float64, device=device)
+        return self.engine.batch_curves_device(rows, out)
+
+    def curves_all_device(self, out):
+        """Every chain's curve of the last call into the device tensor out
+        [chains x points] (one device copy)."""
+        return self.engine.batch_curves_device(None, out)
+
 
 def _proposal(rng, theta, chol):
     return theta + rng.standard_normal(theta.shape) @ chol.T
@@ -115,6 +138,62 @@ def _put(dst, idx, src):
     else:
         import torch
         dst[torch.as_tensor(idx, device=dst.device)] = src
+
+
+def _delayed_acceptance_device(exact, sur, theta0, cov, steps, seed, box_check, record):
+    """delayed_acceptance with the anchored surrogate kept on the device: the
+    exact curves of every chain are copied from the engine in one device
+    copy, the screening and reverse chi**2 run over all chains (no index
+    gathers), and accepted rows are merged with masked selects. The same
+    random draws and decisions as the general loop."""
+    torch = sur.torch
+    dev = sur.sur.dev
+    rng = np.random.default_rng(seed)
+    chol = np.linalg.cholesky(cov)
+    theta = np.array(theta0, np.float64)
+    nc = theta.shape[0]
+    chi = exact(theta)
+    F = torch.empty((nc, exact.engine._n), dtype=torch.float64, device=dev)
+    exact.curves_all_device(F)
+    f = F.clone()  # exact curves at the states
+    sx = sur.state(theta)
+    last = theta.copy()
+    chain = np.empty((steps,) + theta.shape) if record else None
+    acc = stage1 = 0
+    t0 = time.perf_counter()
+    for s in range(steps):
+        prop = _proposal(rng, theta, chol)
+        ok = box_check(prop)
+        sy = sur.state(prop)
+        chi_a = sur.chi2(sy, sx, f)  # chi**2 of exact(x) s(y) / s(x)
+        chi_a[~ok] = np.inf
+        log_g = np.minimum(0.0, -(chi_a - chi) / 2)
+        a1 = ok & (np.log(rng.random(nc)) < log_g)
+        u2 = np.log(rng.random(nc))
+        if a1.any():
+            ev = np.where(a1[:, None], prop, last)
+            chi_p = exact(ev)
+            last = ev
+            exact.curves_all_device(F)  # F rows of a1 chains: exact(y)
+            chi_rev = sur.chi2(sx, sy, F)  # exact(y) s(x) / s(y), used where a1
+            log_g_rev = np.where(a1, np.minimum(0.0, -(chi_rev - chi_p) / 2), 0.0)
+            with np.errstate(invalid="ignore"):
+                log_rho = -(chi_p - chi) / 2 + log_g_rev - log_g
+            a2 = a1 & (u2 < log_rho)
+            theta[a2] = prop[a2]
+            chi[a2] = chi_p[a2]
+            if a2.any():
+                m = torch.as_tensor(a2, device=dev)[:, None]
+                f = torch.where(m, F, f)
+                sx = torch.where(m, sy, sx)
+            acc += int(a2.sum())
+            stage1 += int(a1.sum())
+        if record:
+            chain[s] = theta
+    wall = time.perf_counter() - t0
+    n = steps * nc
+    return chain, theta, chi, acc / n, wall, {"stage1_rate": stage1 / n,
+                                              "stage2_rate": acc / max(stage1, 1)}
 
 
 def metropolis(exact, theta0, cov, steps, seed=0, box_check=in_box, record=True):
@@ -157,10 +236,17 @@ def delayed_acceptance(exact, sur, theta0, cov, steps, seed=0, box_check=in_box,
     chol = np.linalg.cholesky(cov)
     theta = np.array(theta0, np.float64)
     anchored = hasattr(sur, "state")
+    if anchored and hasattr(exact, "curves_all_device") and hasattr(sur, "torch"):
+        return _delayed_acceptance_device(exact, sur, theta0, cov, steps, seed, box_check,
+                                          record)
     place = getattr(sur, "anchor", lambda rows: np.array(rows, np.float64))
+    if anchored and hasattr(exact, "curves_device") and hasattr(sur, "sur"):
+        fetch = lambda rows: exact.curves_device(rows, sur.sur.dev)  # stays on the device
+    else:
+        fetch = lambda rows: place(exact.curves_of(rows))
     chi = exact(theta)
     if anchored:
-        f = place(exact.curves_of(np.arange(theta.shape[0])))  # exact curves at the states
+        f = fetch(np.arange(theta.shape[0]))  # exact curves at the states
         sx = sur.state(theta)
     else:
         chi_s = sur(theta)
@@ -191,7 +277,7 @@ def delayed_acceptance(exact, sur, theta0, cov, steps, seed=0, box_check=in_box,
             if anchored:
                 # only the chains that reached the engine need their new curve
                 i1 = np.nonzero(a1)[0]
-                fp = place(exact.curves_of(i1))
+                fp = fetch(i1)
                 chi_r = np.full(nc, np.inf)
                 chi_r[i1] = sur.chi2(_take(sx, i1), _take(sy, i1), fp)  # exact(y) s(x)/s(y)
                 log_g_rev = np.minimum(0.0, -(chi_r - chi_p) / 2)

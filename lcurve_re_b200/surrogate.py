@@ -66,19 +66,24 @@ class ModelFactory:
         self.base = (base if base is not None else W.model()).to_c()
         self.dtype = np.dtype(abi.LcgModel)  # the struct layout, parsed once
         self.base_row = np.frombuffer(bytes(self.base), dtype=self.dtype)[0]
-        self._arr = None
+        self._arr = self._view = None
 
     def __call__(self, theta, out=None):
         """lcg_model array for the rows of theta. Without out, the array is
-        reused between calls of the same size (valid until the next call)."""
+        reused between calls of the same size (valid until the next call):
+        it holds the base model already, so only the sampled fields are
+        written."""
         theta = np.atleast_2d(np.asarray(theta, np.float64))
         n = theta.shape[0]
         if out is None:
             if self._arr is None or len(self._arr) != n:
                 self._arr = (abi.LcgModel * n)()
-            out = self._arr
-        view = np.frombuffer(out, dtype=self.dtype)
-        view[:] = self.base_row
+                self._view = np.frombuffer(self._arr, dtype=self.dtype)
+                self._view[:] = self.base_row
+            out, view = self._arr, self._view
+        else:
+            view = np.frombuffer(out, dtype=self.dtype)
+            view[:] = self.base_row
         for k, name in enumerate(PARAMS):
             view[name] = theta[:, k]
         return out
@@ -169,6 +174,8 @@ class Surrogate:
         vectors theta [n x 9]."""
         torch = self.torch
         x = torch.as_tensor(to_unit(theta), device=self.dev, dtype=torch.float32)
+        if x.shape[0] <= self.net.B:
+            return self.net.forward(x).clone()
         outs = []
         for i0 in range(0, x.shape[0], self.net.B):
             outs.append(self.net.forward(x[i0:i0 + self.net.B]).clone())

@@ -188,3 +188,16 @@ def test_training_reduces_the_loss():
         net.step(1e-3)
     net.check()
     assert losses[-1] < 0.1 * losses[0], (losses[0], losses[-1])
+
+
+def test_inference_on_the_rows_present_matches_the_full_batch():
+    """Inference runs only ceil(n / 128) x 128 rows; the outputs of those rows
+    equal a full-batch pass (FP32 sums of the same BF16 products)."""
+    import torch
+    from lcurve_re_b200.mlp import MLP
+    net = MLP(nin=9, nout=64, batch=1024, device="cuda", seed=3)
+    x = torch.rand(1024, 9, device="cuda")
+    full = net.forward(x).clone()
+    for n in (1, 130, 512):
+        part = net.forward(x[:n]).clone()
+        torch.testing.assert_close(part, full[:n], rtol=1e-5, atol=1e-6)

@@ -91,3 +91,41 @@ def test_delayed_acceptance_calls_the_engine_less(trained):
     assert exact2.evals < n_plain
     assert accp > 0 and accd > 0 and 0 < st["stage1_rate"] < 1
     assert np.all(np.isfinite(chd))
+
+
+def test_device_delayed_acceptance_equals_the_general_loop(trained):
+    """The device-resident anchored loop (whole-matrix curve copies, masked
+    merges) takes the same decisions as the general loop (row gathers)."""
+    from lcurve_re_b200.sampler import ExactChi2, delayed_acceptance
+    e, sur, theta, curves, _ = trained
+    idx = np.arange(0, S.NGRID, 2)
+    truth = np.array([0.25, 86.0, 0.015, 0.20, 20000.0, 3200.0, 0.08, 0.5, 0.0])
+    calc = e.light_curve_comp(S.ModelFactory()(truth[None])[0], W.data(S.NGRID, -0.2, 1.2),
+                              scale=False, rdata=False, sfac=np.ones(5), diagnostics=False)[0]
+    d = W.add_noise(W.data(S.NGRID, -0.2, 1.2)[idx], calc[idx], 9)
+    sur_chi = S.SurrogateChi2(sur, d, idx)
+    rng = np.random.default_rng(4)
+    scale = (S.BOX[:, 1] - S.BOX[:, 0]) * 2e-3
+    theta0 = truth + rng.standard_normal((24, 9)) * scale
+    cov = np.diag(scale ** 2) * 4.0
+
+    class General:  # an ExactChi2 without the whole-matrix copy: the general loop
+        def __init__(self, ex):
+            self.ex = ex
+
+        def __call__(self, theta):
+            return self.ex(theta)
+
+        def curves_of(self, rows):
+            return self.ex.curves_of(rows)
+
+        def curves_device(self, rows, device="cuda"):
+            return self.ex.curves_device(rows, device)
+
+    out = []
+    for wrap in (lambda x: x, General):
+        ex = wrap(ExactChi2(e, d, curves=True))
+        ch, th, chi, acc, _, st = delayed_acceptance(ex, sur_chi, theta0, cov, 40, seed=3)
+        out.append((ch, chi, st))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])

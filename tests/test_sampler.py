@@ -135,3 +135,19 @@ def test_anchored_delayed_acceptance_samples_the_posterior():
     assert np.all(np.abs(s.mean(axis=0) - MU) < 0.05 * SIG)
     assert np.all(np.abs(s.std(axis=0) / SIG - 1) < 0.05)
     assert st["stage2_rate"] > 0.5 and ex.evals < chains * steps
+
+
+def test_between_chain_ess_matches_geyer_on_ar1_chains():
+    """For AR(1) chains started in stationarity both estimators recover the
+    known ESS n (1 - a) / (1 + a)."""
+    from lcurve_re_b200.sampler import ess_between_chains, ess_total
+    rng = np.random.default_rng(3)
+    a, n, nc = 0.9, 4000, 400
+    x = np.empty((n, nc, 2))
+    x[0] = rng.standard_normal((nc, 2))
+    for t in range(1, n):
+        x[t] = a * x[t - 1] + np.sqrt(1 - a * a) * rng.standard_normal((nc, 2))
+    want = nc * n * (1 - a) / (1 + a)
+    g, _ = ess_total(x)
+    b, _ = ess_between_chains(x)
+    assert abs(g / want - 1) < 0.1 and abs(b / want - 1) < 0.25, (g, b, want)
