@@ -196,6 +196,56 @@ def _delayed_acceptance_device(exact, sur, theta0, cov, steps, seed, box_check, 
                                               "stage2_rate": acc / max(stage1, 1)}
 
 
+def _delayed_acceptance_graphs(exact, sur, theta0, cov, steps, seed, box_check, record):
+    """The device loop with the surrogate's two per-step passes replayed as
+    CUDA graphs on static buffers (sur.bind): one launch each instead of the
+    network's layer-by-layer launches and allocations. Same draws and
+    decisions as the other loops."""
+    import torch
+    rng = np.random.default_rng(seed)
+    chol = np.linalg.cholesky(cov)
+    theta = np.array(theta0, np.float64)
+    nc = theta.shape[0]
+    chi = exact(theta)
+    F = torch.empty((nc, exact.engine._n), dtype=torch.float64, device=sur.sur.dev)
+    exact.curves_all_device(F)
+    sur.bind(sur.state(theta), F)
+    last = theta.copy()
+    chain = np.empty((steps,) + theta.shape) if record else None
+    acc = stage1 = 0
+    t0 = time.perf_counter()
+    for s in range(steps):
+        prop = _proposal(rng, theta, chol)
+        ok = box_check(prop)
+        chi_a = sur.screen(prop)  # chi**2 of exact(x) s(y) / s(x)
+        chi_a[~ok] = np.inf
+        log_g = np.minimum(0.0, -(chi_a - chi) / 2)
+        a1 = ok & (np.log(rng.random(nc)) < log_g)
+        u2 = np.log(rng.random(nc))
+        if a1.any():
+            ev = np.where(a1[:, None], prop, last)
+            chi_p = exact(ev)
+            last = ev
+            exact.curves_all_device(sur.g_F)  # rows of a1 chains: exact(y)
+            chi_rev = sur.reverse()
+            log_g_rev = np.where(a1, np.minimum(0.0, -(chi_rev - chi_p) / 2), 0.0)
+            with np.errstate(invalid="ignore"):
+                log_rho = -(chi_p - chi) / 2 + log_g_rev - log_g
+            a2 = a1 & (u2 < log_rho)
+            theta[a2] = prop[a2]
+            chi[a2] = chi_p[a2]
+            if a2.any():
+                sur.merge(a2)
+            acc += int(a2.sum())
+            stage1 += int(a1.sum())
+        if record:
+            chain[s] = theta
+    wall = time.perf_counter() - t0
+    n = steps * nc
+    return chain, theta, chi, acc / n, wall, {"stage1_rate": stage1 / n,
+                                              "stage2_rate": acc / max(stage1, 1)}
+
+
 def metropolis(exact, theta0, cov, steps, seed=0, box_check=in_box, record=True):
     """Plain random-walk Metropolis on every chain at once. Returns
     (chain [steps x chains x params] or None, final theta, final chi**2,
@@ -236,6 +286,9 @@ def delayed_acceptance(exact, sur, theta0, cov, steps, seed=0, box_check=in_box,
     chol = np.linalg.cholesky(cov)
     theta = np.array(theta0, np.float64)
     anchored = hasattr(sur, "state")
+    if anchored and hasattr(exact, "curves_all_device") and hasattr(sur, "bind"):
+        return _delayed_acceptance_graphs(exact, sur, theta0, cov, steps, seed, box_check,
+                                          record)
     if anchored and hasattr(exact, "curves_all_device") and hasattr(sur, "torch"):
         return _delayed_acceptance_device(exact, sur, theta0, cov, steps, seed, box_check,
                                           record)

@@ -253,22 +253,81 @@ class SurrogateChi2:
         """The surrogate's coefficients at theta (device tensor)."""
         return self.sur.coefficients(theta).contiguous()
 
+    def _pca(self, coef, coef_x, anchor, chi):
+        torch = self.torch
+        p = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
+        st = self.lib.lcg_mlp_pca_chisq(C.c_void_p(torch.cuda.current_stream().cuda_stream),
+                                        p(coef), coef.shape[0], coef.shape[1], p(self.basis),
+                                        p(self.mean), self.npts, p(self.flux), p(self.ferr),
+                                        p(self.wgt), p(coef_x), p(anchor), p(chi), None)
+        if st != abi.OK:
+            raise RuntimeError("lcg_mlp_pca_chisq failed")
+
     def chi2(self, coef, coef_x=None, anchor=None):
         """chi**2 of s(coef), or of anchor * s(coef) / s(coef_x) (anchor: exact
         curves at the data points, one row per chain)."""
         torch = self.torch
-        m = coef.shape[0]
-        chi = torch.empty(m, dtype=torch.float64, device=self.sur.dev)
+        chi = torch.empty(coef.shape[0], dtype=torch.float64, device=self.sur.dev)
         an = None
         if anchor is not None:
             an = anchor if isinstance(anchor, torch.Tensor) else self.anchor(anchor)
             an = an.contiguous()
-        p = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
-        st = self.lib.lcg_mlp_pca_chisq(C.c_void_p(torch.cuda.current_stream().cuda_stream),
-                                        p(coef), m, coef.shape[1], p(self.basis), p(self.mean),
-                                        self.npts, p(self.flux), p(self.ferr), p(self.wgt),
-                                        p(coef_x.contiguous() if coef_x is not None else None),
-                                        p(an), p(chi), None)
-        if st != abi.OK:
-            raise RuntimeError("lcg_mlp_pca_chisq failed")
+        self._pca(coef, coef_x.contiguous() if coef_x is not None else None, an, chi)
         return chi.cpu().numpy()
+
+    # -- fixed-shape passes of the device delayed-acceptance loop -------------
+    def bind(self, sx0, f0):
+        """Static buffers for the chains of sx0 (their states) and f0 (their
+        exact curves), and CUDA graphs of the two passes the sampler runs
+        every step: screening (network forward on the proposals in g_x, then
+        chi**2 of f s(y)/s(x) into g_chi) and reverse (chi**2 of F s(x)/s(y)
+        into g_chr, F the exact curves of the proposals in g_F)."""
+        torch = self.torch
+        dev = self.sur.dev
+        nc = sx0.shape[0]
+        self.g_x = torch.zeros(nc, len(PARAMS), dtype=torch.float32, device=dev)
+        self.h_x = torch.zeros(nc, len(PARAMS), dtype=torch.float32, pin_memory=True)
+        self.g_sx, self.g_sy = sx0.clone(), torch.zeros_like(sx0)
+        self.g_f, self.g_F = f0.clone(), torch.zeros_like(f0)
+        self.g_chi = torch.empty(nc, dtype=torch.float64, device=dev)
+        self.g_chr = torch.empty(nc, dtype=torch.float64, device=dev)
+
+        def screen():
+            self.g_sy.copy_(self.sur.net.forward(self.g_x))
+            self._pca(self.g_sy, self.g_sx, self.g_f, self.g_chi)
+
+        def reverse():
+            self._pca(self.g_sx, self.g_sy, self.g_F, self.g_chr)
+        self.gr_screen = self._capture(screen)
+        self.gr_reverse = self._capture(reverse)
+
+    def _capture(self, fn):
+        torch = self.torch
+        s = torch.cuda.Stream(device=self.sur.dev)
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            fn()  # first run outside the graph
+        torch.cuda.current_stream().wait_stream(s)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            fn()
+        return g
+
+    def screen(self, theta):
+        """The bound screening pass on proposals theta: chi**2 per chain."""
+        self.h_x.numpy()[:] = to_unit(theta)
+        self.g_x.copy_(self.h_x, non_blocking=True)
+        self.gr_screen.replay()
+        return self.g_chi.cpu().numpy()
+
+    def reverse(self):
+        """The bound reverse pass (g_F holds the proposals' exact curves)."""
+        self.gr_reverse.replay()
+        return self.g_chr.cpu().numpy()
+
+    def merge(self, accepted):
+        """Chains accepted this step take the proposal's state and curve."""
+        torch = self.torch
+        m = torch.as_tensor(accepted, device=self.sur.dev)[:, None]
+        self.g_sx.copy_(torch.where(m, self.g_sy, self.g_sx))
+        self.g_f.copy_(torch.where(m, self.g_F, self.g_f))
