@@ -24,6 +24,7 @@
 
 #include <algorithm>
 #include <map>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -73,6 +74,8 @@ struct BatchState {
     int32_t nslots = 0;
     int64_t nfaces = 0, nflat = 0, nblk = 0, ldp = 0;
     FluxPlan plan{};
+    bool tuned = false;      // the flux plan was chosen by autotune_flux
+    DBuf<int64_t> tune_pre;  // chunk offsets of a candidate plan while timing
     std::vector<int64_t> face0, flat0, blk0, chunk_pre;
     std::vector<RingSet> slot_rings;
     // ring pool, one table per nlat
@@ -131,7 +134,7 @@ struct BatchState {
         area.release(); grav.release(); flux.release(); fp.release(); necl.release();
         ecl.release(); n0.release(); blockcnt.release(); queue.release(); counters.release();
         st.release(); ef.release(); runb.release(); rings.release(); es.release(); ehit.release(); d_tab.release();
-        rows.release(); gathered.release();
+        rows.release(); gathered.release(); tune_pre.release();
         if (h_rows) cudaFreeHost(h_rows);
         h_rows = nullptr;
         h_rows_cap = 0;
@@ -206,6 +209,7 @@ void ring_set(BatchState &B, int32_t nlat, RingSet &out) {
 lcg_status relayout(lcg_ctx *c, BatchState &B, const lcg_model *models, int32_t nmodels,
                     int32_t flags, int want_calc) {
     B.drop_graph();
+    B.tuned = false;
     B.nmodels = nmodels;
     B.n = c->data_n;
     B.nent = c->data_nent;
@@ -369,24 +373,133 @@ bool batchable(const lcg_model &m) {
            (!m.npole || (m.nlatfill == 0 && m.nlngfill == 0));
 }
 
+// Flux-plan autotuner. On the first call of a layout, once the stages before
+// the sweep have built the records and phases, each candidate plan (phase
+// entries per thread 4, 2 or 1; face chunks of 1024, 512, 256 or 128 faces) times
+// the batched sweep on them (one warm-up launch, then the mean of two timed
+// ones) and the fastest becomes the layout's plan for that call and every
+// later one (the captured graph included). The choice is kept per layout
+// (slot face counts, phase entries, SM count) for the whole process, so every
+// context evaluating that layout sums in the same chunks and gives the same
+// results; a new process measures again.
+struct PlanChoice {
+    int ppt;
+    int64_t chunk;
+};
+std::mutex g_plan_mu;
+std::map<std::vector<int64_t>, PlanChoice> g_plans;
+
+FluxPlan plan_for(const BatchState &B, int ppt, int64_t chunk, std::vector<int64_t> &pre) {
+    FluxPlan p = B.plan;
+    p.ppt = ppt;
+    p.chunk = chunk;
+    p.ntile = (B.nent + (int64_t)256 * ppt - 1) / ((int64_t)256 * ppt);
+    pre.assign((size_t)B.nslots + 1, 0);
+    for (int sl = 0; sl < B.nslots; sl++)
+        pre[sl + 1] = pre[sl] + (B.slot_rings[sl].nface + chunk - 1) / chunk;
+    p.nchunk = pre[B.nslots];
+    return p;
+}
+
+cudaError_t autotune_flux(lcg_ctx *c, BatchState &B) {
+    cudaStream_t s = c->stream;
+    cudaError_t e;
+    std::vector<int64_t> key = {B.nent, (int64_t)c->nsm, (int64_t)B.nslots};
+    for (int sl = 0; sl < B.nslots; sl++) key.push_back(B.slot_rings[sl].nface);
+    PlanChoice choice{0, 0};
+    {
+        std::lock_guard<std::mutex> lk(g_plan_mu);
+        auto it = g_plans.find(key);
+        if (it != g_plans.end()) choice = it->second;
+    }
+    if (!choice.ppt) {
+        const int ppts[] = {4, 2, 1};
+        const int64_t chunks[] = {1024, 512, 256, 128};
+        std::vector<FluxPlan> plans;
+        std::vector<std::vector<int64_t>> pres;
+        int64_t most = 0;
+        for (int64_t ch : chunks)
+            for (int ppt : ppts) {
+                std::vector<int64_t> pre;
+                FluxPlan p = plan_for(B, ppt, ch, pre);
+                if (p.nchunk * p.ntile >= (int64_t)0x7fffffff) continue;
+                most = std::max(most, p.nchunk);
+                plans.push_back(p);
+                pres.push_back(std::move(pre));
+            }
+        if (plans.empty()) return cudaSuccess;
+        if ((e = B.part.ensure((size_t)std::max<int64_t>(most, 1) * (size_t)B.ldp)) ||
+            (e = B.tune_pre.ensure((size_t)B.nslots + 1)))
+            return e;
+        cudaEvent_t ev0, ev1;
+        if ((e = cudaEventCreate(&ev0))) return e;
+        if ((e = cudaEventCreate(&ev1))) {
+            cudaEventDestroy(ev0);
+            return e;
+        }
+        const BatchPhases ph = B.phases();
+        double best = 1e300;
+        size_t pick = 0;
+        for (size_t i = 0; i < plans.size(); i++) {
+            cudaMemcpyAsync(B.tune_pre.p, pres[i].data(), pres[i].size() * sizeof(int64_t),
+                            cudaMemcpyHostToDevice, s);
+            BatchDev b = B.dev();
+            b.chunk_pre = B.tune_pre.p;
+            launch_batch_flux(b, ph, plans[i], B.part.p, B.ldp, s);  // warm-up
+            cudaEventRecord(ev0, s);
+            for (int r = 0; r < 2; r++) launch_batch_flux(b, ph, plans[i], B.part.p, B.ldp, s);
+            cudaEventRecord(ev1, s);
+            if ((e = cudaEventSynchronize(ev1))) break;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev0, ev1);
+            if (ms < best) {
+                best = ms;
+                pick = i;
+            }
+        }
+        cudaEventDestroy(ev0);
+        cudaEventDestroy(ev1);
+        if (e) return e;
+        choice = PlanChoice{plans[pick].ppt, plans[pick].chunk};
+        std::lock_guard<std::mutex> lk(g_plan_mu);
+        g_plans.emplace(key, choice);  // a concurrent first measurement keeps its own
+        choice = g_plans[key];
+    }
+    std::vector<int64_t> pre;
+    B.plan = plan_for(B, choice.ppt, choice.chunk, pre);
+    B.chunk_pre = pre;
+    if ((e = B.part.ensure((size_t)std::max<int64_t>(B.plan.nchunk, 1) * (size_t)B.ldp)))
+        return e;
+    const size_t bytes = pre.size() * sizeof(int64_t);
+    memcpy(B.tab<int64_t>(B.o_chunk), pre.data(), bytes);
+    cudaMemcpyAsync(B.d_tab.p + B.o_chunk, B.h_tab + B.o_chunk, bytes, cudaMemcpyHostToDevice, s);
+    return cudaSuccess;
+}
+
 // The stages of one batch on the context's stream.
-void enqueue(lcg_ctx *c, BatchState &B, bool timed) {
+// part: 0 every stage; 1 the table and the stages up to the phases; 2 the
+// sweep, the reduction and the result copies (the first call of a layout
+// runs 1, the flux autotuner, then 2).
+void enqueue(lcg_ctx *c, BatchState &B, bool timed, int part = 0) {
     cudaStream_t s = c->stream;
     const BatchDev b = B.dev();
     const BatchPhases ph = B.phases();
-    cudaMemcpyAsync(B.d_tab.p, B.h_tab, B.tab_bytes, cudaMemcpyHostToDevice, s);
-    cudaMemsetAsync(B.st.p, 0, (size_t)B.nmodels * sizeof(DevStatus), s);
     auto stage = [&](int id, auto &&fn) {
         Timer t;
         if (timed) c->stage_begin(id, t);
         fn();
         if (timed) c->stage_end(id, t);
     };
-    stage(LCG_STAGE_GRID, [&] { launch_batch_grid(b, c->nsm, s); });
-    stage(LCG_STAGE_ECLIPSE, [&] { launch_batch_eclipse(b, c->nsm, c->eclipse_warp, s); });
-    stage(LCG_STAGE_CONTINUUM, [&] { launch_batch_continuum(b, c->nsm, s); });
-    stage(LCG_STAGE_FLATTEN, [&] { launch_batch_flatten(b, c->nsm, s); });
-    stage(LCG_STAGE_PHASES, [&] { launch_batch_phases(b, c->data.p, c->off.p, B.n, ph, s); });
+    if (part != 2) {
+        cudaMemcpyAsync(B.d_tab.p, B.h_tab, B.tab_bytes, cudaMemcpyHostToDevice, s);
+        cudaMemsetAsync(B.st.p, 0, (size_t)B.nmodels * sizeof(DevStatus), s);
+        stage(LCG_STAGE_GRID, [&] { launch_batch_grid(b, c->nsm, s); });
+        stage(LCG_STAGE_ECLIPSE, [&] { launch_batch_eclipse(b, c->nsm, c->eclipse_warp, s); });
+        stage(LCG_STAGE_CONTINUUM, [&] { launch_batch_continuum(b, c->nsm, s); });
+        stage(LCG_STAGE_FLATTEN, [&] { launch_batch_flatten(b, c->nsm, s); });
+        stage(LCG_STAGE_PHASES, [&] { launch_batch_phases(b, c->data.p, c->off.p, B.n, ph, s); });
+    }
+    if (part == 1) return;
     stage(LCG_STAGE_FLUX, [&] { launch_batch_flux(b, ph, B.plan, B.part.p, B.ldp, s); });
     stage(LCG_STAGE_REDUCE, [&] {
         launch_batch_reduce(b, ph, B.part.p, B.ldp, B.osum.p, c->data.p, c->off.p, B.n,
@@ -575,7 +688,19 @@ extern "C" lcg_status lcg_light_curve_batch_resident(lcg_ctx *c, const lcg_model
         counts[1] = nc;
 
         cudaError_t e;
-        if (c->profiling) {
+        if (!B.tuned) {
+            // first call on this layout: the stages up to the phases, the
+            // measured flux plan, then the sweep with it
+            enqueue(c, B, c->profiling, 1);
+            if ((e = autotune_flux(c, B))) {
+                cudaStreamSynchronize(c->stream);
+                c->collect_timers();
+                B.nmodels = -1;
+                return c->cuda_fail(e, "flux autotuning");
+            }
+            B.tuned = true;
+            enqueue(c, B, c->profiling, 2);
+        } else if (c->profiling) {
             enqueue(c, B, true);
         } else {
             if (!B.exec) {
