@@ -53,6 +53,9 @@ def parse():
                              "surrogate_da", "cv_disc"))
     ap.add_argument("--batch-models", type=int, default=256,
                     help="models per step of mcmc_batch (256 is the benchmark)")
+    ap.add_argument("--batch-variant", choices=("geometry", "brightness"), default="geometry",
+                    help="mcmc_batch: q alternates between steps (every grid rebuilt), or only "
+                         "T1/T2 alternate (grids reused, continuum and flux recomputed)")
     ap.add_argument("--train-curves", type=int, default=200000)
     ap.add_argument("--epochs", type=int, default=60)
     ap.add_argument("--chains", type=int, default=512)
@@ -399,23 +402,35 @@ BATCH_DESC = ("mcmc_batch: 256 models around wd_dm_small (q~N(0.25,0.02), i~N(86
               "2000 points")
 
 
-def batch_workload(nmodels=256):
-    """The models, a second set with every q scaled by 1 + 1e-4 (so that
-    alternating steps rebuild every grid, as an MCMC step does), and noisy data
-    from the first model's curve."""
+BATCH_GRIDS = {
+    "geometry": "every model's grids rebuilt every step (q alternates by 1e-4)",
+    "brightness": "grids reused, continuum and flux recomputed every step (T1, T2 alternate by "
+                  "1e-4; geometry unchanged)",
+}
+
+
+def batch_workload(nmodels=256, variant="geometry"):
+    """The models, a second set with every q (variant "geometry": alternating
+    steps rebuild every grid, as an MCMC step does) or every T1 and T2
+    (variant "brightness": the grids stay, the continuum changes) scaled by
+    1 + 1e-4, and noisy data from the first model's curve."""
     from lcurve_re_b200 import workloads as W
     ms, d = W.mcmc_batch(nmodels)
     alt = []
+    fq, ft = (1 + 1e-4, 1.0) if variant == "geometry" else (1.0, 1 + 1e-4)
     for m in ms:
         c = m.to_c()
-        alt.append(W.model(q=c.q * (1 + 1e-4), iangle=c.iangle, r1=c.r1, r2=c.r2, t1=c.t1,
-                           t2=c.t2, nlat1f=c.nlat1f, nlat2f=c.nlat2f))
+        alt.append(W.model(q=c.q * fq, iangle=c.iangle, r1=c.r1, r2=c.r2, t1=c.t1 * ft,
+                           t2=c.t2 * ft, nlat1f=c.nlat1f, nlat2f=c.nlat2f))
     return ms, alt, d
 
 
-def cpu_batch_rate(models, data, sample=8, budget_s=20.0):
+def cpu_batch_rate(models, data, sample=8, budget_s=20.0, warm=None):
     """The reference CPU path on the first `sample` models of the batch (each
-    a cold call: grids rebuilt), scaled to the batch by total face count."""
+    a cold call: grids rebuilt), scaled to the batch by total face count.
+    With warm (the same models with only T1/T2 changed), each timed call
+    follows an untimed call on its warm partner, so the reference's own
+    per-thread grid cache (light_curve_comp.cpp:156-170) skips the grids."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_lib as OL
     kind = "reference"
@@ -428,7 +443,9 @@ def cpu_batch_rate(models, data, sample=8, budget_s=20.0):
     face_count_host = lambda m: counter.face_count(m, 0) + counter.face_count(m, 1)
     t_used, k = 0.0, 0
     f_used = 0
-    for m in models[:sample]:
+    for i, m in enumerate(models[:sample]):
+        if warm is not None:
+            lib.light_curve(warm[i], data)
         t = time.perf_counter()
         st, err, *_ = lib.light_curve(m, data)
         t_used += time.perf_counter() - t
@@ -442,9 +459,13 @@ def cpu_batch_rate(models, data, sample=8, budget_s=20.0):
     t_batch = t_used * f_all / f_used
     v = len(models) / t_batch
     return {"value": v, "unit": METRIC, "cores": os.cpu_count(), "kind": kind,
-            "sample": "%d of %d models, full %d points each, cold grids (%.2f s); scaled to the "
-                      "batch by total faces (%d of %d)" % (k, len(models), data.shape[0], t_used,
-                                                           f_used, f_all)}
+            "sample": "%d of %d models, full %d points each, %s (%.2f s); scaled to the "
+                      "batch by total faces (%d of %d)" % (
+                          k, len(models), data.shape[0],
+                          "cold grids" if warm is None else
+                          "grids from the reference's cache (only T1/T2 changed)" if
+                          kind == "reference" else "grids rebuilt (the port has no cache)",
+                          t_used, f_used, f_all)}
 
 
 def run_batch(args):
@@ -461,7 +482,7 @@ def run_batch(args):
     from lcurve_re_b200 import workloads as W
     from lcurve_re_b200.engine import Engine
 
-    ms, alt, data = batch_workload(args.batch_models)
+    ms, alt, data = batch_workload(args.batch_models, args.batch_variant)
     eng = Engine(device=local, precision="mixed")
     lib, ctx = eng.lib, eng.ctx
     calc0 = eng.light_curve_comp(ms[0], data, scale=False, rdata=False, diagnostics=False)[0]
@@ -572,7 +593,8 @@ def run_batch(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cpu = cpu_batch_rate(ms, data)
+            cpu = cpu_batch_rate(ms, data, warm=alt if args.batch_variant == "brightness"
+                                 else None)
         except Exception as ex:
             cpu = {"value": None, "unit": METRIC, "cores": os.cpu_count(), "kind": "unavailable",
                    "sample": str(ex)}
@@ -585,7 +607,7 @@ def run_batch(args):
         "data": "synthetic (seeded models + Gaussian noise sigma=1.5e-3)",
         "config": {"workload": BATCH_DESC, "models_per_step": nm, "faces_per_step": int(sum(faces)),
                    "points": n, "precision": "mixed",
-                   "grids": "every model's grids rebuilt every step (q alternates by 1e-4)",
+                   "grids": BATCH_GRIDS[args.batch_variant],
                    "l2": "flushed by a 256 MiB write between timed steps (untimed)",
                    "graph": "one CUDA graph per step", "parallelism": "replicas x%d" % world},
         "roofline": {"bound": "fp32", "kernel": "k_flux_batch", "achieved": achieved,
@@ -614,18 +636,21 @@ def run_reference_batch(args):
     if rank != 0:
         return 0
     from lcurve_re_b200 import workloads as W
-    ms, alt, data = batch_workload()
+    ms, alt, data = batch_workload(variant=args.batch_variant)
+    warm = alt if args.batch_variant == "brightness" else None
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_lib as OL
     calc0 = OL.Oracle().light_curve(ms[0], data, scale=False, rdata=False)[2]
     data = W.add_noise(data, calc0, seed=1234)
-    vals = [cpu_batch_rate(ms, data, sample=2, budget_s=8.0) for _ in range(args.warmup + args.steps)]
+    vals = [cpu_batch_rate(ms, data, sample=2, budget_s=8.0, warm=warm)
+            for _ in range(args.warmup + args.steps)]
     vals = vals[args.warmup:]
     v = float(np.mean([x["value"] for x in vals]))
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 256 / v * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": BATCH_DESC, "precision": "fp64 (reference CPU)"},
+            "data": "synthetic", "config": {"workload": BATCH_DESC, "precision": "fp64 (reference CPU)",
+                                            "grids": BATCH_GRIDS[args.batch_variant]},
             "cpu_baseline": dict(vals[-1], value=v),
             "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)

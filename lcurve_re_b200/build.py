@@ -34,7 +34,8 @@ SOURCES = {
     "mlp.cu": ["--fmad=true"],
     "components.cu": ["--fmad=false"],
 }
-HEADERS = ["roche.cuh", "eclipse.cuh", "disc.cuh", "engine.h", "tma.cuh", "context.h"]
+HEADERS = ["roche.cuh", "eclipse.cuh", "disc.cuh", "ecl_screen.cuh", "engine.h", "tma.cuh",
+           "context.h"]
 
 
 def nvcc():

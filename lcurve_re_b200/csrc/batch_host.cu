@@ -161,6 +161,7 @@ struct BatchState {
         b.n0 = n0.p;
         b.blockcnt = blockcnt.p;
         b.queue = queue.p;
+        b.qcap = nfaces;
         b.counters = counters.p;
         b.es = es.p;
         b.ehit = ehit.p;
@@ -315,7 +316,7 @@ lcg_status relayout(lcg_ctx *c, BatchState &B, const lcg_model *models, int32_t 
         (e = B.fp.ensure(8 * (size_t)B.nflat)) || (e = B.ecl.ensure((size_t)B.nflat)) ||
         (e = B.runb.ensure((size_t)B.nflat / 64)) ||
         (e = B.n0.ensure(ns)) || (e = B.blockcnt.ensure((size_t)B.nblk)) ||
-        (e = B.counters.ensure(4)) || (e = B.st.ensure(nm)) ||
+        (e = B.counters.ensure(8)) || (e = B.st.ensure(nm)) ||
         (e = B.es.ensure(nf)) || (e = B.ehit.ensure(nf)) ||
         (e = B.ef.ensure(nm * (size_t)B.ldp)) || (e = B.w1.ensure(nm * (size_t)B.ldp)) ||
         (e = B.w2.ensure(nm * (size_t)B.ldp)) ||
@@ -633,6 +634,7 @@ extern "C" lcg_status lcg_light_curve_batch_resident(lcg_ctx *c, const lcg_model
                     ep.cosi = cos(ri);
                     ep.sini = sin(ri);
                     ep.delta = M.delta_phase;
+                    set_ecl_screen(ep, 1, star == kStar1 ? su.r1 : su.r2);  // batches are mixed
                     X.eclipse_on = su.eclipse;
                 }
             }

@@ -451,6 +451,7 @@ lcg_status build_geometry(lcg_ctx *c, const lcg_model &m, int star, int fine, Gr
     ep.cosi = cos(ri);
     ep.sini = sin(ri);
     ep.delta = m.delta_phase;
+    set_ecl_screen(ep, c->precision == LCG_PREC_MIXED, star == kStar1 ? s.r1 : s.r2);
     {
         StageScope t(c, LCG_STAGE_ECLIPSE);
         launch_eclipse(ep, s.eclipse, g.dev(), g.queue.p, g.counters.p, g.es.p, g.ehit.p,

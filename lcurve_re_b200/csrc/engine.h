@@ -7,6 +7,7 @@
 
 #include "roche.cuh"
 #include "disc.cuh"
+#include "ecl_screen.cuh"
 
 namespace lcg {
 
@@ -51,7 +52,16 @@ struct EclParams {
     int32_t comp_star;   // the eclipsing star
     int32_t comp_roche;  // Roche-distorted eclipser (else a sphere of radius comp_r)
     double q, comp_spin, comp_rref, comp_pref, comp_r, cosi, sini, delta;
+    EclScreen scr;       // FP32 screen of the bisections' line-of-sight tests
 };
+
+// The FP32 screen runs in mixed contexts when neither the eclipsed star
+// (radius r_face) nor the eclipser (reference sphere rref) is tiny: a white
+// dwarf's own eclipse boundaries, and eclipses by one, stay with FP64 alone.
+inline void set_ecl_screen(EclParams &ep, int mixed, double r_face) {
+    ep.scr = make_ecl_screen(ep.comp_star, ep.q, ep.comp_spin, ep.comp_rref, ep.comp_pref);
+    ep.scr.on = mixed && ep.comp_roche && r_face >= 0.01 && ep.comp_rref >= 0.05;
+}
 
 // Continuum of one star (set_star_continuum.cpp:26-297).
 struct ContParams {
@@ -198,7 +208,12 @@ struct BatchDev {
     float4 *runb;  // FlatDev::runb per slot, from flat0 / 64
     uint2 *ecl;
     int64_t *n0;  // per slot
-    int32_t *blockcnt, *queue, *counters;  // counters: 4 work counters
+    // eclipse candidates: those whose bisections the FP32 screen serves go to
+    // the front of queue, the others (FP64 alone) to the back, so that warps
+    // do not mix the two; counters: [0] candidates, [1]-[3] work counters of
+    // the passes, [4] back-of-queue candidates, [5] front-of-queue ones
+    int32_t *blockcnt, *queue, *counters;
+    int64_t qcap;  // queue capacity (faces of the batch)
     // eclipse candidates between the two passes of the thread mode: per queue
     // entry (phase of the potential minimum, phi1, phi2, ACC) and a hit flag
     double4 *es;

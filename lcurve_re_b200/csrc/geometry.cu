@@ -9,6 +9,8 @@
 //   k_scatter    merge of the flux partials into the light curve (:457-498)
 //   k_finalize   scale factor and chi**2 (re_scale.cpp:16-42, light_curve_comp.cpp:557-585)
 //   k_diag       sums behind logg and the volume-averaged radius (comp_gravity.cpp, comp_radius.cpp)
+#include <stdlib.h>
+
 #include "eclipse.cuh"
 #include "engine.h"
 
@@ -191,6 +193,65 @@ __global__ void __launch_bounds__(128, 4) k_ecl_roche(EclParams p, GridDev g,
     }
 }
 
+// One test of a bisection: the FP32 screen where p.scr allows it (it decides
+// only where the FP64 test's answer is certain, so the bisection takes the
+// same midpoints), else Roche::fblink in FP64. u0: the point relative to the
+// eclipser's centre, in FP32.
+__device__ __noinline__ int ecl_screen_test(const EclScreen scr, float cosi, float sini,
+                                            double pmid, float u0x, float u0y, float u0z,
+                                            float acc) {
+    const double ph = pmid - rint(pmid);  // |ph| <= 1/2 keeps the FP32 angle fine
+    float sn, cs;
+    sincospif(2.f * (float)ph, &sn, &cs);
+    return fblink_screen(scr, u0x, u0y, u0z, sini * cs, -sini * sn, cosi, acc);
+}
+
+// The bisection of ingress (side 0) or egress (side 1) of ingress_egress
+// (ingress_egress.cpp:61-86) from the pot_min state, for every lane of a warp
+// at once (all 32 lanes call it; lanes with live false only vote). Each lane
+// screens its midpoints in FP32 until one is unsure; when no live lane can go
+// on, the warp runs Roche::fblink in FP64 for all the lanes waiting on one, in
+// a single pass, and the screening resumes. The FP64 passes are thus packed
+// (one per test of the lane that needs the most, instead of one per step
+// whenever any lane needs one), and the lanes take the FP64 decisions at the
+// same midpoints as the plain loop. With the screen off it is the plain loop.
+__device__ __forceinline__ double ecl_bisect_warp(const EclParams &p, bool live, double pin,
+                                                  double pout, double acc, V3 pos, int &s) {
+    // what the screening loop reads, in registers (p may be global memory;
+    // the FP64 test, a third of the steps, reads the rest from it)
+    const EclScreen scr = p.scr;
+    const double delta = p.delta;
+    const float cif = (float)p.cosi, sif = (float)p.sini, accf = (float)acc;
+    const float u0x = (float)(pos.x - (p.comp_star == kStar1 ? 0. : 1.));
+    const float u0y = (float)pos.y, u0z = (float)pos.z;
+    bool done = !live;
+    int guard = 0;
+    double pmid = 0.;
+    for (;;) {
+        bool need = false;
+        while (!done) {
+            if (!(fabs(pin - pout) > delta)) { done = true; break; }
+            if (++guard > 400) { s = kEclNoConverge; done = true; break; }
+            pmid = (pin + pout) / 2.;
+            if (!scr.on) { need = true; break; }
+            const int d = ecl_screen_test(scr, cif, sif, pmid, u0x, u0y, u0z, accf);
+            if (d == kScreenUnsure) { need = true; break; }
+            if (d == kScreenTrue) pin = pmid;
+            else pout = pmid;
+        }
+        if (!__any_sync(0xffffffffu, need)) break;
+        if (need) {
+            if (fblink(p.comp_star, p.q, p.comp_spin, acc, set_earth(p.cosi, p.sini, pmid), pos,
+                       p.comp_rref, p.comp_pref, s))
+                pin = pmid;
+            else
+                pout = pmid;
+            if (s) done = true;
+        }
+    }
+    return (pin + pout) / 2.;
+}
+
 // Thread mode (more candidates than warp_max), in two passes with a small code
 // footprint each, as for the batch (k_ecl_potmin_b / k_ecl_bisect_b): the
 // sphere test and pot_min per candidate, then ingress and egress on the two
@@ -230,14 +291,13 @@ __global__ void __launch_bounds__(128, 4) k_ecl_potmin(EclParams p, GridDev g,
     }
 }
 
-__global__ void __launch_bounds__(128, 6) k_ecl_bisect(EclParams p, GridDev g,
-                                                    const int32_t *__restrict__ queue,
-                                                    int32_t *counters, const double4 *es,
-                                                    const uint8_t *ehit, DevStatus *st,
-                                                    int32_t warp_max) {
+template <int NB>
+__global__ void __launch_bounds__(128, NB)
+    k_ecl_bisect(__grid_constant__ const EclParams p, __grid_constant__ const GridDev g,
+                 const int32_t *__restrict__ queue, int32_t *counters, const double4 *es,
+                 const uint8_t *ehit, DevStatus *st, int32_t warp_max) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    const unsigned pair = 3u << (lane & ~1);
     const int total = counters[0];
     if (total <= warp_max) return;
     const int64_t n2 = 2 * (int64_t)total;
@@ -246,30 +306,20 @@ __global__ void __launch_bounds__(128, 6) k_ecl_bisect(EclParams p, GridDev g,
         if (lane == 0) base = atomicAdd(&counters[3], 32);
         base = __shfl_sync(full, base, 0);
         if (base >= n2) break;
+        // every lane stays here (ecl_bisect_warp votes over the warp); both
+        // lanes of a pair agree on live
         const int64_t u = base + lane;
-        if (u >= n2) continue;
         const int k = (int)(u >> 1), side = (int)(u & 1);
-        if (!ehit[k]) continue;  // both lanes of a pair
-        const int32_t i = queue[k];
-        const double4 E = es[k];
-        const V3 pos = v3(g.px[i], g.py[i], g.pz[i]);
-        double pin = E.x, pout = side ? E.z : E.y, pmid;
-        int s = 0, guard = 0;
-        while (fabs(pin - pout) > p.delta) {
-            if (++guard > 400) { s = kEclNoConverge; break; }
-            pmid = (pin + pout) / 2.;
-            if (fblink(p.comp_star, p.q, p.comp_spin, E.w, set_earth(p.cosi, p.sini, pmid), pos,
-                       p.comp_rref, p.comp_pref, s))
-                pin = pmid;
-            else
-                pout = pmid;
-            if (s) break;
-        }
-        double v = (pin + pout) / 2.;
+        const bool live = u < n2 && ehit[k];
+        const int32_t i = live ? queue[k] : 0;
+        const double4 E = live ? es[k] : make_double4(0., 0., 0., 0.);
+        const V3 pos = live ? v3(g.px[i], g.py[i], g.pz[i]) : v3(0., 0., 0.);
+        int s = 0;
+        double v = ecl_bisect_warp(p, live, E.x, side ? E.z : E.y, E.w, pos, s);
         v = v - floor(v);
-        const double other = __shfl_xor_sync(pair, v, 1);
-        const int os = __shfl_xor_sync(pair, s, 1);
-        if (side == 0) {
+        const double other = __shfl_xor_sync(full, v, 1);
+        const int os = __shfl_xor_sync(full, s, 1);
+        if (live && side == 0) {
             if (s || os) {
                 set_status(st, s ? s : os, i);
             } else {
@@ -948,7 +998,7 @@ __global__ void k_ecl_pre_b(BatchDev b) {
     for (int64_t u0 = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31); u0 < total;
          u0 += stride) {
         const int64_t u = u0 + lane;
-        bool cand = false;
+        bool cand = false, scr = false;
         int32_t item = 0;
         if (u < total) {
             const int k = find_seg(b.geo_face, nk, u);
@@ -956,9 +1006,35 @@ __global__ void k_ecl_pre_b(BatchDev b) {
             const int64_t i = u - b.geo_face[k];
             cand = ecl_pre_face(S.ep, S.eclipse_on, slot_grid(b.g, S.face0, S.nface, S.ntiled), i);
             item = (int32_t)(S.face0 + i);
+            scr = S.ep.scr.on;
         }
-        queue_push(cand, item, b.queue, b.counters);
+        // screened candidates to the front of the queue, the others to the back
+        const unsigned back = __ballot_sync(0xffffffffu, cand && !scr);
+        queue_push(cand && scr, item, b.queue, b.counters);
+        if (back) {
+            const int leader = __ffs(back) - 1;
+            int base = 0;
+            if (lane == leader) base = atomicAdd(&b.counters[4], __popc(back));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (cand && !scr)
+                b.queue[b.qcap - 1 - (base + __popc(back & ((1u << lane) - 1u)))] = item;
+        }
     }
+}
+
+// After k_ecl_pre_b: the candidate count covers both ends of the queue;
+// counters[5] keeps the front's.
+__global__ void k_ecl_join_b(BatchDev b) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        b.counters[5] = b.counters[0];
+        b.counters[0] += b.counters[4];
+    }
+}
+
+// Candidate k of the batch queue (front, then back in push order).
+__device__ __forceinline__ int32_t queue_at(const BatchDev &b, int k) {
+    const int front = b.counters[5];
+    return k < front ? b.queue[k] : b.queue[b.qcap - 1 - (k - front)];
 }
 
 // k_ecl_roche over the batch queue: each candidate finds its slot by its
@@ -977,7 +1053,7 @@ __global__ void __launch_bounds__(128, 4) k_ecl_roche_b(BatchDev b, int32_t warp
             if (lane == 0) k = atomicAdd(&b.counters[1], 1);
             k = __shfl_sync(full, k, 0);
             if (k >= total) break;
-            const int32_t i = b.queue[k];
+            const int32_t i = queue_at(b, k);
             const SlotDev &S = b.slots[find_seg(b.face0, b.nslots, i)];
             const EclParams &p = S.ep;
             const V3 pos = v3(g.px[i], g.py[i], g.pz[i]);
@@ -1019,7 +1095,7 @@ __global__ void __launch_bounds__(128, 4) k_ecl_potmin_b(BatchDev b, int32_t war
         if (base >= total) break;
         const int k = base + lane;
         if (k >= total) continue;
-        const int32_t i = b.queue[k];
+        const int32_t i = queue_at(b, k);
         const SlotDev &S = b.slots[find_seg(b.face0, b.nslots, i)];
         const EclParams &p = S.ep;
         const V3 pos = v3(g.px[i], g.py[i], g.pz[i]);
@@ -1043,53 +1119,41 @@ __global__ void __launch_bounds__(128, 4) k_ecl_potmin_b(BatchDev b, int32_t war
 
 // 6 blocks of 4 warps per SM (a sweep of 4, 5, 6 and 8 on B200 chose 6: more
 // warps hide the FP64 latency, fewer registers spill more)
-__global__ void __launch_bounds__(128, 6) k_ecl_bisect_b(BatchDev b, int32_t warp_max) {
+template <int NB>
+__global__ void __launch_bounds__(128, NB)
+    k_ecl_bisect_b(__grid_constant__ const BatchDev b, int32_t warp_max) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    const unsigned pair = 3u << (lane & ~1);
     const int total = b.counters[0];
     if (total <= warp_max) return;
-    const GridDev g = b.g;
     const int64_t n2 = 2 * (int64_t)total;
     for (;;) {
         int64_t base = 0;
         if (lane == 0) base = atomicAdd(&b.counters[3], 32);
         base = __shfl_sync(full, base, 0);
         if (base >= n2) break;
-        const int64_t u = base + lane;  // both lanes of a pair agree on u < n2
-        if (u >= n2) continue;
+        const int64_t u = base + lane;
         const int k = (int)(u >> 1), side = (int)(u & 1);
-        if (!b.ehit[k]) continue;  // so do both lanes of a pair here
-        const int32_t i = b.queue[k];
-        const SlotDev &S = b.slots[find_seg(b.face0, b.nslots, i)];
-        const EclParams &p = S.ep;
-        const double4 E = b.es[k];
-        const V3 pos = v3(g.px[i], g.py[i], g.pz[i]);
-        double pin = E.x, pout = side ? E.z : E.y, pmid;
-        int s = 0, guard = 0;
-        while (fabs(pin - pout) > p.delta) {
-            if (++guard > 400) { s = kEclNoConverge; break; }
-            pmid = (pin + pout) / 2.;
-            if (fblink(p.comp_star, p.q, p.comp_spin, E.w, set_earth(p.cosi, p.sini, pmid), pos,
-                       p.comp_rref, p.comp_pref, s))
-                pin = pmid;
-            else
-                pout = pmid;
-            if (s) break;
-        }
-        double v = (pin + pout) / 2.;
+        const bool live = u < n2 && b.ehit[k];
+        const int32_t i = live ? queue_at(b, k) : 0;
+        const int sl = find_seg(b.face0, b.nslots, i);
+        const double4 E = live ? b.es[k] : make_double4(0., 0., 0., 0.);
+        const V3 pos = live ? v3(b.g.px[i], b.g.py[i], b.g.pz[i]) : v3(0., 0., 0.);
+        int s = 0;
+        double v = ecl_bisect_warp(b.slots[sl].ep, live, E.x, side ? E.z : E.y, E.w, pos, s);
         v = v - floor(v);
-        const double other = __shfl_xor_sync(pair, v, 1);
-        const int os = __shfl_xor_sync(pair, s, 1);
-        if (side == 0) {
+        const double other = __shfl_xor_sync(full, v, 1);
+        const int os = __shfl_xor_sync(full, s, 1);
+        if (live && side == 0) {
+            const SlotDev &S = b.slots[sl];
             if (s || os) {
                 set_status(b.st + S.model, s ? s : os, i - S.face0);
             } else {
                 double egr = other;
                 if (egr < v) egr++;
-                g.necl[i] = 1;
-                g.ein[i] = v;
-                g.eout[i] = egr;
+                b.g.necl[i] = 1;
+                b.g.ein[i] = v;
+                b.g.eout[i] = egr;
             }
         }
     }
@@ -1270,6 +1334,18 @@ void launch_grid(const GridParams &p, const RingRec *rings, GridDev g, DevStatus
     count_launch();
 }
 
+// Resident blocks of 128 threads per SM for the bisection kernels: 4 (no
+// register spills, 128 registers a thread) or 6 (80 registers, a few
+// spills, more warps to hide FP64 latency); LCG_ECL_BISECT_BLOCKS=6 selects
+// the second, for measurement.
+int bisect_blocks_per_sm() {
+    static const int nb = [] {
+        const char *v = getenv("LCG_ECL_BISECT_BLOCKS");
+        return (v && atoi(v) == 6) ? 6 : 4;
+    }();
+    return nb;
+}
+
 void launch_eclipse(const EclParams &p, int32_t eclipse_on, GridDev g, int32_t *queue,
                     int32_t *counters, double4 *es, uint8_t *ehit, DevStatus *st, int nsm,
                     int32_t warp_mode, cudaStream_t s) {
@@ -1288,8 +1364,13 @@ void launch_eclipse(const EclParams &p, int32_t eclipse_on, GridDev g, int32_t *
         count_launch();
         k_ecl_potmin<<<nb, 128, 0, s>>>(p, g, queue, counters, es, ehit, st, warp_max);
         count_launch();
-        const unsigned nb6 = need < (unsigned)nsm * 6u ? need : (unsigned)nsm * 6u;
-        k_ecl_bisect<<<nb6, 128, 0, s>>>(p, g, queue, counters, es, ehit, st, warp_max);
+        const int nbs = bisect_blocks_per_sm();
+        const unsigned cap = (unsigned)nsm * (unsigned)nbs;
+        const unsigned nbb = need < cap ? need : cap;
+        if (nbs == 6)
+            k_ecl_bisect<6><<<nbb, 128, 0, s>>>(p, g, queue, counters, es, ehit, st, warp_max);
+        else
+            k_ecl_bisect<4><<<nbb, 128, 0, s>>>(p, g, queue, counters, es, ehit, st, warp_max);
         count_launch();
     }
 }
@@ -1394,8 +1475,10 @@ void launch_batch_grid(const BatchDev &b, int nsm, cudaStream_t s) {
 }
 
 void launch_batch_eclipse(const BatchDev &b, int nsm, int32_t warp_mode, cudaStream_t s) {
-    cudaMemsetAsync(b.counters, 0, 4 * sizeof(int32_t), s);
+    cudaMemsetAsync(b.counters, 0, 8 * sizeof(int32_t), s);
     k_ecl_pre_b<<<nsm * 4, 256, 0, s>>>(b);
+    count_launch();
+    k_ecl_join_b<<<1, 32, 0, s>>>(b);
     count_launch();
     const int32_t warps = nsm * 16;
     const int32_t warp_max = warp_mode < 0 ? -1 : warp_mode > 0 ? warp_mode : 2 * warps;
@@ -1403,7 +1486,10 @@ void launch_batch_eclipse(const BatchDev &b, int nsm, int32_t warp_mode, cudaStr
     count_launch();
     k_ecl_potmin_b<<<nsm * 4, 128, 0, s>>>(b, warp_max);
     count_launch();
-    k_ecl_bisect_b<<<nsm * 6, 128, 0, s>>>(b, warp_max);
+    if (bisect_blocks_per_sm() == 6)
+        k_ecl_bisect_b<6><<<nsm * 6, 128, 0, s>>>(b, warp_max);
+    else
+        k_ecl_bisect_b<4><<<nsm * 4, 128, 0, s>>>(b, warp_max);
     count_launch();
 }
 

@@ -80,6 +80,27 @@ def test_eclipse_warp_and_thread_modes_agree(oracle):
         thread.close()
 
 
+def test_eclipse_fp32_screen_keeps_the_fp64_decisions():
+    """Mixed contexts screen the bisections' line-of-sight tests in FP32 and
+    run the FP64 test only where the screen is unsure: eclipse flags and
+    phases equal the FP64 context's bit for bit (thread mode, where the
+    screen runs), on the parity cases and on batch models."""
+    from lcurve_re_b200.engine import Engine
+    fp64 = Engine(precision="fp64", eclipse_warp=-1)
+    mixed = Engine(precision="mixed", eclipse_warp=-1)
+    try:
+        ms, _ = W.mcmc_batch(256)
+        cases = [(n, m) for n, m, _ in CASES] + [("batch%d" % k, ms[k]) for k in range(0, 256, 16)]
+        for name, m in cases:
+            for star in (0, 1):
+                a, b = fp64.star_grid(m, star), mixed.star_grid(m, star)
+                for k in ("neclipse", "ecl_in", "ecl_out"):
+                    assert np.array_equal(a[k], b[k]), (name, star, k)
+    finally:
+        fp64.close()
+        mixed.close()
+
+
 def test_flux_fp64_bit_exact(engine_fp64, oracle):
     m, d = W.wd_dm_small()
     ph = oracle.phase_batch(m, W.data(700, ndiv=3, expose=0.002))
