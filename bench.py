@@ -66,10 +66,6 @@ def parse():
     ap.add_argument("--refine-epochs", type=int, default=600)
     ap.add_argument("--da-scale", type=float, default=2.6)
     ap.add_argument("--local-widen", type=float, default=2.0)
-    ap.add_argument("--equilibrate", type=int, default=0,
-                    help="surrogate_da: further burn-in steps, run with delayed acceptance in "
-                         "two rounds that adapt the proposal (the network refined again "
-                         "after them), so that both timed samplers start from equilibrium")
     ap.add_argument("--precision", choices=("mixed", "fp64"), default="mixed")
     ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -751,35 +747,6 @@ def run_surrogate(args):
     glob_err_loc = float(np.sqrt(np.mean((sur.curves(th_lh) - cu_lh) ** 2)))
     exact = ExactChi2(eng, data)
     sur_loc_chi = S.SurrogateChi2(sur_loc, data, idx)
-    # optional equilibration (untimed burn-in, shared by both samplers): delayed
-    # acceptance keeps the exact posterior invariant and is cheap per step, so
-    # it carries the chains along the posterior's ridges far sooner than plain
-    # Metropolis; each round re-adapts the proposal, and the network is
-    # refined again around where the chains went
-    eq_acc = []
-    if args.equilibrate > 0:
-        for k in range(2):
-            ex_eq = ExactChi2(eng, data, curves=True)
-            che, theta0, _, acc_e, _, _ = delayed_acceptance(
-                ex_eq, sur_loc_chi, theta0, cov * args.da_scale ** 2, args.equilibrate // 2,
-                seed=31 + k)
-            eq_acc.append(float(acc_e))
-            samp = che[che.shape[0] // 2:].reshape(-1, 9)
-            cov = np.cov(samp.T) * 2.38 ** 2 / 9 + np.diag((scale0 * 1e-3) ** 2)
-            del che
-        th_loc = S.local_draws(samp.mean(0), np.cov(samp.T), args.local_curves, seed=6 + rank,
-                               widen=args.local_widen)
-        t0 = time.perf_counter()
-        _, cu_loc = S.training_set(eng, 0, theta=th_loc, batch=2048)
-        sur_loc = S.Surrogate(ncoef=args.ncoef, batch=4096, seed=rank + 2)
-        losses_loc = sur_loc.fit(th_loc, cu_loc, epochs=args.refine_epochs)
-        t_ref += time.perf_counter() - t0
-        th_lh = S.local_draws(samp.mean(0), np.cov(samp.T), 2048, seed=78 + rank,
-                              widen=args.local_widen)
-        _, cu_lh = S.training_set(eng, 0, theta=th_lh, batch=2048)
-        loc_err = float(np.sqrt(np.mean((sur_loc.curves(th_lh) - cu_lh) ** 2)))
-        glob_err_loc = float(np.sqrt(np.mean((sur.curves(th_lh) - cu_lh) ** 2)))
-        sur_loc_chi = S.SurrogateChi2(sur_loc, data, idx)
     # inference throughput of the network alone (the DA screening pass)
     xin = torch.rand(args.chains, 9, device="cuda") * 2 - 1
     for _ in range(3):
@@ -863,8 +830,6 @@ def run_surrogate(args):
         "gpu_launches": launches_da,
         "gpu_launches_plain": launches_plain,
         "da_proposal_scale": args.da_scale,
-        "equilibration": {"steps": args.equilibrate, "sampler": "delayed acceptance, 2 rounds",
-                          "acceptance": eq_acc},
         "clocks": clk,
     }
     if rank == 0:
