@@ -61,6 +61,13 @@ def parse():
     ap.add_argument("--chains", type=int, default=512)
     ap.add_argument("--mcmc-steps", type=int, default=2000)
     ap.add_argument("--burn", type=int, default=400)
+    ap.add_argument("--compact", type=int, default=32,
+                    help="surrogate_da: delayed acceptance's exact evaluations through a "
+                         "batch of this many slots on a second engine context (0: the "
+                         "whole-chain batch)")
+    ap.add_argument("--burn-fixed", type=int, default=2000,
+                    help="surrogate_da: plain Metropolis steps after the adaptive burn-in, "
+                         "with its final proposal kept (no further adaptation)")
     ap.add_argument("--ncoef", type=int, default=64)
     ap.add_argument("--local-curves", type=int, default=131072)
     ap.add_argument("--refine-epochs", type=int, default=600)
@@ -683,8 +690,8 @@ def run_surrogate(args):
     from lcurve_re_b200 import surrogate as S
     from lcurve_re_b200 import workloads as W
     from lcurve_re_b200.engine import Engine
-    from lcurve_re_b200.sampler import (ExactChi2, delayed_acceptance, ess_between_chains,
-                                        ess_total, metropolis)
+    from lcurve_re_b200.sampler import (CompactExact, ExactChi2, delayed_acceptance,
+                                        ess_between_chains, ess_total, metropolis)
 
     eng = Engine(device=local, precision="mixed")
     clocks = Clocks(local)
@@ -730,9 +737,13 @@ def run_surrogate(args):
         ch, theta0, _, acc_b, _ = metropolis(exact, theta0, cov, args.burn // 2, seed=11 + k)
         samp = ch[ch.shape[0] // 2:].reshape(-1, 9)
         cov = np.cov(samp.T) * 2.38 ** 2 / 9 + np.diag((scale0 * 1e-3) ** 2)
+    if args.burn_fixed > 0:
+        chf, theta0, _, _, _ = metropolis(exact, theta0, cov, args.burn_fixed, seed=13)
+        samp_f = chf[chf.shape[0] // 2:].reshape(-1, 9)
+        del chf
     # refinement: the same network trained again on engine curves around the
     # burn-in posterior (Gaussian, local_widen x its spread, inside the box)
-    samp = ch[ch.shape[0] // 2:].reshape(-1, 9)
+    samp = ch[ch.shape[0] // 2:].reshape(-1, 9) if args.burn_fixed <= 0 else samp_f
     th_loc = S.local_draws(samp.mean(0), np.cov(samp.T), args.local_curves, seed=5 + rank,
                            widen=args.local_widen)
     t0 = time.perf_counter()
@@ -765,13 +776,16 @@ def run_surrogate(args):
     # delayed acceptance can afford bolder proposals: the surrogate screens them
     cov_da = cov * args.da_scale ** 2
     n_plain = exact.evals - e_plain0
+    eng_c = Engine(device=local, precision="mixed") if args.compact > 0 else None
     exact_g = ExactChi2(eng, data, curves=True)
+    comp_g = CompactExact(eng_c, data, k=args.compact) if eng_c else None
     chg, _, _, accg, wall_g, stg = delayed_acceptance(exact_g, sur_chi, theta0, cov_da,
-                                                       args.mcmc_steps, seed=21)
+                                                       args.mcmc_steps, seed=21, compact=comp_g)
     exact2 = ExactChi2(eng, data, curves=True)
+    comp2 = CompactExact(eng_c, data, k=args.compact) if eng_c else None
     lib.lcg_kernel_launches(1)
     chd, _, _, accd, wall_d, st = delayed_acceptance(exact2, sur_loc_chi, theta0, cov_da,
-                                                      args.mcmc_steps, seed=21)
+                                                      args.mcmc_steps, seed=21, compact=comp2)
     launches_da = int(lib.lcg_kernel_launches(1))
     clk = clocks.stop()
     ess_g, _ = ess_total(chg)
@@ -786,7 +800,7 @@ def run_surrogate(args):
     line = {
         "metric": "MCMC effective samples/s", "value": ess_d / wall_d,
         "unit": "effective samples/s", "n_gpus": world, "steps": args.mcmc_steps,
-        "warmup": args.burn, "ms_per_step": wall_d / args.mcmc_steps * 1e3,
+        "warmup": args.burn + args.burn_fixed, "ms_per_step": wall_d / args.mcmc_steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "bf16 tensor-core MLP (fp32 accumulate) + f32/f64 engine",
         "data": "synthetic (wd_dm_small physics at 500 points + noise sigma=1.5e-3)",
@@ -801,12 +815,15 @@ def run_surrogate(args):
                   "ess_between_chains": ess_between_chains(chp)[0]},
         "delayed_acceptance": {"surrogate": "refined around the burn-in posterior",
                                "ess": ess_d, "ess_per_s": ess_d / wall_d, "wall_s": wall_d,
-                               "acceptance": accd, "exact_evals": exact2.evals,
+                               "acceptance": accd,
+                               "exact_evals": exact2.evals + (comp2.evals if comp2 else 0),
+                               "exact_batch": "%d slots" % args.compact if comp2 else "chains",
                                "ess_between_chains": ess_between_chains(chd)[0], **st},
         "delayed_acceptance_global": {"surrogate": "prior box only",
                                       "ess": ess_g, "ess_per_s": ess_g / wall_g,
                                       "wall_s": wall_g, "acceptance": accg,
-                                      "exact_evals": exact_g.evals,
+                                      "exact_evals": exact_g.evals +
+                                      (comp_g.evals if comp_g else 0),
                                       "posterior_mean_shift_sigma_max": float(shift_g.max()),
                                       **stg},
         "ess_per_s_ratio": (ess_d / wall_d) / (ess_p / wall_p),
@@ -834,6 +851,8 @@ def run_surrogate(args):
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
+    if eng_c is not None:
+        eng_c.close()
     eng.close()
     return 0
 

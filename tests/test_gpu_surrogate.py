@@ -129,3 +129,48 @@ def test_device_delayed_acceptance_equals_the_general_loop(trained):
         out.append((ch, chi, st))
     assert np.array_equal(out[0][0], out[1][0])
     assert np.array_equal(out[0][1], out[1][1])
+
+
+def test_compact_exact_matches_the_whole_chain_batch(trained):
+    """CompactExact (the stage-1 chains through a small batch on a second
+    context) gives the chi**2 and curves of the whole-chain batch for those
+    chains, including across calls that refill only some slots, and a delayed
+    acceptance run through it keeps the exact posterior's checks. The two
+    batch layouts may sum their flux chunks differently (each layout's plan is
+    tuned on its own), so they agree to the batch tolerances: curves 2e-6,
+    chi**2 1e-5 relative."""
+    from lcurve_re_b200.engine import Engine
+    from lcurve_re_b200.sampler import CompactExact, ExactChi2, delayed_acceptance
+    import torch
+    e, sur, theta, curves, _ = trained
+    idx = np.arange(0, S.NGRID, 2)
+    truth = np.array([0.25, 86.0, 0.015, 0.20, 20000.0, 3200.0, 0.08, 0.5, 0.0])
+    calc = e.light_curve_comp(S.ModelFactory()(truth[None])[0], W.data(S.NGRID, -0.2, 1.2),
+                              scale=False, rdata=False, sfac=np.ones(5), diagnostics=False)[0]
+    d = W.add_noise(W.data(S.NGRID, -0.2, 1.2)[idx], calc[idx], 9)
+    rng = np.random.default_rng(8)
+    scale = (S.BOX[:, 1] - S.BOX[:, 0]) * 2e-3
+    nc = 40
+    exact = ExactChi2(e, d, curves=True)
+    with Engine(precision="mixed") as ec:
+        comp = CompactExact(ec, d, k=8)
+        out = torch.zeros((nc, len(idx)), dtype=torch.float64, device="cuda")
+        for trial in range(3):
+            th = truth + rng.standard_normal((nc, 9)) * scale
+            full = exact(th)
+            ref = torch.empty((nc, len(idx)), dtype=torch.float64, device="cuda")
+            exact.curves_all_device(ref)
+            sel = np.sort(rng.choice(nc, 5 + 4 * trial, replace=False))  # one or two groups
+            got = comp(sel, th, out)
+            np.testing.assert_allclose(got, full[sel], rtol=1e-5)
+            np.testing.assert_allclose(out[sel].cpu().numpy(), ref[sel].cpu().numpy(),
+                                       rtol=2e-6, atol=0)
+        assert comp.evals == 5 + 9 + 13
+        sur_chi = S.SurrogateChi2(sur, d, idx)
+        theta0 = truth + rng.standard_normal((24, 9)) * scale
+        cov = np.diag(scale ** 2) * 4.0
+        comp2 = CompactExact(ec, d, k=8)
+        ch, th, chi, acc, _, st = delayed_acceptance(ExactChi2(e, d, curves=True), sur_chi,
+                                                     theta0, cov, 40, seed=3, compact=comp2)
+        assert 0 < st["stage1_rate"] < 1 and acc > 0 and np.all(np.isfinite(chi))
+        np.testing.assert_allclose(chi, exact(th), rtol=1e-5)
