@@ -641,6 +641,7 @@ extern "C" lcg_status lcg_light_curve_batch_resident(lcg_ctx *c, const lcg_model
             if (k) {
                 for (int star = 0; star < 2; star++) {
                     S[star].cp = continuum_params(M, star);
+                    S[star].cp.fp32 = 1;  // batches are mixed
                     S[star].fc = fast_coef(M, star, 1);
                 }
             }

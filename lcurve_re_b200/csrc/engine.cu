@@ -340,6 +340,10 @@ ContParams continuum_params(const lcg_model &m, int star) {
     p.absorb = m.absorb;
     p.wavelength = m.wavelength;
     p.efac = sqrt(8. * log(2.));
+    p.fp32 = 0;  // the callers that run mixed turn it on
+    p.irr32 = (float)(m.absorb * pow(star == kStar1 ? m.t2 : m.t1, 4.));
+    p.planck_c1 = (float)(2.e27 * kH * kC / (m.wavelength * m.wavelength * m.wavelength));
+    p.planck_c2 = (float)(1.e9 * kH * kC / kK / m.wavelength);
     if (star == kStar1) {
         p.t_own = m.t1;
         p.t_other = m.t2;
@@ -940,6 +944,7 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
             gl[k]->disc = false;
             if (!use[k]) continue;
             ContParams cp = continuum_params(m, stars[k]);
+            cp.fp32 = c->precision == LCG_PREC_MIXED;
             {
                 StageScope t(c, LCG_STAGE_CONTINUUM);
                 launch_continuum(cp, gl[k]->dev(), c->stream);

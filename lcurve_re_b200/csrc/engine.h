@@ -70,6 +70,12 @@ struct ContParams {
     double absorb, gdcbol, wavelength, rcomp, efac;
     double spot_dir[3][3], spot_fwhm[3], spot_tcen[3];
     double uesp_dir[3], uesp_longhw, uesp_lathw, uesp_taper, uesp_temp;
+    // mixed contexts: the intensity (gravity darkening, irradiated temperature,
+    // Planck) in FP32 from the FP64 geometry and temperature; irr32 = absorb
+    // t_other^4, planck_c1 = 2e27 h c / wavelength^3 (the reference's FAC1 over
+    // lambda^3), planck_c2 = 1e9 h c / k / wavelength
+    int32_t fp32;
+    float irr32, planck_c1, planck_c2;
 };
 
 // One light-curve point, the byte layout of lcg_datum / Lcurve::Datum.

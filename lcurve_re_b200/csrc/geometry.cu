@@ -385,6 +385,34 @@ __device__ __forceinline__ void continuum_face(const ContParams &p, GridDev g, i
             t += (p.spot_tcen[k] - t) * exp(-sq(dist / (p.spot_fwhm[k] / EFAC)) / 2.);
         }
     }
+    if (p.fp32) {
+        // the intensity in FP32 (the face's flux is stored as a float): the same
+        // formulas as below; x^(1/4) as two square roots, Planck from its
+        // constants over the wavelength, set on the host
+        const float gd = powf(g.grav[i], (float)p.gdcbol);
+        const float tg = (float)t * gd, tg2 = tg * tg;
+        const double rc = p.rcomp;
+        double geom = 0.;
+        float temp = tg;
+        if (mu > -rc) {
+            if (mu >= rc) {
+                geom = sq(rc / r) * mu;
+            } else {
+                double x0 = -mu / rc;
+                geom = sq(rc / r) * rc *
+                       (sqrt(1. - x0 * x0) * (2 + x0 * x0) / 3 - x0 * (kPi / 2 - asin(x0))) / kPi;
+            }
+            temp = sqrtf(sqrtf(fmaf(tg2, tg2, p.irr32 * (float)geom)));
+        }
+        const float area = g.area[i];
+        float f = area * (p.planck_c1 / (expf(p.planck_c2 / temp) - 1.f));
+        if (p.mirror) {
+            const float tm = (float)(p.star == kStar1 ? fabs(p.t_other) : p.t_other);
+            f = fmaf(area * (float)geom, p.planck_c1 / (expf(p.planck_c2 / tm) - 1.f), f);
+        }
+        g.flux[i] = f;
+        return;
+    }
     const double gd = pow((double)g.grav[i], p.gdcbol);
     const double rc = p.rcomp;
     // pow(t_other, 4) for star 1 and pow(t_other, 4.) for star 2 are the same call
