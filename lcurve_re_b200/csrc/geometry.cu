@@ -1070,12 +1070,21 @@ __device__ __forceinline__ int32_t queue_at(const BatchDev &b, int k) {
 // Warp mode of the batched eclipse (few candidates): one warp per candidate.
 // With more candidates than warp_max, k_ecl_potmin_b and k_ecl_bisect_b do
 // the work and this kernel returns at once (the choice is made on the device).
-__global__ void __launch_bounds__(128, 4) k_ecl_roche_b(BatchDev b, int32_t warp_max) {
+// Warp mode for this call: at most warp_max candidates and, when the mode is
+// chosen automatically, none that the FP32 screen serves (the front of the
+// queue): thread mode with the screen has the shorter latency even for few.
+__device__ __forceinline__ bool batch_warp_mode(const BatchDev &b, int32_t warp_max,
+                                                int32_t auto_mode) {
+    return b.counters[0] <= warp_max && !(auto_mode && b.counters[5] > 0);
+}
+
+__global__ void __launch_bounds__(128, 4) k_ecl_roche_b(BatchDev b, int32_t warp_max,
+                                                     int32_t auto_mode) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int total = b.counters[0];
     const GridDev g = b.g;
-    if (total <= warp_max) {
+    if (batch_warp_mode(b, warp_max, auto_mode)) {
         for (;;) {
             int k = 0;
             if (lane == 0) k = atomicAdd(&b.counters[1], 1);
@@ -1110,11 +1119,12 @@ __global__ void __launch_bounds__(128, 4) k_ecl_roche_b(BatchDev b, int32_t warp
 // egress bisections (ingress_egress.cpp:61-86) on the two lanes of a pair.
 // Warps take consecutive candidates (similar iteration counts run together).
 // Same arithmetic and decisions as ingress_egress: identical results.
-__global__ void __launch_bounds__(128, 4) k_ecl_potmin_b(BatchDev b, int32_t warp_max) {
+__global__ void __launch_bounds__(128, 4) k_ecl_potmin_b(BatchDev b, int32_t warp_max,
+                                                      int32_t auto_mode) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int total = b.counters[0];
-    if (total <= warp_max) return;
+    if (batch_warp_mode(b, warp_max, auto_mode)) return;
     const GridDev g = b.g;
     for (;;) {
         int base = 0;
@@ -1149,11 +1159,11 @@ __global__ void __launch_bounds__(128, 4) k_ecl_potmin_b(BatchDev b, int32_t war
 // warps hide the FP64 latency, fewer registers spill more)
 template <int NB>
 __global__ void __launch_bounds__(128, NB)
-    k_ecl_bisect_b(__grid_constant__ const BatchDev b, int32_t warp_max) {
+    k_ecl_bisect_b(__grid_constant__ const BatchDev b, int32_t warp_max, int32_t auto_mode) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int total = b.counters[0];
-    if (total <= warp_max) return;
+    if (batch_warp_mode(b, warp_max, auto_mode)) return;
     const int64_t n2 = 2 * (int64_t)total;
     for (;;) {
         int64_t base = 0;
@@ -1387,7 +1397,10 @@ void launch_eclipse(const EclParams &p, int32_t eclipse_on, GridDev g, int32_t *
         const unsigned need = nblocks(g.n, 4);
         if (need < nb) nb = need;
         const int32_t warps = (int32_t)nb * 4;
-        const int32_t warp_max = warp_mode < 0 ? -1 : warp_mode > 0 ? warp_mode : 2 * warps;
+        // auto: warp mode for few candidates, unless the FP32 screen serves them
+        // (thread mode with the screen has the shorter latency even then)
+        const int32_t warp_max =
+            warp_mode < 0 ? -1 : warp_mode > 0 ? warp_mode : (p.scr.on ? -1 : 2 * warps);
         k_ecl_roche<<<nb, 128, 0, s>>>(p, g, queue, counters, st, warp_max);
         count_launch();
         k_ecl_potmin<<<nb, 128, 0, s>>>(p, g, queue, counters, es, ehit, st, warp_max);
@@ -1510,14 +1523,15 @@ void launch_batch_eclipse(const BatchDev &b, int nsm, int32_t warp_mode, cudaStr
     count_launch();
     const int32_t warps = nsm * 16;
     const int32_t warp_max = warp_mode < 0 ? -1 : warp_mode > 0 ? warp_mode : 2 * warps;
-    k_ecl_roche_b<<<nsm * 4, 128, 0, s>>>(b, warp_max);
+    const int32_t auto_mode = warp_mode == 0;
+    k_ecl_roche_b<<<nsm * 4, 128, 0, s>>>(b, warp_max, auto_mode);
     count_launch();
-    k_ecl_potmin_b<<<nsm * 4, 128, 0, s>>>(b, warp_max);
+    k_ecl_potmin_b<<<nsm * 4, 128, 0, s>>>(b, warp_max, auto_mode);
     count_launch();
     if (bisect_blocks_per_sm() == 6)
-        k_ecl_bisect_b<6><<<nsm * 6, 128, 0, s>>>(b, warp_max);
+        k_ecl_bisect_b<6><<<nsm * 6, 128, 0, s>>>(b, warp_max, auto_mode);
     else
-        k_ecl_bisect_b<4><<<nsm * 4, 128, 0, s>>>(b, warp_max);
+        k_ecl_bisect_b<4><<<nsm * 4, 128, 0, s>>>(b, warp_max, auto_mode);
     count_launch();
 }
 
