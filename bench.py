@@ -12,8 +12,8 @@ in an MCMC step whose geometry changes.
   e2e    the same through lcg_light_curve with pinned host buffers: the
          points go host->device and the curve device->host every step
   roofline  the flux sweep (the dominant kernel): 16 FLOP per element
-         (5 for mu, 8 for the Claret Horner form, 2 for
-         mu*flux*I, 1 accumulate) over its CUDA-event time, against the FP32
+         (5 for mu, 8 for the Claret Horner form, 2 for mu*flux*I,
+         1 accumulate) over its CUDA-event time, against the FP32
          FMA peak measured live by lcg_measure_fp32_peak
   cpu_baseline  lcurve_re's own CPU path (oracle/_ref, Release flags,
          OpenMP on all host cores) on a bounded sample
