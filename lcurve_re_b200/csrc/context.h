@@ -165,6 +165,7 @@ struct lcg_ctx {
     // work buffers
     DBuf<DevStatus> status;
     DBuf<int32_t> queue, counters, blockcnt;
+    DBuf<int32_t> blockcnt2;  // star 2's partition scratch when it flattens on side[0]
     DBuf<DatumRec> data;
     DBuf<int64_t> off;
     DBuf<double> pex, pey, pez, pphin, pw1, pw2, part1f, part1c, part2f, part2c, calc, scratch,
@@ -180,8 +181,12 @@ struct lcg_ctx {
     // side streams: star 2's grids (side[0]) and the component elements
     // (side[1]) run beside star 1's; their eclipse solves are latency-bound,
     // so they overlap well. Created by the first call.
+    // With fine grids only (no coarse ones, no opaque disc), star 2's continuum,
+    // partition and flux sweep also stay on side[0], which waits for the phase
+    // entries (ev_phases) and joins before the scatter: star 1's sweep fills
+    // the SMs that star 2's latency-bound geometry leaves idle.
     cudaStream_t side[2] = {nullptr, nullptr};
-    cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
+    cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr}, ev_phases = nullptr;
     std::vector<int64_t> h_off;
     std::vector<double> h_diag;
     // resident light-curve points (lcg_set_data)

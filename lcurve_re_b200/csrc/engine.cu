@@ -487,17 +487,20 @@ FastCoef fast_coef(const lcg_model &m, int star, int mixed) {
     return f;
 }
 
-lcg_status flatten(lcg_ctx *c, Grid &g, int need_pos, const FastCoef &fc) {
+// side: run on side[0] with its own partition scratch (star 2, concurrent
+// order); otherwise on the context's stream.
+lcg_status flatten(lcg_ctx *c, Grid &g, int need_pos, const FastCoef &fc, bool side = false) {
     const int mixed = c->precision == LCG_PREC_MIXED;
     cudaError_t e;
     if ((e = g.alloc_flat(mixed, need_pos, fc.on)) != cudaSuccess)
         return c->cuda_fail(e, "flat grid");
     g.fast = fc.on;
-    if ((e = c->blockcnt.ensure(2 * ((g.n + 1023) / 1024) + 1)) != cudaSuccess)
+    DBuf<int32_t> &bc = side ? c->blockcnt2 : c->blockcnt;
+    if ((e = bc.ensure(2 * ((g.n + 1023) / 1024) + 1)) != cudaSuccess)
         return c->cuda_fail(e, "partition");
     StageScope t(c, LCG_STAGE_FLATTEN);
-    launch_flatten(g.dev(), g.flat(), c->blockcnt.p, mixed, need_pos, fc, c->status.p,
-                   c->stream);
+    launch_flatten(g.dev(), g.flat(), bc.p, mixed, need_pos, fc, c->status.p,
+                   side ? c->side[0] : c->stream);
     return LCG_OK;
 }
 
@@ -671,6 +674,7 @@ lcg_status lcg_create(lcg_ctx **out, const lcg_options *opt) {
         (e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&c->ev_join[0], cudaEventDisableTiming)) != cudaSuccess ||
         (e = cudaEventCreateWithFlags(&c->ev_join[1], cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&c->ev_phases, cudaEventDisableTiming)) != cudaSuccess ||
         (e = c->status.ensure(1)) != cudaSuccess || (e = c->counters.ensure(2)) != cudaSuccess ||
         (e = c->sfac.ensure(8)) != cudaSuccess || (e = c->out.ensure(4)) != cudaSuccess) {
         g_create_error = cudaGetErrorString(e);
@@ -700,6 +704,7 @@ void lcg_destroy(lcg_ctx *c) {
                          &c->out, &c->diag, &c->osum};
     for (auto *b : d) b->release();
     c->status.release(); c->queue.release(); c->counters.release(); c->blockcnt.release();
+    c->blockcnt2.release();
     c->data.release(); c->off.release(); c->pef.release(); c->ptype.release();
     c->fdata.release(); c->fidx.release(); c->fcalc.release(); c->fout.release();
     c->elem.release(); c->epos.release(); c->drings.release(); c->csum.release();
@@ -713,6 +718,7 @@ void lcg_destroy(lcg_ctx *c) {
             cudaEventDestroy(c->ev_join[k]);
         }
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_phases) cudaEventDestroy(c->ev_phases);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -894,6 +900,13 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
                    (!m.npole || r1 >= r2 || (m.nlatfill == 0 && m.nlngfill == 0));
         if (!c->copy1 && (rc = build_geometry(c, m, kStar1, 0, c->g1c, c->stream))) return rc;
         if (!c->copy2 && (rc = build_geometry(c, m, kStar2, 0, c->g2c, c->side[0]))) return rc;
+    }
+    // concurrent order (see lcg_ctx::side): star 2 stays on side[0] up to its
+    // sweep; otherwise the streams join here
+    const bool conc = c->copy1 && c->copy2 && !opaque && !c->profiling;
+    if (conc) {
+        cudaStreamWaitEvent(c->side[0], c->ev_fork, 0);  // also when the grids were reused
+    } else if (!geom_hit) {
         cudaEventRecord(c->ev_join[0], c->side[0]);
         cudaStreamWaitEvent(c->stream, c->ev_join[0], 0);
     }
@@ -945,15 +958,17 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
             if (!use[k]) continue;
             ContParams cp = continuum_params(m, stars[k]);
             cp.fp32 = c->precision == LCG_PREC_MIXED;
+            const bool on_side = conc && k == 1;  // star 2's fine grid
             {
                 StageScope t(c, LCG_STAGE_CONTINUUM);
-                launch_continuum(cp, gl[k]->dev(), c->stream);
+                launch_continuum(cp, gl[k]->dev(), on_side ? c->side[0] : c->stream);
             }
             // (with an opaque disc the grids are flattened below, after the
             // disc's ranges; first without them when the Ginterp scales need it)
             if (!opaque || !c->copy1 || !c->copy2)
                 if ((rc = flatten(c, *gl[k], need_pos,
-                                  fast_coef(m, stars[k], c->precision == LCG_PREC_MIXED))))
+                                  fast_coef(m, stars[k], c->precision == LCG_PREC_MIXED),
+                                  on_side)))
                     return rc;
         }
         c->gi = Ginterp{m.phase1, m.phase2, 1., 1., 1., 1.};
@@ -1027,6 +1042,10 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
             launch_pack_phases(one, c->stream);
         }
     }
+    if (conc) {
+        cudaEventRecord(c->ev_phases, c->stream);
+        cudaStreamWaitEvent(c->side[0], c->ev_phases, 0);
+    }
 
     // flux sweeps (light_curve_comp.cpp:457-473)
     struct Sweep {
@@ -1055,12 +1074,17 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
         phk.nent = s.nent;
         FluxConsts kc = flux_consts(m, s.star, s.spin, rlens1);
         StageScope t(c, LCG_STAGE_FLUX);
+        cudaStream_t fs = (conc && k == 2) ? c->side[0] : c->stream;  // star 2's fine sweep
         launch_flux(mixed, s.star, kc, s.g->flat(), phk, s.plan, s.part->p, ldp, c->status.p,
-                    c->stream);
+                    fs);
         if (s.g->disc)
             launch_flux_ragged(s.star, kc, s.g->flat(), s.g->dev(), phk, s.plan.chunk,
-                               s.plan.nchunk, s.part->p, ldp, c->stream);
+                               s.plan.nchunk, s.part->p, ldp, fs);
         c->flux_elements += s.g->n * s.nent;
+    }
+    if (conc) {
+        cudaEventRecord(c->ev_join[0], c->side[0]);
+        cudaStreamWaitEvent(c->stream, c->ev_join[0], 0);
     }
     if (comps) {
         if ((e = c->csum.ensure(3 * (size_t)ldp + (size_t)comp_sums_scratch(ncomp, ldp))))
