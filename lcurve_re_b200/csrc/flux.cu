@@ -279,7 +279,7 @@ __device__ __forceinline__ void sweep_pairs(const float4 *sp, const uint4 *se, i
             uint4 E = make_uint4(0u, 0u, 0u, 0u);
             if constexpr (ECL) E = ep[i];
             float2 m[PPT];
-            bool vis = false;
+            uint32_t vis = 0u;  // ma, mb >= 0: their bits are nonzero iff they are > 0
 #pragma unroll
             for (int j = 0; j < PPT; j++) {
                 const float2 mu = __ffma2_rn(ex[j], nx, __ffma2_rn(ey[j], ny, cz));
@@ -289,9 +289,9 @@ __device__ __forceinline__ void sweep_pairs(const float4 *sp, const uint4 *se, i
                     mb = ((pf[j] - E.z) >= E.w) ? mb : 0.f;
                 }
                 m[j] = f2(ma, mb);
-                vis = vis || ma > 0.f || mb > 0.f;
+                vis |= __float_as_uint(ma) | __float_as_uint(mb);
             }
-            if (!__any_sync(0xffffffffu, vis)) continue;
+            if (!__any_sync(0xffffffffu, vis != 0u)) continue;
             const float4 P2 = rp[4 * i + 2], P3 = rp[4 * i + 3];
             const float2 p0 = f2(P1.z, P1.w), p1 = f2(P2.x, P2.y), p2 = f2(P2.z, P2.w);
             const float2 p3 = f2(P3.x, P3.y), p4 = f2(P3.z, P3.w);
