@@ -1511,7 +1511,17 @@ void launch_diagnostics(int star, GridDev g, double *out, cudaStream_t s) {
 // ---- batched launchers -------------------------------------------------------
 
 void launch_batch_grid(const BatchDev &b, int nsm, cudaStream_t s) {
-    k_grid_b<<<nsm * 8, 128, 0, s>>>(b);
+    // one wave of the blocks that fit (its registers allow 5 of 128 threads per
+    // SM): a grid-stride loop over more blocks than fit runs a second, partial
+    // wave after the first
+    static const int per_sm = [] {
+        int nb = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_grid_b, 128, 0) != cudaSuccess ||
+            nb < 1)
+            nb = 4;
+        return nb;
+    }();
+    k_grid_b<<<nsm * per_sm, 128, 0, s>>>(b);
     count_launch();
 }
 
