@@ -145,7 +145,11 @@ typedef struct lcg_options {
     int32_t verbose;       /* print per-stage timings at destroy when > 0  */
     int32_t eclipse_warp;  /* Roche eclipse candidates up to which one warp
                               bisects each face (the rest: one thread per
-                              face); 0 automatic, -1 never                 */
+                              face); -1 never. 0 automatic: one thread per
+                              face whenever the FP32 screen of the
+                              bisections serves the faces (mixed contexts,
+                              stars with r >= 0.01), else a warp per face
+                              up to twice the GPU's resident warps       */
     int32_t reserved[4];
 } lcg_options;
 
