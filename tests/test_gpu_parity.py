@@ -91,6 +91,10 @@ def test_eclipse_fp32_screen_keeps_the_fp64_decisions():
     try:
         ms, _ = W.mcmc_batch(256)
         cases = [(n, m) for n, m, _ in CASES] + [("batch%d" % k, ms[k]) for k in range(0, 256, 16)]
+        # a donor star beside a disc (FP32 screen on its faces) and a tiny white
+        # dwarf (r1 < 0.01: its faces stay with the FP64 test alone)
+        cases += [("cv_disc", W.cv_disc(nlat1f=40, nlat2f=80, nrad=12, nspot=10)),
+                  ("tiny", W.model(r1=0.005, q=0.2, iangle=87.0, nlat1f=120, nlat2f=60))]
         for name, m in cases:
             for star in (0, 1):
                 a, b = fp64.star_grid(m, star), mixed.star_grid(m, star)
