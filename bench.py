@@ -16,7 +16,9 @@ in an MCMC step whose geometry changes.
          1 accumulate) over its CUDA-event time, against the FP32
          FMA peak measured live by lcg_measure_fp32_peak
   cpu_baseline  lcurve_re's own CPU path (oracle/_ref, Release flags,
-         OpenMP on all host cores) on a bounded sample
+         OpenMP on all host cores) on whole light curves of the workload
+         (grids rebuilt each call) for about 20 s; its curve of the exact
+         model also gives the benched curve's error ("parity")
 
 --impl reference times that reference CPU path alone (rank 0).
 Multi-GPU: one process per GPU; each rank evaluates its own light curves
@@ -36,6 +38,8 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+
+from lcurve_re_b200 import abi  # noqa: E402  (ctypes declarations only)
 
 METRIC = "light curves/s"
 FLOP_PER_ELEMENT = 16
@@ -158,20 +162,14 @@ class Clocks:
 # ---- CPU baseline: the reference's own CPU path ------------------------------------
 class RefTimer:
     """Times lcurve_re's CPU light_curve_comp (oracle/_ref Release build, OpenMP
-    over all host cores; the C port in oracle/ if that build is absent).
+    over all host cores; the C port in oracle/ if that build is absent) on
+    whole light curves: every timed call evaluates all points of the
+    workload with the geometry perturbed (q x (1 + 1e-13 k)), so that the
+    reference's grid cache (light_curve_comp.cpp:156-170) misses and the
+    grids, eclipses, continuum and FlatGrids are rebuilt, as the GPU arm's
+    FLAG_NO_CACHE does. Nothing is extrapolated."""
 
-    Bounded sample: one light curve costs t_grid + frac * t_sample, where
-    t_grid is a cold call on 1 point (the geometry perturbed by 1e-13 so the
-    reference's grid cache misses: grids, eclipses, continuum, FlatGrids) and
-    t_sample a warm call (cache hit) on 1/frac of the points. A model with an
-    opaque disc bypasses the reference's cache (light_curve_comp.cpp:163) and
-    rebuilds its disc every call, so each timed call is a whole light curve
-    (frac 1, no separate grid term)."""
-
-    def __init__(self, model, data, frac=50):
-        self.full = bool(model["add_disc"] or model["add_spot"])
-        if self.full:
-            frac = 1
+    def __init__(self, model, data):
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         import oracle_lib as OL
         self.kind = "reference"
@@ -181,56 +179,53 @@ class RefTimer:
             self.kind = "port"
             self.lib = OL.Oracle()
         self.model = model
+        self.data = data
         self.n = data.shape[0]
-        step = max(1, frac)
-        self.sub = np.ascontiguousarray(data[::step])  # strided: covers eclipses too
-        self.ns = self.sub.shape[0]
-        self.frac = self.n / self.ns
-        self.one = np.ascontiguousarray(data[:1])
         self.k = 0
-        st, err, *_ = self.lib.light_curve(model, self.one)
+
+    def exact_curve(self):
+        """The unperturbed model's curve, chi**2 and scale factors (untimed)."""
+        st, err, calc, sfac, sc = self.lib.light_curve(self.model, self.data)
         if st:
             raise RuntimeError(err)
+        return calc, sc[abi.OUT_CHISQ], sfac
 
-    def cold_grid(self, reps=3):
-        if self.full:
-            self.t_grid = 0.0
-            return 0.0
-        ts = []
-        for _ in range(reps):
-            self.k += 1
-            m = self.model.copy()
-            m["q"] = m["q"] * (1 + 1e-13 * self.k)
-            t = time.perf_counter()
-            self.lib.light_curve(m, self.one)
-            ts.append(time.perf_counter() - t)
-        self.t_grid = float(np.median(ts))
-        self.lib.light_curve(self.model, self.sub)  # re-warm the cache on the model
-        return self.t_grid
-
-    def sample(self):
+    def curve(self):
+        """One timed whole light curve with the grids rebuilt: seconds."""
+        self.k += 1
+        m = self.model.copy()
+        m["q"] = m["q"] * (1 + 1e-13 * self.k)
         t = time.perf_counter()
-        self.lib.light_curve(self.model, self.sub)
-        return time.perf_counter() - t
+        st, err, *_ = self.lib.light_curve(m, self.data)
+        dt = time.perf_counter() - t
+        if st:
+            raise RuntimeError(err)
+        return dt
 
     def describe(self, reps, t_curve):
-        if self.full:
-            return ("whole light curves (%d points; grids, disc, rim and spot rebuilt each call); "
-                    "%d calls; one light curve = %.3f s" % (self.n, reps, t_curve))
-        return ("every %dth point (%d of %d) per timed call (warm grids), x%.0f, plus a cold 1-point call for "
-                "grids+eclipses+continuum (%.3f s); %d calls; one light curve = %.3f s"
-                % (round(self.frac), self.ns, self.n, self.frac, self.t_grid, reps, t_curve))
+        return ("whole light curves (%d points each, grids rebuilt every call), %d timed calls; "
+                "one light curve = %.3f s" % (self.n, reps, t_curve))
 
 
-def cpu_reference_rate(model, data, budget_s=15.0):
+def cpu_reference_rate(model, data, budget_s=20.0, gpu_calc=None, gpu_chisq=None):
+    """The reference CPU path on whole light curves of the workload: one
+    untimed call on the exact model (its curve checks the GPU's benched curve
+    when gpu_calc is given), then timed calls until budget_s is spent (at
+    least two)."""
     r = RefTimer(model, data)
-    r.cold_grid()
-    t_probe = r.sample()
-    reps = int(max(3, min(50, budget_s // max(t_probe, 1e-3))))
-    ts = [r.sample() for _ in range(reps)]
-    t_curve = r.t_grid + r.frac * float(np.median(ts))
-    return {"value": 1.0 / t_curve, "unit": METRIC, "cores": os.cpu_count(), "kind": r.kind,
-            "sample": r.describe(reps, t_curve)}
+    calc, chisq, _ = r.exact_curve()
+    ts = []
+    while len(ts) < 2 or (sum(ts) < budget_s and len(ts) < 50):
+        ts.append(r.curve())
+    t_curve = float(np.mean(ts))
+    out = {"value": 1.0 / t_curve, "unit": METRIC, "cores": os.cpu_count(), "kind": r.kind,
+           "sample": r.describe(len(ts), t_curve)}
+    if gpu_calc is not None:
+        out["parity"] = {
+            "checker": "this reference build's curve of the same model and points",
+            "max_rel_flux_error": float(np.max(np.abs(gpu_calc - calc) / np.abs(calc))),
+            "chi2_rel_error": (abs(gpu_chisq - chisq) / abs(chisq)) if gpu_chisq else None}
+    return out
 
 
 def run_reference(args):
@@ -239,10 +234,10 @@ def run_reference(args):
         return 0
     model, data, desc = workload(args.workload)
     r = RefTimer(model, data)
-    r.cold_grid()
+    r.exact_curve()
     for _ in range(args.warmup):
-        r.sample()
-    ts = [r.t_grid + r.frac * r.sample() for _ in range(args.steps)]
+        r.curve()
+    ts = [r.curve() for _ in range(args.steps)]
     mean_t = float(np.mean(ts))
     v = 1.0 / mean_t
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": world,
@@ -356,7 +351,8 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cpu = cpu_reference_rate(model, data)
+            cpu = cpu_reference_rate(model, data, gpu_calc=hcalc.copy(),
+                                     gpu_chisq=float(scal[abi.OUT_CHISQ]))
         except Exception as ex:  # the baseline is reported, never required
             cpu = {"value": None, "unit": METRIC, "cores": os.cpu_count(), "kind": "unavailable",
                    "sample": str(ex)}

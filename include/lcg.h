@@ -312,8 +312,13 @@ lcg_status lcg_sum_star_multi(lcg_ctx *ctx, int32_t star, int64_t n,
  *   All arrays are DEVICE arrays owned by the caller (same meaning as in
  *   lcg_sum_star_multi; in1/out1 of length n-n0); ldc is a host array of 4.
  *   Runs on `stream` (a cudaStream_t; NULL = the legacy default stream) on
- *   the device that owns `out`; returns without waiting for the GPU.
+ *   the device that owns `out`, and leaves the caller's current device as it
+ *   found it; returns without waiting for the GPU.
+ *   Only faces with zero or one eclipse range ([0,n0) and [n0,n)): faces with
+ *   several ranges (opaque discs) have no place in this form's arguments.
  *   No beaming or lensing in this form; FP64 arithmetic of the reference.
+ *   A launch failure returns LCG_E_CUDA and consumes the runtime's record of
+ *   that failure; errors left by the caller's earlier work are not cleared.
  * Scratch: a fixed 16 MiB device array inside the library (held by every GPU
  * that loads it, until exit): ceil(n/1024) * nent must not exceed 2,097,152
  * and ceil(n/1024) must not exceed 65,535, else LCG_E_CAPACITY is returned

@@ -145,6 +145,29 @@ __global__ void k_merge_noalloc(const double *__restrict__ scratch, int64_t nblk
 std::mutex g_setup_mutex;
 double *g_scratch_addr[kMaxDevices] = {};
 
+// Puts the caller's current device back on every return path: this entry point
+// runs inside other programs, whose later runtime calls must not land on the
+// device that owned `out`.
+struct CurrentDeviceGuard {
+    int saved = -1;
+    CurrentDeviceGuard() {
+        if (cudaGetDevice(&saved) != cudaSuccess) {
+            saved = -1;
+            cudaGetLastError();
+        }
+    }
+    ~CurrentDeviceGuard() {
+        if (saved >= 0 && cudaSetDevice(saved) != cudaSuccess) cudaGetLastError();
+    }
+};
+
+// A failure this call caused: consume the runtime's record of it, so that the
+// caller's next cudaGetLastError does not report it a second time.
+lcg_status own_cuda_failure() {
+    cudaGetLastError();
+    return LCG_E_CUDA;
+}
+
 }  // namespace
 
 extern "C" lcg_status lcg_sum_star_multi_noalloc(
@@ -171,26 +194,38 @@ extern "C" lcg_status lcg_sum_star_multi_noalloc(
         cudaGetLastError();
         return LCG_E_INVALID;
     }
-    if (cudaSetDevice(attr.device) != cudaSuccess) return LCG_E_CUDA;
+    CurrentDeviceGuard keep_callers_device;
+    if (cudaSetDevice(attr.device) != cudaSuccess) return own_cuda_failure();
     double *scratch;
     {
         std::lock_guard<std::mutex> lock(g_setup_mutex);
         if (!g_scratch_addr[attr.device]) {
             void *p = nullptr;
-            if (cudaGetSymbolAddress(&p, g_sweep_scratch) != cudaSuccess || !p) return LCG_E_CUDA;
+            if (cudaGetSymbolAddress(&p, g_sweep_scratch) != cudaSuccess || !p)
+                return own_cuda_failure();
             g_scratch_addr[attr.device] = static_cast<double *>(p);
         }
         scratch = g_scratch_addr[attr.device];
     }
-    const Limb L{ldc[0], ldc[1], ldc[2], ldc[3], 1.0 - (ldc[0] + ldc[1] + ldc[2] + ldc[3]),
-                 mucrit, ltype};
+    Limb L{ldc[0], ldc[1], ldc[2], ldc[3], 1.0 - (ldc[0] + ldc[1] + ldc[2] + ldc[3]), mucrit,
+           ltype};
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // cudaLaunchKernel reports this launch's own status; an error left by the
+    // caller's earlier work is neither consumed nor blamed on this call unless
+    // it is a sticky one that also fails these launches.
     if (nblk > 0) {
         dim3 grid((unsigned)((nent + kThreads * kPPT - 1) / (kThreads * kPPT)), (unsigned)nblk);
-        k_sweep_noalloc<<<grid, kThreads, 0, s>>>(n, n0, dx, dy, dz, flux, in1, out1, nent, ex, ey,
-                                                  ez, phin, L, scratch);
+        void *args[] = {&n,  &n0, &dx, &dy, &dz, &flux, &in1, &out1, &nent,
+                        &ex, &ey, &ez, &phin, &L, &scratch};
+        if (cudaLaunchKernel((const void *)k_sweep_noalloc, grid, dim3(kThreads), args, 0, s) !=
+            cudaSuccess)
+            return own_cuda_failure();
     }
-    k_merge_noalloc<<<(unsigned)((nent + 255) / 256), 256, 0, s>>>(scratch, nblk, nent, out);
-    if (cudaGetLastError() != cudaSuccess) return LCG_E_CUDA;
+    const double *partials = scratch;
+    int64_t nb = nblk;
+    void *margs[] = {&partials, &nb, &nent, &out};
+    if (cudaLaunchKernel((const void *)k_merge_noalloc, dim3((unsigned)((nent + 255) / 256)),
+                         dim3(256), margs, 0, s) != cudaSuccess)
+        return own_cuda_failure();
     return LCG_OK;
 }
