@@ -69,9 +69,10 @@ def parse():
                     help="surrogate_da: delayed acceptance's exact evaluations through a "
                          "batch of this many slots on a second engine context (0: the "
                          "whole-chain batch)")
-    ap.add_argument("--burn-fixed", type=int, default=2000,
+    ap.add_argument("--burn-fixed", type=int, default=0,
                     help="surrogate_da: plain Metropolis steps after the adaptive burn-in, "
-                         "with its final proposal kept (no further adaptation)")
+                         "with its final proposal kept (no further adaptation), before the "
+                         "local draws")
     ap.add_argument("--ncoef", type=int, default=64)
     ap.add_argument("--local-curves", type=int, default=131072)
     ap.add_argument("--refine-epochs", type=int, default=600)
@@ -80,6 +81,8 @@ def parse():
     ap.add_argument("--precision", choices=("mixed", "fp64"), default="mixed")
     ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="report the named workload alone (no batch and surrogate sub-objects)")
     ap.add_argument("--eclipse-warp", type=int, default=0,
                     help="Roche eclipse candidates up to which one warp bisects each face "
                          "(0 automatic, -1 never)")
@@ -231,7 +234,7 @@ def cpu_reference_rate(model, data, budget_s=20.0, gpu_calc=None, gpu_chisq=None
 def run_reference(args):
     rank, _, world = rank_info()
     if rank != 0:
-        return 0
+        return None
     model, data, desc = workload(args.workload)
     r = RefTimer(model, data)
     r.exact_curve()
@@ -247,21 +250,15 @@ def run_reference(args):
             "cpu_baseline": {"value": v, "unit": METRIC, "cores": os.cpu_count(), "kind": r.kind,
                              "sample": r.describe(args.steps, mean_t)},
             "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 # ---- our arm -------------------------------------------------------------------------
-def run_ours(args):
+def run_ours(args, dist=None):
     import ctypes as C
     import torch
     from lcurve_re_b200.replicas import max_over_ranks
     rank, local, world = rank_info()
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     from lcurve_re_b200 import abi
     from lcurve_re_b200 import workloads as W
     from lcurve_re_b200.engine import Engine
@@ -391,12 +388,8 @@ def run_ours(args):
         "cpu_baseline": cpu,
         "clocks": clk,
     }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
     eng.close()
-    if dist is not None:
-        dist.destroy_process_group()
-    return 0
+    return line if rank == 0 else None
 
 
 # ---- batched workload: 256 models per step -------------------------------------------
@@ -428,59 +421,70 @@ def batch_workload(nmodels=256, variant="geometry"):
     return ms, alt, d
 
 
-def cpu_batch_rate(models, data, sample=8, budget_s=20.0, warm=None):
-    """The reference CPU path on the first `sample` models of the batch (each
-    a cold call: grids rebuilt), scaled to the batch by total face count.
-    With warm (the same models with only T1/T2 changed), each timed call
-    follows an untimed call on its warm partner, so the reference's own
-    per-thread grid cache (light_curve_comp.cpp:156-170) skips the grids."""
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import oracle_lib as OL
-    kind = "reference"
-    if os.path.exists(OL.REF_RELEASE_SO):
-        lib = OL.Reference(OL.REF_RELEASE_SO)
-    else:
-        kind = "port"
-        lib = OL.Oracle()
-    counter = OL.Oracle()
-    face_count_host = lambda m: counter.face_count(m, 0) + counter.face_count(m, 1)
-    t_used, k = 0.0, 0
-    f_used = 0
-    for i, m in enumerate(models[:sample]):
-        if warm is not None:
-            lib.light_curve(warm[i], data)
-        t = time.perf_counter()
-        st, err, *_ = lib.light_curve(m, data)
-        t_used += time.perf_counter() - t
-        if st:
-            raise RuntimeError(err)
-        f_used += face_count_host(m)
-        k += 1
-        if t_used > budget_s:
-            break
-    f_all = sum(face_count_host(m) for m in models)
-    t_batch = t_used * f_all / f_used
-    v = len(models) / t_batch
-    return {"value": v, "unit": METRIC, "cores": os.cpu_count(), "kind": kind,
-            "sample": "%d of %d models, full %d points each, %s (%.2f s); scaled to the "
-                      "batch by total faces (%d of %d)" % (
-                          k, len(models), data.shape[0],
-                          "cold grids" if warm is None else
-                          "grids from the reference's cache (only T1/T2 changed)" if
-                          kind == "reference" else "grids rebuilt (the port has no cache)",
-                          t_used, f_used, f_all)}
+class RefBatch:
+    """The reference CPU path (oracle/_ref Release build, OpenMP on all host
+    cores; the C port if that build is absent) over every model of a batch,
+    one whole light curve per model. Consecutive models differ in geometry,
+    so each call rebuilds its grids. With warm (the same models with only T1
+    and T2 changed), each timed call follows an untimed call on its warm
+    partner, so the reference's own per-thread grid cache
+    (light_curve_comp.cpp:156-170) skips the grids, as the engine does."""
+
+    def __init__(self, models, data, warm=None):
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_lib as OL
+        from lcurve_re_b200 import workloads as W
+        self.kind = "reference"
+        if os.path.exists(OL.REF_RELEASE_SO):
+            self.lib = OL.Reference(OL.REF_RELEASE_SO)
+        else:
+            self.kind = "port"
+            self.lib = OL.Oracle()
+        # models whose nlat makes the reference's grid build write past its
+        # own vector cannot run in this process: the rate is over the others
+        keep = [i for i, m in enumerate(models) if W.reference_safe(m)]
+        self.left_out = len(models) - len(keep)
+        self.models = [models[i] for i in keep]
+        self.warm = [warm[i] for i in keep] if warm is not None else None
+        self.data = data
+
+    def batch(self):
+        """Seconds for one pass over the whole batch (timed calls only)."""
+        t_used = 0.0
+        for i, m in enumerate(self.models):
+            if self.warm is not None:
+                self.lib.light_curve(self.warm[i], self.data)
+            t = time.perf_counter()
+            st, err, *_ = self.lib.light_curve(m, self.data)
+            t_used += time.perf_counter() - t
+            if st:
+                raise RuntimeError(err)
+        return t_used
+
+    def describe(self, passes, t_batch):
+        return ("%d models of the batch (%d left out: their nlat makes the reference's ring "
+                "tiling write past its Point vector), one whole %d-point light curve each, %s; "
+                "%d pass(es); %.2f s per pass" % (
+                    len(self.models), self.left_out, self.data.shape[0],
+                    "cold grids" if self.warm is None else
+                    "grids from the reference's cache (only T1/T2 changed)" if
+                    self.kind == "reference" else "grids rebuilt (the port has no cache)",
+                    passes, t_batch))
 
 
-def run_batch(args):
+def cpu_batch_rate(models, data, warm=None, passes=1):
+    r = RefBatch(models, data, warm)
+    ts = [r.batch() for _ in range(passes)]
+    t = float(np.mean(ts))
+    return {"value": len(r.models) / t, "unit": METRIC, "cores": os.cpu_count(), "kind": r.kind,
+            "sample": r.describe(passes, t)}
+
+
+def run_batch(args, dist=None):
     import ctypes as C
     import torch
     from lcurve_re_b200.replicas import max_over_ranks
     rank, local, world = rank_info()
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     from lcurve_re_b200 import abi
     from lcurve_re_b200 import workloads as W
     from lcurve_re_b200.engine import Engine
@@ -626,18 +630,14 @@ def run_batch(args):
         "cpu_baseline": cpu,
         "clocks": clk,
     }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
     eng.close()
-    if dist is not None:
-        dist.destroy_process_group()
-    return 0
+    return line if rank == 0 else None
 
 
 def run_reference_batch(args):
     rank, _, world = rank_info()
     if rank != 0:
-        return 0
+        return None
     from lcurve_re_b200 import workloads as W
     ms, alt, data = batch_workload(variant=args.batch_variant)
     warm = alt if args.batch_variant == "brightness" else None
@@ -645,19 +645,21 @@ def run_reference_batch(args):
     import oracle_lib as OL
     calc0 = OL.Oracle().light_curve(ms[0], data, scale=False, rdata=False)[2]
     data = W.add_noise(data, calc0, seed=1234)
-    vals = [cpu_batch_rate(ms, data, sample=2, budget_s=8.0, warm=warm)
-            for _ in range(args.warmup + args.steps)]
-    vals = vals[args.warmup:]
-    v = float(np.mean([x["value"] for x in vals]))
+    r = RefBatch(ms, data, warm)
+    for _ in range(args.warmup):
+        r.batch()
+    ts = [r.batch() for _ in range(args.steps)]
+    t = float(np.mean(ts))
+    v = len(r.models) / t
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 256 / v * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": {"workload": BATCH_DESC, "precision": "fp64 (reference CPU)",
                                             "grids": BATCH_GRIDS[args.batch_variant]},
-            "cpu_baseline": dict(vals[-1], value=v),
+            "cpu_baseline": {"value": v, "unit": METRIC, "cores": os.cpu_count(), "kind": r.kind,
+                             "sample": r.describe(args.steps, t)},
             "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 # ---- learned surrogate + delayed acceptance ---------------------------------------------
@@ -678,16 +680,29 @@ def _bf16_peak():
 
 def run_surrogate(args):
     """cfg4: the surrogate trained on engine curves over the prior box, then
-    plain vs delayed-acceptance Metropolis (same proposals, same start) on
-    wd_dm_small data; effective samples per second of sampling."""
+    plain vs delayed-acceptance Metropolis (same start states, same draws) on
+    wd_dm_small data; effective samples per second of sampling.
+
+    Start states: a first adaptive burn-in locates the posterior; every exact
+    curve computed so far (the box-uniform training set and the local draws
+    the network is refined on) then gives an importance sample of the
+    posterior (each row weighted by its exact likelihood over the density of
+    the mixture it was drawn from), and the chains start from a resample of
+    it, so both samplers begin at (close to) the stationary distribution and
+    their means can be compared against their Monte Carlo errors. The
+    proposal covariance is that sample's weighted covariance x 2.38^2 / 9.
+
+    value: bulk ESS (rank-normalised multi-chain ESS over split chains,
+    minimum over parameters) per second of delayed-acceptance sampling; the
+    reference's Geyer estimator and a between-chain estimate are reported
+    beside it."""
     import torch
     rank, local, world = rank_info()
-    torch.cuda.set_device(local)
     from lcurve_re_b200 import surrogate as S
     from lcurve_re_b200 import workloads as W
     from lcurve_re_b200.engine import Engine
     from lcurve_re_b200.sampler import (CompactExact, ExactChi2, delayed_acceptance,
-                                        ess_between_chains, ess_total, metropolis)
+                                        mean_shift, metropolis, shift_verdict, summary)
 
     eng = Engine(device=local, precision="mixed")
     clocks = Clocks(local)
@@ -721,37 +736,51 @@ def run_surrogate(args):
     rng = np.random.default_rng(7 + rank)
     scale0 = (S.BOX[:, 1] - S.BOX[:, 0]) * 1e-3
     theta0 = truth + rng.standard_normal((args.chains, 9)) * scale0
-    # burn-in with plain Metropolis in two rounds, each adapting the proposal
-    # to 2.38^2 / d times the covariance of its second half (pooled over the
-    # chains); both samplers then start from the same burn-in end states. The
-    # posterior is nearly degenerate (correlations to 0.995, two parameters
-    # bounded only by the prior box), so neither sampler mixes over all of it
-    # within the run: the comparison is of how fast each explores the same
-    # region from the same states.
+    # adaptive burn-in with plain Metropolis in two rounds, each adapting the
+    # proposal to 2.38^2 / d times the covariance of its second half (pooled
+    # over the chains): it locates the posterior for the local draws
     cov = np.diag(scale0 ** 2)
     for k in range(2):
         ch, theta0, _, acc_b, _ = metropolis(exact, theta0, cov, args.burn // 2, seed=11 + k)
         samp = ch[ch.shape[0] // 2:].reshape(-1, 9)
         cov = np.cov(samp.T) * 2.38 ** 2 / 9 + np.diag((scale0 * 1e-3) ** 2)
+    del ch
     if args.burn_fixed > 0:
         chf, theta0, _, _, _ = metropolis(exact, theta0, cov, args.burn_fixed, seed=13)
-        samp_f = chf[chf.shape[0] // 2:].reshape(-1, 9)
+        samp = chf[chf.shape[0] // 2:].reshape(-1, 9)
         del chf
     # refinement: the same network trained again on engine curves around the
     # burn-in posterior (Gaussian, local_widen x its spread, inside the box)
-    samp = ch[ch.shape[0] // 2:].reshape(-1, 9) if args.burn_fixed <= 0 else samp_f
-    th_loc = S.local_draws(samp.mean(0), np.cov(samp.T), args.local_curves, seed=5 + rank,
-                           widen=args.local_widen)
+    mu_b, cov_b = samp.mean(0), np.cov(samp.T)
+    th_loc = S.local_draws(mu_b, cov_b, args.local_curves, seed=5 + rank, widen=args.local_widen)
     t0 = time.perf_counter()
     _, cu_loc = S.training_set(eng, 0, theta=th_loc, batch=2048)
     sur_loc = S.Surrogate(ncoef=args.ncoef, batch=4096, seed=rank + 1)
     losses_loc = sur_loc.fit(th_loc, cu_loc, epochs=args.refine_epochs)
     t_ref = time.perf_counter() - t0
-    th_lh = S.local_draws(samp.mean(0), np.cov(samp.T), 2048, seed=77 + rank,
-                          widen=args.local_widen)
+    th_lh = S.local_draws(mu_b, cov_b, 2048, seed=77 + rank, widen=args.local_widen)
     _, cu_lh = S.training_set(eng, 0, theta=th_lh, batch=2048)
     loc_err = float(np.sqrt(np.mean((sur_loc.curves(th_lh) - cu_lh) ** 2)))
     glob_err_loc = float(np.sqrt(np.mean((sur.curves(th_lh) - cu_lh) ** 2)))
+    # start states and proposal: importance resampling of the posterior from
+    # every exact curve made so far, in two stages: the first weighted
+    # estimate places a second, tighter pool of exact curves (1.5 x its
+    # spread), and the three pools together give the final sample
+    t0 = time.perf_counter()
+    chi_pool = np.r_[S.curves_chi2(curves, data, idx), S.curves_chi2(cu_loc, data, idx)]
+    del curves, cu_loc
+    pools = [(theta, S.log_uniform_box()),
+             (th_loc, S.log_gaussian_in_box(mu_b, cov_b, args.local_widen))]
+    _, mu_1, cov_1, ess_1 = S.posterior_resample(pools, chi_pool, 1, seed=17 + rank)
+    th_2 = S.local_draws(mu_1, cov_1, args.local_curves, seed=19 + rank, widen=1.5)
+    _, cu_2 = S.training_set(eng, 0, theta=th_2, batch=2048)
+    chi_pool = np.r_[chi_pool, S.curves_chi2(cu_2, data, idx)]
+    del cu_2
+    pools.append((th_2, S.log_gaussian_in_box(mu_1, cov_1, 1.5)))
+    theta0, mu_is, cov_is, ess_is = S.posterior_resample(pools, chi_pool, args.chains,
+                                                         seed=17 + rank)
+    t_sir = time.perf_counter() - t0
+    cov = cov_is * 2.38 ** 2 / 9 + np.diag((scale0 * 1e-3) ** 2)
     exact = ExactChi2(eng, data)
     sur_loc_chi = S.SurrogateChi2(sur_loc, data, idx)
     # inference throughput of the network alone (the DA screening pass)
@@ -784,17 +813,20 @@ def run_surrogate(args):
                                                       args.mcmc_steps, seed=21, compact=comp2)
     launches_da = int(lib.lcg_kernel_launches(1))
     clk = clocks.stop()
-    ess_g, _ = ess_total(chg)
-    shift_g = np.abs(chg.reshape(-1, 9).mean(0) - chp.reshape(-1, 9).mean(0)) / \
-        chp.reshape(-1, 9).std(0)
-    ess_p, per_p = ess_total(chp)
-    ess_d, per_d = ess_total(chd)
-    sp, sd = chp.reshape(-1, 9), chd.reshape(-1, 9)
-    shift = np.abs(sd.mean(0) - sp.mean(0)) / sp.std(0)
+    sum_p, sum_d, sum_g = summary(chp, wall_p), summary(chd, wall_d), summary(chg, wall_g)
+    shift, mcse = mean_shift(chd, chp)
+    shift_g, mcse_g = mean_shift(chg, chp)
+    sd_p = chp.reshape(-1, 9).std(0)
+    mcse_is = np.sqrt(np.diag(cov_is) / ess_is) / sd_p
+    shift_is = {k: (np.abs(c.reshape(-1, 9).mean(0) - mu_is) / sd_p).max()
+                for k, c in (("plain", chp), ("delayed_acceptance", chd))}
+    del chg
     peak, peak_src = _bf16_peak()
     train_tflops = train_flop / t_fit / 1e12
+    value = sum_d["ess_bulk_per_s"]
+    nbytes_model = C_sizeof_model()
     line = {
-        "metric": "MCMC effective samples/s", "value": ess_d / wall_d,
+        "metric": "MCMC effective samples/s", "value": value,
         "unit": "effective samples/s", "n_gpus": world, "steps": args.mcmc_steps,
         "warmup": args.burn + args.burn_fixed, "ms_per_step": wall_d / args.mcmc_steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -804,28 +836,38 @@ def run_surrogate(args):
                                "9 -> 4x256 GELU -> 64 PCA coefficients of a %d-point curve, "
                                "%d training curves" % (args.chains, args.mcmc_steps, S.NGRID,
                                                        args.train_curves),
-                   "ess": "Geyer initial positive sequence, min over parameters of the sum "
-                          "over chains (new_scripts/mcmc_solver.cpp:80-115)"},
-        "plain": {"ess": ess_p, "ess_per_s": ess_p / wall_p, "wall_s": wall_p,
-                  "acceptance": accp, "exact_evals": n_plain,
-                  "ess_between_chains": ess_between_chains(chp)[0]},
-        "delayed_acceptance": {"surrogate": "refined around the burn-in posterior",
-                               "ess": ess_d, "ess_per_s": ess_d / wall_d, "wall_s": wall_d,
-                               "acceptance": accd,
-                               "exact_evals": exact2.evals + (comp2.evals if comp2 else 0),
-                               "exact_batch": "%d slots" % args.compact if comp2 else "chains",
-                               "ess_between_chains": ess_between_chains(chd)[0], **st},
-        "delayed_acceptance_global": {"surrogate": "prior box only",
-                                      "ess": ess_g, "ess_per_s": ess_g / wall_g,
-                                      "wall_s": wall_g, "acceptance": accg,
-                                      "exact_evals": exact_g.evals +
-                                      (comp_g.evals if comp_g else 0),
-                                      "posterior_mean_shift_sigma_max": float(shift_g.max()),
-                                      **stg},
-        "ess_per_s_ratio": (ess_d / wall_d) / (ess_p / wall_p),
-        "ess_per_s_ratio_between_chains": (ess_between_chains(chd)[0] / wall_d) /
-                                          (ess_between_chains(chp)[0] / wall_p),
-        "posterior_mean_shift_sigma_max": float(shift.max()),
+                   "ess": "bulk ESS: rank-normalised multi-chain ESS of the split chains "
+                          "(Vehtari, Gelman, Simpson, Carpenter & Buerkner 2021), minimum "
+                          "over parameters; ess_geyer: the reference's estimator "
+                          "(new_scripts/mcmc_solver.cpp:80-115) summed over chains, frozen "
+                          "chains counted as zero",
+                   "start": "both samplers from the same %d states, resampled from an "
+                            "importance sample of the posterior (%d exact curves in three "
+                            "pools, effective size %.0f; %.0f after the first two)"
+                            % (args.chains, len(chi_pool), ess_is, ess_1)},
+        "plain": dict(sum_p, acceptance=accp, exact_evals=n_plain),
+        "delayed_acceptance": dict(sum_d, surrogate="refined around the burn-in posterior",
+                                   acceptance=accd,
+                                   exact_evals=exact2.evals + (comp2.evals if comp2 else 0),
+                                   exact_batch="%d slots" % args.compact if comp2 else "chains",
+                                   **st),
+        "delayed_acceptance_global": dict(sum_g, surrogate="prior box only", acceptance=accg,
+                                          exact_evals=exact_g.evals +
+                                          (comp_g.evals if comp_g else 0),
+                                          posterior_mean_shift_sigma_max=float(shift_g.max()),
+                                          **stg),
+        "ess_per_s_ratio": value / sum_p["ess_bulk_per_s"],
+        "ess_per_s_ratio_geyer": sum_d["ess_geyer_per_s"] / sum_p["ess_geyer_per_s"],
+        "ess_per_s_ratio_between_chains": (sum_d["ess_between_chains"] / wall_d) /
+                                          (sum_p["ess_between_chains"] / wall_p),
+        "posterior_mean_shift": {
+            "sigma_max": float(shift.max()), "per_parameter": shift.tolist(),
+            "mcse_per_parameter": mcse.tolist(),
+            "verdict_0.1_sigma": shift_verdict(shift, mcse),
+            "rule": "within: every |mean_DA - mean_plain| / sd_plain + 2 mcse < 0.1; outside: "
+                    "some shift - 2 mcse > 0.1",
+            "vs_importance_sample": {k: float(v) for k, v in shift_is.items()},
+            "importance_sample_mcse_max": float(mcse_is.max())},
         "surrogate": {"train_curves": args.train_curves, "curve_generation_s": t_gen,
                       "curves_per_s": args.train_curves / t_gen, "fit_s": t_fit,
                       "epochs": args.epochs, "final_loss": losses[-1],
@@ -835,22 +877,33 @@ def run_surrogate(args):
                                   "final_loss": losses_loc[-1],
                                   "local_rms_curve_error": loc_err,
                                   "global_net_local_rms_curve_error": glob_err_loc,
-                                  "pca_max_error": sur_loc.pca_max_err}},
+                                  "pca_max_error": sur_loc.pca_max_err},
+                      "importance_resampling_s": t_sir},
         "roofline": {"bound": "tensor", "kernel": "k_gemm (training, all layers)",
                      "achieved": train_tflops, "peak": peak, "unit": "TFLOP/s",
                      "frac": train_tflops / peak, "traffic": None, "peak_source": peak_src,
                      "flop_per_sample_train": sur.net.flops_per_sample(train=True)},
+        # the samplers' wall clock already covers every per-step transfer: the
+        # proposals (models) to the device, chi**2 back to the host
+        "e2e": {"value": value, "unit": "effective samples/s",
+                "h2d_bytes_per_step": int(args.chains * 9 * 4 +
+                                          st["stage1_rate"] * args.chains * nbytes_model),
+                "d2h_bytes_per_step": int(2 * args.chains * 8),
+                "note": "wall-clock sampling: every step sends the proposals and reads chi**2"},
         "gpu_launches": launches_da,
         "gpu_launches_plain": launches_plain,
         "da_proposal_scale": args.da_scale,
         "clocks": clk,
     }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
     if eng_c is not None:
         eng_c.close()
     eng.close()
-    return 0
+    return line if rank == 0 else None
+
+
+def C_sizeof_model():
+    import ctypes as C
+    return C.sizeof(abi.LcgModel)
 
 
 def run_reference_da(args):
@@ -859,12 +912,12 @@ def run_reference_da(args):
     steps, so the run takes seconds; ESS/s by the same estimator."""
     rank, _, world = rank_info()
     if rank != 0:
-        return 0
+        return None
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_lib as OL
     from lcurve_re_b200 import surrogate as S
     from lcurve_re_b200 import workloads as W
-    from lcurve_re_b200.sampler import ess_total, metropolis
+    from lcurve_re_b200.sampler import metropolis, summary
     kind = "reference" if os.path.exists(OL.REF_RELEASE_SO) else "port"
     lib = OL.Reference(OL.REF_RELEASE_SO) if kind == "reference" else OL.Oracle()
     fac = S.ModelFactory()
@@ -897,15 +950,18 @@ def run_reference_da(args):
     cov = np.cov(samp.T) * 2.38 ** 2 / 9 + np.diag((scale0 * 1e-3) ** 2)
     steps = min(400, max(40, args.steps * 20))  # about half a minute of CPU
     chp, _, _, acc, wall = metropolis(exact, theta0, cov, steps, seed=21)
-    ess, _ = ess_total(chp)
-    v = ess / wall
+    sm = summary(chp, wall)
+    v = sm["ess_bulk_per_s"]
     line = {"impl": "reference", "metric": "MCMC effective samples/s", "value": v,
             "unit": "effective samples/s", "n_gpus": world, "steps": steps, "warmup": burn,
             "ms_per_step": wall / steps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (wd_dm_small physics at 500 points + noise sigma=1.5e-3)",
             "config": {"workload": "surrogate_da reference arm: plain Metropolis, %d chains x "
-                                   "%d steps on the reference CPU path" % (chains, steps)},
+                                   "%d steps on the reference CPU path" % (chains, steps),
+                       "ess": "bulk ESS (rank-normalised multi-chain ESS of the split chains), "
+                              "minimum over parameters"},
+            "plain": sm,
             "cpu_baseline": {"value": v, "unit": "effective samples/s", "cores": os.cpu_count(),
                              "kind": kind,
                              "sample": "%d chains x %d steps after %d burn-in steps, one light "
@@ -913,21 +969,99 @@ def run_reference_da(args):
                                        % (chains, steps, burn, acc)},
             "e2e": {"value": v, "unit": "effective samples/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
+
+
+def launch_ranks(n):
+    """bench.py --gpus N started without a launcher: one process per GPU on
+    this node, with RANK / LOCAL_RANK / WORLD_SIZE / MASTER_* set as
+    torch.distributed.run sets them, and the same arguments. Only rank 0
+    prints. Returns the first non-zero exit status of the ranks."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    procs = []
+    for r in range(n):
+        env = dict(os.environ, RANK=str(r), LOCAL_RANK=str(r), WORLD_SIZE=str(n),
+                   LOCAL_WORLD_SIZE=str(n), MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+        procs.append(subprocess.Popen([sys.executable, os.path.abspath(__file__)] + sys.argv[1:],
+                                      env=env))
+    rcs = [p.wait() for p in procs]
+    return next((rc for rc in rcs if rc), 0)
+
+
+def init_dist(world):
+    """The process group for max-over-ranks timing (NCCL on GPUs, gloo where
+    CUDA is absent); None for one rank."""
+    if world <= 1:
+        return None
+    import torch
+    import torch.distributed as dist
+    backend = "nccl" if torch.cuda.is_available() else "gloo"
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return dist
+
+
+def sub_args(args, **over):
+    a = argparse.Namespace(**vars(args))
+    for k, v in over.items():
+        setattr(a, k, v)
+    return a
+
+
+def extra_workloads(args, world):
+    """The default run at one GPU also reports the batched engine (cfg2) and
+    the surrogate's delayed acceptance (cfg4, the named 512 chains x 20,000
+    steps), each as a sub-object with its own value, e2e, cpu_baseline and
+    clocks."""
+    return (world == 1 and args.workload == "wd_dm_large" and args.precision == "mixed"
+            and not args.headline_only)
+
+
+MCMC_NAMED = dict(mcmc_steps=20000)
 
 
 def main():
     args = parse()
-    if args.impl == "ours" and args.workload == "surrogate_da":
-        return run_surrogate(args)
-    if args.impl == "reference" and args.workload == "surrogate_da":
-        return run_reference_da(args)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return launch_ranks(args.gpus)
+    rank, local, world = rank_info()
+    more = extra_workloads(args, world)
     if args.impl == "reference":
-        return run_reference_batch(args) if args.workload == "mcmc_batch" else run_reference(args)
-    if args.workload == "mcmc_batch":
-        return run_batch(args)
-    return run_ours(args)
+        if args.workload == "surrogate_da":
+            line = run_reference_da(args)
+        elif args.workload == "mcmc_batch":
+            line = run_reference_batch(args)
+        else:
+            line = run_reference(args)
+        if line is not None and more:
+            line["workloads"] = {
+                "mcmc_batch": run_reference_batch(sub_args(args, steps=1, warmup=0)),
+                "surrogate_da": run_reference_da(sub_args(args, **MCMC_NAMED))}
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return 0
+    import torch
+    torch.cuda.set_device(local)
+    dist = init_dist(world)
+    try:
+        if args.workload == "surrogate_da":
+            line = run_surrogate(args)
+        elif args.workload == "mcmc_batch":
+            line = run_batch(args, dist)
+        else:
+            line = run_ours(args, dist)
+            if line is not None and more:
+                line["workloads"] = {
+                    "mcmc_batch": run_batch(sub_args(args, steps=min(args.steps, 20)), dist),
+                    "surrogate_da": run_surrogate(sub_args(args, **MCMC_NAMED))}
+        if line is not None:
+            print(json.dumps(line), flush=True)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+    return 0
 
 
 if __name__ == "__main__":

@@ -1,6 +1,6 @@
 """Random-walk Metropolis over many parallel chains, plain or with delayed
-acceptance screened by a surrogate, and the effective-sample-size
-estimator of the reference sampler.
+acceptance screened by a surrogate; the effective-sample-size estimator of
+the reference sampler and the rank-normalised multi-chain ESS and R-hat.
 
 The likelihood is exp(-chi**2 / 2) with chi**2 from a callable over a batch
 of parameter vectors (one row per chain): the exact GPU engine
@@ -30,7 +30,12 @@ def ess_geyer(x):
     """Geyer's initial-positive-sequence ESS of one chain, as the reference
     sampler computes it (new_scripts/mcmc_solver.cpp:80-115): autocorrelations
     summed in consecutive pairs up to the first negative pair sum, lags up to
-    min(n/2, 10000). Autocovariances come from an FFT (the same sums)."""
+    min(n/2, 10000). Autocovariances come from an FFT (the same sums).
+
+    One deliberate difference: a chain that never moved (zero variance) has
+    no effective samples here, where the reference returns n for it. Counted
+    as n, frozen chains of a sticky sampler would inflate the sum over
+    chains."""
     x = np.asarray(x, np.float64)
     n = x.shape[0]
     if n < 4:
@@ -38,7 +43,7 @@ def ess_geyer(x):
     xc = x - x.mean()
     c0 = float(np.dot(xc, xc)) / n
     if c0 < 1e-30:
-        return float(n)
+        return 0.0
     size = 1 << int(np.ceil(np.log2(2 * n)))
     f = np.fft.rfft(xc, size)
     acov = np.fft.irfft(f * np.conj(f), size)[:n]  # acov[k] = sum_i xc[i] xc[i+k]
@@ -61,6 +66,134 @@ def ess_total(chain):
     steps, nc, npar = chain.shape
     per = np.array([[ess_geyer(chain[:, c, k]) for c in range(nc)] for k in range(npar)])
     return float(per.sum(axis=1).min()), per.sum(axis=1)
+
+
+def _split(chain):
+    """[steps x chains] -> [2*chains x steps//2]: each chain cut in two halves
+    (a chain that drifts then shows as two chains that disagree)."""
+    h = chain.shape[0] // 2
+    return np.concatenate([chain[:h].T, chain[chain.shape[0] - h:].T], axis=0)
+
+
+def _rank_normal(x):
+    """Pooled ranks of all draws mapped to normal scores,
+    Phi^-1((r - 3/8) / (S + 1/4)), ties given their average rank."""
+    from scipy.special import ndtri
+    from scipy.stats import rankdata
+    r = rankdata(x.ravel(), method="average").reshape(x.shape)
+    return ndtri((r - 0.375) / (x.size + 0.25))
+
+
+def _ess_chains(x):
+    """Multi-chain effective sample size of x [chains x draws] (Vehtari,
+    Gelman, Simpson, Carpenter & Buerkner 2021, "Rank-normalization,
+    folding, and localization: an improved R-hat"): the autocorrelation at
+    each lag combines the chains' mean autocovariance with the between-chain
+    variance, rho_t = 1 - (W - mean_m acov_m(t)) / var_plus; the sum is cut
+    by Geyer's initial positive sequence made monotone."""
+    m, n = x.shape
+    if n < 4:
+        return float(m * n)
+    xc = x - x.mean(axis=1, keepdims=True)
+    size = 1 << int(np.ceil(np.log2(2 * n)))
+    f = np.fft.rfft(xc, size, axis=1)
+    acov = np.fft.irfft(f * np.conj(f), size, axis=1)[:, :n] / n  # biased, per chain
+    w = float((acov[:, 0] * n / (n - 1)).mean())                    # within-chain variance
+    var_plus = w * (n - 1) / n + (float(x.mean(axis=1).var(ddof=1)) if m > 1 else 0.0)
+    if var_plus <= 0.0:
+        return 0.0
+    rho = 1.0 - (w - acov.mean(axis=0)) / var_plus
+    rho[0] = 1.0
+    # pairs (rho_2k + rho_2k+1) while positive, then made non-increasing
+    pairs = []
+    for t in range(0, n - 1, 2):
+        p = rho[t] + rho[t + 1]
+        if p <= 0.0:
+            break
+        pairs.append(p if not pairs else min(p, pairs[-1]))
+    tau = -1.0 + 2.0 * float(np.sum(pairs))
+    return float(m * n / max(tau, 1.0 / np.log10(max(m * n, 10))))
+
+
+def ess_bulk(chain):
+    """Bulk ESS per parameter: the multi-chain ESS of the rank-normalised
+    split chains. chain [steps x chains x params] -> array [params]. Chains
+    that have not mixed (different halves, different chains in different
+    places) lower it through the between-chain variance, which per-chain
+    estimators do not see."""
+    return np.array([_ess_chains(_rank_normal(_split(chain[:, :, k])))
+                     for k in range(chain.shape[2])])
+
+
+def ess_mean(chain):
+    """ESS for the posterior mean per parameter: the multi-chain ESS of the
+    split chains on the original scale (the one the Monte Carlo standard
+    error of a mean needs)."""
+    return np.array([_ess_chains(_split(chain[:, :, k])) for k in range(chain.shape[2])])
+
+
+def _rhat(z):
+    """Potential scale reduction of z [chains x draws]: sqrt(var_plus / W)."""
+    n = z.shape[1]
+    w = z.var(axis=1, ddof=1).mean()
+    b = n * z.mean(axis=1).var(ddof=1)
+    return float(np.sqrt(((n - 1) / n * w + b / n) / w)) if w > 0 else np.inf
+
+
+def _rhat_split(s, z=None):
+    """Rank-normalised split R-hat of split chains s (the same paper): the
+    larger of the bulk value and the folded (|x - median|) one."""
+    z = _rank_normal(s) if z is None else z
+    return max(_rhat(z), _rhat(_rank_normal(np.abs(s - np.median(s)))))
+
+
+def rhat(chain):
+    """Rank-normalised split R-hat per parameter; near 1 for chains that
+    sample the same distribution."""
+    return np.array([_rhat_split(_split(chain[:, :, k])) for k in range(chain.shape[2])])
+
+
+def summary(chain, wall):
+    """Per-sampler figures for one run (chain [steps x chains x params],
+    wall seconds): bulk ESS and R-hat (rank-normalised, split chains), the
+    reference's Geyer estimator (frozen chains counted as zero) and the
+    between-chain estimate, each as a minimum over parameters, and ESS/s."""
+    bulk, rh = [], []
+    for k in range(chain.shape[2]):
+        s = _split(chain[:, :, k])
+        z = _rank_normal(s)
+        bulk.append(_ess_chains(z))
+        rh.append(_rhat_split(s, z))
+    geyer, _ = ess_total(chain)
+    bulk = float(np.min(bulk))
+    return {"ess_bulk": bulk, "ess_bulk_per_s": bulk / wall, "ess_geyer": geyer,
+            "ess_geyer_per_s": geyer / wall,
+            "ess_between_chains": ess_between_chains(chain)[0], "rhat_max": float(np.max(rh)),
+            "wall_s": wall}
+
+
+def mean_shift(chain_a, chain_b):
+    """Posterior-mean difference of two samplers per parameter, in units of
+    chain_b's posterior standard deviation, with its Monte Carlo standard
+    error (the two means' errors sd / sqrt(ESS_mean) combined). Returns
+    (shift, mcse) arrays [params]."""
+    sa, sb = chain_a.reshape(-1, chain_a.shape[2]), chain_b.reshape(-1, chain_b.shape[2])
+    sd_b = sb.std(axis=0)
+    shift = np.abs(sa.mean(axis=0) - sb.mean(axis=0)) / sd_b
+    mcse_a = sa.std(axis=0) / np.sqrt(np.maximum(ess_mean(chain_a), 1.0))
+    mcse_b = sd_b / np.sqrt(np.maximum(ess_mean(chain_b), 1.0))
+    return shift, np.sqrt(mcse_a ** 2 + mcse_b ** 2) / sd_b
+
+
+def shift_verdict(shift, mcse, bar=0.1, z=2.0):
+    """'within' when every parameter's shift + z * mcse is below bar,
+    'outside' when some parameter's shift - z * mcse is above it,
+    'undecided' otherwise (more effective samples needed)."""
+    if np.all(shift + z * mcse < bar):
+        return "within"
+    if np.any(shift - z * mcse > bar):
+        return "outside"
+    return "undecided"
 
 
 def ess_between_chains(chain):

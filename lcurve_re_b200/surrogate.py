@@ -220,6 +220,82 @@ def local_draws(mean, cov, n, seed=0, widen=3.0):
     return out[:n]
 
 
+def gaussian_in_box_fraction(mean, cov, widen, n=1 << 20, seed=99):
+    """Monte Carlo estimate of the probability that local_draws' Gaussian
+    lands inside the box (its truncation constant)."""
+    rng = np.random.default_rng(seed)
+    L = np.linalg.cholesky(np.asarray(cov) * widen ** 2)
+    t = np.asarray(mean) + rng.standard_normal((n, len(PARAMS))) @ L.T
+    return float(in_box(t).mean())
+
+
+def curves_chi2(curves, data, index):
+    """Exact chi**2 of the data for unit-mean engine curves on the grid: the
+    curves at the data points (index), the optimal scale as re_scale fits it
+    (re_scale.cpp:16-42), and sum w ((f - s m) / sigma)**2. Rows of curves
+    [n x NGRID] (float32 or float64) -> array [n]."""
+    import torch
+    d = np.ascontiguousarray(data)
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    f = torch.as_tensor(d["flux"].copy(), device=dev)
+    wt = torch.as_tensor((d["weight"] / d["ferr"] ** 2).copy(), device=dev)
+    idx = torch.as_tensor(np.asarray(index), device=dev)
+    out = np.empty(curves.shape[0])
+    for i0 in range(0, curves.shape[0], 65536):
+        m = torch.as_tensor(curves[i0:i0 + 65536], device=dev)[:, idx].to(torch.float64)
+        sc = (m * (wt * f)).sum(1) / (m * m * wt).sum(1)
+        out[i0:i0 + m.shape[0]] = (((f - sc[:, None] * m) ** 2) * wt).sum(1).cpu().numpy()
+    return out
+
+
+def posterior_resample(pools, chi2, n, seed=0):
+    """Sampling-importance-resampling of the posterior (uniform prior over the
+    box, likelihood exp(-chi**2 / 2)) from parameter vectors whose exact
+    chi**2 is known. pools: list of (theta [k x 9], log density of the
+    distribution they were drawn from at each row); together they are one
+    draw from the mixture sum_j (k_j / K) q_j, whose density weighs each row.
+    Returns (n resampled rows, the weighted mean, the weighted covariance,
+    the importance sample's effective size 1 / sum w**2)."""
+    theta = np.vstack([p[0] for p in pools])
+    K = theta.shape[0]
+    logq = np.full(K, -np.inf)
+    for t, logq_j in pools:
+        logq = np.logaddexp(logq, logq_j(theta) + np.log(t.shape[0] / K))
+    logw = -0.5 * np.asarray(chi2) - logq
+    logw[~np.isfinite(logw)] = -np.inf
+    w = np.exp(logw - logw.max())
+    w /= w.sum()
+    mean = w @ theta
+    xc = theta - mean
+    cov = (xc * w[:, None]).T @ xc
+    rng = np.random.default_rng(seed)
+    # systematic resampling
+    u = (rng.random() + np.arange(n)) / n
+    rows = np.minimum(np.searchsorted(np.cumsum(w), u), K - 1)
+    return theta[rows].copy(), mean, cov, float(1.0 / np.sum(w ** 2))
+
+
+def log_uniform_box():
+    """Log density of uniform draws over the box."""
+    vol = float(np.prod(BOX[:, 1] - BOX[:, 0]))
+    return lambda theta: np.full(np.asarray(theta).shape[0], -np.log(vol))
+
+
+def log_gaussian_in_box(mean, cov, widen):
+    """Log density of local_draws(mean, cov, widen): the Gaussian truncated
+    to the box (its normalisation from gaussian_in_box_fraction)."""
+    C = np.asarray(cov) * widen ** 2
+    L = np.linalg.cholesky(C)
+    logdet = 2.0 * np.sum(np.log(np.diag(L)))
+    z = gaussian_in_box_fraction(mean, cov, widen)
+    d = len(PARAMS)
+
+    def f(theta):
+        y = np.linalg.solve(L, (np.asarray(theta) - mean).T)
+        return -0.5 * (y * y).sum(0) - 0.5 * (d * np.log(2 * np.pi) + logdet) - np.log(z)
+    return f
+
+
 class SurrogateChi2:
     """chi**2 of the data under the surrogate, on the GPU: the MLP forward
     pass, then lcg_mlp_pca_chisq (curve at the data points, optimal scale,

@@ -13,6 +13,8 @@ Gaussian noise drawn from a seeded numpy Generator.
   cv_disc        cataclysmic variable: white dwarf, Roche-filling donor, flared
                  accretion disc with its rim, and the bright spot
 """
+import math
+
 import numpy as np
 
 from . import abi
@@ -141,6 +143,49 @@ def cv_disc(**over):
     kw = dict(CV_DISC)
     kw.update(over)
     return model(**kw)
+
+
+def _rings(nlat):
+    """Ring count and spacing of a full star without infill: dtheta = pi / nlat
+    and ceil(pi / dtheta) rings (numface.cpp:46-50, set_star_grid.cpp:249-250),
+    one more than nlat where the quotient rounds above it."""
+    dtheta = math.pi / nlat
+    return int(math.ceil(math.pi / dtheta)), dtheta
+
+
+def _numface(nlat):
+    """Faces numface gives a full star without infill (numface.cpp:14-52)."""
+    nl, dtheta = _rings(nlat)
+    return sum(max(16, int(2 * math.pi / (dtheta / math.sin(math.pi * (i + 0.5) / nl))))
+               for i in range(nl))
+
+
+def _tiled(nlat):
+    """Faces the ring tiling of add_faces lays on a full star without infill
+    (set_star_grid.cpp:241-320): the same rings, nphi from 2 pi sin(theta) /
+    dtheta, which rounds differently from numface's expression at a few nlat."""
+    nl, dtheta = _rings(nlat)
+    return sum(max(16, int(2 * math.pi * math.sin(math.pi * (i + 0.5) / nl) / dtheta))
+               for i in range(nl))
+
+
+def tiling_overflows(nlat):
+    """True at the nlat (153, 297, 315, 333, 339, 549, ... up to 1200: 16
+    values) where the ring tiling has more faces than numface, with which the
+    reference sizes its Point vector: its add_faces then writes past the
+    vector's end (set_star_grid.cpp:490,508), undefined behaviour that can
+    corrupt the heap of the process running it. The engine keeps the numface
+    faces the vector holds."""
+    return _tiled(nlat) > _numface(nlat)
+
+
+def reference_safe(m):
+    """False for a model (without infill) whose fine or coarse grid of either
+    star has an nlat at which the reference's grid build writes past its
+    vector: such models are not run through the reference's own code."""
+    c = m.to_c() if hasattr(m, "to_c") else m
+    return not any(tiling_overflows(int(v)) for v in (c.nlat1f, c.nlat2f, c.nlat1c, c.nlat2c)
+                   if v > 0)
 
 
 def elements(nface1, nface2, nent):

@@ -153,7 +153,8 @@ def batch_checked(reference, oracle):
     ms, d = _batch_models()
     out = []
     for m, nl in zip(ms, BATCH_NLAT):
-        checker = oracle if nl in OVERFLOWING_NLAT else reference
+        checker = reference if W.reference_safe(m) else oracle
+        assert (checker is oracle) == (nl in OVERFLOWING_NLAT)
         out.append((nl, checker, _Checked(checker, m, d)))
     return out
 

@@ -82,7 +82,8 @@ def test_vary_order_and_set_param():
 
 
 def test_reference_example_config_parses(tmp_path):
-    ref = "/root/reference/example/example.json"
+    ref = os.path.join(os.environ.get("LCURVE_REF_DIR", "/root/reference"), "example",
+                       "example.json")
     if not os.path.exists(ref):
         pytest.skip("reference example not present")
     text = open(ref).read()
@@ -99,3 +100,19 @@ def test_read_data_rules(tmp_path):
     assert d.shape[0] == 2
     assert d["ferr"][1] == 0.0 and d["weight"][1] == 0.0 and d["ndiv"][1] == 3
     assert d.dtype.itemsize == 48
+
+
+def test_tiling_overflow_nlat_match_numface_and_the_known_list(oracle):
+    """workloads.tiling_overflows: the nlat at which the ring tiling lays more
+    faces than numface sizes the reference's Point vector with. Its numface
+    equals the oracle's face count (numface.cpp), and up to 1200 the overflow
+    set is the one the GPU face-count tests pin."""
+    for nlat in (30, 40, 80, 153, 200, 297, 306, 375, 393, 400, 813, 879):
+        m = W.model(nlat1f=nlat, nlat2f=nlat)
+        assert W._numface(nlat) == oracle.face_count(m, 0) == oracle.face_count(m, 1), nlat
+    over = [k for k in range(1, 1201) if W.tiling_overflows(k)]
+    assert over == [153, 297, 315, 333, 339, 549, 609, 621, 645, 686, 687, 705, 710, 758, 1173,
+                    1191]
+    assert [k for k in range(1, 1201) if W._tiled(k) < W._numface(k)] == [813, 879]
+    ms, _ = W.mcmc_batch(256)
+    assert sum(not W.reference_safe(m) for m in ms) == 8

@@ -77,3 +77,23 @@ def test_two_gloo_ranks_match_one_process():
     for rank, full, t in res:
         assert np.array_equal(full, serial), rank
         assert t == 2.0
+
+
+def test_bench_gpus_flag_launches_one_process_per_rank():
+    """bench.py --gpus 2 without a launcher starts two ranks itself (RANK,
+    LOCAL_RANK, WORLD_SIZE, MASTER_* set as torch.distributed.run sets them);
+    rank 0 alone prints one line, which reports n_gpus 2. The reference arm
+    needs no GPU, so it runs here."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = {k: v for k, v in os.environ.items()
+           if k not in ("RANK", "LOCAL_RANK", "WORLD_SIZE", "MASTER_ADDR", "MASTER_PORT")}
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference",
+                        "--gpus", "2", "--workload", "wd_dm_small", "--steps", "1", "--warmup",
+                        "0"], capture_output=True, text=True, timeout=600, env=env, cwd=root)
+    assert r.returncode == 0, r.stderr
+    lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    assert len(lines) == 1
+    assert lines[0]["n_gpus"] == 2 and lines[0]["impl"] == "reference"

@@ -8,7 +8,9 @@ still sample the exact posterior while calling the exact model less often.
 """
 import numpy as np
 
-from lcurve_re_b200.sampler import delayed_acceptance, ess_geyer, ess_total, metropolis
+from lcurve_re_b200.sampler import (delayed_acceptance, ess_bulk, ess_geyer, ess_mean,
+                                    ess_total, mean_shift, metropolis, rhat, shift_verdict,
+                                    summary)
 
 
 def _ess_loop(x):
@@ -41,7 +43,8 @@ def test_ess_matches_the_reference_loop():
     for phi, seed in ((0.0, 1), (0.5, 2), (0.9, 3)):
         x = _ar1(400, phi, seed)
         assert abs(ess_geyer(x) - _ess_loop(list(x))) <= 1e-9 * _ess_loop(list(x))
-    assert ess_geyer(np.ones(10)) == 10.0 and ess_geyer(np.arange(3.0)) == 3.0
+    # a chain that never moved has no effective samples (the reference counts n)
+    assert ess_geyer(np.ones(10)) == 0.0 and ess_geyer(np.arange(3.0)) == 3.0
 
 
 def test_ess_of_ar1_series():
@@ -151,3 +154,80 @@ def test_between_chain_ess_matches_geyer_on_ar1_chains():
     g, _ = ess_total(x)
     b, _ = ess_between_chains(x)
     assert abs(g / want - 1) < 0.1 and abs(b / want - 1) < 0.25, (g, b, want)
+
+
+def _ar1_chains(steps, chains, phi, seed, offsets=None):
+    rng = np.random.default_rng(seed)
+    x = np.empty((steps, chains))
+    x[0] = rng.standard_normal(chains)
+    for i in range(1, steps):
+        x[i] = phi * x[i - 1] + np.sqrt(1 - phi * phi) * rng.standard_normal(chains)
+    if offsets is not None:
+        x += offsets[None, :]
+    return x[:, :, None]
+
+
+def test_multichain_ess_and_rhat_on_ar1_chains():
+    """Stationary AR(1) chains: bulk and mean ESS near steps x chains x
+    (1 - phi) / (1 + phi), R-hat near 1. The same chains with different
+    offsets (chains that have not mixed): R-hat well above 1 and a bulk ESS
+    that collapses, where the per-chain Geyer sum does not notice."""
+    steps, chains = 4000, 16
+    for phi in (0.0, 0.7):
+        ch = _ar1_chains(steps, chains, phi, 11)
+        expect = steps * chains * (1 - phi) / (1 + phi)
+        assert abs(ess_bulk(ch)[0] - expect) < 0.15 * expect, (phi, ess_bulk(ch), expect)
+        assert abs(ess_mean(ch)[0] - expect) < 0.15 * expect
+        assert rhat(ch)[0] < 1.01
+    ch = _ar1_chains(steps, chains, 0.7, 12, offsets=np.linspace(-2, 2, chains))
+    assert rhat(ch)[0] > 1.5
+    assert ess_bulk(ch)[0] < 0.05 * ess_total(ch)[0]
+
+
+def test_summary_counts_frozen_chains_as_zero():
+    ch = _ar1_chains(2000, 8, 0.5, 3)
+    stuck = np.array([-1.5, -1.0, -0.5, 0.3, 0.8, 1.2, 1.6, 2.0])  # states chains stuck at
+    frozen = np.concatenate([ch, np.broadcast_to(stuck[None, :, None], (2000, 8, 1))], axis=1)
+    a, b = summary(ch, 1.0), summary(frozen, 1.0)
+    assert b["ess_geyer"] == a["ess_geyer"]  # the frozen chains add nothing
+    assert b["ess_bulk"] < a["ess_bulk"]  # and they split the distribution
+
+
+def test_mean_shift_and_verdict():
+    a = _ar1_chains(4000, 16, 0.5, 21)
+    b = _ar1_chains(4000, 16, 0.5, 22)
+    shift, mcse = mean_shift(a, b)
+    assert shift[0] < 4 * mcse[0] and 0.002 < mcse[0] < 0.02
+    assert shift_verdict(shift, mcse) == "within"
+    c = a + 0.3
+    shift, mcse = mean_shift(c, b)
+    assert abs(shift[0] - 0.3) < 5 * mcse[0]
+    assert shift_verdict(shift, mcse) == "outside"
+    assert shift_verdict(np.array([0.09]), np.array([0.02])) == "undecided"
+
+
+def test_posterior_resample_recovers_a_gaussian_posterior():
+    """Importance resampling in two stages, as the delayed-acceptance
+    benchmark does it: box-uniform and a wide Gaussian pool give a first
+    estimate, a second Gaussian pool at 1.5x its spread is added, and the
+    final weighted mean, covariance and resampled rows match the Gaussian
+    posterior (chi**2 known in closed form)."""
+    from lcurve_re_b200 import surrogate as S
+    rng = np.random.default_rng(5)
+    lo, hi = S.BOX[:, 0], S.BOX[:, 1]
+    mu = (lo + hi) / 2 + 0.1 * (hi - lo)
+    sd = 0.04 * (hi - lo)
+    chi2 = lambda t: np.sum(((t - mu) / sd) ** 2, axis=1)
+    th_u = lo + rng.random((50000, 9)) * (hi - lo)
+    guess_mu, guess_cov = mu + 0.5 * sd, np.diag((1.3 * sd) ** 2)
+    th_g = S.local_draws(guess_mu, guess_cov, 60000, seed=3, widen=2.0)
+    pools = [(th_u, S.log_uniform_box()), (th_g, S.log_gaussian_in_box(guess_mu, guess_cov, 2.0))]
+    _, m1, c1, ess1 = S.posterior_resample(pools, chi2(np.vstack([th_u, th_g])), 10, seed=1)
+    th_2 = S.local_draws(m1, c1, 60000, seed=4, widen=1.5)
+    pools.append((th_2, S.log_gaussian_in_box(m1, c1, 1.5)))
+    rows, mean, cov, ess = S.posterior_resample(pools, chi2(np.vstack([th_u, th_g, th_2])),
+                                                4000, seed=1)
+    assert ess > 10 * ess1 and ess > 5000, (ess1, ess)
+    assert np.all(np.abs(mean - mu) < 0.05 * sd)
+    assert np.all(np.abs(np.sqrt(np.diag(cov)) / sd - 1) < 0.05)
+    assert np.all(np.abs(rows.mean(0) - mu) < 0.1 * sd)
