@@ -13,8 +13,25 @@
 //     reference's messages for lobe overflow), which the solvers treat as a
 //     rejected model (mcmc_solver.cpp:1071, levmarq_solver.cpp:682).
 // One engine context per host thread: the reference keeps its caches
-// thread_local too (light_curve_comp.cpp:161). Disc, bright-spot and iscale
-// models raise Lcurve_Error: the engine has no CPU fallback.
+// thread_local too (light_curve_comp.cpp:161). Every model the reference
+// evaluates runs on the engine, discs, rims, bright spots and iscale included;
+// there is no CPU fallback.
+//
+// The environment variables the reference's CUDA path reads select the same
+// things here (comp_light_cuda.cu:415,523-533): LCURVE_CUDA_PRECISION = double,
+// fp64 or 64 gives FP64 contexts (every stage FP64, the sweep bit-identical
+// to the CPU path); anything else, or unset, gives the mixed-precision default,
+// as the reference's CUDA sweeps default to FP32. LCURVE_CUDA_DEVICE picks the
+// device (default 0).
+//
+// The two offload counters the reference's CUDA sources define and
+// levmarq_solver.cpp reports (comp_light_cuda.h:23, set_star_grid_cuda.h:24)
+// are defined here too: light curves this thread evaluated on the engine (both
+// stars' grids and flux sweeps run on the device for each).
+#include <algorithm>
+#include <cctype>
+#include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -89,16 +106,30 @@ lcg_model to_lcg(const Lcurve::Model &m) {
 
 struct Context {
     lcg_ctx *ctx = nullptr;
+    std::uint64_t curves = 0;
     ~Context() {
         if (ctx) lcg_destroy(ctx);
     }
 };
 
+thread_local Context t_context;
+
+int32_t precision_from_env() {
+    const char *env = std::getenv("LCURVE_CUDA_PRECISION");
+    if (!env) return LCG_PREC_MIXED;
+    std::string mode(env);
+    std::transform(mode.begin(), mode.end(), mode.begin(),
+                   [](unsigned char ch) { return (char)std::tolower(ch); });
+    return (mode == "double" || mode == "fp64" || mode == "64") ? LCG_PREC_FP64 : LCG_PREC_MIXED;
+}
+
 lcg_ctx *context() {
-    static thread_local Context c;
+    Context &c = t_context;
     if (!c.ctx) {
         lcg_options o;
         lcg_default_options(&o);
+        o.precision = precision_from_env();
+        if (const char *dev = std::getenv("LCURVE_CUDA_DEVICE")) o.device = std::atoi(dev);
         if (lcg_create(&c.ctx, &o) != LCG_OK) {
             c.ctx = nullptr;
             throw Lcurve::Lcurve_Error(std::string("light_curve_comp: ") + lcg_last_error(nullptr));
@@ -126,6 +157,7 @@ void Lcurve::light_curve_comp(const Lcurve::Model &mdl, const Lcurve::Data &data
         lcg_light_curve(ctx, &m, reinterpret_cast<const lcg_datum *>(data.data()),
                         (int32_t)data.size(), flags, sfac.data(), calc.data(), s);
     if (st != LCG_OK) throw Lcurve::Lcurve_Error(lcg_last_error(ctx));
+    t_context.curves++;
     wdwarf = s[LCG_OUT_WDWARF];
     if (scale || rdata) {
         chisq = s[LCG_OUT_CHISQ];
@@ -136,3 +168,8 @@ void Lcurve::light_curve_comp(const Lcurve::Model &mdl, const Lcurve::Data &data
     rv1 = s[LCG_OUT_RV1];
     rv2 = s[LCG_OUT_RV2];
 }
+
+namespace Lcurve {
+std::uint64_t cuda_flux_evaluation_count() { return t_context.curves; }
+std::uint64_t cuda_grid_evaluation_count() { return t_context.curves; }
+}  // namespace Lcurve
