@@ -9,7 +9,16 @@ the range when both sides would leave it), steps halved when an evaluation
 fails, non-finite derivatives set to zero. The reference divides a first
 backward step by sign * (p' - p) = +h (levmarq_solver.cpp:843-849), which
 gives that column the derivative's opposite sign; that is kept, so a solver
-driven by this Jacobian takes the reference's steps.
+driven by this Jacobian takes the reference's steps. The scheme is pinned to
+the reference's own executable: evaluated through the compiled reference, it
+reproduces the uncertainties and correlations lcurve_levmarq prints from the
+covariance of its Jacobian, on a model that runs every branch
+(tests/test_solvers.py).
+
+Precision: on a mixed-precision engine context a round of perturbed models is
+one graph-captured batch. On an FP64 context lcg_light_curve_batch evaluates
+the models of the round one after another on the GPU (the batched flux sweep
+is the mixed-precision one), with the same results as single calls.
 """
 import numpy as np
 
