@@ -13,8 +13,9 @@ in an MCMC step whose geometry changes.
          points go host->device and the curve device->host every step
   roofline  the flux sweep (the dominant kernel): 16 FLOP per element
          (5 for mu, 8 for the Claret Horner form, 2 for mu*flux*I,
-         1 accumulate) over its CUDA-event time, against the FP32
-         FMA peak measured live by lcg_measure_fp32_peak
+         1 accumulate) over its CUDA-event time, against the FMA peak
+         of the sweep's arithmetic measured live (lcg_measure_fp32_peak,
+         or lcg_measure_fp64_peak with --precision fp64)
   cpu_baseline  lcurve_re's own CPU path (oracle/_ref, Release flags,
          OpenMP on all host cores) on whole light curves of the workload
          (grids rebuilt each call) for about 20 s; its curve of the exact
@@ -275,7 +276,8 @@ def run_ours(args, dist=None):
     sfac = np.ones(5)
     scal = np.zeros(abi.NOUT)
     dptr = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
-    peak = eng.fp32_peak_tflops()
+    fp64 = args.precision == "fp64"
+    peak = eng.fp64_peak_tflops() if fp64 else eng.fp32_peak_tflops()
 
     ext = torch.cuda.ExternalStream(eng.stream_ptr)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
@@ -373,11 +375,13 @@ def run_ours(args, dist=None):
                    "precision": args.precision, "grids": "rebuilt every step",
                    "l2": "flushed by a 256 MiB write between timed steps (untimed)",
                    "parallelism": "replicas x%d" % world},
-        "roofline": {"bound": "fp32", "kernel": "k_flux_fast" if args.precision == "mixed"
-                     else "k_flux64",
+        "roofline": {"bound": "fp64" if fp64 else "fp32",
+                     "kernel": "k_flux64" if fp64 else "k_flux_fast",
                      "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                     "peak_source": "measured live: FFMA-chain kernel (lcg_measure_fp32_peak)",
+                     "peak_source": ("measured live: DFMA-chain kernel (lcg_measure_fp64_peak)"
+                                     if fp64 else
+                                     "measured live: FFMA-chain kernel (lcg_measure_fp32_peak)"),
                      "flop_per_element": FLOP_PER_ELEMENT,
                      "flux_ms_per_step": flux_ms / args.steps,
                      "flux_launches_per_step": flux_n / args.steps},

@@ -361,6 +361,10 @@ int64_t lcg_kernel_launches(int32_t reset);
  * roofline. */
 lcg_status lcg_measure_fp32_peak(lcg_ctx *ctx, double *tflops);
 
+/* The same with a DFMA chain: the device's FP64 FMA throughput, the
+ * denominator of the FP64 sweep's roofline. */
+lcg_status lcg_measure_fp64_peak(lcg_ctx *ctx, double *tflops);
+
 /* ---- surrogate network kernels (no reference counterpart) -------------
  * The delayed-acceptance sampler screens proposals with a small MLP whose
  * training and inference run on these kernels. Device pointers, all on the

@@ -114,6 +114,7 @@ PROTOTYPES = {
     "lcg_stage_times": (None, [P, D, I64, C.c_int32]),
     "lcg_flux_elements": (C.c_int64, [P, C.c_int32]),
     "lcg_measure_fp32_peak": (C.c_int, [P, D]),
+    "lcg_measure_fp64_peak": (C.c_int, [P, D]),
     "lcg_set_data": (C.c_int, [P, P, C.c_int32]),
     "lcg_batch_curves": (C.c_int, [P, I32, C.c_int32, D]),
     "lcg_batch_curves_device": (C.c_int, [P, I32, C.c_int32, C.c_void_p]),

@@ -625,6 +625,41 @@ void lcg::count_launches(int64_t k) { g_launches.fetch_add(k, std::memory_order_
 
 // ---- C ABI --------------------------------------------------------------------
 
+// Best of five timed launches of an FMA-chain probe on the context's stream,
+// after one warm-up: TFLOP/s (2 FLOP per FMA).
+template <class Launch>
+lcg_status measure_peak(lcg_ctx *c, double *tflops, Launch launch) {
+    if (!c || !tflops) return LCG_E_INVALID;
+    cudaSetDevice(c->device);
+    void *sink = nullptr;
+    cudaError_t e = cudaMalloc(&sink, 16);
+    if (e) return c->cuda_fail(e, "probe");
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const int blocks = c->nsm * 8, iters = 4096;
+    double gflop = 0.;
+    launch(sink, blocks, iters, &gflop, c->stream);  // warm-up
+    double best = 0.;
+    for (int r = 0; r < 5; r++) {
+        cudaEventRecord(a, c->stream);
+        launch(sink, blocks, iters, &gflop, c->stream);
+        cudaEventRecord(b, c->stream);
+        cudaEventSynchronize(b);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        const double t = gflop / (ms * 1e-3) * 1e-3;
+        if (t > best) best = t;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(sink);
+    e = cudaGetLastError();
+    if (e) return c->cuda_fail(e, "probe");
+    *tflops = best;
+    return LCG_OK;
+}
+
 extern "C" {
 
 void lcg_default_options(lcg_options *opt) {
@@ -1428,35 +1463,17 @@ int64_t lcg_kernel_launches(int32_t reset) {
 }
 
 lcg_status lcg_measure_fp32_peak(lcg_ctx *c, double *tflops) {
-    if (!c || !tflops) return LCG_E_INVALID;
-    cudaSetDevice(c->device);
-    float *sink = nullptr;
-    cudaError_t e = cudaMalloc(&sink, 16);
-    if (e) return c->cuda_fail(e, "probe");
-    cudaEvent_t a, b;
-    cudaEventCreate(&a);
-    cudaEventCreate(&b);
-    const int blocks = c->nsm * 8, iters = 4096;
-    double gflop = 0.;
-    launch_fma_probe(sink, blocks, iters, &gflop, c->stream);  // warm-up
-    double best = 0.;
-    for (int r = 0; r < 5; r++) {
-        cudaEventRecord(a, c->stream);
-        launch_fma_probe(sink, blocks, iters, &gflop, c->stream);
-        cudaEventRecord(b, c->stream);
-        cudaEventSynchronize(b);
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, a, b);
-        const double t = gflop / (ms * 1e-3) * 1e-3;
-        if (t > best) best = t;
-    }
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
-    cudaFree(sink);
-    e = cudaGetLastError();
-    if (e) return c->cuda_fail(e, "probe");
-    *tflops = best;
-    return LCG_OK;
+    return measure_peak(c, tflops, [](void *sink, int blocks, int iters, double *gflop,
+                                      cudaStream_t s) {
+        launch_fma_probe(static_cast<float *>(sink), blocks, iters, gflop, s);
+    });
+}
+
+lcg_status lcg_measure_fp64_peak(lcg_ctx *c, double *tflops) {
+    return measure_peak(c, tflops, [](void *sink, int blocks, int iters, double *gflop,
+                                      cudaStream_t s) {
+        launch_dfma_probe(static_cast<double *>(sink), blocks, iters, gflop, s);
+    });
 }
 
 }  // extern "C"

@@ -324,6 +324,7 @@ void launch_batch_flux(const BatchDev &b, const BatchPhases &ph, const FluxPlan 
                        double *part, int64_t ldp, cudaStream_t s);
 // FP32 FMA throughput probe: fills *gflop with the FLOPs it executed.
 void launch_fma_probe(float *sink, int blocks, int iters, double *gflop, cudaStream_t s);
+void launch_dfma_probe(double *sink, int blocks, int iters, double *gflop, cudaStream_t s);
 void launch_flux64(int star, const FluxConsts &k, const FlatDev &f, const PhaseDev &ph,
                    const FluxPlan &plan, double *part, int64_t ldp, DevStatus *st,
                    cudaStream_t s);

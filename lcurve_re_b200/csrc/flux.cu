@@ -165,7 +165,8 @@ __global__ void __launch_bounds__(kThreads)
     const float vfac = (float)k.vfac, spin = (float)k.spin, xcofm = (float)k.xcofm;
     const float beam = (float)k.beam;
 
-    if (!mbar_wait_bounded(&bar, 0)) {
+    // warp-uniform: a warp leaves together, so no lane is missing at the votes
+    if (!__all_sync(0xffffffffu, mbar_wait_bounded(&bar, 0))) {
         if (tid == 0) {
             if (atomicCAS(&st->code, 0, 6) == 0) st->face = (int32_t)c0;
         }
@@ -344,7 +345,8 @@ __global__ void __launch_bounds__(kThreads, 2)
         exy[j] = sqrtf(fmaf(v.x, v.x, v.y * v.y));
         pf[j] = __float_as_uint(v.w);
     }
-    if (!mbar_wait_bounded(&bar, 0)) {
+    // warp-uniform: a warp leaves together, so no lane is missing at the votes
+    if (!__all_sync(0xffffffffu, mbar_wait_bounded(&bar, 0))) {
         if (tid == 0) {
             if (atomicCAS(&st->code, 0, 6) == 0) st->face = (int32_t)c0;
         }
@@ -415,7 +417,8 @@ __global__ void __launch_bounds__(kThreads, 2)
         exy[j] = sqrtf(fmaf(v.x, v.x, v.y * v.y));
         pf[j] = __float_as_uint(v.w);
     }
-    if (!mbar_wait_bounded(&bar, 0)) {
+    // warp-uniform: a warp leaves together, so no lane is missing at the votes
+    if (!__all_sync(0xffffffffu, mbar_wait_bounded(&bar, 0))) {
         if (tid == 0) {
             if (atomicCAS(&b.st[model].code, 0, 6) == 0) b.st[model].face = (int32_t)c0;
         }

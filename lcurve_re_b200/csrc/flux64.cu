@@ -39,12 +39,24 @@ __device__ __forceinline__ double imu_bl(double mu, const Consts64 &L) {
     return (double)(mu > 0.0) * im;
 }
 
-// s1_elem / s2_elem (comp_light_flat.cpp:109-168)
+// mu = e . n, in the reference's order of operations
+__device__ __forceinline__ double mu_of(double ex, double ey, double ez, double dx, double dy,
+                                        double dz) {
+    return ex * dx + ey * dy + ez * dz;
+}
+
+// Elements at or below this mu are exactly zero: the factor (mu > mucrit)
+// and, without beaming, (mu > 0) inside imu_bl multiply a finite value.
+template <bool BEAM>
+__device__ __forceinline__ double zero_below(const Consts64 &L) {
+    return BEAM ? L.mucrit : (L.mucrit > 0.0 ? L.mucrit : 0.0);
+}
+
+// s1_elem / s2_elem (comp_light_flat.cpp:109-168), given mu
 template <int LT, bool BEAM, bool GLENS, int STAR>
-__device__ __forceinline__ double elem(double ex, double ey, double ez, double dx, double dy,
-                                       double dz, double px, double py, double pz, double flux,
-                                       const Consts64 &L) {
-    const double mu = ex * dx + ey * dy + ez * dz;
+__device__ __forceinline__ double elem_mu(double mu, double ex, double ey, double ez, double dx,
+                                          double dy, double px, double py, double pz,
+                                          double flux, const Consts64 &L) {
     double magn = 1.0;
     if constexpr (GLENS) {
         const double d = -(px * ex + py * ey + pz * ez);
@@ -72,6 +84,14 @@ __device__ __forceinline__ double elem(double ex, double ey, double ez, double d
     }
     if constexpr (GLENS) return mu > L.mucrit ? val : 0.0;
     return (double)(mu > L.mucrit) * val;
+}
+
+template <int LT, bool BEAM, bool GLENS, int STAR>
+__device__ __forceinline__ double elem(double ex, double ey, double ez, double dx, double dy,
+                                       double dz, double px, double py, double pz, double flux,
+                                       const Consts64 &L) {
+    return elem_mu<LT, BEAM, GLENS, STAR>(mu_of(ex, ey, ez, dx, dy, dz), ex, ey, ez, dx, dy, px,
+                                          py, pz, flux, L);
 }
 
 template <int PPT, int LT, bool BEAM, bool GLENS, int STAR>
@@ -126,34 +146,63 @@ __global__ void __launch_bounds__(kThreads64)
     }
     const Consts64 L{k.c[0], k.c[1], k.c[2], k.c[3], k.base, k.mucrit,
                      k.beam, k.spin, k.vfac, k.xcofm, k.rlens1};
-    if (!mbar_wait_bounded(&bar, 0)) {
+    // a warp leaves together whether its copies arrived or the wait gave up,
+    // so every lane reaches the votes below
+    const bool staged = __all_sync(0xffffffffu, mbar_wait_bounded(&bar, 0));
+    if (!staged) {
         if (tid == 0) {
             if (atomicCAS(&st->code, 0, 6) == 0) st->face = (int32_t)lo;
         }
         mbar_wait_bounded(&bar, 0);
         return;
     }
+    // Per face, one vote of the warp: when the face is at or below zero_below
+    // (exactly zero) or eclipsed at every entry of the warp, its elements
+    // would add exact zeros, and the warp moves on. The warp's entries are
+    // 32 consecutive sub-phases per j, so a face's visibility is shared by
+    // nearly all of them. Skipped or not, every sum is bit-identical.
+    const double zb = zero_below<BEAM>(L);
     for (int64_t i = lo; i < a1; i++) {
         const int t = (int)(i - lo);
-        const double dx = s_dx[t], dy = s_dy[t], dz = s_dz[t], fl = s_fl[t];
+        const double dx = s_dx[t], dy = s_dy[t], dz = s_dz[t];
+        double mu[PPT];
+        bool live = false;
+#pragma unroll
+        for (int j = 0; j < PPT; j++) {
+            mu[j] = mu_of(ex[j], ey[j], ez[j], dx, dy, dz);
+            live |= mu[j] > zb;
+        }
+        if (!__any_sync(0xffffffffu, live)) continue;
+        const double fl = s_fl[t];
         double px = 0., py = 0., pz = 0.;
         if constexpr (need_pos) { px = s_px[t]; py = s_py[t]; pz = s_pz[t]; }
 #pragma unroll
         for (int j = 0; j < PPT; j++)
-            br[j] += elem<LT, BEAM, GLENS, STAR>(ex[j], ey[j], ez[j], dx, dy, dz, px, py, pz, fl, L);
+            br[j] += elem_mu<LT, BEAM, GLENS, STAR>(mu[j], ex[j], ey[j], ez[j], dx, dy, px, py,
+                                                    pz, fl, L);
     }
     for (int64_t i = b0; i < hi; i++) {
         const int t = (int)(i - lo);
-        const double dx = s_dx[t], dy = s_dy[t], dz = s_dz[t], fl = s_fl[t];
+        const double dx = s_dx[t], dy = s_dy[t], dz = s_dz[t];
         const double ein = s_in[t], eout = s_out[t];
+        double mu[PPT];
+        bool ecl[PPT];
+        bool live = false;
+#pragma unroll
+        for (int j = 0; j < PPT; j++) {
+            mu[j] = mu_of(ex[j], ey[j], ez[j], dx, dy, dz);
+            ecl[j] = (pn[j] >= ein && pn[j] <= eout) || pn[j] <= eout - 1.0;
+            live |= (mu[j] > zb) && !ecl[j];
+        }
+        if (!__any_sync(0xffffffffu, live)) continue;
+        const double fl = s_fl[t];
         double px = 0., py = 0., pz = 0.;
         if constexpr (need_pos) { px = s_px[t]; py = s_py[t]; pz = s_pz[t]; }
 #pragma unroll
         for (int j = 0; j < PPT; j++) {
-            const double v =
-                elem<LT, BEAM, GLENS, STAR>(ex[j], ey[j], ez[j], dx, dy, dz, px, py, pz, fl, L);
-            const bool ecl = (pn[j] >= ein && pn[j] <= eout) || pn[j] <= eout - 1.0;
-            br[j] += ecl ? 0.0 : v;
+            const double v = elem_mu<LT, BEAM, GLENS, STAR>(mu[j], ex[j], ey[j], ez[j], dx, dy,
+                                                            px, py, pz, fl, L);
+            br[j] += ecl[j] ? 0.0 : v;
         }
     }
 #pragma unroll
@@ -258,7 +307,28 @@ void launch_ppt(int star, const FluxConsts &k, const FlatDev &f, const PhaseDev 
     else launch_lt<PPT, 0>(star, k, f, ph, plan, part, ldp, st, s);
 }
 
+// 8 independent DFMA chains per thread keep the FP64 pipe full.
+__global__ void __launch_bounds__(256) k_dfma_probe(double *sink, int iters) {
+    double a0 = threadIdx.x * 1e-3, a1 = a0 + 1., a2 = a0 + 2., a3 = a0 + 3.;
+    double a4 = a0 + 4., a5 = a0 + 5., a6 = a0 + 6., a7 = a0 + 7.;
+    const double m = 0.999999, c = 1e-6;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+            a0 = fma(a0, m, c); a1 = fma(a1, m, c); a2 = fma(a2, m, c); a3 = fma(a3, m, c);
+            a4 = fma(a4, m, c); a5 = fma(a5, m, c); a6 = fma(a6, m, c); a7 = fma(a7, m, c);
+        }
+    }
+    const double r = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+    if (r == 12345.) sink[0] = r;  // keeps the chains live
+}
+
 }  // namespace
+
+void launch_dfma_probe(double *sink, int blocks, int iters, double *gflop, cudaStream_t s) {
+    k_dfma_probe<<<blocks, 256, 0, s>>>(sink, iters);
+    *gflop = 2.0 * 8 * 16 * (double)iters * 256.0 * blocks * 1e-9;
+}
 
 void launch_flux_ragged(int star, const FluxConsts &k, const FlatDev &f, const GridDev &g,
                         const PhaseDev &ph, int64_t blk, int64_t nblk, double *part,

@@ -281,3 +281,8 @@ class Engine:
         t = C.c_double()
         self._check(self.lib.lcg_measure_fp32_peak(self.ctx, C.byref(t)))
         return t.value
+
+    def fp64_peak_tflops(self):
+        t = C.c_double()
+        self._check(self.lib.lcg_measure_fp64_peak(self.ctx, C.byref(t)))
+        return t.value
