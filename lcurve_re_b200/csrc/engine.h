@@ -313,6 +313,10 @@ struct FluxPlan {
     int64_t chunk;  // faces per CTA
     int64_t nchunk;
     int64_t ntile;  // phase tiles
+    int64_t group = 1;  // consecutive chunks summed into one partial row (a cluster)
+    // partial rows the sweep writes, and the faces each row covers
+    int64_t rows() const { return group > 1 ? (nchunk + group - 1) / group : nchunk; }
+    int64_t row_faces() const { return chunk * group; }
 };
 FluxPlan plan_flux(int mixed, int fast, int64_t nface, int64_t nent, int nsm);
 void launch_flux(int mixed, int star, const FluxConsts &k, const FlatDev &f,

@@ -17,8 +17,12 @@
 //    merged in chunk order by k_scatter (deterministic, no atomics).
 //  * eclipse test in 32-bit fixed-point phase: (phase - ingress) mod 2^32 <
 //    width + 1, exact except within 2^-32 of a boundary.
+#include <cooperative_groups.h>
+
 #include "engine.h"
 #include "tma.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace lcg {
 
@@ -311,8 +315,17 @@ __device__ __forceinline__ void sweep_pairs(const float4 *sp, const uint4 *se, i
     }
 }
 
-template <int PPT, int LT>
-__global__ void __launch_bounds__(kThreads, 2)
+// 3 CTAs per SM for PPT <= 4 (80 registers, no spills): 24 warps hide the
+// FFMA2 and MUFU latencies better than 16; larger PPT keeps 2
+//
+// CLUSTER: the CTAs of a thread-block cluster (1 x G along the chunks) hold G
+// consecutive chunks of one phase tile; rank 0 adds their FP64 partials in
+// chunk order through distributed shared memory and writes one partial row
+// per group, so the partials that reach HBM (and the chunk reduction's
+// reads) shrink G-fold. Chunks past the grid (the grid's chunk count is
+// padded to a multiple of G) add zero.
+template <int PPT, int LT, bool CLUSTER>
+__global__ void __launch_bounds__(kThreads, (PPT <= 4) ? 3 : 2)
     k_flux_fast(FlatDev f, PhaseDev ph, int64_t chunk, int64_t ntile, double *part, int64_t ldp,
                 DevStatus *st) {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -320,13 +333,14 @@ __global__ void __launch_bounds__(kThreads, 2)
     const int tid = threadIdx.x;
     const int64_t c0 = (int64_t)blockIdx.y * chunk;
     const int64_t n = f.n, n0 = *f.n0;
+    const bool live = c0 < n;  // false only for the padding chunks of a cluster grid
     const int64_t cend = (c0 + chunk < n) ? c0 + chunk : n;
     const bool need_ecl = cend > n0;
     float4 *sp = reinterpret_cast<float4 *>(smem);
     uint4 *se = reinterpret_cast<uint4 *>(smem + chunk * 32);
     if (tid == 0) mbar_init(&bar, 1);
     __syncthreads();
-    if (tid == 0) {
+    if (tid == 0 && live) {
         const uint32_t bytes = (uint32_t)(chunk * 32) + (need_ecl ? (uint32_t)(chunk * 8) : 0u);
         mbar_arrive_expect_tx(&bar, bytes);
         bulk_g2s(sp, f.fp + 8 * c0, (uint32_t)(chunk * 32), &bar);
@@ -346,30 +360,58 @@ __global__ void __launch_bounds__(kThreads, 2)
         pf[j] = __float_as_uint(v.w);
     }
     // warp-uniform: a warp leaves together, so no lane is missing at the votes
-    if (!__all_sync(0xffffffffu, mbar_wait_bounded(&bar, 0))) {
-        if (tid == 0) {
-            if (atomicCAS(&st->code, 0, 6) == 0) st->face = (int32_t)c0;
-        }
-        mbar_wait_bounded(&bar, 0);
-        return;
+    const bool staged = !live || __all_sync(0xffffffffu, mbar_wait_bounded(&bar, 0));
+    if (!staged && tid == 0) {
+        if (atomicCAS(&st->code, 0, 6) == 0) st->face = (int32_t)c0;
     }
     // two-level FP32 sums: runs of <= 64 faces, then the runs of the chunk;
     // the chunk partial goes out in FP64 and chunks are added in FP64
     float acc[PPT];
 #pragma unroll
     for (int j = 0; j < PPT; j++) acc[j] = 0.f;
-    // pairs: the pair holding face n0 and those after it take the eclipse
-    // test (a never-eclipsed face in that pair has an empty range); faces past
-    // n in the last pair carry zero coefficients
-    const int64_t q0 = c0 >> 1, qend = (cend + 1) >> 1, qn0 = n0 >> 1;
-    const int64_t qa = qn0 < qend ? qn0 : qend;
-    sweep_pairs<PPT, LT, false>(sp, se, q0, q0, qa > q0 ? qa : q0, ex, ey, exy, pf, f.runb, acc);
-    sweep_pairs<PPT, LT, true>(sp, se, q0, qa > q0 ? qa : q0, qend, ex, ey, exy, pf, f.runb, acc);
-#pragma unroll
-    for (int j = 0; j < PPT; j++) {
-        const int64_t e = (int64_t)blockIdx.x * (kThreads * PPT) + tid * PPT + j;
-        if (e < ph.nent) part[(int64_t)blockIdx.y * ldp + e] = (double)acc[j];
+    if (live && staged) {
+        // pairs: the pair holding face n0 and those after it take the eclipse
+        // test (a never-eclipsed face in that pair has an empty range); faces
+        // past n in the last pair carry zero coefficients
+        const int64_t q0 = c0 >> 1, qend = (cend + 1) >> 1, qn0 = n0 >> 1;
+        const int64_t qa = qn0 < qend ? qn0 : qend;
+        sweep_pairs<PPT, LT, false>(sp, se, q0, q0, qa > q0 ? qa : q0, ex, ey, exy, pf, f.runb,
+                                    acc);
+        sweep_pairs<PPT, LT, true>(sp, se, q0, qa > q0 ? qa : q0, qend, ex, ey, exy, pf, f.runb,
+                                   acc);
     }
+    if constexpr (!CLUSTER) {
+#pragma unroll
+        for (int j = 0; j < PPT; j++) {
+            const int64_t e = (int64_t)blockIdx.x * (kThreads * PPT) + tid * PPT + j;
+            if (e < ph.nent) part[(int64_t)blockIdx.y * ldp + e] = (double)acc[j];
+        }
+    } else {
+        __shared__ double red[PPT * kThreads];
+        cg::cluster_group cluster = cg::this_cluster();
+#pragma unroll
+        for (int j = 0; j < PPT; j++) red[j * kThreads + tid] = (double)acc[j];
+        cluster.sync();
+        if (cluster.block_rank() == 0) {
+            const unsigned G = cluster.num_blocks();
+            double o[PPT];
+#pragma unroll
+            for (int j = 0; j < PPT; j++) o[j] = 0.0;
+            for (unsigned r = 0; r < G; r++) {
+                const double *rr = cluster.map_shared_rank(red, r);
+#pragma unroll
+                for (int j = 0; j < PPT; j++) o[j] += rr[j * kThreads + tid];
+            }
+            const int64_t row = (int64_t)blockIdx.y / G;
+#pragma unroll
+            for (int j = 0; j < PPT; j++) {
+                const int64_t e = (int64_t)blockIdx.x * (kThreads * PPT) + tid * PPT + j;
+                if (e < ph.nent) part[row * ldp + e] = o[j];
+            }
+        }
+        cluster.sync();  // every rank's shared memory stays until rank 0 has read it
+    }
+    if (live && !staged) mbar_wait_bounded(&bar, 0);  // let the copy land before the CTA exits
 }
 
 // The batched fast sweep: CTA w takes phase tile w % ntile of batch chunk
@@ -377,7 +419,7 @@ __global__ void __launch_bounds__(kThreads, 2)
 // its limb-darkening law. Same per-element arithmetic and sums as
 // k_flux_fast.
 template <int PPT>
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, (PPT <= 4) ? 3 : 2)
     k_flux_batch(BatchDev b, BatchPhases ph, int64_t chunk, int64_t ntile, double *part,
                  int64_t ldp) {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -461,11 +503,32 @@ template <int PPT, int LT>
 void launch_fast_t(const FlatDev &f, const PhaseDev &ph, const FluxPlan &plan, double *part,
                    int64_t ldp, DevStatus *st, cudaStream_t s) {
     const size_t smem = (size_t)plan.chunk * 40;  // 32 B records + 8 B eclipse ranges
-    auto kern = k_flux_fast<PPT, LT>;
+    if (plan.group <= 1) {
+        auto kern = k_flux_fast<PPT, LT, false>;
+        if (smem > 48 * 1024)
+            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        dim3 grid((unsigned)plan.ntile, (unsigned)plan.nchunk);
+        kern<<<grid, kThreads, smem, s>>>(f, ph, plan.chunk, plan.ntile, part, ldp, st);
+        count_launch();
+        return;
+    }
+    auto kern = k_flux_fast<PPT, LT, true>;
     if (smem > 48 * 1024)
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    dim3 grid((unsigned)plan.ntile, (unsigned)plan.nchunk);
-    kern<<<grid, kThreads, smem, s>>>(f, ph, plan.chunk, plan.ntile, part, ldp, st);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)plan.ntile, (unsigned)(plan.rows() * plan.group));
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 1;
+    attr[0].val.clusterDim.y = (unsigned)plan.group;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int64_t chunk = plan.chunk, ntile = plan.ntile;
+    cudaLaunchKernelEx(&cfg, kern, f, ph, chunk, ntile, part, ldp, st);
     count_launch();
 }
 
@@ -552,6 +615,8 @@ FluxPlan plan_flux(int mixed, int fast, int64_t nface, int64_t nent, int nsm) {
         p.chunk = 1024;  // FACE_BLOCK of comp_light_flat.cpp:239
     }
     p.nchunk = nface > 0 ? (nface + p.chunk - 1) / p.chunk : 0;
+    // the fast sweep adds up to 8 consecutive chunks in a thread-block cluster
+    if (p.fast) p.group = p.nchunk >= 32 ? 8 : p.nchunk >= 8 ? 4 : p.nchunk >= 4 ? 2 : 1;
     return p;
 }
 
