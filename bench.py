@@ -776,6 +776,7 @@ def run_surrogate(args):
     pools = [(theta, S.log_uniform_box()),
              (th_loc, S.log_gaussian_in_box(mu_b, cov_b, args.local_widen))]
     _, mu_1, cov_1, ess_1 = S.posterior_resample(pools, chi_pool, 1, seed=17 + rank)
+    cov_1 = cov_1 + np.diag(np.diag(cov_b) * 1e-6)  # keeps it positive definite
     th_2 = S.local_draws(mu_1, cov_1, args.local_curves, seed=19 + rank, widen=1.5)
     _, cu_2 = S.training_set(eng, 0, theta=th_2, batch=2048)
     chi_pool = np.r_[chi_pool, S.curves_chi2(cu_2, data, idx)]
