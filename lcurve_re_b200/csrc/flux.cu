@@ -512,9 +512,11 @@ void launch_fast_t(const FlatDev &f, const PhaseDev &ph, const FluxPlan &plan, d
         count_launch();
         return;
     }
+    // the reduction's static shared memory (PPT x 256 doubles) comes on top of
+    // the staging buffer: opt in whatever the dynamic size, as the sum can pass
+    // the 48 KB default
     auto kern = k_flux_fast<PPT, LT, true>;
-    if (smem > 48 * 1024)
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)plan.ntile, (unsigned)(plan.rows() * plan.group));
     cfg.blockDim = dim3(kThreads);
