@@ -35,7 +35,7 @@ SOURCES = {
     "components.cu": ["--fmad=false"],
 }
 HEADERS = ["roche.cuh", "eclipse.cuh", "disc.cuh", "ecl_screen.cuh", "engine.h", "tma.cuh",
-           "context.h"]
+           "context.h", "fixed_phase.cuh"]
 
 
 def nvcc():

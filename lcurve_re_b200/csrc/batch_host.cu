@@ -98,11 +98,12 @@ struct BatchState {
     DBuf<double> px, py, pz, nx, ny, nz, ein, eout;
     DBuf<float> area, grav, flux, fp;
     DBuf<uint8_t> necl;
-    DBuf<uint2> ecl;
+    DBuf<ulonglong2> ecl;
     DBuf<int64_t> n0;
     DBuf<int32_t> blockcnt, queue, counters;
     DBuf<DevStatus> st;
     DBuf<float4> ef, runb;
+    DBuf<unsigned long long> pfx;
     DBuf<double4> es;
     DBuf<uint8_t> ehit;
     DBuf<double> w1, w2, part, osum, calc, sfac, out;
@@ -133,7 +134,7 @@ struct BatchState {
         for (auto *b : d) b->release();
         area.release(); grav.release(); flux.release(); fp.release(); necl.release();
         ecl.release(); n0.release(); blockcnt.release(); queue.release(); counters.release();
-        st.release(); ef.release(); runb.release(); rings.release(); es.release(); ehit.release(); d_tab.release();
+        st.release(); ef.release(); pfx.release(); runb.release(); rings.release(); es.release(); ehit.release(); d_tab.release();
         rows.release(); gathered.release(); tune_pre.release();
         if (h_rows) cudaFreeHost(h_rows);
         h_rows = nullptr;
@@ -175,7 +176,7 @@ struct BatchState {
         b.cont_blk = reinterpret_cast<const int64_t *>(d + o_cont_blk);
         return b;
     }
-    BatchPhases phases() { return BatchPhases{ef.p, w1.p, w2.p, ldp, nent}; }
+    BatchPhases phases() { return BatchPhases{ef.p, w1.p, w2.p, ldp, nent, pfx.p}; }
 };
 
 void batch_release(BatchState *b) {
@@ -319,7 +320,7 @@ lcg_status relayout(lcg_ctx *c, BatchState &B, const lcg_model *models, int32_t 
         (e = B.n0.ensure(ns)) || (e = B.blockcnt.ensure((size_t)B.nblk)) ||
         (e = B.counters.ensure(8)) || (e = B.st.ensure(nm)) ||
         (e = B.es.ensure(nf)) || (e = B.ehit.ensure(nf)) ||
-        (e = B.ef.ensure(nm * (size_t)B.ldp)) || (e = B.w1.ensure(nm * (size_t)B.ldp)) ||
+        (e = B.ef.ensure(nm * (size_t)B.ldp)) || (e = B.pfx.ensure(nm * (size_t)B.ldp)) || (e = B.w1.ensure(nm * (size_t)B.ldp)) ||
         (e = B.w2.ensure(nm * (size_t)B.ldp)) ||
         (e = B.part.ensure((size_t)std::max<int64_t>(B.plan.nchunk, 1) * (size_t)B.ldp)) ||
         (e = B.osum.ensure(ns * (size_t)B.ldp)) || (e = B.calc.ensure(nm * (size_t)B.n)) ||
@@ -333,7 +334,7 @@ lcg_status relayout(lcg_ctx *c, BatchState &B, const lcg_model *models, int32_t 
     }
     // an odd pad record or a never-built slot must read as zeros
     cudaMemsetAsync(B.fp.p, 0, 8 * (size_t)B.nflat * sizeof(float), c->stream);
-    cudaMemsetAsync(B.ecl.p, 0, (size_t)B.nflat * sizeof(uint2), c->stream);
+    cudaMemsetAsync(B.ecl.p, 0, (size_t)B.nflat * sizeof(ulonglong2), c->stream);
     cudaMemsetAsync(B.runb.p, 0, (size_t)B.nflat / 64 * sizeof(float4), c->stream);
     cudaMemsetAsync(B.n0.p, 0, ns * sizeof(int64_t), c->stream);
     B.key.assign(nm, lcg_model{});

@@ -63,7 +63,7 @@ struct Grid {
     // flat
     DBuf<int64_t> n0;
     DBuf<float4> geo, pos;
-    DBuf<uint2> ecl;
+    DBuf<ulonglong2> ecl;
     DBuf<double> fdx, fdy, fdz, fpx, fpy, fpz, fflux, fin, fout;
     DBuf<float> fp;
     DBuf<float4> runb;
@@ -171,6 +171,7 @@ struct lcg_ctx {
     DBuf<double> pex, pey, pez, pphin, pw1, pw2, part1f, part1c, part2f, part2c, calc, scratch,
         sfac, out, diag, osum;
     DBuf<float4> pef;
+    DBuf<unsigned long long> ppfx;
     DBuf<uint8_t> ptype;
     // disc, rim and bright spot of the last model; iscale components
     DBuf<lcg::ElemRec> elem;

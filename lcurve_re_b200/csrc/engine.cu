@@ -512,13 +512,14 @@ lcg_status sweep_one(lcg_ctx *c, const lcg_model &m, Grid &g, int star, double p
     double v[4] = {e.x, e.y, e.z, phase - floor(phase)};
     cudaError_t err;
     if ((err = c->pex.ensure(1)) || (err = c->pey.ensure(1)) || (err = c->pez.ensure(1)) ||
-        (err = c->pphin.ensure(1)) || (err = c->pef.ensure(1)))
+        (err = c->pphin.ensure(1)) || (err = c->pef.ensure(1)) || (err = c->ppfx.ensure(1)))
         return c->cuda_fail(err, "phases");
     cudaMemcpyAsync(c->pex.p, &v[0], 8, cudaMemcpyHostToDevice, c->stream);
     cudaMemcpyAsync(c->pey.p, &v[1], 8, cudaMemcpyHostToDevice, c->stream);
     cudaMemcpyAsync(c->pez.p, &v[2], 8, cudaMemcpyHostToDevice, c->stream);
     cudaMemcpyAsync(c->pphin.p, &v[3], 8, cudaMemcpyHostToDevice, c->stream);
-    PhaseDev ph{c->pex.p, c->pey.p, c->pez.p, c->pphin.p, nullptr, nullptr, c->pef.p, nullptr, 1};
+    PhaseDev ph{c->pex.p, c->pey.p, c->pez.p, c->pphin.p, nullptr, nullptr, c->pef.p, nullptr, 1,
+                c->ppfx.p};
     const int mixed = c->precision == LCG_PREC_MIXED;
     if (mixed) launch_pack_phases(ph, c->stream);
     FluxPlan plan = plan_flux(mixed, g.fast, g.n, 1, c->nsm);
@@ -740,7 +741,7 @@ void lcg_destroy(lcg_ctx *c) {
     for (auto *b : d) b->release();
     c->status.release(); c->queue.release(); c->counters.release(); c->blockcnt.release();
     c->blockcnt2.release();
-    c->data.release(); c->off.release(); c->pef.release(); c->ptype.release();
+    c->data.release(); c->off.release(); c->pef.release(); c->ppfx.release(); c->ptype.release();
     c->fdata.release(); c->fidx.release(); c->fcalc.release(); c->fout.release();
     c->elem.release(); c->epos.release(); c->drings.release(); c->csum.release();
     c->fcomp.release(); c->iwork.release();
@@ -1046,11 +1047,11 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
     const int64_t ldp = ((nall + 3) / 4) * 4;
     if ((e = c->pex.ensure(nall)) || (e = c->pey.ensure(nall)) || (e = c->pez.ensure(nall)) ||
         (e = c->pphin.ensure(nall)) || (e = c->pw1.ensure(nall)) || (e = c->pw2.ensure(nall)) ||
-        (e = c->pef.ensure(nall)) || (e = c->ptype.ensure(nall)) || (e = c->calc.ensure(n)) ||
+        (e = c->pef.ensure(nall)) || (e = c->ppfx.ensure(nall)) || (e = c->ptype.ensure(nall)) || (e = c->calc.ensure(n)) ||
         (e = c->scratch.ensure(3 * (size_t)n)))
         return c->cuda_fail(e, "phase buffers");
     PhaseDev ph{c->pex.p, c->pey.p, c->pez.p, c->pphin.p, c->pw1.p, c->pw2.p,
-                c->pef.p, c->ptype.p, nall};
+                c->pef.p, c->ptype.p, nall, c->ppfx.p};
     const double ri = deg2rad(m.iangle);
     const double cosi = cos(ri), sini = sin(ri);
     PhaseParams pp{};
@@ -1073,6 +1074,7 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
             cudaMemcpyAsync(c->pphin.p + nent, &v[3], 8, cudaMemcpyHostToDevice, c->stream);
             PhaseDev one = ph;
             one.ex += nent; one.ey += nent; one.ez += nent; one.phin += nent; one.ef += nent;
+            one.pfx += nent;
             one.nent = 1;
             launch_pack_phases(one, c->stream);
         }
@@ -1412,7 +1414,7 @@ lcg_status lcg_sum_star_multi(lcg_ctx *c, int32_t star, int64_t n, int64_t n0, c
     cudaMemcpyAsync(g.n0.p, &n0, sizeof(int64_t), cudaMemcpyHostToDevice, c->stream);
     if (mixed) launch_pack_flat(g.flat(), n0, need_pos, c->stream);
     if ((e = c->pex.ensure(nent)) || (e = c->pey.ensure(nent)) || (e = c->pez.ensure(nent)) ||
-        (e = c->pphin.ensure(nent)) || (e = c->pef.ensure(nent)))
+        (e = c->pphin.ensure(nent)) || (e = c->pef.ensure(nent)) || (e = c->ppfx.ensure(nent)))
         return c->cuda_fail(e, "phases");
     if (nent) {
         cudaMemcpyAsync(c->pex.p, ex, (size_t)nent * 8, cudaMemcpyHostToDevice, c->stream);
@@ -1420,7 +1422,8 @@ lcg_status lcg_sum_star_multi(lcg_ctx *c, int32_t star, int64_t n, int64_t n0, c
         cudaMemcpyAsync(c->pez.p, ez, (size_t)nent * 8, cudaMemcpyHostToDevice, c->stream);
         cudaMemcpyAsync(c->pphin.p, phin, (size_t)nent * 8, cudaMemcpyHostToDevice, c->stream);
     }
-    PhaseDev ph{c->pex.p, c->pey.p, c->pez.p, c->pphin.p, nullptr, nullptr, c->pef.p, nullptr, nent};
+    PhaseDev ph{c->pex.p, c->pey.p, c->pez.p, c->pphin.p, nullptr, nullptr, c->pef.p, nullptr, nent,
+                c->ppfx.p};
     if (mixed) launch_pack_phases(ph, c->stream);
     FluxConsts k{};
     for (int i = 0; i < 4; i++) k.c[i] = ldc[i];

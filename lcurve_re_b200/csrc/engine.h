@@ -93,13 +93,14 @@ struct DevStatus {
 // Flattened grid for the flux sweep (FlatGrid, comp_light_flat.cpp:26-65).
 // Faces [0,n0) are never eclipsed, [n0,n) have one eclipse range. The
 // mixed-precision view packs (nx,ny,nz,flux) as float4 and the eclipse range
-// as 32-bit fixed-point phase (start, width+1); the FP64 view keeps the
-// reference's doubles. Arrays are padded with zero faces to npad.
+// as 64-bit fixed-point phase (ingress, width; ecl_fx64 in geometry.cu); the
+// FP64 view keeps the reference's doubles. Arrays are padded with zero faces
+// to npad.
 struct FlatDev {
     int64_t n, npad;
     int64_t *n0;  // device scalar, written by the partition
     float4 *geo;  // mixed, general: (nx, ny, nz, flux)
-    uint2 *ecl;
+    ulonglong2 *ecl;  // mixed: (ingress, width) as 64-bit fixed-point phase
     float4 *pos;  // (px,py,pz,0): beaming and lensing only
     double *dx, *dy, *dz, *px, *py, *pz, *flux, *in1, *out1;  // FP64
     // mixed, fast: per PAIR of faces (a, b) four float4
@@ -135,9 +136,10 @@ struct FastCoef {
 // Sub-exposure phase entries of all data points (light_curve_comp.cpp:416-455).
 struct PhaseDev {
     double *ex, *ey, *ez, *phin, *w1, *w2;
-    float4 *ef;     // (ex, ey, ez, phin as 32-bit fixed point bits)
+    float4 *ef;     // (ex, ey, ez, unused) for the mixed sweeps
     uint8_t *type;  // Ginterp::type
     int64_t nent;
+    unsigned long long *pfx;  // phin as a 64-bit fixed-point fraction (mixed)
 };
 
 struct PhaseParams {
@@ -212,7 +214,7 @@ struct BatchDev {
     GridDev g;  // every face of the batch
     float *fp;  // fast sweep records (FlatDev::fp layout per slot)
     float4 *runb;  // FlatDev::runb per slot, from flat0 / 64
-    uint2 *ecl;
+    ulonglong2 *ecl;
     int64_t *n0;  // per slot
     // eclipse candidates: those whose bisections the FP32 screen serves go to
     // the front of queue, the others (FP64 alone) to the back, so that warps
@@ -251,6 +253,7 @@ struct BatchPhases {
     float4 *ef;
     double *w1, *w2;
     int64_t ldp, nent;
+    unsigned long long *pfx;  // PhaseDev::pfx, ldp per model
 };
 
 // ---- launchers (geometry.cu) ------------------------------------------------

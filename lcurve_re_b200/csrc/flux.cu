@@ -8,15 +8,16 @@
 //
 // Layout and schedule:
 //  * grid (phase tiles, face chunks). A CTA stages its face chunk
-//    (float4 n/flux records, uint2 fixed-point eclipse ranges) into shared
+//    (float4 n/flux records, 64-bit fixed-point eclipse ranges) into shared
 //    memory with one bulk TMA copy per array, completed on an mbarrier.
 //  * each thread keeps PPT phase entries in registers and walks the staged
 //    faces; all lanes read the same face record (shared-memory broadcast).
 //  * element math in FP32; sums over at most 64 faces in FP32, folded into
 //    FP64 accumulators; one FP64 partial per (chunk, entry) is written and
 //    merged in chunk order by k_scatter (deterministic, no atomics).
-//  * eclipse test in 32-bit fixed-point phase: (phase - ingress) mod 2^32 <
-//    width + 1, exact except within 2^-32 of a boundary.
+//  * eclipse test in 64-bit fixed-point phase: visible iff (phase - ingress)
+//    mod 2^64 >= width + 1 (ecl_fx64, geometry.cu), the reference's double
+//    comparisons decision for decision.
 #include <cooperative_groups.h>
 
 #include "engine.h"
@@ -70,15 +71,16 @@ struct FaceConsts {
 // Sums faces [lo, hi) of the staged chunk (first face c0) into acc, in FP32
 // runs of kFold faces folded into FP64.
 template <int PPT, int LT, bool BEAM, bool GLENS, int STAR, bool ECL>
-__device__ __forceinline__ void sweep(const float4 *sgeo, const uint2 *secl, const float4 *spos,
-                                      int64_t c0, int64_t lo, int64_t hi, const float *ex,
-                                      const float *ey, const float *ez, const uint32_t *pf,
+__device__ __forceinline__ void sweep(const float4 *sgeo, const ulonglong2 *secl,
+                                      const float4 *spos, int64_t c0, int64_t lo, int64_t hi,
+                                      const float *ex, const float *ey, const float *ez,
+                                      const unsigned long long *pf,
                                       const FaceConsts &k, double *acc) {
     constexpr bool need_pos = BEAM || GLENS;
     for (int64_t b = lo; b < hi; b += kFold) {
         const int cnt = (int)((b + kFold < hi) ? kFold : hi - b);
         const float4 *gp = sgeo + (b - c0);
-        const uint2 *ep = secl + (b - c0);
+        const ulonglong2 *ep = secl + (b - c0);
         const float4 *pp4 = spos + (b - c0);
         float s[PPT];
 #pragma unroll
@@ -86,7 +88,7 @@ __device__ __forceinline__ void sweep(const float4 *sgeo, const uint2 *secl, con
 #pragma unroll 4
         for (int i = 0; i < cnt; i++) {
             const float4 g = gp[i];
-            uint2 ec = make_uint2(0u, 0u);
+            ulonglong2 ec = make_ulonglong2(0ull, 0ull);
             if constexpr (ECL) ec = ep[i];
             float4 pp = make_float4(0.f, 0.f, 0.f, 0.f);
             float vx = 0.f, vy = 0.f, vn = 0.f;
@@ -135,33 +137,37 @@ __global__ void __launch_bounds__(kThreads)
     const bool need_ecl = cend > n0;
     constexpr bool need_pos = BEAM || GLENS;
     float4 *sgeo = reinterpret_cast<float4 *>(smem);
-    uint2 *secl = reinterpret_cast<uint2 *>(smem + chunk * 16);
-    float4 *spos = reinterpret_cast<float4 *>(smem + chunk * 24);
+    ulonglong2 *secl = reinterpret_cast<ulonglong2 *>(smem + chunk * 16);
+    float4 *spos = reinterpret_cast<float4 *>(smem + chunk * 32);
 
     if (tid == 0) mbar_init(&bar, 1);
     __syncthreads();
     if (tid == 0) {
-        uint32_t bytes = (uint32_t)(chunk * 16) + (need_ecl ? (uint32_t)(chunk * 8) : 0u) +
+        uint32_t bytes = (uint32_t)(chunk * 16) + (need_ecl ? (uint32_t)(chunk * 16) : 0u) +
                          (need_pos ? (uint32_t)(chunk * 16) : 0u);
         mbar_arrive_expect_tx(&bar, bytes);
         bulk_g2s(sgeo, f.geo + c0, (uint32_t)(chunk * 16), &bar);
-        if (need_ecl) bulk_g2s(secl, f.ecl + c0, (uint32_t)(chunk * 8), &bar);
+        if (need_ecl) bulk_g2s(secl, f.ecl + c0, (uint32_t)(chunk * 16), &bar);
         if (need_pos) bulk_g2s(spos, f.pos + c0, (uint32_t)(chunk * 16), &bar);
     }
 
     // phase entries of this thread, loaded while the faces stream in
     float ex[PPT], ey[PPT], ez[PPT];
-    uint32_t pf[PPT];
+    unsigned long long pf[PPT];
     const int64_t ebase = (int64_t)blockIdx.x * kThreads * PPT + tid;
 #pragma unroll
     for (int j = 0; j < PPT; j++) {
         const int64_t e = ebase + (int64_t)j * kThreads;
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (e < ph.nent) v = ph.ef[e];
+        unsigned long long p = 0ull;
+        if (e < ph.nent) {
+            v = ph.ef[e];
+            p = ph.pfx[e];
+        }
         ex[j] = v.x;
         ey[j] = v.y;
         ez[j] = v.z;
-        pf[j] = __float_as_uint(v.w);
+        pf[j] = p;
     }
     const float c1 = (float)k.c[0], c2 = (float)k.c[1], c3 = (float)k.c[2], c4 = (float)k.c[3];
     const float base = (float)k.base;
@@ -198,7 +204,7 @@ __global__ void __launch_bounds__(kThreads)
 template <int PPT, int LT, bool BEAM, bool GLENS, int STAR>
 void launch_t(const FluxConsts &k, const FlatDev &f, const PhaseDev &ph, const FluxPlan &plan,
               double *part, int64_t ldp, DevStatus *st, cudaStream_t s) {
-    const size_t smem = (size_t)plan.chunk * ((BEAM || GLENS) ? 40 : 24);
+    const size_t smem = (size_t)plan.chunk * ((BEAM || GLENS) ? 48 : 32);
     auto kern = k_flux_mixed<PPT, LT, BEAM, GLENS, STAR>;
     if (smem > 48 * 1024)
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -241,7 +247,8 @@ void launch_ppt(int star, const FluxConsts &k, const FlatDev &f, const PhaseDev 
 //   t   = sqrt(m) (Claret) or m (polynomial)           2 MUFU / 0
 //   fI  = flux * I(t), Horner on per-face coefficients 4 FFMA2
 //   s  += m * fI                                       1 FFMA2
-// one-range faces add the fixed-point eclipse test (IADD, ISETP, FSEL per face).
+// one-range faces add the fixed-point eclipse test (a 64-bit subtract and
+// compare, and a select, per face).
 // Each thread holds PPT consecutive phase entries, so a warp covers 32 * PPT
 // consecutive entries: a narrow arc of the orbit for time-ordered points.
 // A face pair that faces away (mu <= 0) or is eclipsed at every entry of the
@@ -251,10 +258,11 @@ void launch_ppt(int star, const FluxConsts &k, const FlatDev &f, const PhaseDev 
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 
 template <int PPT, int LT, bool ECL>
-__device__ __forceinline__ void sweep_pairs(const float4 *sp, const uint4 *se, int64_t q0,
+__device__ __forceinline__ void sweep_pairs(const float4 *sp, const ulonglong2 *se, int64_t q0,
                                             int64_t lo, int64_t hi, const float2 *ex,
                                             const float2 *ey, const float *exy,
-                                            const uint32_t *pf, const float4 *__restrict__ runb,
+                                            const unsigned long long *pf,
+                                            const float4 *__restrict__ runb,
                                             float *acc) {
     constexpr int kFoldPairs = kFold / 2;
     for (int64_t b = lo; b < hi; b += kFoldPairs) {
@@ -273,7 +281,7 @@ __device__ __forceinline__ void sweep_pairs(const float4 *sp, const uint4 *se, i
             if (!__any_sync(0xffffffffu, vis)) continue;
         }
         const float4 *rp = sp + 4 * (b - q0);
-        const uint4 *ep = se + (b - q0);
+        const ulonglong2 *ep = se + 2 * (b - q0);
         float2 s[PPT];
 #pragma unroll
         for (int j = 0; j < PPT; j++) s[j] = f2(0.f, 0.f);
@@ -281,8 +289,11 @@ __device__ __forceinline__ void sweep_pairs(const float4 *sp, const uint4 *se, i
         for (int i = 0; i < cnt; i++) {
             const float4 P0 = rp[4 * i], P1 = rp[4 * i + 1];
             const float2 nx = f2(P0.x, P0.y), ny = f2(P0.z, P0.w), cz = f2(P1.x, P1.y);
-            uint4 E = make_uint4(0u, 0u, 0u, 0u);
-            if constexpr (ECL) E = ep[i];
+            ulonglong2 Ea = make_ulonglong2(0ull, 0ull), Eb = Ea;
+            if constexpr (ECL) {
+                Ea = ep[2 * i];
+                Eb = ep[2 * i + 1];
+            }
             float2 m[PPT];
             uint32_t vis = 0u;  // ma, mb >= 0: their bits are nonzero iff they are > 0
 #pragma unroll
@@ -290,8 +301,8 @@ __device__ __forceinline__ void sweep_pairs(const float4 *sp, const uint4 *se, i
                 const float2 mu = __ffma2_rn(ex[j], nx, __ffma2_rn(ey[j], ny, cz));
                 float ma = fmaxf(mu.x, 0.f), mb = fmaxf(mu.y, 0.f);
                 if constexpr (ECL) {
-                    ma = ((pf[j] - E.x) >= E.y) ? ma : 0.f;
-                    mb = ((pf[j] - E.z) >= E.w) ? mb : 0.f;
+                    ma = ((pf[j] - Ea.x) >= Ea.y) ? ma : 0.f;
+                    mb = ((pf[j] - Eb.x) >= Eb.y) ? mb : 0.f;
                 }
                 m[j] = f2(ma, mb);
                 vis |= __float_as_uint(ma) | __float_as_uint(mb);
@@ -337,27 +348,31 @@ __global__ void __launch_bounds__(kThreads, (PPT <= 4) ? 3 : 2)
     const int64_t cend = (c0 + chunk < n) ? c0 + chunk : n;
     const bool need_ecl = cend > n0;
     float4 *sp = reinterpret_cast<float4 *>(smem);
-    uint4 *se = reinterpret_cast<uint4 *>(smem + chunk * 32);
+    ulonglong2 *se = reinterpret_cast<ulonglong2 *>(smem + chunk * 32);
     if (tid == 0) mbar_init(&bar, 1);
     __syncthreads();
     if (tid == 0 && live) {
-        const uint32_t bytes = (uint32_t)(chunk * 32) + (need_ecl ? (uint32_t)(chunk * 8) : 0u);
+        const uint32_t bytes = (uint32_t)(chunk * 32) + (need_ecl ? (uint32_t)(chunk * 16) : 0u);
         mbar_arrive_expect_tx(&bar, bytes);
         bulk_g2s(sp, f.fp + 8 * c0, (uint32_t)(chunk * 32), &bar);
-        if (need_ecl) bulk_g2s(se, f.ecl + c0, (uint32_t)(chunk * 8), &bar);
+        if (need_ecl) bulk_g2s(se, f.ecl + c0, (uint32_t)(chunk * 16), &bar);
     }
     float2 ex[PPT], ey[PPT];
     float exy[PPT];
-    uint32_t pf[PPT];
+    unsigned long long pf[PPT];
 #pragma unroll
     for (int j = 0; j < PPT; j++) {
         const int64_t e = (int64_t)blockIdx.x * (kThreads * PPT) + tid * PPT + j;
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (e < ph.nent) v = ph.ef[e];
+        unsigned long long p = 0ull;
+        if (e < ph.nent) {
+            v = ph.ef[e];
+            p = ph.pfx[e];
+        }
         ex[j] = f2(v.x, v.x);
         ey[j] = f2(v.y, v.y);
         exy[j] = sqrtf(fmaf(v.x, v.x, v.y * v.y));
-        pf[j] = __float_as_uint(v.w);
+        pf[j] = p;
     }
     // warp-uniform: a warp leaves together, so no lane is missing at the votes
     const bool staged = !live || __all_sync(0xffffffffu, mbar_wait_bounded(&bar, 0));
@@ -435,29 +450,34 @@ __global__ void __launch_bounds__(kThreads, (PPT <= 4) ? 3 : 2)
     const int model = S.model, ltype = S.fc.ltype;
     const bool need_ecl = cend > n0;
     float4 *sp = reinterpret_cast<float4 *>(smem);
-    uint4 *se = reinterpret_cast<uint4 *>(smem + chunk * 32);
+    ulonglong2 *se = reinterpret_cast<ulonglong2 *>(smem + chunk * 32);
     if (tid == 0) mbar_init(&bar, 1);
     __syncthreads();
     if (tid == 0) {
-        const uint32_t bytes = (uint32_t)(chunk * 32) + (need_ecl ? (uint32_t)(chunk * 8) : 0u);
+        const uint32_t bytes = (uint32_t)(chunk * 32) + (need_ecl ? (uint32_t)(chunk * 16) : 0u);
         mbar_arrive_expect_tx(&bar, bytes);
         bulk_g2s(sp, b.fp + 8 * (S.flat0 + c0), (uint32_t)(chunk * 32), &bar);
-        if (need_ecl) bulk_g2s(se, b.ecl + S.flat0 + c0, (uint32_t)(chunk * 8), &bar);
+        if (need_ecl) bulk_g2s(se, b.ecl + S.flat0 + c0, (uint32_t)(chunk * 16), &bar);
     }
     const float4 *ef = ph.ef + model * ph.ldp;
+    const unsigned long long *pfx = ph.pfx + model * ph.ldp;
     const float4 *runb = b.runb + S.flat0 / 64;
     float2 ex[PPT], ey[PPT];
     float exy[PPT];
-    uint32_t pf[PPT];
+    unsigned long long pf[PPT];
 #pragma unroll
     for (int j = 0; j < PPT; j++) {
         const int64_t e = tile * (kThreads * PPT) + tid * PPT + j;
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (e < ph.nent) v = ef[e];
+        unsigned long long p = 0ull;
+        if (e < ph.nent) {
+            v = ef[e];
+            p = pfx[e];
+        }
         ex[j] = f2(v.x, v.x);
         ey[j] = f2(v.y, v.y);
         exy[j] = sqrtf(fmaf(v.x, v.x, v.y * v.y));
-        pf[j] = __float_as_uint(v.w);
+        pf[j] = p;
     }
     // warp-uniform: a warp leaves together, so no lane is missing at the votes
     if (!__all_sync(0xffffffffu, mbar_wait_bounded(&bar, 0))) {
@@ -490,10 +510,9 @@ __global__ void __launch_bounds__(kThreads, (PPT <= 4) ? 3 : 2)
 template <int PPT>
 void launch_batch_t(const BatchDev &b, const BatchPhases &ph, const FluxPlan &plan, double *part,
                     int64_t ldp, cudaStream_t s) {
-    const size_t smem = (size_t)plan.chunk * 40;
+    const size_t smem = (size_t)plan.chunk * 48;  // 32 B records + 16 B eclipse ranges
     auto kern = k_flux_batch<PPT>;
-    if (smem > 48 * 1024)
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int64_t nblk = plan.nchunk * plan.ntile;
     kern<<<(unsigned)nblk, kThreads, smem, s>>>(b, ph, plan.chunk, plan.ntile, part, ldp);
     count_launch();
@@ -502,11 +521,10 @@ void launch_batch_t(const BatchDev &b, const BatchPhases &ph, const FluxPlan &pl
 template <int PPT, int LT>
 void launch_fast_t(const FlatDev &f, const PhaseDev &ph, const FluxPlan &plan, double *part,
                    int64_t ldp, DevStatus *st, cudaStream_t s) {
-    const size_t smem = (size_t)plan.chunk * 40;  // 32 B records + 8 B eclipse ranges
+    const size_t smem = (size_t)plan.chunk * 48;  // 32 B records + 16 B eclipse ranges
     if (plan.group <= 1) {
         auto kern = k_flux_fast<PPT, LT, false>;
-        if (smem > 48 * 1024)
-            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         dim3 grid((unsigned)plan.ntile, (unsigned)plan.nchunk);
         kern<<<grid, kThreads, smem, s>>>(f, ph, plan.chunk, plan.ntile, part, ldp, st);
         count_launch();
@@ -595,7 +613,7 @@ FluxPlan plan_flux(int mixed, int fast, int64_t nface, int64_t nent, int nsm) {
         p.ntile = (nent + (int64_t)kThreads * p.ppt - 1) / ((int64_t)kThreads * p.ppt);
         if (p.ntile < 1) p.ntile = 1;
         const int64_t want = ((int64_t)nsm * 4 + p.ntile - 1) / p.ntile;
-        int64_t chunk = 1024;  // 40 B per face: 40 KB of shared memory per CTA
+        int64_t chunk = 1024;  // 48 B per face: 48 KB of shared memory per CTA
         while (chunk > 64 && (nface + chunk - 1) / chunk < want) chunk >>= 1;
         p.chunk = chunk;
     } else if (mixed) {

@@ -13,6 +13,7 @@
 
 #include "eclipse.cuh"
 #include "engine.h"
+#include "fixed_phase.cuh"
 
 namespace lcg {
 
@@ -575,18 +576,6 @@ __global__ void k_flat_scan(int32_t *blockcnt, int32_t nb, int64_t n, int64_t *n
     if (threadIdx.x == 0) n0[1] = n - t2;
 }
 
-__device__ __forceinline__ uint32_t phase_fx(double ph) {
-    return (uint32_t)((unsigned long long)llrint(ph * 4294967296.0) & 0xffffffffull);
-}
-
-// Eclipse range [in1, out1] as 32-bit fixed-point phase (start, width + 1).
-__device__ __forceinline__ uint2 ecl_fx(double in1, double out1) {
-    long long w64 = llrint((out1 - in1) * 4294967296.0);
-    if (w64 < 0) w64 = 0;
-    if (w64 > 4294967294ll) w64 = 4294967294ll;
-    return make_uint2(phase_fx(in1), (uint32_t)(w64 + 1));
-}
-
 // Face i's record of the fast mixed sweep at flat position dest (pairs of
 // faces interleaved, FlatDev::fp).
 __device__ __forceinline__ void fast_record(float *fp, int64_t dest, GridDev g, int64_t i,
@@ -654,7 +643,7 @@ __global__ void k_flat_scatter(GridDev g, FlatDev f, const int32_t *__restrict__
                                              g.flux[i])
                                : make_float4(0.f, 0.f, 0.f, 0.f);
         }
-        f.ecl[dest] = cls == 1 ? ecl_fx(ein, eout) : make_uint2(0u, 0u);
+        f.ecl[dest] = cls == 1 ? ecl_fx64(ein, eout) : make_ulonglong2(0ull, 0ull);
         if (need_pos)
             f.pos[dest] = live ? make_float4((float)g.px[i], (float)g.py[i], (float)g.pz[i], 0.f)
                                : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -726,8 +715,8 @@ __global__ void k_phases(PhaseParams p, const DatumRec *__restrict__ data,
         ph.w1[e] = slfac * wgt * gi_scale1(p.gi, phi) / norm;
         ph.w2[e] = slfac * wgt * gi_scale2(p.gi, phi) / norm;
         ph.type[e] = (uint8_t)gi_type(p.gi, phi);
-        ph.ef[e] = make_float4((float)earth.x, (float)earth.y, (float)earth.z,
-                               __uint_as_float(phase_fx(phin)));
+        ph.ef[e] = make_float4((float)earth.x, (float)earth.y, (float)earth.z, 0.f);
+        ph.pfx[e] = phase_fx64(phin);
     }
 }
 
@@ -1042,22 +1031,15 @@ __global__ void k_pack_flat(FlatDev f, int64_t n0, int need_pos) {
     if (i == 0) *f.n0 = n0;
     if (i >= f.n) return;
     f.geo[i] = make_float4((float)f.dx[i], (float)f.dy[i], (float)f.dz[i], (float)f.flux[i]);
-    uint2 e = make_uint2(0u, 0u);
-    if (i >= n0) {
-        long long w64 = llrint((f.out1[i] - f.in1[i]) * 4294967296.0);
-        if (w64 < 0) w64 = 0;
-        if (w64 > 4294967294ll) w64 = 4294967294ll;
-        e = make_uint2(phase_fx(f.in1[i]), (uint32_t)(w64 + 1));
-    }
-    f.ecl[i] = e;
+    f.ecl[i] = i >= n0 ? ecl_fx64(f.in1[i], f.out1[i]) : make_ulonglong2(0ull, 0ull);
     if (need_pos) f.pos[i] = make_float4((float)f.px[i], (float)f.py[i], (float)f.pz[i], 0.f);
 }
 
 __global__ void k_pack_phases(PhaseDev ph) {
     const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (e >= ph.nent) return;
-    ph.ef[e] = make_float4((float)ph.ex[e], (float)ph.ey[e], (float)ph.ez[e],
-                           __uint_as_float(phase_fx(ph.phin[e])));
+    ph.ef[e] = make_float4((float)ph.ex[e], (float)ph.ey[e], (float)ph.ez[e], 0.f);
+    ph.pfx[e] = phase_fx64(ph.phin[e]);
 }
 
 // ---- batched stages ---------------------------------------------------------
@@ -1325,18 +1307,18 @@ __global__ void __launch_bounds__(kFlatBlock) k_flat_scatter_b(BatchDev b) {
         __syncthreads();
         const int rank = before + __popc(m & ((1u << lane) - 1u));
         float *fp = b.fp + 8 * S.flat0;
-        uint2 *ecl = b.ecl + S.flat0;
+        ulonglong2 *ecl = b.ecl + S.flat0;
         if (in) {
             const GridDev g = slot_grid(b.g, S.face0, n, S.ntiled);
             const int64_t n0 = b.n0[s];
             const int64_t boff = b.blockcnt[S.blk0 + lb];
             const int64_t dest = flag ? n0 + boff + rank : lb * kFlatBlock - boff + (t - rank);
             fast_record(fp, dest, g, i, S.fc);
-            ecl[dest] = flag ? ecl_fx(g.ein[i], g.eout[i]) : make_uint2(0u, 0u);
+            ecl[dest] = flag ? ecl_fx64(g.ein[i], g.eout[i]) : make_ulonglong2(0ull, 0ull);
         } else if (i == n && (n & 1)) {
             float *r = fp + 16 * (n >> 1) + 1;
             for (int q = 0; q < 16; q += 2) r[q] = 0.f;
-            ecl[n] = make_uint2(0u, 0u);
+            ecl[n] = make_ulonglong2(0ull, 0ull);
         }
     }
 }
@@ -1361,8 +1343,8 @@ __global__ void k_phases_b(BatchDev b, const DatumRec *__restrict__ data,
         const double phin = phi - floor(phi);
         ph.w1[e] = slfac * wgt * gi_scale1(p.gi, phi) / norm;
         ph.w2[e] = slfac * wgt * gi_scale2(p.gi, phi) / norm;
-        ph.ef[e] = make_float4((float)earth.x, (float)earth.y, (float)earth.z,
-                               __uint_as_float(phase_fx(phin)));
+        ph.ef[e] = make_float4((float)earth.x, (float)earth.y, (float)earth.z, 0.f);
+        ph.pfx[e] = phase_fx64(phin);
     }
 }
 
