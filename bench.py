@@ -79,6 +79,12 @@ def parse():
     ap.add_argument("--refine-epochs", type=int, default=600)
     ap.add_argument("--da-scale", type=float, default=2.6)
     ap.add_argument("--local-widen", type=float, default=2.0)
+    ap.add_argument("--is-rounds", type=int, default=8,
+                    help="surrogate_da: rounds of adaptive importance sampling of the posterior")
+    ap.add_argument("--is-pool", type=int, default=65536,
+                    help="surrogate_da: exact curves per importance-sampling round")
+    ap.add_argument("--is-target", type=float, default=20000.0,
+                    help="surrogate_da: effective size at which the importance sampling stops")
     ap.add_argument("--precision", choices=("mixed", "fp64"), default="mixed")
     ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -687,14 +693,15 @@ def run_surrogate(args):
     plain vs delayed-acceptance Metropolis (same start states, same draws) on
     wd_dm_small data; effective samples per second of sampling.
 
-    Start states: a first adaptive burn-in locates the posterior; every exact
-    curve computed so far (the box-uniform training set and the local draws
-    the network is refined on) then gives an importance sample of the
-    posterior (each row weighted by its exact likelihood over the density of
-    the mixture it was drawn from), and the chains start from a resample of
-    it, so both samplers begin at (close to) the stationary distribution and
-    their means can be compared against their Monte Carlo errors. The
-    proposal covariance is that sample's weighted covariance x 2.38^2 / 9.
+    Start states: a first adaptive burn-in locates the posterior; adaptive
+    importance sampling of exact engine curves (the box-uniform training set,
+    then Gaussian pools around the running weighted estimate, then the local
+    draws the network is refined on; each row weighted by its exact
+    likelihood over the density of the mixture of the pools) gives the
+    posterior's sample, and the chains start from a resample of it, so both
+    samplers begin at (close to) the stationary distribution and their means
+    can be compared against their Monte Carlo errors. The proposal covariance
+    is that sample's weighted covariance x 2.38^2 / 9.
 
     value: bulk ESS (rank-normalised multi-chain ESS over split chains,
     minimum over parameters) per second of delayed-acceptance sampling; the
@@ -753,38 +760,40 @@ def run_surrogate(args):
         chf, theta0, _, _, _ = metropolis(exact, theta0, cov, args.burn_fixed, seed=13)
         samp = chf[chf.shape[0] // 2:].reshape(-1, 9)
         del chf
+    # the posterior by adaptive importance sampling of exact engine curves
+    # (surrogate.adaptive_posterior; the box-uniform training set is the first
+    # pool, the burn-in's spread places the first Gaussian one)
+    t0 = time.perf_counter()
+    chi_box = S.curves_chi2(curves, data, idx)
+    del curves
+
+    def exact_chi2(th):
+        _, cu = S.training_set(eng, 0, theta=th, batch=2048)
+        return S.curves_chi2(cu, data, idx)
+    pools, chi_pool, mu_k, cov_k, ess_rounds = S.adaptive_posterior(
+        exact_chi2, [(theta, S.log_uniform_box())], chi_box, samp.mean(0), np.cov(samp.T),
+        rounds=args.is_rounds, pool=args.is_pool, target=args.is_target,
+        widen0=args.local_widen, seed=19 + rank)
+    jitter = np.diag(np.diag(cov_k) * 1e-6)
     # refinement: the same network trained again on engine curves around the
-    # burn-in posterior (Gaussian, local_widen x its spread, inside the box)
-    mu_b, cov_b = samp.mean(0), np.cov(samp.T)
-    th_loc = S.local_draws(mu_b, cov_b, args.local_curves, seed=5 + rank, widen=args.local_widen)
-    t0 = time.perf_counter()
+    # posterior (Gaussian, local_widen x its spread, inside the box); those
+    # curves are the importance sample's last pool too
+    th_loc = S.local_draws(mu_k, cov_k, args.local_curves, seed=5 + rank, widen=args.local_widen)
     _, cu_loc = S.training_set(eng, 0, theta=th_loc, batch=2048)
-    sur_loc = S.Surrogate(ncoef=args.ncoef, batch=4096, seed=rank + 1)
-    losses_loc = sur_loc.fit(th_loc, cu_loc, epochs=args.refine_epochs)
-    t_ref = time.perf_counter() - t0
-    th_lh = S.local_draws(mu_b, cov_b, 2048, seed=77 + rank, widen=args.local_widen)
-    _, cu_lh = S.training_set(eng, 0, theta=th_lh, batch=2048)
-    loc_err = float(np.sqrt(np.mean((sur_loc.curves(th_lh) - cu_lh) ** 2)))
-    glob_err_loc = float(np.sqrt(np.mean((sur.curves(th_lh) - cu_lh) ** 2)))
-    # start states and proposal: importance resampling of the posterior from
-    # every exact curve made so far, in two stages: the first weighted
-    # estimate places a second, tighter pool of exact curves (1.5 x its
-    # spread), and the three pools together give the final sample
-    t0 = time.perf_counter()
-    chi_pool = np.r_[S.curves_chi2(curves, data, idx), S.curves_chi2(cu_loc, data, idx)]
-    del curves, cu_loc
-    pools = [(theta, S.log_uniform_box()),
-             (th_loc, S.log_gaussian_in_box(mu_b, cov_b, args.local_widen))]
-    _, mu_1, cov_1, ess_1 = S.posterior_resample(pools, chi_pool, 1, seed=17 + rank)
-    cov_1 = cov_1 + np.diag(np.diag(cov_b) * 1e-6)  # keeps it positive definite
-    th_2 = S.local_draws(mu_1, cov_1, args.local_curves, seed=19 + rank, widen=1.5)
-    _, cu_2 = S.training_set(eng, 0, theta=th_2, batch=2048)
-    chi_pool = np.r_[chi_pool, S.curves_chi2(cu_2, data, idx)]
-    del cu_2
-    pools.append((th_2, S.log_gaussian_in_box(mu_1, cov_1, 1.5)))
+    chi_pool = np.r_[chi_pool, S.curves_chi2(cu_loc, data, idx)]
+    pools.append((th_loc, S.log_gaussian_in_box(mu_k, cov_k, args.local_widen)))
     theta0, mu_is, cov_is, ess_is = S.posterior_resample(pools, chi_pool, args.chains,
                                                          seed=17 + rank)
     t_sir = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    sur_loc = S.Surrogate(ncoef=args.ncoef, batch=4096, seed=rank + 1)
+    losses_loc = sur_loc.fit(th_loc, cu_loc, epochs=args.refine_epochs)
+    t_ref = time.perf_counter() - t0
+    del cu_loc
+    th_lh = S.local_draws(mu_is, cov_is + jitter, 2048, seed=77 + rank, widen=args.local_widen)
+    _, cu_lh = S.training_set(eng, 0, theta=th_lh, batch=2048)
+    loc_err = float(np.sqrt(np.mean((sur_loc.curves(th_lh) - cu_lh) ** 2)))
+    glob_err_loc = float(np.sqrt(np.mean((sur.curves(th_lh) - cu_lh) ** 2)))
     cov = cov_is * 2.38 ** 2 / 9 + np.diag((scale0 * 1e-3) ** 2)
     exact = ExactChi2(eng, data)
     sur_loc_chi = S.SurrogateChi2(sur_loc, data, idx)
@@ -847,9 +856,10 @@ def run_surrogate(args):
                           "(new_scripts/mcmc_solver.cpp:80-115) summed over chains, frozen "
                           "chains counted as zero",
                    "start": "both samplers from the same %d states, resampled from an "
-                            "importance sample of the posterior (%d exact curves in three "
-                            "pools, effective size %.0f; %.0f after the first two)"
-                            % (args.chains, len(chi_pool), ess_is, ess_1)},
+                            "importance sample of the posterior (%d exact curves in %d pools, "
+                            "effective size %.0f; after each adaptive round: %s)"
+                            % (args.chains, len(chi_pool), len(pools), ess_is,
+                               [round(x) for x in ess_rounds])},
         "plain": dict(sum_p, acceptance=accp, exact_evals=n_plain),
         "delayed_acceptance": dict(sum_d, surrogate="refined around the burn-in posterior",
                                    acceptance=accd,

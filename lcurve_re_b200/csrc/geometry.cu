@@ -207,117 +207,50 @@ __device__ __noinline__ int ecl_screen_test(const EclScreen scr, float cosi, flo
     return fblink_screen(scr, u0x, u0y, u0z, sini * cs, -sini * sn, cosi, acc);
 }
 
-// The bisections of ingress (side 0) and egress (side 1) of ingress_egress
-// (ingress_egress.cpp:61-86) from the pot_min state, as a pool worked by the
-// lanes of a warp: a task is one (candidate, side); every lane holds one task
-// at a time, and a lane whose bisection has ended writes its result and takes
-// the next task from the queue (one atomic per warp and refill), so lanes do
-// not sit idle while the slowest bisection of the warp runs on. Each lane
-// screens its midpoints in FP32 until one is unsure; when every lane that
-// holds a task is waiting on an unsure test, the warp runs Roche::fblink in
-// FP64 for all of them in a single pass, and the screening resumes. A task
-// takes the FP64 decisions at the same midpoints as the plain loop (with the
-// screen off, every midpoint is an FP64 test): the phases are bit-identical
-// to those of ingress_egress, whatever the order in which tasks run.
-//
-// Source supplies the tasks: load(u, ...) fills a task's state and returns
-// false for a candidate without an eclipse (the lane then draws again), and
-// finish(u, v, s) takes the bisection's phase (or a failure status).
-template <class Source>
-__device__ __forceinline__ void ecl_bisect_pool(Source &src, int32_t ntask, int32_t *counter) {
-    const unsigned full = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    const unsigned below = (1u << lane) - 1u;
-    bool has = false, exhausted = false, done = false, need = false;
-    int32_t u = 0;
-    const EclParams *p = nullptr;
-    double pin = 0., pout = 0., acc = 0.;
-    V3 pos = v3(0., 0., 0.);
-    float u0x = 0.f, u0y = 0.f, u0z = 0.f, cif = 0.f, sif = 0.f;
-    EclScreen scr{};  // the task's screen and step, in registers for the loop
-    double delta = 0.;
-    int guard = 0, s = 0;
+// The bisection of ingress (side 0) or egress (side 1) of ingress_egress
+// (ingress_egress.cpp:61-86) from the pot_min state, for every lane of a warp
+// at once (all 32 lanes call it; lanes with live false only vote). Each lane
+// screens its midpoints in FP32 until one is unsure; when no live lane can go
+// on, the warp runs Roche::fblink in FP64 for all the lanes waiting on one, in
+// a single pass, and the screening resumes. The FP64 passes are thus packed
+// (one per test of the lane that needs the most, instead of one per step
+// whenever any lane needs one), and the lanes take the FP64 decisions at the
+// same midpoints as the plain loop. With the screen off it is the plain loop.
+__device__ __forceinline__ double ecl_bisect_warp(const EclParams &p, bool live, double pin,
+                                                  double pout, double acc, V3 pos, int &s) {
+    // what the screening loop reads, in registers (p may be global memory;
+    // the FP64 test, a third of the steps, reads the rest from it)
+    const EclScreen scr = p.scr;
+    const double delta = p.delta;
+    const float cif = (float)p.cosi, sif = (float)p.sini, accf = (float)acc;
+    const float u0x = (float)(pos.x - (p.comp_star == kStar1 ? 0. : 1.));
+    const float u0y = (float)pos.y, u0z = (float)pos.z;
+    bool done = !live;
+    int guard = 0;
+    double pmid = 0.;
     for (;;) {
-        // every lane advances until it waits on an FP64 test or the pool has
-        // nothing left for it; a waiting lane's midpoint is (pin + pout) / 2
-        for (;;) {
-            while (has && !done && !need) {
-                if (!(fabs(pin - pout) > delta)) { done = true; break; }
-                if (++guard > 400) { s = kEclNoConverge; done = true; break; }
-                const double pmid = (pin + pout) / 2.;
-                if (!scr.on) { need = true; break; }
-                const int d = ecl_screen_test(scr, cif, sif, pmid, u0x, u0y, u0z, (float)acc);
-                if (d == kScreenUnsure) { need = true; break; }
-                if (d == kScreenTrue) pin = pmid;
-                else pout = pmid;
-            }
-            if (has && done) {
-                src.finish(u, (pin + pout) / 2., s);
-                has = false;
-            }
-            const unsigned want = __ballot_sync(full, !has && !exhausted);
-            if (!want) break;
-            const int leader = __ffs(want) - 1;
-            int32_t base = 0;
-            if (lane == leader) base = atomicAdd(counter, __popc(want));
-            base = __shfl_sync(full, base, leader);
-            if (!has && !exhausted) {
-                u = base + __popc(want & below);
-                if (u >= ntask) {
-                    exhausted = true;
-                } else if (src.load(u, p, pin, pout, acc, pos)) {
-                    has = true;
-                    done = need = false;
-                    guard = s = 0;
-                    scr = p->scr;
-                    delta = p->delta;
-                    cif = (float)p->cosi;
-                    sif = (float)p->sini;
-                    u0x = (float)(pos.x - (p->comp_star == kStar1 ? 0. : 1.));
-                    u0y = (float)pos.y;
-                    u0z = (float)pos.z;
-                }
-            }
+        bool need = false;
+        while (!done) {
+            if (!(fabs(pin - pout) > delta)) { done = true; break; }
+            if (++guard > 400) { s = kEclNoConverge; done = true; break; }
+            pmid = (pin + pout) / 2.;
+            if (!scr.on) { need = true; break; }
+            const int d = ecl_screen_test(scr, cif, sif, pmid, u0x, u0y, u0z, accf);
+            if (d == kScreenUnsure) { need = true; break; }
+            if (d == kScreenTrue) pin = pmid;
+            else pout = pmid;
         }
-        if (!__any_sync(full, need)) break;  // no task left anywhere in the warp
+        if (!__any_sync(0xffffffffu, need)) break;
         if (need) {
-            const double pmid = (pin + pout) / 2.;
-            if (fblink(p->comp_star, p->q, p->comp_spin, acc, set_earth(p->cosi, p->sini, pmid),
-                       pos, p->comp_rref, p->comp_pref, s))
+            if (fblink(p.comp_star, p.q, p.comp_spin, acc, set_earth(p.cosi, p.sini, pmid), pos,
+                       p.comp_rref, p.comp_pref, s))
                 pin = pmid;
             else
                 pout = pmid;
-            need = false;
             if (s) done = true;
         }
     }
-}
-
-// A side's result goes into its own starting slot of the candidate's pot_min
-// state (es[k] = (phi, phi1, phi2, ACC): side 0 starts from phi1, side 1 from
-// phi2 and nothing else reads them), as a phase in [0, 1), or NaN when the
-// bisection failed; the join writes the grid once both sides are in.
-__device__ __forceinline__ void ecl_task_state(const double4 *es, int32_t u, double &pin,
-                                               double &pout, double &acc) {
-    const double *e = reinterpret_cast<const double *>(es + (u >> 1));
-    pin = e[0];
-    pout = (u & 1) ? e[2] : e[1];
-    acc = e[3];
-}
-
-__device__ __forceinline__ void ecl_task_result(double4 *es, int32_t u, double v, bool ok) {
-    reinterpret_cast<double *>(es + (u >> 1))[1 + (u & 1)] = ok ? v - floor(v) : __longlong_as_double(0x7ff8000000000000LL);
-}
-
-// set_star_grid.cpp:372-386: a face eclipsed from ingress to egress, egress
-// taken past ingress
-__device__ __forceinline__ void ecl_join_face(const GridDev &g, int32_t i, double4 E) {
-    if (isnan(E.y) || isnan(E.z)) return;  // a side failed: its status is set
-    double egr = E.z;
-    if (egr < E.y) egr++;
-    g.necl[i] = 1;
-    g.ein[i] = E.y;
-    g.eout[i] = egr;
+    return (pin + pout) / 2.;
 }
 
 // Thread mode (more candidates than warp_max), in two passes with a small code
@@ -359,47 +292,46 @@ __global__ void __launch_bounds__(128, 4) k_ecl_potmin(EclParams p, GridDev g,
     }
 }
 
-struct EclTasks {
-    const EclParams *p;
-    const GridDev *g;
-    const int32_t *queue;
-    double4 *es;
-    const uint8_t *ehit;
-    DevStatus *st;
-    __device__ bool load(int32_t u, const EclParams *&pp, double &pin, double &pout, double &acc,
-                         V3 &pos) {
-        const int k = u >> 1;
-        if (!ehit[k]) return false;
-        ecl_task_state(es, u, pin, pout, acc);
-        const int32_t i = queue[k];
-        pos = v3(g->px[i], g->py[i], g->pz[i]);
-        pp = p;
-        return true;
-    }
-    __device__ void finish(int32_t u, double v, int s) {
-        if (s) set_status(st, s, queue[u >> 1]);
-        ecl_task_result(es, u, v, s == 0);
-    }
-};
-
 template <int NB>
 __global__ void __launch_bounds__(128, NB)
     k_ecl_bisect(__grid_constant__ const EclParams p, __grid_constant__ const GridDev g,
-                 const int32_t *__restrict__ queue, int32_t *counters, double4 *es,
+                 const int32_t *__restrict__ queue, int32_t *counters, const double4 *es,
                  const uint8_t *ehit, DevStatus *st, int32_t warp_max) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
     const int total = counters[0];
     if (total <= warp_max) return;
-    EclTasks src{&p, &g, queue, es, ehit, st};
-    ecl_bisect_pool(src, 2 * total, &counters[3]);
-}
-
-__global__ void k_ecl_join(GridDev g, const int32_t *__restrict__ queue,
-                           const int32_t *counters, const double4 *es, const uint8_t *ehit,
-                           int32_t warp_max) {
-    const int total = counters[0];
-    if (total <= warp_max) return;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x)
-        if (ehit[k]) ecl_join_face(g, queue[k], es[k]);
+    const int64_t n2 = 2 * (int64_t)total;
+    for (;;) {
+        int64_t base = 0;
+        if (lane == 0) base = atomicAdd(&counters[3], 32);
+        base = __shfl_sync(full, base, 0);
+        if (base >= n2) break;
+        // every lane stays here (ecl_bisect_warp votes over the warp); both
+        // lanes of a pair agree on live
+        const int64_t u = base + lane;
+        const int k = (int)(u >> 1), side = (int)(u & 1);
+        const bool live = u < n2 && ehit[k];
+        const int32_t i = live ? queue[k] : 0;
+        const double4 E = live ? es[k] : make_double4(0., 0., 0., 0.);
+        const V3 pos = live ? v3(g.px[i], g.py[i], g.pz[i]) : v3(0., 0., 0.);
+        int s = 0;
+        double v = ecl_bisect_warp(p, live, E.x, side ? E.z : E.y, E.w, pos, s);
+        v = v - floor(v);
+        const double other = __shfl_xor_sync(full, v, 1);
+        const int os = __shfl_xor_sync(full, s, 1);
+        if (live && side == 0) {
+            if (s || os) {
+                set_status(st, s ? s : os, i);
+            } else {
+                double egr = other;
+                if (egr < v) egr++;
+                g.necl[i] = 1;
+                g.ein[i] = v;
+                g.eout[i] = egr;
+            }
+        }
+    }
 }
 
 __device__ __forceinline__ void continuum_face(const ContParams &p, GridDev g, int64_t i) {
@@ -1205,43 +1137,46 @@ __global__ void __launch_bounds__(128, 4) k_ecl_potmin_b(BatchDev b, int32_t war
     }
 }
 
-struct EclTasksB {
-    const BatchDev *b;
-    __device__ bool load(int32_t u, const EclParams *&pp, double &pin, double &pout, double &acc,
-                         V3 &pos) {
-        const int k = u >> 1;
-        if (!b->ehit[k]) return false;
-        ecl_task_state(b->es, u, pin, pout, acc);
-        const int32_t i = queue_at(*b, k);
-        pos = v3(b->g.px[i], b->g.py[i], b->g.pz[i]);
-        pp = &b->slots[find_seg(b->face0, b->nslots, i)].ep;
-        return true;
-    }
-    __device__ void finish(int32_t u, double v, int s) {
-        if (s) {
-            const int32_t i = queue_at(*b, u >> 1);
-            const SlotDev &S = b->slots[find_seg(b->face0, b->nslots, i)];
-            set_status(b->st + S.model, s, i - S.face0);
-        }
-        ecl_task_result(b->es, u, v, s == 0);
-    }
-};
-
-// 4 blocks of 4 warps per SM by default (LCG_ECL_BISECT_BLOCKS=6 selects 6
-// for measurement); every warp works the lane pool until the queue is empty
+// 6 blocks of 4 warps per SM (a sweep of 4, 5, 6 and 8 on B200 chose 6: more
+// warps hide the FP64 latency, fewer registers spill more)
 template <int NB>
 __global__ void __launch_bounds__(128, NB)
     k_ecl_bisect_b(__grid_constant__ const BatchDev b, int32_t warp_max, int32_t auto_mode) {
-    if (batch_warp_mode(b, warp_max, auto_mode)) return;
-    EclTasksB src{&b};
-    ecl_bisect_pool(src, 2 * b.counters[0], &b.counters[3]);
-}
-
-__global__ void k_ecl_join_bisect_b(BatchDev b, int32_t warp_max, int32_t auto_mode) {
-    if (batch_warp_mode(b, warp_max, auto_mode)) return;
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
     const int total = b.counters[0];
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x)
-        if (b.ehit[k]) ecl_join_face(b.g, queue_at(b, k), b.es[k]);
+    if (batch_warp_mode(b, warp_max, auto_mode)) return;
+    const int64_t n2 = 2 * (int64_t)total;
+    for (;;) {
+        int64_t base = 0;
+        if (lane == 0) base = atomicAdd(&b.counters[3], 32);
+        base = __shfl_sync(full, base, 0);
+        if (base >= n2) break;
+        const int64_t u = base + lane;
+        const int k = (int)(u >> 1), side = (int)(u & 1);
+        const bool live = u < n2 && b.ehit[k];
+        const int32_t i = live ? queue_at(b, k) : 0;
+        const int sl = find_seg(b.face0, b.nslots, i);
+        const double4 E = live ? b.es[k] : make_double4(0., 0., 0., 0.);
+        const V3 pos = live ? v3(b.g.px[i], b.g.py[i], b.g.pz[i]) : v3(0., 0., 0.);
+        int s = 0;
+        double v = ecl_bisect_warp(b.slots[sl].ep, live, E.x, side ? E.z : E.y, E.w, pos, s);
+        v = v - floor(v);
+        const double other = __shfl_xor_sync(full, v, 1);
+        const int os = __shfl_xor_sync(full, s, 1);
+        if (live && side == 0) {
+            const SlotDev &S = b.slots[sl];
+            if (s || os) {
+                set_status(b.st + S.model, s ? s : os, i - S.face0);
+            } else {
+                double egr = other;
+                if (egr < v) egr++;
+                b.g.necl[i] = 1;
+                b.g.ein[i] = v;
+                b.g.eout[i] = egr;
+            }
+        }
+    }
 }
 
 __global__ void k_continuum_b(BatchDev b) {
@@ -1460,8 +1395,6 @@ void launch_eclipse(const EclParams &p, int32_t eclipse_on, GridDev g, int32_t *
         else
             k_ecl_bisect<4><<<nbb, 128, 0, s>>>(p, g, queue, counters, es, ehit, st, warp_max);
         count_launch();
-        k_ecl_join<<<nb, 128, 0, s>>>(g, queue, counters, es, ehit, warp_max);
-        count_launch();
     }
 }
 
@@ -1591,8 +1524,6 @@ void launch_batch_eclipse(const BatchDev &b, int nsm, int32_t warp_mode, cudaStr
         k_ecl_bisect_b<6><<<nsm * 6, 128, 0, s>>>(b, warp_max, auto_mode);
     else
         k_ecl_bisect_b<4><<<nsm * 4, 128, 0, s>>>(b, warp_max, auto_mode);
-    count_launch();
-    k_ecl_join_bisect_b<<<nsm * 4, 256, 0, s>>>(b, warp_max, auto_mode);
     count_launch();
 }
 

@@ -275,6 +275,33 @@ def posterior_resample(pools, chi2, n, seed=0):
     return theta[rows].copy(), mean, cov, float(1.0 / np.sum(w ** 2))
 
 
+def adaptive_posterior(chi2_of, pools, chi, mu, cov, rounds=8, pool=65536, target=2e4,
+                       widen0=2.0, widen=1.3, seed=0):
+    """Adaptive importance sampling of the posterior (uniform prior over the
+    box, likelihood exp(-chi**2 / 2)). pools / chi: the rows already drawn
+    (list of (theta, log density) as posterior_resample takes them) and their
+    chi**2. Each round draws `pool` rows from the Gaussian around the current
+    estimate (widen0 x the spread of (mu, cov) first, then widen x the
+    weighted spread), gets their chi**2 from chi2_of(theta) (the exact engine
+    in the benchmark), adds them as a pool and re-weighs every row over the
+    mixture; it stops once the effective size reaches target. Returns
+    (pools, chi, mean, covariance, effective size per round)."""
+    jitter = np.diag(np.diag(np.asarray(cov)) * 1e-6)  # keeps estimates positive definite
+    w, hist = widen0, []
+    chi = np.asarray(chi, np.float64)
+    for k in range(rounds):
+        th = local_draws(mu, cov, pool, seed=seed + 7 * k, widen=w)
+        chi = np.r_[chi, chi2_of(th)]
+        pools = pools + [(th, log_gaussian_in_box(mu, cov, w))]
+        _, mu, cov, ess = posterior_resample(pools, chi, 1, seed=seed)
+        cov = cov + jitter
+        hist.append(float(ess))
+        w = widen
+        if ess >= target:
+            break
+    return pools, chi, mu, cov, hist
+
+
 def log_uniform_box():
     """Log density of uniform draws over the box."""
     vol = float(np.prod(BOX[:, 1] - BOX[:, 0]))

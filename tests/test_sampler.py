@@ -231,3 +231,28 @@ def test_posterior_resample_recovers_a_gaussian_posterior():
     assert np.all(np.abs(mean - mu) < 0.05 * sd)
     assert np.all(np.abs(np.sqrt(np.diag(cov)) / sd - 1) < 0.05)
     assert np.all(np.abs(rows.mean(0) - mu) < 0.1 * sd)
+
+
+def test_adaptive_posterior_finds_a_correlated_posterior():
+    """Adaptive importance sampling from a poor first estimate (offset mean,
+    three times too wide, no correlation) of a strongly correlated Gaussian
+    posterior (correlation 0.99 between two parameters): the rounds reach the
+    target effective size and the weighted mean and covariance match."""
+    from lcurve_re_b200 import surrogate as S
+    rng = np.random.default_rng(9)
+    lo, hi = S.BOX[:, 0], S.BOX[:, 1]
+    mu = (lo + hi) / 2 + 0.05 * (hi - lo)
+    sd = 0.02 * (hi - lo)
+    corr = np.eye(9)
+    corr[0, 3] = corr[3, 0] = 0.99
+    cov = corr * np.outer(sd, sd)
+    prec = np.linalg.inv(cov)
+    chi2 = lambda t: np.einsum("ij,jk,ik->i", t - mu, prec, t - mu)
+    th_u = lo + rng.random((50000, 9)) * (hi - lo)
+    pools, chi, m, c, hist = S.adaptive_posterior(
+        chi2, [(th_u, S.log_uniform_box())], chi2(th_u), mu + 2 * sd, np.diag((3 * sd) ** 2),
+        rounds=8, pool=30000, target=5000, seed=4)
+    assert hist[-1] >= 5000 and len(hist) <= 8, hist
+    assert np.all(np.abs(m - mu) < 0.05 * sd)
+    assert np.all(np.abs(np.sqrt(np.diag(c)) / sd - 1) < 0.05)
+    assert abs(c[0, 3] / np.sqrt(c[0, 0] * c[3, 3]) - 0.99) < 0.003
