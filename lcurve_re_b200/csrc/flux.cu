@@ -18,12 +18,10 @@
 //  * eclipse test in 64-bit fixed-point phase: visible iff (phase - ingress)
 //    mod 2^64 >= width + 1 (ecl_fx64, geometry.cu), the reference's double
 //    comparisons decision for decision.
-#include <cooperative_groups.h>
+#include <algorithm>
 
 #include "engine.h"
 #include "tma.cuh"
-
-namespace cg = cooperative_groups;
 
 namespace lcg {
 
@@ -31,6 +29,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kFold = 64;  // LCG_MIXED_FOLD
+constexpr int kGroup = 4;  // chunks per work unit of the fast sweep's pool
 
 __device__ __forceinline__ float sqrt_approx(float x) {
     float r;
@@ -328,41 +327,14 @@ __device__ __forceinline__ void sweep_pairs(const float4 *sp, const ulonglong2 *
 
 // 3 CTAs per SM for PPT <= 4 (80 registers, no spills): 24 warps hide the
 // FFMA2 and MUFU latencies better than 16; larger PPT keeps 2
-//
-// CLUSTER: the CTAs of a thread-block cluster (1 x G along the chunks) hold G
-// consecutive chunks of one phase tile; rank 0 adds their FP64 partials in
-// chunk order through distributed shared memory and writes one partial row
-// per group, so the partials that reach HBM (and the chunk reduction's
-// reads) shrink G-fold. Chunks past the grid (the grid's chunk count is
-// padded to a multiple of G) add zero.
-template <int PPT, int LT, bool CLUSTER>
-__global__ void __launch_bounds__(kThreads, (PPT <= 4) ? 3 : 2)
-    k_flux_fast(FlatDev f, PhaseDev ph, int64_t chunk, int64_t ntile, double *part, int64_t ldp,
-                DevStatus *st) {
-    extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ uint64_t bar;
-    const int tid = threadIdx.x;
-    const int64_t c0 = (int64_t)blockIdx.y * chunk;
-    const int64_t n = f.n, n0 = *f.n0;
-    const bool live = c0 < n;  // false only for the padding chunks of a cluster grid
-    const int64_t cend = (c0 + chunk < n) ? c0 + chunk : n;
-    const bool need_ecl = cend > n0;
-    float4 *sp = reinterpret_cast<float4 *>(smem);
-    ulonglong2 *se = reinterpret_cast<ulonglong2 *>(smem + chunk * 32);
-    if (tid == 0) mbar_init(&bar, 1);
-    __syncthreads();
-    if (tid == 0 && live) {
-        const uint32_t bytes = (uint32_t)(chunk * 32) + (need_ecl ? (uint32_t)(chunk * 16) : 0u);
-        mbar_arrive_expect_tx(&bar, bytes);
-        bulk_g2s(sp, f.fp + 8 * c0, (uint32_t)(chunk * 32), &bar);
-        if (need_ecl) bulk_g2s(se, f.ecl + c0, (uint32_t)(chunk * 16), &bar);
-    }
-    float2 ex[PPT], ey[PPT];
-    float exy[PPT];
-    unsigned long long pf[PPT];
+// A thread's PPT consecutive phase entries of phase tile `tile`.
+template <int PPT>
+__device__ __forceinline__ void load_entries(const PhaseDev &ph, int64_t tile, int tid,
+                                             float2 *ex, float2 *ey, float *exy,
+                                             unsigned long long *pf) {
 #pragma unroll
     for (int j = 0; j < PPT; j++) {
-        const int64_t e = (int64_t)blockIdx.x * (kThreads * PPT) + tid * PPT + j;
+        const int64_t e = tile * (kThreads * PPT) + tid * PPT + j;
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
         unsigned long long p = 0ull;
         if (e < ph.nent) {
@@ -374,59 +346,142 @@ __global__ void __launch_bounds__(kThreads, (PPT <= 4) ? 3 : 2)
         exy[j] = sqrtf(fmaf(v.x, v.x, v.y * v.y));
         pf[j] = p;
     }
+}
+
+// One staged chunk [c0, cend): the pairs holding face n0 and those after it
+// take the eclipse test (a never-eclipsed face in that pair has an empty
+// range); faces past n in the last pair carry zero coefficients.
+template <int PPT, int LT>
+__device__ __forceinline__ void sweep_chunk(const FlatDev &f, const float4 *sp,
+                                            const ulonglong2 *se, int64_t c0, int64_t cend,
+                                            int64_t n0, const float2 *ex, const float2 *ey,
+                                            const float *exy, const unsigned long long *pf,
+                                            float *acc) {
+    const int64_t q0 = c0 >> 1, qend = (cend + 1) >> 1, qn0 = n0 >> 1;
+    const int64_t qa = qn0 < qend ? qn0 : qend;
+    sweep_pairs<PPT, LT, false>(sp, se, q0, q0, qa > q0 ? qa : q0, ex, ey, exy, pf, f.runb, acc);
+    sweep_pairs<PPT, LT, true>(sp, se, q0, qa > q0 ? qa : q0, qend, ex, ey, exy, pf, f.runb, acc);
+}
+
+template <int PPT, int LT>
+__global__ void __launch_bounds__(kThreads, (PPT <= 4) ? 3 : 2)
+    k_flux_fast(FlatDev f, PhaseDev ph, int64_t chunk, int64_t ntile, double *part, int64_t ldp,
+                DevStatus *st) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ uint64_t bar;
+    const int tid = threadIdx.x;
+    const int64_t c0 = (int64_t)blockIdx.y * chunk;
+    const int64_t n = f.n, n0 = *f.n0;
+    const int64_t cend = (c0 + chunk < n) ? c0 + chunk : n;
+    const bool need_ecl = cend > n0;
+    float4 *sp = reinterpret_cast<float4 *>(smem);
+    ulonglong2 *se = reinterpret_cast<ulonglong2 *>(smem + chunk * 32);
+    if (tid == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    if (tid == 0) {
+        const uint32_t bytes = (uint32_t)(chunk * 32) + (need_ecl ? (uint32_t)(chunk * 16) : 0u);
+        mbar_arrive_expect_tx(&bar, bytes);
+        bulk_g2s(sp, f.fp + 8 * c0, (uint32_t)(chunk * 32), &bar);
+        if (need_ecl) bulk_g2s(se, f.ecl + c0, (uint32_t)(chunk * 16), &bar);
+    }
+    float2 ex[PPT], ey[PPT];
+    float exy[PPT];
+    unsigned long long pf[PPT];
+    load_entries<PPT>(ph, (int64_t)blockIdx.x, tid, ex, ey, exy, pf);
     // warp-uniform: a warp leaves together, so no lane is missing at the votes
-    const bool staged = !live || __all_sync(0xffffffffu, mbar_wait_bounded(&bar, 0));
-    if (!staged && tid == 0) {
-        if (atomicCAS(&st->code, 0, 6) == 0) st->face = (int32_t)c0;
+    if (!__all_sync(0xffffffffu, mbar_wait_bounded(&bar, 0))) {
+        if (tid == 0) {
+            if (atomicCAS(&st->code, 0, 6) == 0) st->face = (int32_t)c0;
+        }
+        mbar_wait_bounded(&bar, 0);  // let the copy land before the CTA exits
+        return;
     }
     // two-level FP32 sums: runs of <= 64 faces, then the runs of the chunk;
     // the chunk partial goes out in FP64 and chunks are added in FP64
     float acc[PPT];
 #pragma unroll
     for (int j = 0; j < PPT; j++) acc[j] = 0.f;
-    if (live && staged) {
-        // pairs: the pair holding face n0 and those after it take the eclipse
-        // test (a never-eclipsed face in that pair has an empty range); faces
-        // past n in the last pair carry zero coefficients
-        const int64_t q0 = c0 >> 1, qend = (cend + 1) >> 1, qn0 = n0 >> 1;
-        const int64_t qa = qn0 < qend ? qn0 : qend;
-        sweep_pairs<PPT, LT, false>(sp, se, q0, q0, qa > q0 ? qa : q0, ex, ey, exy, pf, f.runb,
-                                    acc);
-        sweep_pairs<PPT, LT, true>(sp, se, q0, qa > q0 ? qa : q0, qend, ex, ey, exy, pf, f.runb,
-                                   acc);
+    sweep_chunk<PPT, LT>(f, sp, se, c0, cend, n0, ex, ey, exy, pf, acc);
+#pragma unroll
+    for (int j = 0; j < PPT; j++) {
+        const int64_t e = (int64_t)blockIdx.x * (kThreads * PPT) + tid * PPT + j;
+        if (e < ph.nent) part[(int64_t)blockIdx.y * ldp + e] = (double)acc[j];
     }
-    if constexpr (!CLUSTER) {
+}
+
+// The same sweep as a persistent pool: CTAs (a few per SM) take work units
+// (phase tile, group of G consecutive chunks) from the counter f.work, one
+// atomic per unit, and walk the group's chunks in order, each staged by TMA
+// into the same buffer, their FP32 chunk sums added into an FP64 row that is
+// written once per group. The rows are the chunk partials summed G at a time
+// in chunk order, whichever CTA ran the unit (deterministic), so the partials
+// that reach HBM, and the chunk reduction's reads, shrink G-fold; no CTA ever
+// waits for another, and units go to whichever CTA is free.
+template <int PPT, int LT>
+__global__ void __launch_bounds__(kThreads, (PPT <= 4) ? 3 : 2)
+    k_flux_fast_pool(FlatDev f, PhaseDev ph, int64_t chunk, int64_t ntile, int64_t group,
+                     int64_t nunit, double *part, int64_t ldp, DevStatus *st) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ uint64_t bar;
+    __shared__ int64_t s_unit;
+    const int tid = threadIdx.x;
+    const int64_t n = f.n, n0 = *f.n0;
+    const int64_t nchunk = (n + chunk - 1) / chunk;
+    float4 *sp = reinterpret_cast<float4 *>(smem);
+    ulonglong2 *se = reinterpret_cast<ulonglong2 *>(smem + chunk * 32);
+    if (tid == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    uint32_t parity = 0;
+    for (;;) {
+        if (tid == 0) s_unit = atomicAdd(f.work, 1);
+        __syncthreads();
+        const int64_t u = s_unit;
+        __syncthreads();  // every thread has the unit before s_unit is written again
+        if (u >= nunit) break;
+        const int64_t tile = u % ntile, grp = u / ntile;
+        float2 ex[PPT], ey[PPT];
+        float exy[PPT];
+        unsigned long long pf[PPT];
+        load_entries<PPT>(ph, tile, tid, ex, ey, exy, pf);
+        double row[PPT];
+#pragma unroll
+        for (int j = 0; j < PPT; j++) row[j] = 0.0;
+        const int64_t cb = grp * group, ce = (cb + group < nchunk) ? cb + group : nchunk;
+        for (int64_t c = cb; c < ce; c++) {
+            const int64_t c0 = c * chunk;
+            const int64_t cend = (c0 + chunk < n) ? c0 + chunk : n;
+            const bool need_ecl = cend > n0;
+            if (tid == 0) {
+                const uint32_t bytes =
+                    (uint32_t)(chunk * 32) + (need_ecl ? (uint32_t)(chunk * 16) : 0u);
+                mbar_arrive_expect_tx(&bar, bytes);
+                bulk_g2s(sp, f.fp + 8 * c0, (uint32_t)(chunk * 32), &bar);
+                if (need_ecl) bulk_g2s(se, f.ecl + c0, (uint32_t)(chunk * 16), &bar);
+            }
+            // a CTA-wide decision: every thread leaves the pool together if a
+            // copy does not arrive, after the copy has had its chance to land
+            if (__syncthreads_or(!mbar_wait_bounded(&bar, parity))) {
+                if (tid == 0) {
+                    if (atomicCAS(&st->code, 0, 6) == 0) st->face = (int32_t)c0;
+                }
+                mbar_wait_bounded(&bar, parity);
+                return;
+            }
+            parity ^= 1u;
+            float acc[PPT];
+#pragma unroll
+            for (int j = 0; j < PPT; j++) acc[j] = 0.f;
+            sweep_chunk<PPT, LT>(f, sp, se, c0, cend, n0, ex, ey, exy, pf, acc);
+#pragma unroll
+            for (int j = 0; j < PPT; j++) row[j] += (double)acc[j];
+            __syncthreads();  // the staging buffer is read by everyone before the next copy
+        }
 #pragma unroll
         for (int j = 0; j < PPT; j++) {
-            const int64_t e = (int64_t)blockIdx.x * (kThreads * PPT) + tid * PPT + j;
-            if (e < ph.nent) part[(int64_t)blockIdx.y * ldp + e] = (double)acc[j];
+            const int64_t e = tile * (kThreads * PPT) + tid * PPT + j;
+            if (e < ph.nent) part[grp * ldp + e] = row[j];
         }
-    } else {
-        __shared__ double red[PPT * kThreads];
-        cg::cluster_group cluster = cg::this_cluster();
-#pragma unroll
-        for (int j = 0; j < PPT; j++) red[j * kThreads + tid] = (double)acc[j];
-        cluster.sync();
-        if (cluster.block_rank() == 0) {
-            const unsigned G = cluster.num_blocks();
-            double o[PPT];
-#pragma unroll
-            for (int j = 0; j < PPT; j++) o[j] = 0.0;
-            for (unsigned r = 0; r < G; r++) {
-                const double *rr = cluster.map_shared_rank(red, r);
-#pragma unroll
-                for (int j = 0; j < PPT; j++) o[j] += rr[j * kThreads + tid];
-            }
-            const int64_t row = (int64_t)blockIdx.y / G;
-#pragma unroll
-            for (int j = 0; j < PPT; j++) {
-                const int64_t e = (int64_t)blockIdx.x * (kThreads * PPT) + tid * PPT + j;
-                if (e < ph.nent) part[row * ldp + e] = o[j];
-            }
-        }
-        cluster.sync();  // every rank's shared memory stays until rank 0 has read it
     }
-    if (live && !staged) mbar_wait_bounded(&bar, 0);  // let the copy land before the CTA exits
 }
 
 // The batched fast sweep: CTA w takes phase tile w % ntile of batch chunk
@@ -522,33 +577,24 @@ template <int PPT, int LT>
 void launch_fast_t(const FlatDev &f, const PhaseDev &ph, const FluxPlan &plan, double *part,
                    int64_t ldp, DevStatus *st, cudaStream_t s) {
     const size_t smem = (size_t)plan.chunk * 48;  // 32 B records + 16 B eclipse ranges
-    if (plan.group <= 1) {
-        auto kern = k_flux_fast<PPT, LT, false>;
+    if (plan.group <= 1 || !f.work) {
+        auto kern = k_flux_fast<PPT, LT>;
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         dim3 grid((unsigned)plan.ntile, (unsigned)plan.nchunk);
         kern<<<grid, kThreads, smem, s>>>(f, ph, plan.chunk, plan.ntile, part, ldp, st);
         count_launch();
         return;
     }
-    // the reduction's static shared memory (PPT x 256 doubles) comes on top of
-    // the staging buffer: opt in whatever the dynamic size, as the sum can pass
-    // the 48 KB default
-    auto kern = k_flux_fast<PPT, LT, true>;
+    auto kern = k_flux_fast_pool<PPT, LT>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)plan.ntile, (unsigned)(plan.rows() * plan.group));
-    cfg.blockDim = dim3(kThreads);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = 1;
-    attr[0].val.clusterDim.y = (unsigned)plan.group;
-    attr[0].val.clusterDim.z = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    int64_t chunk = plan.chunk, ntile = plan.ntile;
-    cudaLaunchKernelEx(&cfg, kern, f, ph, chunk, ntile, part, ldp, st);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem);
+    if (per_sm < 1) per_sm = 1;
+    const int64_t nunit = plan.ntile * plan.rows();
+    const int64_t nblk = std::min<int64_t>(nunit, (int64_t)per_sm * std::max(plan.nsm, 1));
+    cudaMemsetAsync(f.work, 0, sizeof(int32_t), s);
+    kern<<<(unsigned)nblk, kThreads, smem, s>>>(f, ph, plan.chunk, plan.ntile, plan.group, nunit,
+                                                part, ldp, st);
     count_launch();
 }
 
@@ -635,8 +681,11 @@ FluxPlan plan_flux(int mixed, int fast, int64_t nface, int64_t nent, int nsm) {
         p.chunk = 1024;  // FACE_BLOCK of comp_light_flat.cpp:239
     }
     p.nchunk = nface > 0 ? (nface + p.chunk - 1) / p.chunk : 0;
-    // the fast sweep adds up to 8 consecutive chunks in a thread-block cluster
-    if (p.fast) p.group = p.nchunk >= 32 ? 8 : p.nchunk >= 8 ? 4 : p.nchunk >= 4 ? 2 : 1;
+    p.nsm = nsm;
+    // the fast sweep's pool adds kGroup consecutive chunks into one partial row
+    // where there are enough units to keep every SM's CTAs busy
+    if (p.fast && p.ntile * ((p.nchunk + kGroup - 1) / kGroup) >= 8 * (int64_t)nsm)
+        p.group = kGroup;
     return p;
 }
 
