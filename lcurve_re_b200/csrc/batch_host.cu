@@ -248,7 +248,6 @@ lcg_status relayout(lcg_ctx *c, BatchState &B, const lcg_model *models, int32_t 
     // flux plan: the single-grid plan for entries per thread and phase tiles;
     // then the largest chunk (dividing 1024) that still fills the SMs
     B.plan = plan_flux(1, 1, B.nfaces, B.nent, c->nsm);
-    B.plan.group = 1;  // the batched sweep writes one partial row per chunk
     int64_t chunk = 1024, total = 0;
     const int64_t want = (int64_t)c->nsm * 4;
     for (;;) {

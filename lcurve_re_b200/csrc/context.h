@@ -91,7 +91,7 @@ struct Grid {
     cudaError_t alloc_flat(int mixed, int need_pos, int fast_on) {
         npad = ((n + 4095) / 4096) * 4096;
         if (npad == 0) npad = 4096;
-        cudaError_t e = n0.ensure(3);  // n0, n1, the mixed sweep's work counter
+        cudaError_t e = n0.ensure(2);  // n0, n1
         if (e) return e;
         if (disc && ((e = ridx.ensure(n)) || (e = rn.ensure(n)) || (e = rr.ensure(kRagRanges * n))))
             return e;
@@ -118,8 +118,7 @@ struct Grid {
     FlatDev flat() const {
         return FlatDev{n, npad, n0.p, geo.p, ecl.p, pos.p, fdx.p, fdy.p, fdz.p,
                        fpx.p, fpy.p, fpz.p, fflux.p, fin.p, fout.p, fp.p, runb.p,
-                       n0.p ? n0.p + 1 : nullptr, ridx.p, rr.p, rn.p,
-                       n0.p ? reinterpret_cast<int32_t *>(n0.p + 2) : nullptr};
+                       n0.p ? n0.p + 1 : nullptr, ridx.p, rr.p, rn.p};
     }
     void release() {
         DBuf<double> *d[] = {&px, &py, &pz, &nx, &ny, &nz, &ein, &eout, &fdx, &fdy,

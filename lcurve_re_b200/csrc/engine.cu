@@ -523,20 +523,20 @@ lcg_status sweep_one(lcg_ctx *c, const lcg_model &m, Grid &g, int star, double p
     const int mixed = c->precision == LCG_PREC_MIXED;
     if (mixed) launch_pack_phases(ph, c->stream);
     FluxPlan plan = plan_flux(mixed, g.fast, g.n, 1, c->nsm);
-    if ((err = c->part1f.ensure((size_t)std::max<int64_t>(plan.rows(), 1) * 4)))
+    if ((err = c->part1f.ensure((size_t)std::max<int64_t>(plan.nchunk, 1) * 4)))
         return c->cuda_fail(err, "partials");
     FluxConsts k = flux_consts(m, star, 1.0, rlens1);
     launch_flux(mixed, star, k, g.flat(), ph, plan, c->part1f.p, 4, c->status.p, c->stream);
     if (g.disc)
-        launch_flux_ragged(star, k, g.flat(), g.dev(), ph, plan.row_faces(), plan.rows(),
+        launch_flux_ragged(star, k, g.flat(), g.dev(), ph, plan.chunk, plan.nchunk,
                            c->part1f.p, 4, c->stream);
-    std::vector<double> col((size_t)std::max<int64_t>(plan.rows(), 1));
-    if (plan.rows())
-        cudaMemcpy2DAsync(col.data(), 8, c->part1f.p, 4 * 8, 8, (size_t)plan.rows(),
+    std::vector<double> col((size_t)std::max<int64_t>(plan.nchunk, 1));
+    if (plan.nchunk)
+        cudaMemcpy2DAsync(col.data(), 8, c->part1f.p, 4 * 8, 8, (size_t)plan.nchunk,
                           cudaMemcpyDeviceToHost, c->stream);
     if ((err = cudaStreamSynchronize(c->stream))) return c->cuda_fail(err, "sweep");
     sum = 0.0;
-    for (int64_t b = 0; b < plan.rows(); b++) sum += col[(size_t)b];
+    for (int64_t b = 0; b < plan.nchunk; b++) sum += col[(size_t)b];
     return LCG_OK;
 }
 
@@ -1105,7 +1105,7 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
         if (!use_sw[k]) continue;
         Sweep &s = sw[k];
         s.plan = plan_flux(mixed, s.g->fast, s.g->n, s.nent, c->nsm);
-        if ((e = s.part->ensure((size_t)std::max<int64_t>(s.plan.rows(), 1) * ldp)))
+        if ((e = s.part->ensure((size_t)std::max<int64_t>(s.plan.nchunk, 1) * ldp)))
             return c->cuda_fail(e, "flux partials");
         PhaseDev phk = ph;
         phk.nent = s.nent;
@@ -1115,8 +1115,8 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
         launch_flux(mixed, s.star, kc, s.g->flat(), phk, s.plan, s.part->p, ldp, c->status.p,
                     fs);
         if (s.g->disc)
-            launch_flux_ragged(s.star, kc, s.g->flat(), s.g->dev(), phk, s.plan.row_faces(),
-                               s.plan.rows(), s.part->p, ldp, fs);
+            launch_flux_ragged(s.star, kc, s.g->flat(), s.g->dev(), phk, s.plan.chunk,
+                               s.plan.nchunk, s.part->p, ldp, fs);
         c->flux_elements += s.g->n * s.nent;
     }
     if (conc) {
@@ -1153,7 +1153,7 @@ lcg_status lcg_light_curve_resident(lcg_ctx *c, const lcg_model *mp, int32_t fla
         rp.ldp = ldp;
         for (int k = 0; k < 4; k++) {
             rp.part[k] = use_sw[k] ? sw[k].part->p : nullptr;
-            rp.nchunk[k] = use_sw[k] ? sw[k].plan.rows() : 0;
+            rp.nchunk[k] = use_sw[k] ? sw[k].plan.nchunk : 0;
             rp.nent[k] = use_sw[k] ? sw[k].nent : 0;
             rp.osum[k] = c->osum.p + k * ldp;
         }
@@ -1439,7 +1439,7 @@ lcg_status lcg_sum_star_multi(lcg_ctx *c, int32_t star, int64_t n, int64_t n0, c
     k.rlens1 = rlens1;
     FluxPlan plan = plan_flux(mixed, 0, n, nent, c->nsm);
     const int64_t ldp = ((nent + 3) / 4) * 4;
-    if ((e = c->part1f.ensure((size_t)std::max<int64_t>(plan.rows(), 1) * std::max<int64_t>(ldp, 1))))
+    if ((e = c->part1f.ensure((size_t)std::max<int64_t>(plan.nchunk, 1) * std::max<int64_t>(ldp, 1))))
         return c->cuda_fail(e, "partials");
     cudaMemsetAsync(c->status.p, 0, sizeof(DevStatus), c->stream);
     {
@@ -1447,15 +1447,15 @@ lcg_status lcg_sum_star_multi(lcg_ctx *c, int32_t star, int64_t n, int64_t n0, c
         launch_flux(mixed, star, k, g.flat(), ph, plan, c->part1f.p, ldp, c->status.p, c->stream);
     }
     c->flux_elements += n * (int64_t)nent;
-    std::vector<double> part((size_t)plan.rows() * ldp);
-    if (plan.rows() && nent)
+    std::vector<double> part((size_t)plan.nchunk * ldp);
+    if (plan.nchunk && nent)
         cudaMemcpyAsync(part.data(), c->part1f.p, part.size() * 8, cudaMemcpyDeviceToHost,
                         c->stream);
     lcg_status rc = finish_status(c);
     if (rc) return rc;
     for (int32_t j = 0; j < nent; j++) {
         double o = 0.0;
-        for (int64_t b = 0; b < plan.rows(); b++) o += part[(size_t)b * ldp + j];
+        for (int64_t b = 0; b < plan.nchunk; b++) o += part[(size_t)b * ldp + j];
         out[j] = o;
     }
     return LCG_OK;

@@ -120,7 +120,6 @@ struct FlatDev {
     int32_t *ridx;
     double2 *rr;  // kRagRanges per ragged face
     uint8_t *rn;
-    int32_t *work;  // device counter: the fast sweep's next (tile, chunk group) unit
 };
 
 // Face records of the fast mixed sweep (no beaming, no lensing, mucrit <= 0):
@@ -317,11 +316,6 @@ struct FluxPlan {
     int64_t chunk;  // faces per CTA
     int64_t nchunk;
     int64_t ntile;  // phase tiles
-    int64_t group = 1;  // consecutive chunks summed into one partial row
-    int nsm = 0;        // SMs of the device (the persistent sweep's grid)
-    // partial rows the sweep writes, and the faces each row covers
-    int64_t rows() const { return group > 1 ? (nchunk + group - 1) / group : nchunk; }
-    int64_t row_faces() const { return chunk * group; }
 };
 FluxPlan plan_flux(int mixed, int fast, int64_t nface, int64_t nent, int nsm);
 void launch_flux(int mixed, int star, const FluxConsts &k, const FlatDev &f,

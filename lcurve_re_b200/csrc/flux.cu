@@ -18,8 +18,6 @@
 //  * eclipse test in 64-bit fixed-point phase: visible iff (phase - ingress)
 //    mod 2^64 >= width + 1 (ecl_fx64, geometry.cu), the reference's double
 //    comparisons decision for decision.
-#include <algorithm>
-
 #include "engine.h"
 #include "tma.cuh"
 
@@ -29,7 +27,6 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kFold = 64;  // LCG_MIXED_FOLD
-constexpr int kGroup = 4;  // chunks per work unit of the fast sweep's pool
 
 __device__ __forceinline__ float sqrt_approx(float x) {
     float r;
@@ -409,81 +406,6 @@ __global__ void __launch_bounds__(kThreads, (PPT <= 4) ? 3 : 2)
     }
 }
 
-// The same sweep as a persistent pool: CTAs (a few per SM) take work units
-// (phase tile, group of G consecutive chunks) from the counter f.work, one
-// atomic per unit, and walk the group's chunks in order, each staged by TMA
-// into the same buffer, their FP32 chunk sums added into an FP64 row that is
-// written once per group. The rows are the chunk partials summed G at a time
-// in chunk order, whichever CTA ran the unit (deterministic), so the partials
-// that reach HBM, and the chunk reduction's reads, shrink G-fold; no CTA ever
-// waits for another, and units go to whichever CTA is free.
-template <int PPT, int LT>
-__global__ void __launch_bounds__(kThreads, (PPT <= 4) ? 3 : 2)
-    k_flux_fast_pool(FlatDev f, PhaseDev ph, int64_t chunk, int64_t ntile, int64_t group,
-                     int64_t nunit, double *part, int64_t ldp, DevStatus *st) {
-    extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ uint64_t bar;
-    __shared__ int64_t s_unit;
-    const int tid = threadIdx.x;
-    const int64_t n = f.n, n0 = *f.n0;
-    const int64_t nchunk = (n + chunk - 1) / chunk;
-    float4 *sp = reinterpret_cast<float4 *>(smem);
-    ulonglong2 *se = reinterpret_cast<ulonglong2 *>(smem + chunk * 32);
-    if (tid == 0) mbar_init(&bar, 1);
-    __syncthreads();
-    uint32_t parity = 0;
-    for (;;) {
-        if (tid == 0) s_unit = atomicAdd(f.work, 1);
-        __syncthreads();
-        const int64_t u = s_unit;
-        __syncthreads();  // every thread has the unit before s_unit is written again
-        if (u >= nunit) break;
-        const int64_t tile = u % ntile, grp = u / ntile;
-        float2 ex[PPT], ey[PPT];
-        float exy[PPT];
-        unsigned long long pf[PPT];
-        load_entries<PPT>(ph, tile, tid, ex, ey, exy, pf);
-        double row[PPT];
-#pragma unroll
-        for (int j = 0; j < PPT; j++) row[j] = 0.0;
-        const int64_t cb = grp * group, ce = (cb + group < nchunk) ? cb + group : nchunk;
-        for (int64_t c = cb; c < ce; c++) {
-            const int64_t c0 = c * chunk;
-            const int64_t cend = (c0 + chunk < n) ? c0 + chunk : n;
-            const bool need_ecl = cend > n0;
-            if (tid == 0) {
-                const uint32_t bytes =
-                    (uint32_t)(chunk * 32) + (need_ecl ? (uint32_t)(chunk * 16) : 0u);
-                mbar_arrive_expect_tx(&bar, bytes);
-                bulk_g2s(sp, f.fp + 8 * c0, (uint32_t)(chunk * 32), &bar);
-                if (need_ecl) bulk_g2s(se, f.ecl + c0, (uint32_t)(chunk * 16), &bar);
-            }
-            // a CTA-wide decision: every thread leaves the pool together if a
-            // copy does not arrive, after the copy has had its chance to land
-            if (__syncthreads_or(!mbar_wait_bounded(&bar, parity))) {
-                if (tid == 0) {
-                    if (atomicCAS(&st->code, 0, 6) == 0) st->face = (int32_t)c0;
-                }
-                mbar_wait_bounded(&bar, parity);
-                return;
-            }
-            parity ^= 1u;
-            float acc[PPT];
-#pragma unroll
-            for (int j = 0; j < PPT; j++) acc[j] = 0.f;
-            sweep_chunk<PPT, LT>(f, sp, se, c0, cend, n0, ex, ey, exy, pf, acc);
-#pragma unroll
-            for (int j = 0; j < PPT; j++) row[j] += (double)acc[j];
-            __syncthreads();  // the staging buffer is read by everyone before the next copy
-        }
-#pragma unroll
-        for (int j = 0; j < PPT; j++) {
-            const int64_t e = tile * (kThreads * PPT) + tid * PPT + j;
-            if (e < ph.nent) part[grp * ldp + e] = row[j];
-        }
-    }
-}
-
 // The batched fast sweep: CTA w takes phase tile w % ntile of batch chunk
 // w / ntile; the chunk's slot gives its records, its model's phase row and
 // its limb-darkening law. Same per-element arithmetic and sums as
@@ -577,24 +499,10 @@ template <int PPT, int LT>
 void launch_fast_t(const FlatDev &f, const PhaseDev &ph, const FluxPlan &plan, double *part,
                    int64_t ldp, DevStatus *st, cudaStream_t s) {
     const size_t smem = (size_t)plan.chunk * 48;  // 32 B records + 16 B eclipse ranges
-    if (plan.group <= 1 || !f.work) {
-        auto kern = k_flux_fast<PPT, LT>;
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        dim3 grid((unsigned)plan.ntile, (unsigned)plan.nchunk);
-        kern<<<grid, kThreads, smem, s>>>(f, ph, plan.chunk, plan.ntile, part, ldp, st);
-        count_launch();
-        return;
-    }
-    auto kern = k_flux_fast_pool<PPT, LT>;
+    auto kern = k_flux_fast<PPT, LT>;
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads, smem);
-    if (per_sm < 1) per_sm = 1;
-    const int64_t nunit = plan.ntile * plan.rows();
-    const int64_t nblk = std::min<int64_t>(nunit, (int64_t)per_sm * std::max(plan.nsm, 1));
-    cudaMemsetAsync(f.work, 0, sizeof(int32_t), s);
-    kern<<<(unsigned)nblk, kThreads, smem, s>>>(f, ph, plan.chunk, plan.ntile, plan.group, nunit,
-                                                part, ldp, st);
+    dim3 grid((unsigned)plan.ntile, (unsigned)plan.nchunk);
+    kern<<<grid, kThreads, smem, s>>>(f, ph, plan.chunk, plan.ntile, part, ldp, st);
     count_launch();
 }
 
@@ -681,11 +589,6 @@ FluxPlan plan_flux(int mixed, int fast, int64_t nface, int64_t nent, int nsm) {
         p.chunk = 1024;  // FACE_BLOCK of comp_light_flat.cpp:239
     }
     p.nchunk = nface > 0 ? (nface + p.chunk - 1) / p.chunk : 0;
-    p.nsm = nsm;
-    // the fast sweep's pool adds kGroup consecutive chunks into one partial row
-    // where there are enough units to keep every SM's CTAs busy
-    if (p.fast && p.ntile * ((p.nchunk + kGroup - 1) / kGroup) >= 8 * (int64_t)nsm)
-        p.group = kGroup;
     return p;
 }
 
