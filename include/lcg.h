@@ -389,6 +389,19 @@ lcg_status lcg_mlp_gemm(void *stream, int32_t epi, int32_t m, int32_t n, int32_t
 lcg_status lcg_mlp_adam(void *stream, float *w, float *m1, float *m2, const float *g,
                         int32_t rows, int32_t cols, float lr, float beta1, float beta2,
                         float eps, int32_t step, void *w_bf16, void *wt_bf16);
+/* One Adam step on n <= 16 tensors in one launch (tensor j: FP32 weights
+ * w[j] [rows[j] x cols[j]], moments m1[j] and m2[j], gradient g[j]; BF16
+ * copy w_bf16[j] and BF16 transpose wt_bf16[j], either array or entry may
+ * be NULL). The host arrays hold device pointers. Learning rate and bias
+ * corrections come from device memory so that one captured graph serves
+ * every step: sched = {lr_max, lr_min, total_steps, beta1, beta2, eps}
+ * (FP32), step = the number of steps taken before this one (int32);
+ * lr = lr_min + (lr_max - lr_min) (1 + cos(pi step / total_steps)) / 2, or
+ * lr_max when total_steps <= 0. The caller advances *step. */
+lcg_status lcg_mlp_adam_all(void *stream, int32_t n, float *const *w, float *const *m1,
+                            float *const *m2, const float *const *g, const int32_t *rows,
+                            const int32_t *cols, void *const *w_bf16, void *const *wt_bf16,
+                            const float *sched, const int32_t *step);
 /* out[c] = sum over the first rvalid rows of the BF16 [rows x cols] g. */
 lcg_status lcg_mlp_colsum(void *stream, const void *g_bf16, int32_t rows, int32_t cols,
                           int32_t rvalid, float *out);
@@ -406,6 +419,38 @@ lcg_status lcg_mlp_input(void *stream, const float *x, int32_t kin, const float 
 /* dw[n x kin] = g^T x over the first mvalid rows (g BF16 [m x n], x FP32). */
 lcg_status lcg_mlp_input_grad(void *stream, const void *g_bf16, const float *x, int32_t kin,
                               int32_t m, int32_t n, int32_t mvalid, float *dw);
+/* The whole network nin -> (depth - 1) x 256 GELU -> nout (linear) for m
+ * rows (a multiple of 128) in one launch, one CTA per 128 rows, activations
+ * kept on chip between layers:
+ *   layer 0 in FP32 on the CUDA cores from x [m x kin] (kin <= 16), w0
+ *   [256 x kin], b0 [256] (rows >= mvalid are zero); layers 1..depth from
+ *   the BF16 weights w_bf16[l - 1] ([256 x 256], the last [nout x 256]) and
+ *   FP32 biases bias[l - 1] on the tensor cores; out [mvalid x nout] FP32.
+ * Training (z non-NULL): stores the BF16 pre-activations z[l] [m x 256] and
+ * transposed activations yt[l] [256 x ldt] of layers 0..depth-1 (ldt >= m,
+ * a multiple of 8). With target [m x nout] (FP32) also the gradient of the
+ * mean squared error over the first mvalid rows, 2 (out - target) /
+ * (mvalid nout), as BF16 g [m x nout] and its transpose gt [nout x ldt],
+ * and per-row squared-error sums loss_rows [m] (may be NULL). depth <= 5,
+ * nout a multiple of 64 up to 256; host arrays of device pointers; vector
+ * stores need 16-byte aligned out, g, z and yt. *err (may be NULL) is set
+ * if a pipeline wait timed out. */
+lcg_status lcg_mlp_forward(void *stream, const float *x, int32_t kin, int32_t m, int32_t mvalid,
+                           const float *w0, const float *b0, int32_t depth, int32_t nout,
+                           const void *const *w_bf16, const float *const *bias, float *out,
+                           void *const *z, void *const *yt, int32_t ldt, const float *target,
+                           void *g, void *gt, float *loss_rows, int32_t *err);
+/* The backward chain of the same network in one launch: from the output
+ * gradient g_out [m x nout] (BF16), for j = 0..depth-1 the gradient of
+ * layer depth-1-j, g[j] = (g_prev * W) * GELU'(z[j]) with wt_bf16[j] the
+ * BF16 transpose of layer depth-j's weights ([256 x nout] for j = 0, then
+ * [256 x 256]) and z[j] that layer's stored pre-activation [m x 256];
+ * stores g[j] [m x 256] and, where gt and gt[j] are non-NULL, its transpose
+ * [256 x ldt]. */
+lcg_status lcg_mlp_backward_data(void *stream, int32_t m, int32_t depth, int32_t nout,
+                                 const void *g_out, const void *const *wt_bf16,
+                                 const void *const *z, void *const *g, void *const *gt,
+                                 int32_t ldt, int32_t *err);
 /* Per row r of coef [m x ncoef]: the surrogate curve s(c) = mean + c * basis
  * (basis [ncoef x npts]) at the data points, or, with an anchor (exact curves
  * [m x npts] at the points coef_x [m x ncoef] describes), the anchored curve

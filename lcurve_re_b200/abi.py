@@ -124,6 +124,11 @@ PROTOTYPES = {
                                P, P, C.c_int32, C.c_int32, P]),
     "lcg_mlp_adam": (C.c_int, [P, P, P, P, P, C.c_int32, C.c_int32, C.c_float, C.c_float,
                                C.c_float, C.c_float, C.c_int32, P, P]),
+    "lcg_mlp_adam_all": (C.c_int, [P, C.c_int32, P, P, P, P, P, P, P, P, P, P]),
+    "lcg_mlp_forward": (C.c_int, [P, P, C.c_int32, C.c_int32, C.c_int32, P, P, C.c_int32,
+                                  C.c_int32, P, P, P, P, P, C.c_int32, P, P, P, P, P]),
+    "lcg_mlp_backward_data": (C.c_int, [P, C.c_int32, C.c_int32, C.c_int32, P, P, P, P, P,
+                                        C.c_int32, P]),
     "lcg_mlp_colsum": (C.c_int, [P, P, C.c_int32, C.c_int32, C.c_int32, P]),
     "lcg_mlp_input": (C.c_int, [P, P, C.c_int32, P, P, C.c_int32, C.c_int32, C.c_int32, P, P,
                                 P, C.c_int32]),

@@ -32,10 +32,11 @@ SOURCES = {
     "noalloc.cu": ["--fmad=false"],
     "batch_host.cu": ["--fmad=false"],
     "mlp.cu": ["--fmad=true"],
+    "mlp_chain.cu": ["--fmad=true"],
     "components.cu": ["--fmad=false"],
 }
 HEADERS = ["roche.cuh", "eclipse.cuh", "disc.cuh", "ecl_screen.cuh", "engine.h", "tma.cuh",
-           "context.h", "fixed_phase.cuh"]
+           "context.h", "fixed_phase.cuh", "mlp_tc.cuh"]
 
 
 def nvcc():

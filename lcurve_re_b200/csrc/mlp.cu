@@ -30,13 +30,13 @@
 
 #include "engine.h"
 #include "lcg.h"
+#include "mlp_tc.cuh"
 #include "tma.cuh"
 
 namespace lcg {
 namespace {
 
-constexpr int kBM = 128, kBK = 64;
-enum { kEpiGelu = 0, kEpiLinear = 1, kEpiDGelu = 2, kEpiF32 = 3 };
+using namespace mlp;
 
 struct GemmOut {
     const float *bias;   // [N] or NULL
@@ -47,68 +47,6 @@ struct GemmOut {
     int32_t n, mvalid, ldt;
     int32_t *err;
 };
-
-__device__ __forceinline__ uint64_t desc_sw128(uint32_t saddr) {
-    // start address >> 4, LBO 16 B (unused for swizzled K-major), SBO 1024 B
-    // (8 rows of 128 B), version 1, layout SWIZZLE_128B
-    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)64 << 32) |
-           ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
-}
-
-__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, int x, int y,
-                                            uint64_t *bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
-        "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
-        : "memory");
-}
-
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
-                                         uint32_t idesc, uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
-        : "memory");
-}
-
-__device__ __forceinline__ void mma_commit(uint64_t *bar) {
-    asm volatile(
-        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-            smem_u32(bar))
-        : "memory");
-}
-
-__device__ __forceinline__ void fence_before_sync() {
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void fence_after_sync() {
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
-        "%11, %12, %13, %14, %15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
-          "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
-}
-
-__device__ __forceinline__ float gelu(float z) {
-    return 0.5f * z * (1.f + erff(z * 0.70710678118654752f));
-}
-__device__ __forceinline__ float gelu_grad(float z) {
-    return 0.5f * (1.f + erff(z * 0.70710678118654752f)) +
-           z * expf(-0.5f * z * z) * 0.39894228040143268f;
-}
 
 template <int BN, int EPI>
 __global__ void __launch_bounds__(128) k_gemm(const __grid_constant__ CUtensorMap ta,
@@ -300,14 +238,70 @@ __global__ void k_adam(float *w, float *m, float *v, const float *g, int32_t row
     }
 }
 
-// Column sums of a BF16 [rows x cols] matrix (bias gradients), FP32.
+// Column sums of a BF16 [rows x cols] matrix (bias gradients), FP32: a
+// block of 32 columns x 32 row groups, each thread summing rows ty, ty + 32,
+// ... in order, then a fixed-order tree over the groups (deterministic).
 __global__ void k_colsum(const __nv_bfloat16 *g, int32_t rows, int32_t cols, int32_t rvalid,
                          float *out) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= cols) return;
+    __shared__ float sh[32][33];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int c = blockIdx.x * 32 + tx;
     float s = 0.f;
-    for (int r = 0; r < rvalid; r++) s += __bfloat162float(g[(size_t)r * cols + c]);
-    out[c] = s;
+    if (c < cols)
+        for (int r = ty; r < rvalid; r += 32) s += __bfloat162float(g[(size_t)r * cols + c]);
+    sh[ty][tx] = s;
+    __syncthreads();
+    for (int w = 16; w > 0; w >>= 1) {
+        if (ty < w) sh[ty][tx] += sh[ty + w][tx];
+        __syncthreads();
+    }
+    if (ty == 0 && c < cols) out[c] = sh[0][tx];
+}
+
+// One Adam step over up to kAdamMax tensors in one launch. The learning
+// rate follows a cosine schedule read from device memory together with the
+// number of steps taken, so a captured graph serves every step:
+//   sched = {lr_max, lr_min, total_steps, beta1, beta2, eps}
+//   lr(k) = lr_min + (lr_max - lr_min) (1 + cos(pi k / total)) / 2
+//           (lr_max when total <= 0), bias corrections 1 - beta^(k + 1).
+constexpr int kAdamMax = 16;
+struct AdamSet {
+    float *w[kAdamMax], *m1[kAdamMax], *m2[kAdamMax];
+    const float *g[kAdamMax];
+    __nv_bfloat16 *wb[kAdamMax], *wt[kAdamMax];
+    int32_t rows[kAdamMax], cols[kAdamMax];
+    int64_t start[kAdamMax + 1];
+    int32_t n;
+};
+
+__global__ void k_adam_all(const __grid_constant__ AdamSet a, const float *sched,
+                           const int32_t *step) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= a.start[a.n]) return;
+    int j = 0;
+    while (i >= a.start[j + 1]) j++;
+    const int64_t e = i - a.start[j];
+    const int k = *step;
+    const float lr_max = sched[0], lr_min = sched[1], total = sched[2];
+    const float b1 = sched[3], b2 = sched[4], eps = sched[5];
+    const float lr = total > 0.f
+                         ? lr_min + 0.5f * (lr_max - lr_min) *
+                                        (1.f + cosf(3.14159265358979f * (float)k / total))
+                         : lr_max;
+    const float c1 = 1.f - powf(b1, (float)(k + 1)), c2 = 1.f - powf(b2, (float)(k + 1));
+    const float gi = a.g[j][e];
+    const float mi = b1 * a.m1[j][e] + (1.f - b1) * gi;
+    const float vi = b2 * a.m2[j][e] + (1.f - b2) * gi * gi;
+    a.m1[j][e] = mi;
+    a.m2[j][e] = vi;
+    const float wi = a.w[j][e] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    a.w[j][e] = wi;
+    const __nv_bfloat16 b = __float2bfloat16_rn(wi);
+    if (a.wb[j]) a.wb[j][e] = b;
+    if (a.wt[j]) {
+        const int64_t r = e / a.cols[j], c = e % a.cols[j];
+        a.wt[j][c * a.rows[j] + r] = b;
+    }
 }
 
 // Mean-squared-error gradient of out [rows x cols] against target, scaled by
@@ -450,6 +444,10 @@ __global__ void k_pca_chisq(const float *coef, int32_t ncoef, const float *basis
     }
 }
 
+}  // namespace
+
+namespace mlp {
+namespace {
 using EncodeFn = PFN_cuTensorMapEncodeTiled_v12000;
 
 EncodeFn encode_fn() {
@@ -466,8 +464,8 @@ EncodeFn encode_fn() {
     return fn;
 }
 
-// Row-major BF16 [rows x cols] with a box of 64 columns x box_rows rows,
-// 128-byte swizzle.
+}  // namespace
+
 bool make_map(CUtensorMap *map, const void *base, int32_t rows, int32_t cols, int32_t box_rows) {
     EncodeFn fn = encode_fn();
     if (!fn) return false;
@@ -480,6 +478,10 @@ bool make_map(CUtensorMap *map, const void *base, int32_t rows, int32_t cols, in
               CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
+
+}  // namespace mlp
+
+namespace {
 
 template <int BN, int EPI>
 cudaError_t launch_gemm_t(const CUtensorMap &ta, const CUtensorMap &tb, int m, int n, int k,
@@ -567,10 +569,39 @@ lcg_status lcg_mlp_adam(void *stream, float *w, float *m1, float *m2, const floa
     return cudaGetLastError() == cudaSuccess ? LCG_OK : LCG_E_CUDA;
 }
 
+lcg_status lcg_mlp_adam_all(void *stream, int32_t n, float *const *w, float *const *m1,
+                            float *const *m2, const float *const *g, const int32_t *rows,
+                            const int32_t *cols, void *const *w_bf16, void *const *wt_bf16,
+                            const float *sched, const int32_t *step) {
+    if (n <= 0 || n > kAdamMax || !w || !m1 || !m2 || !g || !rows || !cols || !sched || !step)
+        return LCG_E_INVALID;
+    AdamSet a;
+    memset(&a, 0, sizeof(a));
+    a.n = n;
+    a.start[0] = 0;
+    for (int j = 0; j < n; j++) {
+        if (!w[j] || !m1[j] || !m2[j] || !g[j] || rows[j] <= 0 || cols[j] <= 0)
+            return LCG_E_INVALID;
+        a.w[j] = w[j];
+        a.m1[j] = m1[j];
+        a.m2[j] = m2[j];
+        a.g[j] = g[j];
+        a.wb[j] = w_bf16 ? (__nv_bfloat16 *)w_bf16[j] : nullptr;
+        a.wt[j] = wt_bf16 ? (__nv_bfloat16 *)wt_bf16[j] : nullptr;
+        a.rows[j] = rows[j];
+        a.cols[j] = cols[j];
+        a.start[j + 1] = a.start[j] + (int64_t)rows[j] * cols[j];
+    }
+    k_adam_all<<<(unsigned)((a.start[n] + 255) / 256), 256, 0, (cudaStream_t)stream>>>(a, sched,
+                                                                                       step);
+    count_launch();
+    return cudaGetLastError() == cudaSuccess ? LCG_OK : LCG_E_CUDA;
+}
+
 lcg_status lcg_mlp_colsum(void *stream, const void *g_bf16, int32_t rows, int32_t cols,
                           int32_t rvalid, float *out) {
     if (!g_bf16 || !out || rows <= 0 || cols <= 0 || rvalid > rows) return LCG_E_INVALID;
-    k_colsum<<<(unsigned)((cols + 127) / 128), 128, 0, (cudaStream_t)stream>>>(
+    k_colsum<<<(unsigned)((cols + 31) / 32), dim3(32, 32), 0, (cudaStream_t)stream>>>(
         (const __nv_bfloat16 *)g_bf16, rows, cols, rvalid, out);
     count_launch();
     return cudaGetLastError() == cudaSuccess ? LCG_OK : LCG_E_CUDA;

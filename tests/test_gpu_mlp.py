@@ -201,3 +201,171 @@ def test_inference_on_the_rows_present_matches_the_full_batch():
     for n in (1, 130, 512):
         part = net.forward(x[:n]).clone()
         torch.testing.assert_close(part, full[:n], rtol=1e-5, atol=1e-6)
+
+
+@pytest.mark.parametrize("m,n,k,dtype", [(300, 200, 1000, "float64"), (1000, 1000, 5000, "float64"),
+                                         (777, 64, 130, "float32"), (256, 192, 20000, "float64")])
+def test_split_bf16_gemm_reaches_fp32_accuracy(m, n, k, dtype):
+    """gemm_bf16x3 (three BF16 products on lcg_mlp_gemm, K blocks of 8192
+    summed in FP64) against the FP64 product: every entry within 3e-5 of the
+    largest |a| |b|^T entry, which one BF16 product (about 4e-3) misses by
+    two orders of magnitude."""
+    import torch
+    from lcurve_re_b200.mlp import gemm_bf16x3
+    g = torch.Generator(device="cuda").manual_seed(m + n + k)
+    dt = getattr(torch, dtype)
+    a = torch.randn(m, k, device="cuda", generator=g, dtype=torch.float64).to(dt)
+    b = torch.randn(n, k, device="cuda", generator=g, dtype=torch.float64).to(dt)
+    ref = a.double() @ b.double().T
+    bound = (a.double().abs() @ b.double().abs().T).max().item()
+    out = gemm_bf16x3(a, b)
+    torch.cuda.synchronize()
+    assert out.shape == (m, n) and out.dtype == torch.float64
+    err = (out - ref).abs().max().item() / bound
+    assert err <= 3e-5, err
+    one = (a.to(torch.bfloat16).double() @ b.to(torch.bfloat16).double().T - ref).abs().max()
+    assert one.item() / bound > 100 * err
+
+
+def test_pca_on_the_tensor_cores_matches_fp64():
+    """Surrogate.fit_pca (Gram matrix, coefficients and reconstruction on
+    gemm_bf16x3) against the same PCA in FP64 torch on curves of 64 modes
+    (amplitudes 1e-2 .. 1e-4) plus a 16-mode tail (1e-5) and noise, so the
+    retained subspace is well determined: its principal angles' cosines
+    >= 1 - 1e-5 (the Gram matrix carries FP32 rounding, about 1e-7 of its
+    largest eigenvalue, against a gap of 1e-4 of it at the cut: angles up to
+    ~1e-3), the reconstruction residual's maximum within 10% of the FP64 one,
+    and the coefficients within 1e-5 of their largest magnitude."""
+    import torch
+    from lcurve_re_b200.surrogate import Surrogate
+    rng = np.random.default_rng(5)
+    n, npts = 20000, 1000
+    amp = np.r_[np.logspace(-2, -4, 64), np.logspace(-5, -5.5, 16)]
+    modes = rng.standard_normal((80, npts)) * amp[:, None]
+    curves = 1.0 + rng.standard_normal((n, 80)) @ modes + 1e-7 * rng.standard_normal((n, npts))
+    sur = Surrogate(batch=256)
+    err, target = sur.fit_pca(curves)
+    y = torch.as_tensor(curves, device="cuda")
+    yc = y - y.mean(0)
+    ev, V = torch.linalg.eigh(yc.T @ yc / n)
+    basis = V[:, torch.argsort(ev, descending=True)[:sur.ncoef]].T
+    ref_err = float((yc - (yc @ basis.T) @ basis).abs().max())
+    cos = torch.linalg.svdvals(sur.basis @ basis.T)
+    assert float(cos.min()) >= 1 - 1e-5, float(cos.min())
+    assert abs(err - ref_err) <= 0.1 * ref_err, (err, ref_err)
+    coef_ref = (yc @ sur.basis.T) / sur.cscale
+    assert float((target - coef_ref).abs().max()) <= 1e-5 * float(coef_ref.abs().max())
+
+
+def _bits_close(a, b, what):
+    """BF16 tensors equal up to one rounding step of BF16 (the one-launch
+    chain and the per-layer kernels may round a product sum differently in
+    the last FP32 bit)."""
+    import torch
+    a, b = a.float(), b.float()
+    tol = 2 ** -7 * torch.maximum(a.abs(), b.abs()) + 1e-30
+    bad = int(((a - b).abs() > tol).sum())
+    assert bad == 0, (what, bad)
+
+
+@pytest.mark.parametrize("n", [1, 130, 512, 1024])
+def test_fused_forward_matches_the_layer_by_layer_kernels(n):
+    """lcg_mlp_forward (all layers in one launch) against lcg_mlp_input +
+    lcg_mlp_gemm per layer on the same weights: inference outputs within
+    1e-5 relative, and in training the stored pre-activations and
+    transposed activations of every layer within one BF16 rounding."""
+    import torch
+    from lcurve_re_b200.mlp import MLP
+    net = MLP(nin=9, nout=64, batch=1024, seed=11)
+    for l in range(1, net.depth + 1):  # non-zero biases
+        net.b[l].copy_(0.1 * torch.randn_like(net.b[l]))
+    x = torch.rand(n, 9, device="cuda") * 2 - 1
+    fused = net.forward(x).clone()
+    net.fused = False
+    ref = net.forward(x).clone()
+    torch.testing.assert_close(fused, ref, rtol=1e-5, atol=1e-5 * float(ref.abs().max()))
+    if n == 1024:
+        net.forward(x, train=True)
+        ref_z = [z.clone() for z in net.Z]
+        ref_yt = [y.clone() for y in net.Yt]
+        ref_out = net.out.clone()
+        net.fused = True
+        net.forward(x, train=True)
+        for l in range(net.depth):
+            _bits_close(net.Z[l], ref_z[l], ("z", l))
+            _bits_close(net.Yt[l], ref_yt[l], ("yt", l))
+        torch.testing.assert_close(net.out, ref_out, rtol=1e-5,
+                                   atol=1e-5 * float(ref_out.abs().max()))
+
+
+def test_fused_backward_matches_the_layer_by_layer_kernels():
+    """Forward with the fused loss gradient + lcg_mlp_backward_data against
+    lcg_mlp_mse_grad + one GEMM per layer: every layer's gradient (and its
+    transpose) within one BF16 rounding, weight and bias gradients within
+    1e-3 of their largest entry, the same loss to 1e-6."""
+    import torch
+    from lcurve_re_b200.mlp import MLP
+    net = MLP(nin=9, nout=64, batch=512, seed=12)
+    x = torch.rand(512, 9, device="cuda") * 2 - 1
+    t = torch.randn(512, 64, device="cuda").contiguous()
+    net.fused = False
+    net.forward(x, train=True)
+    loss_ref = net.backward(t)
+    G = [g.clone() for g in net.G]
+    Gt = [g.clone() for g in net.Gt]
+    dW = [d.clone() for d in net.dW]
+    db = [d.clone() for d in net.db]
+    net.fused = True
+    net.x.copy_(x)
+    net.tgt.copy_(t)
+    net.forward(net.x, train=True, target=net.tgt)
+    loss = net.backward()
+    net.check()
+    assert abs(loss - loss_ref) <= 1e-6 * loss_ref
+    for l in range(net.depth + 1):
+        _bits_close(net.G[l], G[l], ("g", l))
+        if l >= 1:
+            _bits_close(net.Gt[l], Gt[l], ("gt", l))
+        tol = 1e-3 * float(dW[l].abs().max())
+        assert float((net.dW[l] - dW[l]).abs().max()) <= tol, ("dW", l)
+        assert float((net.db[l] - db[l]).abs().max()) <= 1e-3 * float(db[l].abs().max()), l
+
+
+def test_graph_training_steps_follow_the_eager_steps():
+    """graph_step (one captured graph: fused chains, weight gradients and
+    the one-launch Adam on the device-side cosine schedule) against eager
+    forward/backward/step with the same learning rates: weights within 1e-4
+    relative after 20 steps, and the loss falls over 300 steps."""
+    import torch
+    from lcurve_re_b200.mlp import MLP
+    g = torch.Generator(device="cuda").manual_seed(0)
+    x = torch.rand(1024, 9, device="cuda", generator=g) * 2 - 1
+    proj = torch.randn(9, 64, device="cuda", generator=g)
+    t = torch.sin(2 * x @ proj).contiguous()
+    a, b = MLP(batch=1024, seed=5), MLP(batch=1024, seed=5)
+    total, lr, lr_min = 20, 2e-3, 2e-4
+    b.set_schedule(lr, lr_min, total)
+    for k in range(total):
+        a.forward(x, train=True)
+        a.backward(t)
+        a.step(lr_min + 0.5 * (lr - lr_min) * (1 + np.cos(np.pi * k / total)))
+        b.x.copy_(x)
+        b.tgt.copy_(t)
+        b.graph_step()
+    torch.cuda.synchronize()
+    a.check()
+    b.check()
+    assert int(b.step_dev.item()) == total
+    for l in range(a.depth + 1):
+        rel = float((a.W[l] - b.W[l]).norm() / a.W[l].norm())
+        assert rel <= 1e-4, (l, rel)
+    b.set_schedule(1e-3)
+    first = None
+    for k in range(300):
+        b.graph_step()
+        if k == 0:
+            first = b.take_loss()
+    b.take_loss()
+    b.graph_step()
+    last = b.take_loss()
+    assert last < 0.1 * first, (first, last)
