@@ -1,6 +1,9 @@
 """Random-walk Metropolis over many parallel chains, plain or with delayed
 acceptance screened by a surrogate; the effective-sample-size estimator of
 the reference sampler and the rank-normalised multi-chain ESS and R-hat.
+Proposals: the Gaussian walk with one covariance (GaussianWalk), or the same
+walk in coordinates that straighten a curved posterior ridge
+(TriangularWalk, a volume-preserving map fitted to a posterior sample).
 
 The likelihood is exp(-chi**2 / 2) with chi**2 from a callable over a batch
 of parameter vectors (one row per chain): the exact GPU engine
@@ -19,6 +22,7 @@ fetches just the rows it needs from the engine). Chains whose proposal the
 approximation rejects pass the engine the model it evaluated for them last,
 so the batched engine skips them entirely.
 """
+import copy
 import time
 
 import numpy as np
@@ -297,8 +301,92 @@ class CompactExact:
         return res
 
 
-def _proposal(rng, theta, chol):
-    return theta + rng.standard_normal(theta.shape) @ chol.T
+class GaussianWalk:
+    """The random-walk proposal y = x + N(0, cov)."""
+
+    def __init__(self, cov):
+        self.chol = np.linalg.cholesky(cov)
+
+    def __call__(self, rng, theta):
+        return theta + rng.standard_normal(theta.shape) @ self.chol.T
+
+
+def _quadratic_features(z):
+    """[n x (1 + k + k (k + 1) / 2)]: 1, z_i, z_i z_j (i <= j) of z [n x k]."""
+    n, k = z.shape
+    cols = [np.ones(n)] + [z[:, i] for i in range(k)]
+    cols += [z[:, i] * z[:, j] for i in range(k) for j in range(i, k)]
+    return np.stack(cols, axis=1)
+
+
+class TriangularWalk:
+    """Gaussian random walk in coordinates that straighten a curved
+    posterior ridge. With z = (x - m) / s standardised on a sample of the
+    posterior, u_1 = z_1 and u_k = z_k - P_k(z_1 .. z_{k-1}), P_k the
+    least-squares quadratic in the earlier coordinates (a triangular map
+    with unit diagonal: Jacobian determinant 1, inverted coordinate by
+    coordinate). The proposal y = T^-1(T(x) + N(0, scale^2 2.38^2 / d
+    cov(u))) is therefore symmetric in x, so Metropolis and delayed
+    acceptance use it with the plain ratio pi(y) / pi(x). A random walk with
+    one global covariance is limited to steps of a curved ridge's local
+    width; in u the ridge is straight and its spread is the covariance."""
+
+    def __init__(self, sample, scale=1.0):
+        sample = np.asarray(sample, np.float64)
+        self.m = sample.mean(0)
+        self.s = sample.std(0)
+        self.s[self.s == 0] = 1.0
+        z = (sample - self.m) / self.s
+        self.d = d = z.shape[1]
+        self.coef = [None] + [np.linalg.lstsq(_quadratic_features(z[:, :k]), z[:, k],
+                                              rcond=None)[0] for k in range(1, d)]
+        u = self._forward_z(z)
+        self.mean_u = u.mean(0)
+        self.cov_u = np.cov(u.T)
+        self.set_scale(scale)
+
+    def set_scale(self, scale):
+        self.scale = scale
+        self.chol = np.linalg.cholesky(self.cov_u * (scale * 2.38) ** 2 / self.d)
+        return self
+
+    def with_scale(self, scale):
+        """A copy with another step scale (the map is shared)."""
+        return copy.copy(self).set_scale(scale)
+
+    def _forward_z(self, z):
+        u = z.copy()
+        for k in range(1, self.d):
+            u[:, k] = z[:, k] - _quadratic_features(z[:, :k]) @ self.coef[k]
+        return u
+
+    def forward(self, x):
+        return self._forward_z((np.asarray(x, np.float64) - self.m) / self.s)
+
+    def inverse(self, u):
+        z = np.array(u, np.float64)
+        for k in range(1, self.d):
+            z[:, k] = u[:, k] + _quadratic_features(z[:, :k]) @ self.coef[k]
+        return self.m + z * self.s
+
+    def draws(self, n, widen=1.0, seed=0, box_check=None):
+        """n parameter vectors along the fitted posterior: u Gaussian with the
+        sample's mean and widen^2 x its covariance, mapped back (the curved
+        ridge's shape, widened across and along it); with box_check, redrawn
+        until n lie inside."""
+        rng = np.random.default_rng(seed)
+        L = np.linalg.cholesky(self.cov_u) * widen
+        out = np.empty((0, self.d))
+        while len(out) < n:
+            x = self.inverse(self.mean_u + rng.standard_normal((2 * n, self.d)) @ L.T)
+            if box_check is not None:
+                x = x[box_check(x)]
+            out = np.r_[out, x]
+        return out[:n]
+
+    def __call__(self, rng, theta):
+        u = self.forward(theta)
+        return self.inverse(u + rng.standard_normal(u.shape) @ self.chol.T)
 
 
 def _take(x, idx):
@@ -317,7 +405,7 @@ def _put(dst, idx, src):
         dst[torch.as_tensor(idx, device=dst.device)] = src
 
 
-def _delayed_acceptance_device(exact, sur, theta0, cov, steps, seed, box_check, record):
+def _delayed_acceptance_device(exact, sur, theta0, propose, steps, seed, box_check, record):
     """delayed_acceptance with the anchored surrogate kept on the device: the
     exact curves of every chain are copied from the engine in one device
     copy, the screening and reverse chi**2 run over all chains (no index
@@ -326,7 +414,6 @@ def _delayed_acceptance_device(exact, sur, theta0, cov, steps, seed, box_check, 
     torch = sur.torch
     dev = sur.sur.dev
     rng = np.random.default_rng(seed)
-    chol = np.linalg.cholesky(cov)
     theta = np.array(theta0, np.float64)
     nc = theta.shape[0]
     chi = exact(theta)
@@ -339,7 +426,7 @@ def _delayed_acceptance_device(exact, sur, theta0, cov, steps, seed, box_check, 
     acc = stage1 = 0
     t0 = time.perf_counter()
     for s in range(steps):
-        prop = _proposal(rng, theta, chol)
+        prop = propose(rng, theta)
         ok = box_check(prop)
         sy = sur.state(prop)
         chi_a = sur.chi2(sy, sx, f)  # chi**2 of exact(x) s(y) / s(x)
@@ -373,7 +460,7 @@ def _delayed_acceptance_device(exact, sur, theta0, cov, steps, seed, box_check, 
                                               "stage2_rate": acc / max(stage1, 1)}
 
 
-def _delayed_acceptance_graphs(exact, sur, theta0, cov, steps, seed, box_check, record,
+def _delayed_acceptance_graphs(exact, sur, theta0, propose, steps, seed, box_check, record,
                                compact=None):
     """The device loop with the surrogate's two per-step passes replayed as
     CUDA graphs on static buffers (sur.bind): one launch each instead of the
@@ -382,7 +469,6 @@ def _delayed_acceptance_graphs(exact, sur, theta0, cov, steps, seed, box_check, 
     stage-1 chains' exact evaluations go through its small batch."""
     import torch
     rng = np.random.default_rng(seed)
-    chol = np.linalg.cholesky(cov)
     theta = np.array(theta0, np.float64)
     nc = theta.shape[0]
     chi = exact(theta)
@@ -394,7 +480,7 @@ def _delayed_acceptance_graphs(exact, sur, theta0, cov, steps, seed, box_check, 
     acc = stage1 = 0
     t0 = time.perf_counter()
     for s in range(steps):
-        prop = _proposal(rng, theta, chol)
+        prop = propose(rng, theta)
         ok = box_check(prop)
         chi_a = sur.screen(prop)  # chi**2 of exact(x) s(y) / s(x)
         chi_a[~ok] = np.inf
@@ -430,12 +516,14 @@ def _delayed_acceptance_graphs(exact, sur, theta0, cov, steps, seed, box_check, 
                                               "stage2_rate": acc / max(stage1, 1)}
 
 
-def metropolis(exact, theta0, cov, steps, seed=0, box_check=in_box, record=True):
-    """Plain random-walk Metropolis on every chain at once. Returns
-    (chain [steps x chains x params] or None, final theta, final chi**2,
-    acceptance rate, wall seconds)."""
+def metropolis(exact, theta0, cov, steps, seed=0, box_check=in_box, record=True,
+               propose=None):
+    """Plain Metropolis on every chain at once, with the Gaussian random walk
+    of covariance cov or another symmetric proposal (propose(rng, theta) ->
+    proposals, e.g. TriangularWalk). Returns (chain [steps x chains x params]
+    or None, final theta, final chi**2, acceptance rate, wall seconds)."""
     rng = np.random.default_rng(seed)
-    chol = np.linalg.cholesky(cov)
+    propose = propose or GaussianWalk(cov)
     theta = np.array(theta0, np.float64)
     chi = exact(theta)
     last = theta.copy()
@@ -443,7 +531,7 @@ def metropolis(exact, theta0, cov, steps, seed=0, box_check=in_box, record=True)
     acc = 0
     t0 = time.perf_counter()
     for s in range(steps):
-        prop = _proposal(rng, theta, chol)
+        prop = propose(rng, theta)
         ok = box_check(prop)
         ev = np.where(ok[:, None], prop, last)
         chi_p = exact(ev)
@@ -460,7 +548,7 @@ def metropolis(exact, theta0, cov, steps, seed=0, box_check=in_box, record=True)
 
 
 def delayed_acceptance(exact, sur, theta0, cov, steps, seed=0, box_check=in_box, record=True,
-                       compact=None):
+                       compact=None, propose=None):
     """Delayed-acceptance Metropolis: the approximation screens, the exact
     model judges every step that passes. sur is either a chi**2 callable
     (state-independent approximation) or an anchored one with
@@ -468,14 +556,14 @@ def delayed_acceptance(exact, sur, theta0, cov, steps, seed=0, box_check=in_box,
     anchor * s(y) / s(x); the anchored form needs exact.curves_of(rows). Returns
     (chain, final theta, final chi**2, acceptance rate, wall seconds, stats)."""
     rng = np.random.default_rng(seed)
-    chol = np.linalg.cholesky(cov)
+    propose = propose or GaussianWalk(cov)
     theta = np.array(theta0, np.float64)
     anchored = hasattr(sur, "state")
     if anchored and hasattr(exact, "curves_all_device") and hasattr(sur, "bind"):
-        return _delayed_acceptance_graphs(exact, sur, theta0, cov, steps, seed, box_check,
+        return _delayed_acceptance_graphs(exact, sur, theta0, propose, steps, seed, box_check,
                                           record, compact)
     if anchored and hasattr(exact, "curves_all_device") and hasattr(sur, "torch"):
-        return _delayed_acceptance_device(exact, sur, theta0, cov, steps, seed, box_check,
+        return _delayed_acceptance_device(exact, sur, theta0, propose, steps, seed, box_check,
                                           record)
     place = getattr(sur, "anchor", lambda rows: np.array(rows, np.float64))
     if anchored and hasattr(exact, "curves_device") and hasattr(sur, "sur"):
@@ -494,7 +582,7 @@ def delayed_acceptance(exact, sur, theta0, cov, steps, seed=0, box_check=in_box,
     nc = theta.shape[0]
     t0 = time.perf_counter()
     for s in range(steps):
-        prop = _proposal(rng, theta, chol)
+        prop = propose(rng, theta)
         ok = box_check(prop)
         if anchored:
             sy = sur.state(prop)

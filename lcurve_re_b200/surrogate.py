@@ -14,12 +14,13 @@ resolution (nlat 40/80). The box is the mcmc_batch distribution's mean
 in [-0.005, 0.005].
 """
 import ctypes as C
+import time
 
 import numpy as np
 
 from . import abi
 from . import workloads as W
-from .mlp import MLP
+from .mlp import MLP, gemm_bf16x3
 
 PARAMS = ("q", "iangle", "r1", "r2", "t1", "t2", "gravity_dark2", "absorb", "t0")
 BOX = np.array([
@@ -124,24 +125,33 @@ class Surrogate:
 
     # -- fitting ---------------------------------------------------------------
     def fit_pca(self, curves):
+        """Principal components of the centred curves. The Gram matrix, the
+        coefficients and the reconstruction run on lcg_mlp_gemm (gemm_bf16x3:
+        three BF16 products, FP32 accumulation per block of 8192 terms, FP64
+        across blocks); the eigendecomposition of
+        the npts x npts Gram matrix is torch.linalg.eigh in FP64."""
         torch = self.torch
         y = torch.as_tensor(curves, device=self.dev, dtype=torch.float64)
         self.mean = y.mean(dim=0)
         yc = y - self.mean
-        cov = yc.T @ yc / y.shape[0]
+        cov = gemm_bf16x3(yc.T, yc.T, self.net.lib) / y.shape[0]
+        cov = 0.5 * (cov + cov.T)
         evals, evecs = torch.linalg.eigh(cov)
         order = torch.argsort(evals, descending=True)[:self.ncoef]
         self.basis = evecs[:, order].T.contiguous()          # [ncoef x npts]
-        coef = yc @ self.basis.T                              # [n x ncoef]
+        coef = gemm_bf16x3(yc, self.basis, self.net.lib)       # [n x ncoef]
         self.cscale = float(coef[:, 0].std())                 # targets = coef / cscale
-        resid = yc - coef @ self.basis
+        resid = yc - gemm_bf16x3(coef, self.basis.T, self.net.lib)
         return float(resid.abs().max()), coef / self.cscale
 
     def fit(self, theta, curves, epochs=60, lr=2e-3, lr_min=2e-5, seed=1, log=None):
         """PCA, then Adam on the MSE of the scaled coefficients with a cosine
         learning-rate schedule. Returns the per-epoch mean losses."""
         torch = self.torch
+        t0 = time.perf_counter()
         pca_err, target = self.fit_pca(curves)
+        torch.cuda.synchronize(self.dev)
+        self.pca_s = time.perf_counter() - t0
         self.pca_max_err = pca_err
         x = torch.as_tensor(to_unit(theta), device=self.dev, dtype=torch.float32)
         t = target.to(torch.float32)
@@ -151,21 +161,35 @@ class Surrogate:
             raise ValueError("fewer training curves than one batch")
         steps = epochs * (n // B)
         g = torch.Generator(device=self.dev).manual_seed(seed)
+        net = self.net
+        net.set_schedule(lr, lr_min, steps)
         losses, k = [], 0
+        t0 = time.perf_counter()
         for ep in range(epochs):
             perm = torch.randperm(x.shape[0], generator=g, device=self.dev)[:n]
             tot = 0.0
             for i0 in range(0, n, B):
                 idx = perm[i0:i0 + B]
-                rate = lr_min + 0.5 * (lr - lr_min) * (1 + np.cos(np.pi * k / steps))
-                self.net.forward(x[idx], train=True)
-                tot += self.net.backward(t[idx].contiguous())
-                self.net.step(rate)
+                if net.fused:
+                    # one graph per step, schedule and loss kept on the device
+                    torch.index_select(x, 0, idx, out=net.x)
+                    torch.index_select(t, 0, idx, out=net.tgt)
+                    net.graph_step()
+                else:
+                    rate = lr_min + 0.5 * (lr - lr_min) * (1 + np.cos(np.pi * k / steps))
+                    net.forward(x[idx], train=True)
+                    tot += net.backward(t[idx].contiguous())
+                    net.step(rate)
                 k += 1
+            if net.fused:
+                tot = net.take_loss() * (n // B)
             losses.append(tot / (n // B))
             if log:
                 log("epoch %d loss %.3e" % (ep, losses[-1]))
-        self.net.check()
+        torch.cuda.synchronize(self.dev)
+        self.train_s = time.perf_counter() - t0
+        self.train_steps = steps
+        net.check()
         return losses
 
     # -- prediction --------------------------------------------------------------
@@ -183,7 +207,7 @@ class Surrogate:
 
     def curves(self, theta):
         c = self.coefficients(theta).to(self.torch.float64) * self.cscale
-        return (self.mean + c @ self.basis).cpu().numpy()
+        return (self.mean + gemm_bf16x3(c, self.basis.T, self.net.lib)).cpu().numpy()
 
     def head(self, index):
         """The chi**2 head restricted to the grid points index: (basis

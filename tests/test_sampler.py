@@ -256,3 +256,63 @@ def test_adaptive_posterior_finds_a_correlated_posterior():
     assert np.all(np.abs(m - mu) < 0.05 * sd)
     assert np.all(np.abs(np.sqrt(np.diag(c)) / sd - 1) < 0.05)
     assert abs(c[0, 3] / np.sqrt(c[0, 0] * c[3, 3]) - 0.99) < 0.003
+
+
+def _banana_chi(t):
+    """A curved ridge: x1 follows 0.8 x0^2 within 0.05, x2 Gaussian."""
+    return (t[:, 0] ** 2 + ((t[:, 1] - 0.8 * t[:, 0] ** 2) / 0.05) ** 2 + (t[:, 2] / 0.3) ** 2)
+
+
+def _banana_draws(n, seed):
+    r = np.random.default_rng(seed)
+    x0 = r.standard_normal(n)
+    return np.c_[x0, 0.8 * x0 ** 2 + 0.05 * r.standard_normal(n), 0.3 * r.standard_normal(n)]
+
+
+def test_triangular_walk_is_a_volume_preserving_bijection():
+    from lcurve_re_b200.sampler import TriangularWalk
+    tw = TriangularWalk(_banana_draws(20000, 1))
+    x = _banana_draws(500, 2) + 0.1
+    np.testing.assert_allclose(tw.inverse(tw.forward(x)), x, rtol=0, atol=1e-12)
+    # Jacobian of the forward map by central differences: unit determinant
+    h, x0 = 1e-6, x[:7]
+    for row in x0:
+        J = np.stack([(tw.forward((row + h * e)[None]) - tw.forward((row - h * e)[None]))[0]
+                      / (2 * h) for e in np.eye(3)], axis=1)
+        assert abs(np.linalg.det(J * tw.s[None, :]) - 1) < 1e-6
+    # the fitted map straightens the ridge: u's second coordinate is the
+    # ridge's width (0.05 / its spread) and uncorrelated with the first
+    u = tw.forward(_banana_draws(20000, 3))
+    assert abs(np.corrcoef(u.T)[0, 1]) < 0.02
+    assert u[:, 1].std() < 0.1 * u[:, 0].std()
+
+
+def test_triangular_walk_mixes_a_curved_ridge_where_the_gaussian_walk_does_not():
+    """On a banana-shaped target, plain Metropolis with the triangular walk
+    (fitted to a posterior sample, the step scale 2.38 / sqrt(d)) accepts
+    0.15-0.45 of its moves (near the Gaussian optimum for 3 dimensions) and
+    has at least 5x the bulk ESS of the best-scaled Gaussian walk with the
+    sample's covariance; delayed acceptance with the
+    same proposal and a shifted, too-wide surrogate keeps the target: both
+    chains' means within 4 Monte Carlo errors of the exact ones."""
+    from lcurve_re_b200.sampler import TriangularWalk
+    chains, steps = 128, 1500
+    sample = _banana_draws(20000, 4)
+    theta0 = _banana_draws(chains, 5)
+    tw = TriangularWalk(sample)
+    cg = max((metropolis(_banana_chi, theta0, np.cov(sample.T) * f * f * 2.38 ** 2 / 3, steps,
+                         seed=6, box_check=_everywhere) for f in (1.0, 0.5, 0.25)),
+             key=lambda r: ess_bulk(r[0]).min())
+    ct, _, _, acc, _ = metropolis(_banana_chi, theta0, None, steps, seed=6,
+                                  box_check=_everywhere, propose=tw)
+    assert 0.15 < acc < 0.45, acc
+    assert ess_bulk(ct).min() >= 5 * ess_bulk(cg[0]).min(), (ess_bulk(ct), ess_bulk(cg[0]))
+    sur = lambda t: _banana_chi(t - 0.05) * 0.8
+    cd, _, _, acc_d, _, _ = delayed_acceptance(_banana_chi, sur, theta0, None,
+                                               steps, seed=7, box_check=_everywhere,
+                                               propose=tw.with_scale(1.5))
+    exact_mean = np.array([0.0, 0.8, 0.0])
+    for c in (ct, cd):
+        s = c.reshape(-1, 3)
+        mcse = s.std(0) / np.sqrt(ess_bulk(c))
+        assert np.all(np.abs(s.mean(0) - exact_mean) < 4 * mcse), (s.mean(0), mcse)
