@@ -105,7 +105,7 @@ struct BatchState {
     DBuf<float4> ef, runb;
     DBuf<unsigned long long> pfx;
     DBuf<double4> es;
-    DBuf<uint8_t> ehit;
+    DBuf<int32_t> hits;
     DBuf<double> w1, w2, part, osum, calc, sfac, out;
     // results (pinned): calc, sfac, out, status
     unsigned char *h_res = nullptr;
@@ -134,7 +134,7 @@ struct BatchState {
         for (auto *b : d) b->release();
         area.release(); grav.release(); flux.release(); fp.release(); necl.release();
         ecl.release(); n0.release(); blockcnt.release(); queue.release(); counters.release();
-        st.release(); ef.release(); pfx.release(); runb.release(); rings.release(); es.release(); ehit.release(); d_tab.release();
+        st.release(); ef.release(); pfx.release(); runb.release(); rings.release(); es.release(); hits.release(); d_tab.release();
         rows.release(); gathered.release(); tune_pre.release();
         if (h_rows) cudaFreeHost(h_rows);
         h_rows = nullptr;
@@ -165,7 +165,7 @@ struct BatchState {
         b.qcap = nfaces;
         b.counters = counters.p;
         b.es = es.p;
-        b.ehit = ehit.p;
+        b.hits = hits.p;
         b.st = st.p;
         b.counts = reinterpret_cast<const int32_t *>(d + o_counts);
         b.geo_slot = reinterpret_cast<const int32_t *>(d + o_geo_slot);
@@ -318,7 +318,7 @@ lcg_status relayout(lcg_ctx *c, BatchState &B, const lcg_model *models, int32_t 
         (e = B.runb.ensure((size_t)B.nflat / 64)) ||
         (e = B.n0.ensure(ns)) || (e = B.blockcnt.ensure((size_t)B.nblk)) ||
         (e = B.counters.ensure(8)) || (e = B.st.ensure(nm)) ||
-        (e = B.es.ensure(nf)) || (e = B.ehit.ensure(nf)) ||
+        (e = B.es.ensure(nf)) || (e = B.hits.ensure(nf)) ||
         (e = B.ef.ensure(nm * (size_t)B.ldp)) || (e = B.pfx.ensure(nm * (size_t)B.ldp)) || (e = B.w1.ensure(nm * (size_t)B.ldp)) ||
         (e = B.w2.ensure(nm * (size_t)B.ldp)) ||
         (e = B.part.ensure((size_t)std::max<int64_t>(B.plan.nchunk, 1) * (size_t)B.ldp)) ||

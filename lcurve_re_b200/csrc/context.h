@@ -59,7 +59,7 @@ struct Grid {
     DBuf<RingRec> rings;
     DBuf<int32_t> queue, counters;  // eclipse candidates of this grid
     DBuf<double4> es;               // and their state between the two passes
-    DBuf<uint8_t> ehit;
+    DBuf<int32_t> hits;
     // flat
     DBuf<int64_t> n0;
     DBuf<float4> geo, pos;
@@ -125,7 +125,7 @@ struct Grid {
                              &fdz, &fpx, &fpy, &fpz, &fflux, &fin, &fout};
         for (auto *b : d) b->release();
         area.release(); grav.release(); flux.release(); necl.release(); rings.release();
-        queue.release(); counters.release(); es.release(); ehit.release();
+        queue.release(); counters.release(); es.release(); hits.release();
         n0.release(); geo.release(); pos.release(); ecl.release(); fp.release();
         runb.release(); ndx.release(); rn.release(); xr.release(); rr.release(); ridx.release();
         disc = false;

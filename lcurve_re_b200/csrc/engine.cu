@@ -440,8 +440,8 @@ lcg_status build_geometry(lcg_ctx *c, const lcg_model &m, int star, int fine, Gr
         StageScope t(c, LCG_STAGE_GRID);
         launch_grid(gp, g.rings.p, g.dev(), c->status.p, st);
     }
-    if ((e = g.queue.ensure(s.nface)) || (e = g.counters.ensure(4)) ||
-        (e = g.es.ensure(s.nface)) || (e = g.ehit.ensure(s.nface)))
+    if ((e = g.queue.ensure(s.nface)) || (e = g.counters.ensure(8)) ||
+        (e = g.es.ensure(s.nface)) || (e = g.hits.ensure(s.nface)))
         return c->cuda_fail(e, "queue");
     EclParams ep{};
     ep.comp_star = star == kStar1 ? kStar2 : kStar1;
@@ -458,7 +458,7 @@ lcg_status build_geometry(lcg_ctx *c, const lcg_model &m, int star, int fine, Gr
     set_ecl_screen(ep, c->precision == LCG_PREC_MIXED, star == kStar1 ? s.r1 : s.r2);
     {
         StageScope t(c, LCG_STAGE_ECLIPSE);
-        launch_eclipse(ep, s.eclipse, g.dev(), g.queue.p, g.counters.p, g.es.p, g.ehit.p,
+        launch_eclipse(ep, s.eclipse, g.dev(), g.queue.p, g.counters.p, g.es.p, g.hits.p,
                        c->status.p, c->nsm, c->eclipse_warp, st);
     }
     return LCG_OK;

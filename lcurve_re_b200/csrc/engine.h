@@ -219,13 +219,15 @@ struct BatchDev {
     // eclipse candidates: those whose bisections the FP32 screen serves go to
     // the front of queue, the others (FP64 alone) to the back, so that warps
     // do not mix the two; counters: [0] candidates, [1]-[3] work counters of
-    // the passes, [4] back-of-queue candidates, [5] front-of-queue ones
+    // the passes, [4] back-of-queue candidates, [5] front-of-queue ones, [6]
+    // candidates pot_min found eclipsed
     int32_t *blockcnt, *queue, *counters;
     int64_t qcap;  // queue capacity (faces of the batch)
     // eclipse candidates between the two passes of the thread mode: per queue
-    // entry (phase of the potential minimum, phi1, phi2, ACC) and a hit flag
+    // entry (phase of the potential minimum, phi1, phi2, ACC), and the list of
+    // the entries pot_min found eclipsed (the bisections' work, compacted)
     double4 *es;
-    uint8_t *ehit;
+    int32_t *hits;
     DevStatus *st;  // per model
     // work lists: counts[0] geometry slots, counts[1] continuum slots; each
     // list has its slots and prefix sums (count + 1 entries) of its units
@@ -259,10 +261,11 @@ struct BatchPhases {
 // ---- launchers (geometry.cu) ------------------------------------------------
 void launch_grid(const GridParams &p, const RingRec *rings, GridDev g, DevStatus *st,
                  cudaStream_t s);
-// queue: one int per face; counters: 4 work counters; es / ehit: per-candidate
-// state between the thread mode's two passes (one per face).
+// queue: one int per face; counters: 8 (candidates, work counters, hits);
+// es / hits: per-candidate state between the thread mode's two passes and the
+// compacted list of the eclipsed candidates (one per face each).
 void launch_eclipse(const EclParams &p, int32_t eclipse_on, GridDev g, int32_t *queue,
-                    int32_t *counters, double4 *es, uint8_t *ehit, DevStatus *st, int nsm,
+                    int32_t *counters, double4 *es, int32_t *hits, DevStatus *st, int nsm,
                     int32_t warp_mode, cudaStream_t s);
 void launch_continuum(const ContParams &p, GridDev g, cudaStream_t s);
 void launch_flatten(GridDev g, FlatDev f, int32_t *blockcnt, int mixed, int need_pos,

@@ -194,6 +194,20 @@ __global__ void __launch_bounds__(128, 4) k_ecl_roche(EclParams p, GridDev g,
     }
 }
 
+// Appends the eclipsed candidates k of a warp's 32 (lanes with hit) to the
+// list the bisection pass walks, in lane order, so that warps bisect only
+// faces pot_min found eclipsed (consecutive candidates stay together). All 32
+// lanes call it.
+__device__ __forceinline__ void push_hits(bool hit, int k, int32_t *hits, int32_t *count) {
+    const unsigned m = __ballot_sync(0xffffffffu, hit);
+    if (!m) return;
+    const int lane = threadIdx.x & 31;
+    int at = 0;
+    if (lane == 0) at = atomicAdd(count, __popc(m));
+    at = __shfl_sync(0xffffffffu, at, 0);
+    if (hit) hits[at + __popc(m & ((1u << lane) - 1u))] = k;
+}
+
 // One test of a bisection: the FP32 screen where p.scr allows it (it decides
 // only where the FP64 test's answer is certain, so the bisection takes the
 // same midpoints), else Roche::fblink in FP64. u0: the point relative to the
@@ -256,10 +270,11 @@ __device__ __forceinline__ double ecl_bisect_warp(const EclParams &p, bool live,
 // Thread mode (more candidates than warp_max), in two passes with a small code
 // footprint each, as for the batch (k_ecl_potmin_b / k_ecl_bisect_b): the
 // sphere test and pot_min per candidate, then ingress and egress on the two
-// lanes of a pair. es / ehit hold each candidate's state between the passes.
+// lanes of a pair. es holds each candidate's state between the passes, hits
+// the candidates pot_min found eclipsed.
 __global__ void __launch_bounds__(128, 4) k_ecl_potmin(EclParams p, GridDev g,
                                                     const int32_t *__restrict__ queue,
-                                                    int32_t *counters, double4 *es, uint8_t *ehit,
+                                                    int32_t *counters, double4 *es, int32_t *hits,
                                                     DevStatus *st, int32_t warp_max) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
@@ -272,23 +287,25 @@ __global__ void __launch_bounds__(128, 4) k_ecl_potmin(EclParams p, GridDev g,
         base = __shfl_sync(full, base, 0);
         if (base >= total) break;
         const int k = base + lane;
-        if (k >= total) continue;
-        const int32_t i = queue[k];
-        const V3 pos = v3(g.px[i], g.py[i], g.pz[i]);
-        double phi1, phi2, lam1, lam2, phi = 0., lam = 0.;
-        uint8_t hit = 0;
-        if (sphere_eclipse_ph(p.cosi, p.sini, pos, cofm, p.comp_rref, phi1, phi2, lam1, lam2)) {
-            const double ACC = 2. * sqrt(2. * kTwoPi * (lam2 - lam1) * p.delta);
-            int s = 0;
-            hit = pot_min(p.comp_star, p.q, p.comp_spin, p.cosi, p.sini, pos, phi1, phi2, lam1,
-                          lam2, p.comp_rref, p.comp_pref, ACC, phi, lam, s);
-            if (s) {
-                set_status(st, s, i);
-                hit = 0;
+        bool hit = false;
+        if (k < total) {
+            const int32_t i = queue[k];
+            const V3 pos = v3(g.px[i], g.py[i], g.pz[i]);
+            double phi1, phi2, lam1, lam2, phi = 0., lam = 0.;
+            if (sphere_eclipse_ph(p.cosi, p.sini, pos, cofm, p.comp_rref, phi1, phi2, lam1,
+                                  lam2)) {
+                const double ACC = 2. * sqrt(2. * kTwoPi * (lam2 - lam1) * p.delta);
+                int s = 0;
+                hit = pot_min(p.comp_star, p.q, p.comp_spin, p.cosi, p.sini, pos, phi1, phi2,
+                              lam1, lam2, p.comp_rref, p.comp_pref, ACC, phi, lam, s);
+                if (s) {
+                    set_status(st, s, i);
+                    hit = false;
+                }
+                es[k] = make_double4(phi, phi1, phi2, ACC);
             }
-            es[k] = make_double4(phi, phi1, phi2, ACC);
         }
-        ehit[k] = hit;
+        push_hits(hit, k, hits, &counters[6]);
     }
 }
 
@@ -296,12 +313,12 @@ template <int NB>
 __global__ void __launch_bounds__(128, NB)
     k_ecl_bisect(__grid_constant__ const EclParams p, __grid_constant__ const GridDev g,
                  const int32_t *__restrict__ queue, int32_t *counters, const double4 *es,
-                 const uint8_t *ehit, DevStatus *st, int32_t warp_max) {
+                 const int32_t *__restrict__ hits, DevStatus *st, int32_t warp_max) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int total = counters[0];
     if (total <= warp_max) return;
-    const int64_t n2 = 2 * (int64_t)total;
+    const int64_t n2 = 2 * (int64_t)counters[6];
     for (;;) {
         int64_t base = 0;
         if (lane == 0) base = atomicAdd(&counters[3], 32);
@@ -310,8 +327,9 @@ __global__ void __launch_bounds__(128, NB)
         // every lane stays here (ecl_bisect_warp votes over the warp); both
         // lanes of a pair agree on live
         const int64_t u = base + lane;
-        const int k = (int)(u >> 1), side = (int)(u & 1);
-        const bool live = u < n2 && ehit[k];
+        const int side = (int)(u & 1);
+        const bool live = u < n2;
+        const int k = live ? hits[u >> 1] : 0;
         const int32_t i = live ? queue[k] : 0;
         const double4 E = live ? es[k] : make_double4(0., 0., 0., 0.);
         const V3 pos = live ? v3(g.px[i], g.py[i], g.pz[i]) : v3(0., 0., 0.);
@@ -1114,26 +1132,28 @@ __global__ void __launch_bounds__(128, 4) k_ecl_potmin_b(BatchDev b, int32_t war
         base = __shfl_sync(full, base, 0);
         if (base >= total) break;
         const int k = base + lane;
-        if (k >= total) continue;
-        const int32_t i = queue_at(b, k);
-        const SlotDev &S = b.slots[find_seg(b.face0, b.nslots, i)];
-        const EclParams &p = S.ep;
-        const V3 pos = v3(g.px[i], g.py[i], g.pz[i]);
-        const V3 cofm = p.comp_star == kStar1 ? v3(0., 0., 0.) : v3(1., 0., 0.);
-        double phi1, phi2, lam1, lam2, phi = 0., lam = 0.;
-        uint8_t hit = 0;
-        if (sphere_eclipse_ph(p.cosi, p.sini, pos, cofm, p.comp_rref, phi1, phi2, lam1, lam2)) {
-            const double ACC = 2. * sqrt(2. * kTwoPi * (lam2 - lam1) * p.delta);
-            int s = 0;
-            hit = pot_min(p.comp_star, p.q, p.comp_spin, p.cosi, p.sini, pos, phi1, phi2, lam1,
-                          lam2, p.comp_rref, p.comp_pref, ACC, phi, lam, s);
-            if (s) {
-                set_status(b.st + S.model, s, i - S.face0);
-                hit = 0;
+        bool hit = false;
+        if (k < total) {
+            const int32_t i = queue_at(b, k);
+            const SlotDev &S = b.slots[find_seg(b.face0, b.nslots, i)];
+            const EclParams &p = S.ep;
+            const V3 pos = v3(g.px[i], g.py[i], g.pz[i]);
+            const V3 cofm = p.comp_star == kStar1 ? v3(0., 0., 0.) : v3(1., 0., 0.);
+            double phi1, phi2, lam1, lam2, phi = 0., lam = 0.;
+            if (sphere_eclipse_ph(p.cosi, p.sini, pos, cofm, p.comp_rref, phi1, phi2, lam1,
+                                  lam2)) {
+                const double ACC = 2. * sqrt(2. * kTwoPi * (lam2 - lam1) * p.delta);
+                int s = 0;
+                hit = pot_min(p.comp_star, p.q, p.comp_spin, p.cosi, p.sini, pos, phi1, phi2,
+                              lam1, lam2, p.comp_rref, p.comp_pref, ACC, phi, lam, s);
+                if (s) {
+                    set_status(b.st + S.model, s, i - S.face0);
+                    hit = false;
+                }
+                b.es[k] = make_double4(phi, phi1, phi2, ACC);
             }
-            b.es[k] = make_double4(phi, phi1, phi2, ACC);
         }
-        b.ehit[k] = hit;
+        push_hits(hit, k, b.hits, &b.counters[6]);
     }
 }
 
@@ -1146,15 +1166,16 @@ __global__ void __launch_bounds__(128, NB)
     const int lane = threadIdx.x & 31;
     const int total = b.counters[0];
     if (batch_warp_mode(b, warp_max, auto_mode)) return;
-    const int64_t n2 = 2 * (int64_t)total;
+    const int64_t n2 = 2 * (int64_t)b.counters[6];
     for (;;) {
         int64_t base = 0;
         if (lane == 0) base = atomicAdd(&b.counters[3], 32);
         base = __shfl_sync(full, base, 0);
         if (base >= n2) break;
         const int64_t u = base + lane;
-        const int k = (int)(u >> 1), side = (int)(u & 1);
-        const bool live = u < n2 && b.ehit[k];
+        const int side = (int)(u & 1);
+        const bool live = u < n2;
+        const int k = live ? b.hits[u >> 1] : 0;
         const int32_t i = live ? queue_at(b, k) : 0;
         const int sl = find_seg(b.face0, b.nslots, i);
         const double4 E = live ? b.es[k] : make_double4(0., 0., 0., 0.);
@@ -1367,10 +1388,10 @@ int bisect_blocks_per_sm() {
 }
 
 void launch_eclipse(const EclParams &p, int32_t eclipse_on, GridDev g, int32_t *queue,
-                    int32_t *counters, double4 *es, uint8_t *ehit, DevStatus *st, int nsm,
+                    int32_t *counters, double4 *es, int32_t *hits, DevStatus *st, int nsm,
                     int32_t warp_mode, cudaStream_t s) {
     if (g.n <= 0) return;
-    cudaMemsetAsync(counters, 0, 4 * sizeof(int32_t), s);
+    cudaMemsetAsync(counters, 0, 8 * sizeof(int32_t), s);
     k_ecl_pre<<<nblocks(g.n, 256), 256, 0, s>>>(p, eclipse_on, g, queue, counters);
     count_launch();
     if (eclipse_on && p.comp_roche) {
@@ -1385,15 +1406,15 @@ void launch_eclipse(const EclParams &p, int32_t eclipse_on, GridDev g, int32_t *
             warp_mode < 0 ? -1 : warp_mode > 0 ? warp_mode : (p.scr.on ? -1 : 2 * warps);
         k_ecl_roche<<<nb, 128, 0, s>>>(p, g, queue, counters, st, warp_max);
         count_launch();
-        k_ecl_potmin<<<nb, 128, 0, s>>>(p, g, queue, counters, es, ehit, st, warp_max);
+        k_ecl_potmin<<<nb, 128, 0, s>>>(p, g, queue, counters, es, hits, st, warp_max);
         count_launch();
         const int nbs = bisect_blocks_per_sm();
         const unsigned cap = (unsigned)nsm * (unsigned)nbs;
         const unsigned nbb = need < cap ? need : cap;
         if (nbs == 6)
-            k_ecl_bisect<6><<<nbb, 128, 0, s>>>(p, g, queue, counters, es, ehit, st, warp_max);
+            k_ecl_bisect<6><<<nbb, 128, 0, s>>>(p, g, queue, counters, es, hits, st, warp_max);
         else
-            k_ecl_bisect<4><<<nbb, 128, 0, s>>>(p, g, queue, counters, es, ehit, st, warp_max);
+            k_ecl_bisect<4><<<nbb, 128, 0, s>>>(p, g, queue, counters, es, hits, st, warp_max);
         count_launch();
     }
 }
