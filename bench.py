@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--workload", default="wd_dm_large",
                     choices=("wd_dm_large", "wd_dm_small", "tiny_star", "mcmc_batch",
-                             "surrogate_da", "cv_disc"))
+                             "surrogate_da", "cv_disc", "mlp_train"))
     ap.add_argument("--batch-models", type=int, default=256,
                     help="models per step of mcmc_batch (256 is the benchmark)")
     ap.add_argument("--batch-variant", choices=("geometry", "brightness"), default="geometry",
@@ -66,7 +66,7 @@ def parse():
     ap.add_argument("--chains", type=int, default=512)
     ap.add_argument("--mcmc-steps", type=int, default=2000)
     ap.add_argument("--burn", type=int, default=400)
-    ap.add_argument("--compact", type=int, default=32,
+    ap.add_argument("--compact", type=int, default=64,
                     help="surrogate_da: delayed acceptance's exact evaluations through a "
                          "batch of this many slots on a second engine context (0: the "
                          "whole-chain batch)")
@@ -77,13 +77,16 @@ def parse():
     ap.add_argument("--ncoef", type=int, default=64)
     ap.add_argument("--local-curves", type=int, default=131072)
     ap.add_argument("--refine-epochs", type=int, default=600)
-    ap.add_argument("--da-scale", type=float, default=2.6)
+    ap.add_argument("--da-scales", type=float, nargs="+", default=[1.0, 1.5, 2.0, 3.0],
+                    help="surrogate_da: multiples of the plain step scale tried by the "
+                         "delayed-acceptance pilot runs")
+    ap.add_argument("--adapt-rounds", type=int, default=2,
+                    help="surrogate_da: adaptive burn-in rounds refitting the proposal's map")
     ap.add_argument("--local-widen", type=float, default=2.0)
     ap.add_argument("--tune-steps", type=int, default=200,
                     help="surrogate_da: plain Metropolis steps per pilot run of the proposal scale")
     ap.add_argument("--burn-tuned", type=int, default=2000,
-                    help="surrogate_da: plain Metropolis steps with the tuned proposal from the "
-                         "resampled states before the comparison")
+                    help="surrogate_da: plain Metropolis steps per adaptive burn-in round")
     ap.add_argument("--is-rounds", type=int, default=8,
                     help="surrogate_da: rounds of adaptive importance sampling of the posterior")
     ap.add_argument("--is-pool", type=int, default=65536,
@@ -700,13 +703,17 @@ def run_surrogate(args):
 
     Start states: a first adaptive burn-in locates the posterior; adaptive
     importance sampling of exact engine curves (the box-uniform training set,
-    then Gaussian pools around the running weighted estimate, then the local
-    draws the network is refined on; each row weighted by its exact
-    likelihood over the density of the mixture of the pools) gives the
-    posterior's sample, and the chains start from a resample of it, so both
+    then Gaussian pools around the running weighted estimate; each row
+    weighted by its exact likelihood over the density of the mixture of the
+    pools) gives the posterior's sample, and the chains start from a resample
+    of it, then adaptive burn-in rounds with the final proposal, so both
     samplers begin at (close to) the stationary distribution and their means
-    can be compared against their Monte Carlo errors. The proposal covariance
-    is that sample's weighted covariance x 2.38^2 / 9.
+    can be compared against their Monte Carlo errors. Proposal: a random walk
+    in coordinates that straighten the posterior's curved ridge
+    (sampler.TriangularWalk), refitted over adaptive burn-in rounds; plain
+    Metropolis' step scale by acceptance nearest 0.234, delayed acceptance's
+    boldness by pilot runs (largest squared jump per second). The network is
+    refined on engine curves drawn along the ridge through the same map.
 
     value: bulk ESS (rank-normalised multi-chain ESS over split chains,
     minimum over parameters) per second of delayed-acceptance sampling; the
@@ -717,8 +724,9 @@ def run_surrogate(args):
     from lcurve_re_b200 import surrogate as S
     from lcurve_re_b200 import workloads as W
     from lcurve_re_b200.engine import Engine
-    from lcurve_re_b200.sampler import (CompactExact, ExactChi2, delayed_acceptance,
-                                        mean_shift, metropolis, shift_verdict, summary)
+    from lcurve_re_b200.sampler import (CompactExact, ExactChi2, TriangularWalk,
+                                        delayed_acceptance, mean_shift, metropolis,
+                                        shift_verdict, summary)
 
     eng = Engine(device=local, precision="mixed")
     clocks = Clocks(local)
@@ -779,42 +787,54 @@ def run_surrogate(args):
         exact_chi2, [(theta, S.log_uniform_box())], chi_box, samp.mean(0), np.cov(samp.T),
         rounds=args.is_rounds, pool=args.is_pool, target=args.is_target,
         widen0=args.local_widen, seed=19 + rank)
-    jitter = np.diag(np.diag(cov_k) * 1e-6)
-    # refinement: the same network trained again on engine curves around the
-    # posterior (Gaussian, local_widen x its spread, inside the box); those
-    # curves are the importance sample's last pool too
-    th_loc = S.local_draws(mu_k, cov_k, args.local_curves, seed=5 + rank, widen=args.local_widen)
-    _, cu_loc = S.training_set(eng, 0, theta=th_loc, batch=2048)
-    chi_pool = np.r_[chi_pool, S.curves_chi2(cu_loc, data, idx)]
-    pools.append((th_loc, S.log_gaussian_in_box(mu_k, cov_k, args.local_widen)))
     theta0, mu_is, cov_is, ess_is = S.posterior_resample(pools, chi_pool, args.chains,
                                                          seed=17 + rank)
     t_sir = time.perf_counter() - t0
+    # proposal: the posterior is a curved ridge (iangle, r1, r2 and q follow
+    # one another along a curve: quadratic terms predict them 5-7x better than
+    # linear ones), so a random walk with one covariance moves at the ridge's
+    # local width. sampler.TriangularWalk walks in coordinates that straighten
+    # it (a volume-preserving quadratic map, so the proposal stays symmetric):
+    # fitted to the importance sample first, then refitted on the second half
+    # of each adaptive burn-in round of plain Metropolis; before every round
+    # and the comparison, pilot runs pick the step scale whose acceptance is
+    # nearest 0.234
+    exact = ExactChi2(eng, data)
+    tw = TriangularWalk(S.posterior_resample(pools, chi_pool, 65536, seed=31 + rank)[0])
+    tuning = []
+
+    def tune(walk, start):
+        accs = [(f, metropolis(exact, start, None, args.tune_steps, seed=23, record=False,
+                               propose=walk.with_scale(f))[3])
+                for f in (1.0, 0.7, 0.5, 0.35, 0.25)]
+        tuning.append(accs)
+        return walk.with_scale(min(accs, key=lambda t: abs(t[1] - 0.234))[0])
+    tw = tune(tw, theta0)
+    for r in range(args.adapt_rounds):
+        ch_b, theta0, _, _, _ = metropolis(exact, theta0, None, args.burn_tuned, seed=29 + r,
+                                           propose=tw)
+        tw = tune(TriangularWalk(ch_b[ch_b.shape[0] // 2:].reshape(-1, 9)), theta0)
+        del ch_b
+    f_best = tw.scale
+    # refinement: the same network trained again on engine curves drawn along
+    # the posterior's ridge (Gaussian in the walk's straightened coordinates,
+    # local_widen x its spread there, mapped back, inside the box); its error
+    # is measured on held-out draws of the same kind
     t0 = time.perf_counter()
+    th_loc = tw.draws(args.local_curves, widen=args.local_widen, seed=5 + rank,
+                      box_check=S.in_box)
+    _, cu_loc = S.training_set(eng, 0, theta=th_loc, batch=2048)
     sur_loc = S.Surrogate(ncoef=args.ncoef, batch=4096, seed=rank + 1)
     losses_loc = sur_loc.fit(th_loc, cu_loc, epochs=args.refine_epochs)
     t_ref = time.perf_counter() - t0
     del cu_loc
-    th_lh = S.local_draws(mu_is, cov_is + jitter, 2048, seed=77 + rank, widen=args.local_widen)
+    th_lh = tw.draws(2048, widen=args.local_widen, seed=77 + rank, box_check=S.in_box)
     _, cu_lh = S.training_set(eng, 0, theta=th_lh, batch=2048)
     loc_err = float(np.sqrt(np.mean((sur_loc.curves(th_lh) - cu_lh) ** 2)))
     glob_err_loc = float(np.sqrt(np.mean((sur.curves(th_lh) - cu_lh) ** 2)))
-    # proposal: the importance sample's covariance carries the posterior's
-    # tails, which overshoot the ridges a random walk moves along; short pilot
-    # runs of plain Metropolis pick the scale of it whose acceptance is
-    # nearest 0.234, then a burn-in with that proposal takes the resampled
-    # states into the bulk before both samplers start from them
+    # the training curves above went through the same engine on their own
+    # phase grid: the samplers' evaluator binds the data again
     exact = ExactChi2(eng, data)
-    base = cov_is * 2.38 ** 2 / 9 + np.diag((scale0 * 1e-3) ** 2)
-    tuning = []
-    for f in (1.0, 0.5, 0.25, 0.125, 0.0625):
-        acc_f = metropolis(exact, theta0, base * f * f, args.tune_steps, seed=23,
-                           record=False)[3]
-        tuning.append((f, acc_f))
-    f_best = min(tuning, key=lambda t: abs(t[1] - 0.234))[0]
-    cov = base * f_best * f_best
-    if args.burn_tuned > 0:
-        theta0 = metropolis(exact, theta0, cov, args.burn_tuned, seed=29, record=False)[1]
     sur_loc_chi = S.SurrogateChi2(sur_loc, data, idx)
     # inference throughput of the network alone (the DA screening pass)
     xin = torch.rand(args.chains, 9, device="cuda") * 2 - 1
@@ -829,21 +849,39 @@ def run_surrogate(args):
     lib = eng.lib
     lib.lcg_kernel_launches(1)
     e_plain0 = exact.evals
-    chp, _, _, accp, wall_p = metropolis(exact, theta0, cov, args.mcmc_steps, seed=21)
+    chp, _, _, accp, wall_p = metropolis(exact, theta0, None, args.mcmc_steps, seed=21,
+                                         propose=tw)
     launches_plain = int(lib.lcg_kernel_launches(1))
-    # delayed acceptance can afford bolder proposals: the surrogate screens them
-    cov_da = cov * args.da_scale ** 2
     n_plain = exact.evals - e_plain0
     eng_c = Engine(device=local, precision="mixed") if args.compact > 0 else None
     exact_g = ExactChi2(eng, data, curves=True)
     comp_g = CompactExact(eng_c, data, k=args.compact) if eng_c else None
-    chg, _, _, accg, wall_g, stg = delayed_acceptance(exact_g, sur_chi, theta0, cov_da,
-                                                       args.mcmc_steps, seed=21, compact=comp_g)
+    # delayed acceptance can afford bolder steps, since the surrogate screens
+    # them: short pilot runs pick the multiple of the plain step scale with
+    # the largest expected squared jump (in the walk's whitened coordinates)
+    # per second of sampling
+    da_pilots = []
+    for k in args.da_scales:
+        walk = tw.with_scale(tw.scale * k)
+        ex_p = ExactChi2(eng, data, curves=True)
+        comp_p = CompactExact(eng_c, data, k=args.compact) if eng_c else None
+        cpl, _, _, acc_k, wall_k, _ = delayed_acceptance(ex_p, sur_loc_chi, theta0, None,
+                                                         args.tune_steps, seed=27,
+                                                         compact=comp_p, propose=walk)
+        u = tw.forward(cpl.reshape(-1, 9)).reshape(cpl.shape) @ np.linalg.inv(tw.chol.T)
+        esjd = float(np.mean(np.sum(np.diff(u, axis=0) ** 2, axis=2)))
+        da_pilots.append((k, acc_k, esjd / wall_k))
+    da_scale = max(da_pilots, key=lambda t: t[2])[0]
+    walk_da = tw.with_scale(tw.scale * da_scale)
+    chg, _, _, accg, wall_g, stg = delayed_acceptance(exact_g, sur_chi, theta0, None,
+                                                       args.mcmc_steps, seed=21, compact=comp_g,
+                                                       propose=walk_da)
     exact2 = ExactChi2(eng, data, curves=True)
     comp2 = CompactExact(eng_c, data, k=args.compact) if eng_c else None
     lib.lcg_kernel_launches(1)
-    chd, _, _, accd, wall_d, st = delayed_acceptance(exact2, sur_loc_chi, theta0, cov_da,
-                                                      args.mcmc_steps, seed=21, compact=comp2)
+    chd, _, _, accd, wall_d, st = delayed_acceptance(exact2, sur_loc_chi, theta0, None,
+                                                      args.mcmc_steps, seed=21, compact=comp2,
+                                                      propose=walk_da)
     launches_da = int(lib.lcg_kernel_launches(1))
     clk = clocks.stop()
     sum_p, sum_d, sum_g = summary(chp, wall_p), summary(chd, wall_d), summary(chg, wall_g)
@@ -855,13 +893,13 @@ def run_surrogate(args):
                 for k, c in (("plain", chp), ("delayed_acceptance", chd))}
     del chg
     peak, peak_src = _bf16_peak()
-    train_tflops = train_flop / t_fit / 1e12
+    train_tflops = train_flop / sur.train_s / 1e12
     value = sum_d["ess_bulk_per_s"]
     nbytes_model = C_sizeof_model()
     line = {
         "metric": "MCMC effective samples/s", "value": value,
         "unit": "effective samples/s", "n_gpus": world, "steps": args.mcmc_steps,
-        "warmup": args.burn + args.burn_fixed + args.burn_tuned,
+        "warmup": args.burn + args.burn_fixed + args.adapt_rounds * args.burn_tuned,
         "ms_per_step": wall_d / args.mcmc_steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "bf16 tensor-core MLP (fp32 accumulate) + f32/f64 engine",
@@ -881,7 +919,7 @@ def run_surrogate(args):
                             % (args.chains, len(chi_pool), len(pools), ess_is,
                                [round(x) for x in ess_rounds])},
         "plain": dict(sum_p, acceptance=accp, exact_evals=n_plain),
-        "delayed_acceptance": dict(sum_d, surrogate="refined around the burn-in posterior",
+        "delayed_acceptance": dict(sum_d, surrogate="refined along the posterior's ridge",
                                    acceptance=accd,
                                    exact_evals=exact2.evals + (comp2.evals if comp2 else 0),
                                    exact_batch="%d slots" % args.compact if comp2 else "chains",
@@ -905,6 +943,7 @@ def run_surrogate(args):
             "importance_sample_mcse_max": float(mcse_is.max())},
         "surrogate": {"train_curves": args.train_curves, "curve_generation_s": t_gen,
                       "curves_per_s": args.train_curves / t_gen, "fit_s": t_fit,
+                      "pca_s": sur.pca_s,
                       "epochs": args.epochs, "final_loss": losses[-1],
                       "heldout_rms_curve_error": rel_err, "pca_max_error": sur.pca_max_err,
                       "inference_ms_per_batch": t_inf * 1e3,
@@ -914,10 +953,13 @@ def run_surrogate(args):
                                   "global_net_local_rms_curve_error": glob_err_loc,
                                   "pca_max_error": sur_loc.pca_max_err},
                       "importance_resampling_s": t_sir},
-        "roofline": {"bound": "tensor", "kernel": "k_gemm (training, all layers)",
+        "roofline": {"bound": "tensor",
+                     "kernel": "training steps (one graph each: k_mlp_chain forward and "
+                               "backward, k_gemm weight gradients), PCA excluded",
                      "achieved": train_tflops, "peak": peak, "unit": "TFLOP/s",
                      "frac": train_tflops / peak, "traffic": None, "peak_source": peak_src,
-                     "flop_per_sample_train": sur.net.flops_per_sample(train=True)},
+                     "flop_per_sample_train": sur.net.flops_per_sample(train=True),
+                     "ms_per_training_step": sur.train_s / sur.train_steps * 1e3},
         # the samplers' wall clock already covers every per-step transfer: the
         # proposals (models) to the device, chi**2 back to the host
         "e2e": {"value": value, "unit": "effective samples/s",
@@ -927,15 +969,109 @@ def run_surrogate(args):
                 "note": "wall-clock sampling: every step sends the proposals and reads chi**2"},
         "gpu_launches": launches_da,
         "gpu_launches_plain": launches_plain,
-        "da_proposal_scale": args.da_scale,
+        "proposal": "random walk in coordinates straightening the posterior's curved ridge "
+                    "(sampler.TriangularWalk: volume-preserving quadratic triangular map, "
+                    "refitted on %d adaptive burn-in rounds of %d steps)"
+                    % (args.adapt_rounds, args.burn_tuned),
         "proposal_tuning": {"scale_acceptance": tuning, "chosen": f_best,
-                            "burn_in_steps": args.burn_tuned},
+                            "burn_in_steps": args.adapt_rounds * args.burn_tuned},
+        "da_scale_pilots": [{"scale": k, "acceptance": a, "sq_jump_per_s": e}
+                            for k, a, e in da_pilots],
+        "da_proposal_scale": da_scale,
         "clocks": clk,
     }
     if eng_c is not None:
         eng_c.close()
     eng.close()
     return line if rank == 0 else None
+
+
+def run_mlp_train(args):
+    """The surrogate network's training step alone: cfg4's network (9 -> 4 x
+    256 GELU -> 64) at its training batch of 4096, each step one CUDA graph
+    (fused forward with the loss gradient, fused backward chain, the four
+    weight-gradient GEMMs, bias gradients, the input layer's gradient, one
+    Adam launch), as Surrogate.fit runs it. value: training samples/s with
+    the batch resident; e2e: the batch copied from pinned host memory and the
+    loss read back every step; roofline: the network's FLOPs (3 x forward)
+    per step over its CUDA-event time against the BF16 tensor peak. Also
+    times the one-launch inference of 512 rows (the delayed-acceptance
+    screening batch)."""
+    import torch
+    from lcurve_re_b200.mlp import MLP
+    rank, local, world = rank_info()
+    net = MLP(nin=9, nout=64, batch=4096, seed=rank)
+    g = torch.Generator(device="cuda").manual_seed(rank)
+    x = torch.rand(net.B, 9, device="cuda", generator=g) * 2 - 1
+    t = torch.sin(2 * x @ torch.randn(9, 64, device="cuda", generator=g)).contiguous()
+    net.x.copy_(x)
+    net.tgt.copy_(t)
+    net.set_schedule(1e-3)
+    lib = net.lib
+    lib.lcg_kernel_launches(1)
+    net.graph_step()  # eager, then captured
+    launches = int(lib.lcg_kernel_launches(1))
+    for _ in range(max(args.warmup, 3)):
+        net.graph_step()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        net.graph_step()
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    # end to end: the batch from pinned host memory, the loss back, every step
+    hx, ht = x.cpu().pin_memory(), t.cpu().pin_memory()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        net.x.copy_(hx, non_blocking=True)
+        net.tgt.copy_(ht, non_blocking=True)
+        net.graph_step()
+        loss = net.take_loss()
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    # inference, 512 rows
+    xin = x[:512].contiguous()
+    for _ in range(3):
+        net.forward(xin)
+    ev0.record()
+    for _ in range(50):
+        net.forward(xin)
+    ev1.record()
+    torch.cuda.synchronize()
+    inf_ms = ev0.elapsed_time(ev1) / 50
+    clk = clocks.stop()
+    net.check()
+    flop = net.B * net.flops_per_sample(train=True)
+    peak, peak_src = _bf16_peak()
+    tflops = flop / (ms * 1e-3) / 1e12
+    if rank != 0:
+        return None
+    return {
+        "metric": "surrogate training samples/s", "value": net.B / (ms * 1e-3),
+        "unit": "samples/s", "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3),
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16 tensor-core GEMMs (fp32 accumulate), fp32 input layer and optimiser",
+        "data": "synthetic (uniform inputs, sinusoidal targets)",
+        "config": {"workload": "mlp_train: 9 -> 4x256 GELU -> 64, batch 4096, one CUDA graph "
+                               "per step", "l2": "not flushed (the weights, 0.9 MB, and the "
+                                                 "batch stay in L2 as they do in training)",
+                   "parallelism": "replicas x%d" % world},
+        "roofline": {"bound": "tensor", "kernel": "training step (k_mlp_chain x 2 + k_gemm x 4 "
+                                                  "+ small kernels)",
+                     "achieved": tflops, "peak": peak, "unit": "TFLOP/s", "frac": tflops / peak,
+                     "traffic": None, "peak_source": peak_src,
+                     "flop_per_step": flop},
+        "e2e": {"value": net.B / e2e_s, "unit": "samples/s",
+                "h2d_bytes_per_step": int(hx.numel() * 4 + ht.numel() * 4),
+                "d2h_bytes_per_step": 8, "last_loss": loss},
+        "inference_ms_512_rows": inf_ms,
+        "gpu_launches": launches * args.steps,
+        "gpu_launches_per_step": launches,
+        "clocks": clk,
+    }
 
 
 def C_sizeof_model():
@@ -1085,6 +1221,8 @@ def main():
     try:
         if args.workload == "surrogate_da":
             line = run_surrogate(args)
+        elif args.workload == "mlp_train":
+            line = run_mlp_train(args)
         elif args.workload == "mcmc_batch":
             line = run_batch(args, dist)
         else:

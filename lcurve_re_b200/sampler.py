@@ -338,8 +338,25 @@ class TriangularWalk:
         self.s[self.s == 0] = 1.0
         z = (sample - self.m) / self.s
         self.d = d = z.shape[1]
-        self.coef = [None] + [np.linalg.lstsq(_quadratic_features(z[:, :k]), z[:, k],
-                                              rcond=None)[0] for k in range(1, d)]
+        coef = [None] + [np.linalg.lstsq(_quadratic_features(z[:, :k]), z[:, k],
+                                         rcond=None)[0] for k in range(1, d)]
+        # P_k(z) = c0[k] + z_<k . b[k] + z_<k^T A[k] z_<k (A upper triangular),
+        # and the same for every k at once: C0 + z B + vec(z z^T) Q
+        self.c0 = np.zeros(d)
+        self.b = [np.zeros(0)] + [c[1:k + 1] for k, c in enumerate(coef) if k]
+        self.A = [np.zeros((0, 0))]
+        self.B = np.zeros((d, d))
+        self.Q = np.zeros((d * d, d))
+        for k in range(1, d):
+            c = coef[k]
+            self.c0[k] = c[0]
+            self.B[:k, k] = c[1:k + 1]
+            A = np.zeros((k, k))
+            A[np.triu_indices(k)] = c[k + 1:]
+            self.A.append(A)
+            full = np.zeros((d, d))
+            full[:k, :k] = A
+            self.Q[:, k] = full.ravel()
         u = self._forward_z(z)
         self.mean_u = u.mean(0)
         self.cov_u = np.cov(u.T)
@@ -355,10 +372,8 @@ class TriangularWalk:
         return copy.copy(self).set_scale(scale)
 
     def _forward_z(self, z):
-        u = z.copy()
-        for k in range(1, self.d):
-            u[:, k] = z[:, k] - _quadratic_features(z[:, :k]) @ self.coef[k]
-        return u
+        zz = (z[:, :, None] * z[:, None, :]).reshape(len(z), -1)
+        return z - (self.c0 + z @ self.B + zz @ self.Q)
 
     def forward(self, x):
         return self._forward_z((np.asarray(x, np.float64) - self.m) / self.s)
@@ -366,7 +381,9 @@ class TriangularWalk:
     def inverse(self, u):
         z = np.array(u, np.float64)
         for k in range(1, self.d):
-            z[:, k] = u[:, k] + _quadratic_features(z[:, :k]) @ self.coef[k]
+            zk = z[:, :k]
+            z[:, k] = u[:, k] + self.c0[k] + zk @ self.b[k] + np.einsum(
+                "ni,ni->n", zk @ self.A[k], zk)
         return self.m + z * self.s
 
     def draws(self, n, widen=1.0, seed=0, box_check=None):
