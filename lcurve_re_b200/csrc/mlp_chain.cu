@@ -1,7 +1,7 @@
 // mlp_chain.cu — every layer of the surrogate network for a 128-row tile in
 // one launch (sm_100a).
 //
-// One CTA per 128 rows, 256 threads (8 warps). The tile's activations stay
+// One CTA per 128 rows, 512 threads (16 warps). The tile's activations stay
 // in shared memory between layers as the A operand of the next tcgen05.mma:
 // four 16 KB K-blocks of [128 rows x 64] BF16 in the 128-byte-swizzled
 // K-major layout TMA would write. Each layer:
@@ -11,8 +11,8 @@
 //   * one elected thread issues the MMAs (kind::f16, M = 128, N = n, K = 16
 //     each) into one TMEM accumulator of n columns and commits them to an
 //     mbarrier;
-//   * all eight warps read the accumulator back (warp w: TMEM lanes
-//     32 (w % 4).. = rows, columns half w / 4) and run the epilogue, writing
+//   * all sixteen warps read the accumulator back (warp w: TMEM lanes
+//     32 (w % 4).. = rows, columns quarter w / 4) and run the epilogue, writing
 //     the next A operand into shared memory (generic-proxy stores, then a
 //     proxy fence before the next MMA reads them).
 // Epilogues: bias + GELU (hidden layers; training also stores the
@@ -41,7 +41,9 @@ namespace mlp {
 namespace {
 
 constexpr int kChainMax = 5;          // layers after the first A operand
-constexpr int kChainThreads = 256;
+constexpr int kChainThreads = 512;  // 128 x kGroups: warp w reads TMEM lanes 32 (w % 4)..
+constexpr int kGroups = kChainThreads / 128;  // column groups of the epilogue
+static_assert(kGroups == 2 || kGroups == 4, "64-column layers need 16-column groups");
 constexpr int kSlots = 4;             // weight K-blocks of one layer
 constexpr uint32_t kSlotBytes = 256u * kBK * 2;    // the largest B block, [256 x 64]
 constexpr uint32_t kABlockBytes = (uint32_t)kBM * kBK * 2;
@@ -109,8 +111,8 @@ __global__ void __launch_bounds__(kChainThreads, 1) k_mlp_chain(const __grid_con
     __shared__ uint64_t full[kSlots], accb, abar;
     __shared__ uint32_t tmem_base;
     __shared__ int ok;
-    __shared__ float xs[kBM * 16];
-    __shared__ float lossp[2][kBM];
+    __shared__ __align__(16) float xs[kBM * 16];
+    __shared__ float lossp[kGroups][kBM];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int q = warp & 3, h = warp >> 2;
     const int row = 32 * q + lane;
@@ -162,30 +164,43 @@ __global__ void __launch_bounds__(kChainThreads, 1) k_mlp_chain(const __grid_con
     // ---- first A operand ----------------------------------------------------------------
     if (a.input_layer) {
         const int kin = a.kin;
-        for (int i = tid; i < kBM * kin; i += kChainThreads) {
-            const int r = i / kin, k = i - r * kin;
-            xs[r * 16 + k] = (m0 + r < a.mvalid) ? a.x[(size_t)(m0 + r) * kin + k] : 0.f;
+        // the tile's inputs, zero past kin and for rows >= mvalid
+        for (int i = tid; i < kBM * 16; i += kChainThreads) {
+            const int r = i >> 4, k = i & 15;
+            xs[i] = (k < kin && m0 + r < a.mvalid) ? a.x[(size_t)(m0 + r) * kin + k] : 0.f;
         }
         __syncthreads();
-        const int u = tid;  // unit
+        const int u = tid & 255;  // unit
+        constexpr int kRows = kBM * 256 / kChainThreads;  // rows per thread
+        const int rbase = (tid >> 8) * kRows;
         float wr[16];
 #pragma unroll
         for (int k = 0; k < 16; k++) wr[k] = k < kin ? a.w0[u * kin + k] : 0.f;
         const float bu = a.b0 ? a.b0[u] : 0.f;
-        for (int r0 = 0; r0 < kBM; r0 += 8) {
+        // eight rows at a time, FMA chains interleaved; the sums run in
+        // k_input_fwd's order (the padded terms add exact zeros)
+        for (int r0 = rbase; r0 < rbase + kRows; r0 += 8) {
+            float acc[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) acc[j] = bu;
+#pragma unroll
+            for (int k4 = 0; k4 < 16; k4 += 4) {
+#pragma unroll
+                for (int j = 0; j < 8; j++) {
+                    const float4 xv = *reinterpret_cast<const float4 *>(&xs[(r0 + j) * 16 + k4]);
+                    acc[j] = fmaf(xv.x, wr[k4], acc[j]);
+                    acc[j] = fmaf(xv.y, wr[k4 + 1], acc[j]);
+                    acc[j] = fmaf(xv.z, wr[k4 + 2], acc[j]);
+                    acc[j] = fmaf(xv.w, wr[k4 + 3], acc[j]);
+                }
+            }
             __align__(16) __nv_bfloat16 yb[8];
 #pragma unroll
             for (int j = 0; j < 8; j++) {
                 const int r = r0 + j;
-                float acc = 0.f;
-                if (m0 + r < a.mvalid) {
-                    acc = bu;
-#pragma unroll
-                    for (int k = 0; k < 16; k++)
-                        if (k < kin) acc = fmaf(xs[r * 16 + k], wr[k], acc);
-                }
-                yb[j] = __float2bfloat16_rn(gelu(acc));
-                if (a.z0) a.z0[(size_t)(m0 + r) * kWidth + u] = __float2bfloat16_rn(acc);
+                const float z = m0 + r < a.mvalid ? acc[j] : 0.f;
+                yb[j] = __float2bfloat16_rn(gelu(z));
+                if (a.z0) a.z0[(size_t)(m0 + r) * kWidth + u] = __float2bfloat16_rn(z);
                 act_store1(act, r, u, yb[j]);
             }
             if (a.yt0)
@@ -231,10 +246,10 @@ __global__ void __launch_bounds__(kChainThreads, 1) k_mlp_chain(const __grid_con
         // the next layer's weights load while this epilogue runs
         if (tid == 0 && l + 1 < a.nlayers) load_layer(l + 1);
 
-        const int half = L.n >> 1;
+        const int part = L.n / kGroups;
         float lsum = 0.f;
 #pragma unroll 1
-        for (int c0 = h * half; c0 < (h + 1) * half; c0 += 16) {
+        for (int c0 = h * part; c0 < (h + 1) * part; c0 += 16) {
             float v[16];
             tmem_ld16(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)c0, v);
             if (L.bias) {
@@ -297,8 +312,11 @@ __global__ void __launch_bounds__(kChainThreads, 1) k_mlp_chain(const __grid_con
         fence_before_sync();
         __syncthreads();
     }
-    if (ok && a.target && a.loss_rows && h == 0 && l == a.nlayers)
-        a.loss_rows[m] = lossp[0][row] + lossp[1][row];
+    if (ok && a.target && a.loss_rows && h == 0 && l == a.nlayers) {
+        float sum = lossp[0][row];
+        for (int g = 1; g < kGroups; g++) sum += lossp[g][row];
+        a.loss_rows[m] = sum;
+    }
 
     if (!ok && tid == 0) {
         // drain what is in flight before the shared memory and TMEM go away

@@ -369,7 +369,9 @@ class TriangularWalk:
 
     def with_scale(self, scale):
         """A copy with another step scale (the map is shared)."""
-        return copy.copy(self).set_scale(scale)
+        w = copy.copy(self)
+        w._cache = (None, None)
+        return w.set_scale(scale)
 
     def _forward_z(self, z):
         zz = (z[:, :, None] * z[:, None, :]).reshape(len(z), -1)
@@ -402,7 +404,17 @@ class TriangularWalk:
         return out[:n]
 
     def __call__(self, rng, theta):
-        u = self.forward(theta)
+        # the samplers move few chains per step: map only the rows that
+        # changed since the last call (the cached u of the others is exact)
+        th, u = getattr(self, "_cache", (None, None))
+        if th is None or th.shape != theta.shape:
+            u = self.forward(theta)
+        else:
+            moved = np.any(theta != th, axis=1)
+            if moved.any():
+                u = u.copy()
+                u[moved] = self.forward(theta[moved])
+        self._cache = (theta.copy(), u)
         return self.inverse(u + rng.standard_normal(u.shape) @ self.chol.T)
 
 
