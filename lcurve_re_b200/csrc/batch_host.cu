@@ -103,6 +103,7 @@ struct BatchState {
     DBuf<int32_t> blockcnt, queue, counters;
     DBuf<DevStatus> st;
     DBuf<float4> ef, runb;
+    DBuf<ulonglong2> runh;
     DBuf<unsigned long long> pfx;
     DBuf<double4> es;
     DBuf<int32_t> hits;
@@ -134,7 +135,7 @@ struct BatchState {
         for (auto *b : d) b->release();
         area.release(); grav.release(); flux.release(); fp.release(); necl.release();
         ecl.release(); n0.release(); blockcnt.release(); queue.release(); counters.release();
-        st.release(); ef.release(); pfx.release(); runb.release(); rings.release(); es.release(); hits.release(); d_tab.release();
+        st.release(); ef.release(); pfx.release(); runb.release(); runh.release(); rings.release(); es.release(); hits.release(); d_tab.release();
         rows.release(); gathered.release(); tune_pre.release();
         if (h_rows) cudaFreeHost(h_rows);
         h_rows = nullptr;
@@ -158,6 +159,7 @@ struct BatchState {
                       necl.p, ein.p, eout.p, nfaces};
         b.fp = fp.p;
         b.runb = runb.p;
+        b.runh = runh.p;
         b.ecl = ecl.p;
         b.n0 = n0.p;
         b.blockcnt = blockcnt.p;
@@ -315,7 +317,7 @@ lcg_status relayout(lcg_ctx *c, BatchState &B, const lcg_model *models, int32_t 
     if ((e = B.area.ensure(nf)) || (e = B.grav.ensure(nf)) || (e = B.flux.ensure(nf)) ||
         (e = B.necl.ensure(nf)) || (e = B.queue.ensure(nf)) ||
         (e = B.fp.ensure(8 * (size_t)B.nflat)) || (e = B.ecl.ensure((size_t)B.nflat)) ||
-        (e = B.runb.ensure((size_t)B.nflat / 64)) ||
+        (e = B.runb.ensure((size_t)B.nflat / 64)) || (e = B.runh.ensure((size_t)B.nflat / 64)) ||
         (e = B.n0.ensure(ns)) || (e = B.blockcnt.ensure((size_t)B.nblk)) ||
         (e = B.counters.ensure(8)) || (e = B.st.ensure(nm)) ||
         (e = B.es.ensure(nf)) || (e = B.hits.ensure(nf)) ||
@@ -335,6 +337,7 @@ lcg_status relayout(lcg_ctx *c, BatchState &B, const lcg_model *models, int32_t 
     cudaMemsetAsync(B.fp.p, 0, 8 * (size_t)B.nflat * sizeof(float), c->stream);
     cudaMemsetAsync(B.ecl.p, 0, (size_t)B.nflat * sizeof(ulonglong2), c->stream);
     cudaMemsetAsync(B.runb.p, 0, (size_t)B.nflat / 64 * sizeof(float4), c->stream);
+    cudaMemsetAsync(B.runh.p, 0, (size_t)B.nflat / 64 * sizeof(ulonglong2), c->stream);
     cudaMemsetAsync(B.n0.p, 0, ns * sizeof(int64_t), c->stream);
     B.key.assign(nm, lcg_model{});
     B.key_ok.assign(nm, 0);

@@ -67,6 +67,7 @@ struct Grid {
     DBuf<double> fdx, fdy, fdz, fpx, fpy, fpz, fflux, fin, fout;
     DBuf<float> fp;
     DBuf<float4> runb;
+    DBuf<ulonglong2> runh;
     // opaque disc: per-face disc ranges, and the flat grid's several-range faces
     DBuf<uint8_t> ndx, rn;
     DBuf<double2> xr, rr;
@@ -98,7 +99,9 @@ struct Grid {
         if (mixed) {
             if ((e = ecl.ensure(npad))) return e;
             if (fast_on) {
-                if ((e = fp.ensure(8 * npad)) || (e = runb.ensure(npad / 64))) return e;
+                if ((e = fp.ensure(8 * npad)) || (e = runb.ensure(npad / 64)) ||
+                    (e = runh.ensure(npad / 64)))
+                    return e;
             } else if ((e = geo.ensure(npad))) {
                 return e;
             }
@@ -117,7 +120,7 @@ struct Grid {
     }
     FlatDev flat() const {
         return FlatDev{n, npad, n0.p, geo.p, ecl.p, pos.p, fdx.p, fdy.p, fdz.p,
-                       fpx.p, fpy.p, fpz.p, fflux.p, fin.p, fout.p, fp.p, runb.p,
+                       fpx.p, fpy.p, fpz.p, fflux.p, fin.p, fout.p, fp.p, runb.p, runh.p,
                        n0.p ? n0.p + 1 : nullptr, ridx.p, rr.p, rn.p};
     }
     void release() {
@@ -127,7 +130,7 @@ struct Grid {
         area.release(); grav.release(); flux.release(); necl.release(); rings.release();
         queue.release(); counters.release(); es.release(); hits.release();
         n0.release(); geo.release(); pos.release(); ecl.release(); fp.release();
-        runb.release(); ndx.release(); rn.release(); xr.release(); rr.release(); ridx.release();
+        runb.release(); runh.release(); ndx.release(); rn.release(); xr.release(); rr.release(); ridx.release();
         disc = false;
     }
 };

@@ -113,6 +113,10 @@ struct FlatDev {
     // of the run (C includes a margin over FP32 rounding), so a warp can skip
     // a run that faces away at all its phases
     float4 *runb;
+    // per run: an arc (I, W) of fixed-point phase holding every eclipse range
+    // of the run's faces (W = ~0: test each face; (0, 0): none has a range), so
+    // a warp whose phases all lie outside it skips the run's eclipse tests
+    ulonglong2 *runh;
     // faces with two or more eclipse ranges (opaque discs) sit last, in
     // [*n1, n): their records above are zero (they add nothing to the main
     // sweeps); ridx is each one's face index in the grid, rr its rn ranges
@@ -214,6 +218,7 @@ struct BatchDev {
     GridDev g;  // every face of the batch
     float *fp;  // fast sweep records (FlatDev::fp layout per slot)
     float4 *runb;  // FlatDev::runb per slot, from flat0 / 64
+    ulonglong2 *runh;  // FlatDev::runh per slot, from flat0 / 64
     ulonglong2 *ecl;
     int64_t *n0;  // per slot
     // eclipse candidates: those whose bisections the FP32 screen serves go to
@@ -292,7 +297,8 @@ void launch_interp(const DatumRec *data, int32_t n, const int64_t *idx, int32_t 
 
 void launch_pack_flat(FlatDev f, int64_t n0, int need_pos, cudaStream_t s);
 // run bounds of fast records: npairs pairs from fp, one float4 per 32 pairs
-void launch_run_bounds(const float *fp, int64_t npairs, float4 *runb, cudaStream_t s);
+void launch_run_bounds(const float *fp, const ulonglong2 *ecl, int64_t npairs, float4 *runb,
+                       ulonglong2 *runh, cudaStream_t s);
 void launch_batch_run_bounds(const BatchDev &b, int nsm, cudaStream_t s);
 void launch_pack_phases(PhaseDev ph, cudaStream_t s);
 

@@ -244,7 +244,9 @@ void launch_ppt(int star, const FluxConsts &k, const FlatDev &f, const PhaseDev 
 //   fI  = flux * I(t), Horner on per-face coefficients 4 FFMA2
 //   s  += m * fI                                       1 FFMA2
 // one-range faces add the fixed-point eclipse test (a 64-bit subtract and
-// compare, and a select, per face).
+// compare, and a select, per face), skipped for a run of 32 pairs whose
+// ranges' hull misses the warp's arc of phases (an exact test on the circle,
+// once per run).
 // Each thread holds PPT consecutive phase entries, so a warp covers 32 * PPT
 // consecutive entries: a narrow arc of the orbit for time-ordered points.
 // A face pair that faces away (mu <= 0) or is eclipsed at every entry of the
@@ -253,13 +255,90 @@ void launch_ppt(int star, const FluxConsts &k, const FlatDev &f, const PhaseDev 
 // are bit-identical to evaluating them.
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 
+// The warp's phase arc: every entry of the warp below nent lies in [A, A + L]
+// (mod 2^64), A its first lane's first entry. For time-ordered points it is a
+// short arc of the orbit; in any order it still holds every entry.
+template <int PPT>
+__device__ __forceinline__ void warp_arc(const unsigned long long *pf, int64_t e0, int64_t nent,
+                                         unsigned long long &A, unsigned long long &L) {
+    A = __shfl_sync(0xffffffffu, pf[0], 0);
+    unsigned long long l = 0ull;
+#pragma unroll
+    for (int j = 0; j < PPT; j++) {
+        const unsigned long long d = pf[j] - A;
+        if (e0 + j < nent && d > l) l = d;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long t = __shfl_xor_sync(0xffffffffu, l, o);
+        l = t > l ? t : l;
+    }
+    L = l;
+}
+
+// A run's eclipse-range hull (I, W) (FlatDev::runh) meets the arc [A, A + L]:
+// the hull starts inside the arc, or the arc starts inside the hull; W = ~0
+// means "test every face", W = 0 "no face of the run has a range". Exact on
+// the circle, so a run whose hull misses the arc has every face visible at
+// every entry of the warp.
+__device__ __forceinline__ bool hull_meets_arc(ulonglong2 H, unsigned long long A,
+                                               unsigned long long L) {
+    if (H.y == ~0ull) return true;
+    return H.y != 0ull && ((H.x - A) <= L || (A - H.x) < H.y);
+}
+
+// One fold block of cnt face pairs at rp (eclipse records at ep when ECL):
+// the PPT entries' FP32 sums of the block.
+template <int PPT, int LT, bool ECL>
+__device__ __forceinline__ void fold_block(const float4 *rp, const ulonglong2 *ep, int cnt,
+                                           const float2 *ex, const float2 *ey,
+                                           const unsigned long long *pf, float2 *s) {
+#pragma unroll 2
+    for (int i = 0; i < cnt; i++) {
+        const float4 P0 = rp[4 * i], P1 = rp[4 * i + 1];
+        const float2 nx = f2(P0.x, P0.y), ny = f2(P0.z, P0.w), cz = f2(P1.x, P1.y);
+        ulonglong2 Ea = make_ulonglong2(0ull, 0ull), Eb = Ea;
+        if constexpr (ECL) {
+            Ea = ep[2 * i];
+            Eb = ep[2 * i + 1];
+        }
+        float2 m[PPT];
+        uint32_t vis = 0u;  // ma, mb >= 0: their bits are nonzero iff they are > 0
+#pragma unroll
+        for (int j = 0; j < PPT; j++) {
+            const float2 mu = __ffma2_rn(ex[j], nx, __ffma2_rn(ey[j], ny, cz));
+            float ma = fmaxf(mu.x, 0.f), mb = fmaxf(mu.y, 0.f);
+            if constexpr (ECL) {
+                ma = ((pf[j] - Ea.x) >= Ea.y) ? ma : 0.f;
+                mb = ((pf[j] - Eb.x) >= Eb.y) ? mb : 0.f;
+            }
+            m[j] = f2(ma, mb);
+            vis |= __float_as_uint(ma) | __float_as_uint(mb);
+        }
+        if (!__any_sync(0xffffffffu, vis != 0u)) continue;
+        const float4 P2 = rp[4 * i + 2], P3 = rp[4 * i + 3];
+        const float2 p0 = f2(P1.z, P1.w), p1 = f2(P2.x, P2.y), p2 = f2(P2.z, P2.w);
+        const float2 p3 = f2(P3.x, P3.y), p4 = f2(P3.z, P3.w);
+#pragma unroll
+        for (int j = 0; j < PPT; j++) {
+            float2 t;
+            if constexpr (LT == 1) t = f2(sqrt_approx(m[j].x), sqrt_approx(m[j].y));
+            else t = m[j];
+            const float2 fI =
+                __ffma2_rn(t, __ffma2_rn(t, __ffma2_rn(t, __ffma2_rn(t, p4, p3), p2), p1), p0);
+            s[j] = __ffma2_rn(m[j], fI, s[j]);
+        }
+    }
+}
+
 template <int PPT, int LT, bool ECL>
 __device__ __forceinline__ void sweep_pairs(const float4 *sp, const ulonglong2 *se, int64_t q0,
                                             int64_t lo, int64_t hi, const float2 *ex,
                                             const float2 *ey, const float *exy,
-                                            const unsigned long long *pf,
+                                            const unsigned long long *pf, unsigned long long A,
+                                            unsigned long long L,
                                             const float4 *__restrict__ runb,
-                                            float *acc) {
+                                            const ulonglong2 *__restrict__ runh, float *acc) {
     constexpr int kFoldPairs = kFold / 2;
     for (int64_t b = lo; b < hi; b += kFoldPairs) {
         const int cnt = (int)((b + kFoldPairs < hi) ? kFoldPairs : hi - b);
@@ -281,42 +360,13 @@ __device__ __forceinline__ void sweep_pairs(const float4 *sp, const ulonglong2 *
         float2 s[PPT];
 #pragma unroll
         for (int j = 0; j < PPT; j++) s[j] = f2(0.f, 0.f);
-#pragma unroll 2
-        for (int i = 0; i < cnt; i++) {
-            const float4 P0 = rp[4 * i], P1 = rp[4 * i + 1];
-            const float2 nx = f2(P0.x, P0.y), ny = f2(P0.z, P0.w), cz = f2(P1.x, P1.y);
-            ulonglong2 Ea = make_ulonglong2(0ull, 0ull), Eb = Ea;
-            if constexpr (ECL) {
-                Ea = ep[2 * i];
-                Eb = ep[2 * i + 1];
-            }
-            float2 m[PPT];
-            uint32_t vis = 0u;  // ma, mb >= 0: their bits are nonzero iff they are > 0
-#pragma unroll
-            for (int j = 0; j < PPT; j++) {
-                const float2 mu = __ffma2_rn(ex[j], nx, __ffma2_rn(ey[j], ny, cz));
-                float ma = fmaxf(mu.x, 0.f), mb = fmaxf(mu.y, 0.f);
-                if constexpr (ECL) {
-                    ma = ((pf[j] - Ea.x) >= Ea.y) ? ma : 0.f;
-                    mb = ((pf[j] - Eb.x) >= Eb.y) ? mb : 0.f;
-                }
-                m[j] = f2(ma, mb);
-                vis |= __float_as_uint(ma) | __float_as_uint(mb);
-            }
-            if (!__any_sync(0xffffffffu, vis != 0u)) continue;
-            const float4 P2 = rp[4 * i + 2], P3 = rp[4 * i + 3];
-            const float2 p0 = f2(P1.z, P1.w), p1 = f2(P2.x, P2.y), p2 = f2(P2.z, P2.w);
-            const float2 p3 = f2(P3.x, P3.y), p4 = f2(P3.z, P3.w);
-#pragma unroll
-            for (int j = 0; j < PPT; j++) {
-                float2 t;
-                if constexpr (LT == 1) t = f2(sqrt_approx(m[j].x), sqrt_approx(m[j].y));
-                else t = m[j];
-                const float2 fI =
-                    __ffma2_rn(t, __ffma2_rn(t, __ffma2_rn(t, __ffma2_rn(t, p4, p3), p2), p1), p0);
-                s[j] = __ffma2_rn(m[j], fI, s[j]);
-            }
-        }
+        // the per-entry eclipse tests only where a run's ranges can reach the
+        // warp's arc of phases (warp-uniform: the hulls and the arc are)
+        if (ECL && (hull_meets_arc(runh[b >> 5], A, L) ||
+                    hull_meets_arc(runh[(b + cnt - 1) >> 5], A, L)))
+            fold_block<PPT, LT, true>(rp, ep, cnt, ex, ey, pf, s);
+        else
+            fold_block<PPT, LT, false>(rp, ep, cnt, ex, ey, pf, s);
 #pragma unroll
         for (int j = 0; j < PPT; j++) acc[j] += s[j].x + s[j].y;
     }
@@ -353,11 +403,14 @@ __device__ __forceinline__ void sweep_chunk(const FlatDev &f, const float4 *sp,
                                             const ulonglong2 *se, int64_t c0, int64_t cend,
                                             int64_t n0, const float2 *ex, const float2 *ey,
                                             const float *exy, const unsigned long long *pf,
+                                            unsigned long long A, unsigned long long L,
                                             float *acc) {
     const int64_t q0 = c0 >> 1, qend = (cend + 1) >> 1, qn0 = n0 >> 1;
     const int64_t qa = qn0 < qend ? qn0 : qend;
-    sweep_pairs<PPT, LT, false>(sp, se, q0, q0, qa > q0 ? qa : q0, ex, ey, exy, pf, f.runb, acc);
-    sweep_pairs<PPT, LT, true>(sp, se, q0, qa > q0 ? qa : q0, qend, ex, ey, exy, pf, f.runb, acc);
+    sweep_pairs<PPT, LT, false>(sp, se, q0, q0, qa > q0 ? qa : q0, ex, ey, exy, pf, A, L, f.runb,
+                                f.runh, acc);
+    sweep_pairs<PPT, LT, true>(sp, se, q0, qa > q0 ? qa : q0, qend, ex, ey, exy, pf, A, L, f.runb,
+                               f.runh, acc);
 }
 
 template <int PPT, int LT>
@@ -385,6 +438,8 @@ __global__ void __launch_bounds__(kThreads, (PPT <= 4) ? 3 : 2)
     float exy[PPT];
     unsigned long long pf[PPT];
     load_entries<PPT>(ph, (int64_t)blockIdx.x, tid, ex, ey, exy, pf);
+    unsigned long long A, L;
+    warp_arc<PPT>(pf, (int64_t)blockIdx.x * (kThreads * PPT) + tid * PPT, ph.nent, A, L);
     // warp-uniform: a warp leaves together, so no lane is missing at the votes
     if (!__all_sync(0xffffffffu, mbar_wait_bounded(&bar, 0))) {
         if (tid == 0) {
@@ -398,7 +453,7 @@ __global__ void __launch_bounds__(kThreads, (PPT <= 4) ? 3 : 2)
     float acc[PPT];
 #pragma unroll
     for (int j = 0; j < PPT; j++) acc[j] = 0.f;
-    sweep_chunk<PPT, LT>(f, sp, se, c0, cend, n0, ex, ey, exy, pf, acc);
+    sweep_chunk<PPT, LT>(f, sp, se, c0, cend, n0, ex, ey, exy, pf, A, L, acc);
 #pragma unroll
     for (int j = 0; j < PPT; j++) {
         const int64_t e = (int64_t)blockIdx.x * (kThreads * PPT) + tid * PPT + j;
@@ -439,6 +494,7 @@ __global__ void __launch_bounds__(kThreads, (PPT <= 4) ? 3 : 2)
     const float4 *ef = ph.ef + model * ph.ldp;
     const unsigned long long *pfx = ph.pfx + model * ph.ldp;
     const float4 *runb = b.runb + S.flat0 / 64;
+    const ulonglong2 *runh = b.runh + S.flat0 / 64;
     float2 ex[PPT], ey[PPT];
     float exy[PPT];
     unsigned long long pf[PPT];
@@ -456,6 +512,8 @@ __global__ void __launch_bounds__(kThreads, (PPT <= 4) ? 3 : 2)
         exy[j] = sqrtf(fmaf(v.x, v.x, v.y * v.y));
         pf[j] = p;
     }
+    unsigned long long A, L;
+    warp_arc<PPT>(pf, tile * (kThreads * PPT) + tid * PPT, ph.nent, A, L);
     // warp-uniform: a warp leaves together, so no lane is missing at the votes
     if (!__all_sync(0xffffffffu, mbar_wait_bounded(&bar, 0))) {
         if (tid == 0) {
@@ -471,11 +529,11 @@ __global__ void __launch_bounds__(kThreads, (PPT <= 4) ? 3 : 2)
     const int64_t qa = qn0 < qend ? qn0 : qend;
     const int64_t qb = qa > q0 ? qa : q0;
     if (ltype == 1) {
-        sweep_pairs<PPT, 1, false>(sp, se, q0, q0, qb, ex, ey, exy, pf, runb, acc);
-        sweep_pairs<PPT, 1, true>(sp, se, q0, qb, qend, ex, ey, exy, pf, runb, acc);
+        sweep_pairs<PPT, 1, false>(sp, se, q0, q0, qb, ex, ey, exy, pf, A, L, runb, runh, acc);
+        sweep_pairs<PPT, 1, true>(sp, se, q0, qb, qend, ex, ey, exy, pf, A, L, runb, runh, acc);
     } else {
-        sweep_pairs<PPT, 0, false>(sp, se, q0, q0, qb, ex, ey, exy, pf, runb, acc);
-        sweep_pairs<PPT, 0, true>(sp, se, q0, qb, qend, ex, ey, exy, pf, runb, acc);
+        sweep_pairs<PPT, 0, false>(sp, se, q0, q0, qb, ex, ey, exy, pf, A, L, runb, runh, acc);
+        sweep_pairs<PPT, 0, true>(sp, se, q0, qb, qend, ex, ey, exy, pf, A, L, runb, runh, acc);
     }
 #pragma unroll
     for (int j = 0; j < PPT; j++) {

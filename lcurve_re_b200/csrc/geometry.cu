@@ -882,8 +882,13 @@ __global__ void __launch_bounds__(1024) k_interp(const DatumRec *__restrict__ da
 // is negative the computed mu of every face of the run is <= 0 and the run adds
 // exactly zero. All-zero records (padding) are left out; a run of padding only
 // gets C = -1.
-__device__ __forceinline__ void run_bound(const float *__restrict__ fp, int64_t npairs,
-                                          int64_t run, float4 *out) {
+// With ecl, also the run's eclipse-range hull: an arc [I, I + W) holding every
+// nonempty range (I_f, W_f + 1) of the run's faces, as the record (I, W), or
+// W = ~0 for "test every face" (ranges a quarter orbit long or spread over
+// more than that), (0, 0) when no face of the run has a range.
+__device__ __forceinline__ void run_bound(const float *__restrict__ fp,
+                                          const ulonglong2 *__restrict__ ecl, int64_t npairs,
+                                          int64_t run, float4 *out, ulonglong2 *hull) {
     const unsigned full = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int64_t q = run * 32 + lane;
@@ -917,12 +922,50 @@ __device__ __forceinline__ void run_bound(const float *__restrict__ fp, int64_t 
     if (lane == 0)
         *out = cnt > 0.f ? make_float4(ax, ay, r * (1.f + 1e-6f) + 1e-6f, c + 1e-5f)
                          : make_float4(0.f, 0.f, 0.f, -1.f);
+    if (!ecl) return;
+    ulonglong2 E[2] = {make_ulonglong2(0ull, 0ull), make_ulonglong2(0ull, 0ull)};
+    if (q < npairs) {
+        E[0] = ecl[2 * q];
+        E[1] = ecl[2 * q + 1];
+    }
+    const unsigned m = __ballot_sync(full, E[0].y != 0ull || E[1].y != 0ull);
+    ulonglong2 H = make_ulonglong2(0ull, 0ull);
+    if (m) {
+        // offsets from one range's start, as signed 64-bit distances on the circle
+        const unsigned long long mine = E[0].y != 0ull ? E[0].x : E[1].x;
+        const unsigned long long ref = __shfl_sync(full, mine, __ffs(m) - 1);
+        constexpr long long kQuarter = 1ll << 62;
+        long long lo = LLONG_MAX, hi = LLONG_MIN;
+        bool whole = false;
+        for (int k = 0; k < 2; k++)
+            if (E[k].y != 0ull) {
+                const long long off = (long long)(E[k].x - ref);
+                if (E[k].y >= (unsigned long long)kQuarter || off >= kQuarter || off <= -kQuarter) {
+                    whole = true;
+                } else {
+                    lo = off < lo ? off : lo;
+                    const long long end = off + (long long)E[k].y;
+                    hi = end > hi ? end : hi;
+                }
+            }
+        for (int o = 16; o > 0; o >>= 1) {
+            const long long l2 = __shfl_xor_sync(full, lo, o), h2 = __shfl_xor_sync(full, hi, o);
+            lo = l2 < lo ? l2 : lo;
+            hi = h2 > hi ? h2 : hi;
+        }
+        whole = __any_sync(full, whole);
+        H = whole ? make_ulonglong2(0ull, ~0ull)
+                  : make_ulonglong2(ref + (unsigned long long)lo,
+                                    (unsigned long long)hi - (unsigned long long)lo);
+    }
+    if (lane == 0) *hull = H;
 }
 
-__global__ void k_run_bounds(const float *__restrict__ fp, int64_t npairs, float4 *runb) {
+__global__ void k_run_bounds(const float *__restrict__ fp, const ulonglong2 *__restrict__ ecl,
+                             int64_t npairs, float4 *runb, ulonglong2 *runh) {
     const int64_t run = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     if (run >= (npairs + 31) / 32) return;  // whole warps
-    run_bound(fp, npairs, run, runb + run);
+    run_bound(fp, ecl, npairs, run, runb + run, runh + run);
 }
 
 // Run bounds of the continuum list's slots (16 runs per 1024-face block).
@@ -937,7 +980,8 @@ __global__ void k_run_bounds_b(BatchDev b) {
         const int k = find_seg(b.cont_blk, nk, B);
         const SlotDev &S = b.slots[b.cont_slot[k]];
         const int64_t run = (B - b.cont_blk[k]) * 16 + (w & 15);
-        run_bound(b.fp + 8 * S.flat0, (S.nface + 1) / 2, run, b.runb + S.flat0 / 64 + run);
+        run_bound(b.fp + 8 * S.flat0, b.ecl + S.flat0, (S.nface + 1) / 2, run,
+                  b.runb + S.flat0 / 64 + run, b.runh + S.flat0 / 64 + run);
     }
 }
 
@@ -1446,7 +1490,7 @@ void launch_flatten(GridDev g, FlatDev f, int32_t *blockcnt, int mixed, int need
     count_launch();
     k_flat_scatter<<<nb, kFlatBlock, 0, s>>>(g, f, blockcnt, mixed, need_pos, fc);
     count_launch();
-    if (mixed && fc.on) launch_run_bounds(f.fp, f.npad / 2, f.runb, s);
+    if (mixed && fc.on) launch_run_bounds(f.fp, f.ecl, f.npad / 2, f.runb, f.runh, s);
 }
 
 void launch_phases(const PhaseParams &p, const DatumRec *data, const int64_t *off, int32_t n,
@@ -1485,10 +1529,11 @@ void launch_interp(const DatumRec *data, int32_t n, const int64_t *idx, int32_t 
     count_launch();
 }
 
-void launch_run_bounds(const float *fp, int64_t npairs, float4 *runb, cudaStream_t s) {
+void launch_run_bounds(const float *fp, const ulonglong2 *ecl, int64_t npairs, float4 *runb,
+                       ulonglong2 *runh, cudaStream_t s) {
     const int64_t nruns = (npairs + 31) / 32;
     if (nruns <= 0) return;
-    k_run_bounds<<<nblocks(nruns * 32, 256), 256, 0, s>>>(fp, npairs, runb);
+    k_run_bounds<<<nblocks(nruns * 32, 256), 256, 0, s>>>(fp, ecl, npairs, runb, runh);
     count_launch();
 }
 
