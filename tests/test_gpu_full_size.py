@@ -20,7 +20,7 @@ Configurations:
     60, 153, 211, 297, 315, 333, 339 and 400 (nlat1f = nlat2f / 2), 2000
     points, through lcg_light_curve_batch (mixed) and one by one in FP64.
 
-Bars (north_star): per-point relative flux error <= 1e-6 in FP64 mode and
+Bars: per-point relative flux error <= 1e-6 in FP64 mode and
 <= 1e-5 in mixed mode; chi**2 (re_scale'd, on noisy data) within 1e-6
 relative in FP64 mode and within MIXED_CHI2 relative in mixed mode; per-face
 eclipse flags identical at every sub-phase of the workload except within
