@@ -94,6 +94,7 @@ def parse():
     ap.add_argument("--is-target", type=float, default=20000.0,
                     help="surrogate_da: effective size at which the importance sampling stops")
     ap.add_argument("--precision", choices=("mixed", "fp64"), default="mixed")
+    ap.add_argument("--ref-cuda-child", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--headline-only", action="store_true",
@@ -187,11 +188,13 @@ class RefTimer:
     grids, eclipses, continuum and FlatGrids are rebuilt, as the GPU arm's
     FLAG_NO_CACHE does. Nothing is extrapolated."""
 
-    def __init__(self, model, data):
+    def __init__(self, model, data, path=None):
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         import oracle_lib as OL
         self.kind = "reference"
-        if os.path.exists(OL.REF_RELEASE_SO):
+        if path is not None:
+            self.lib = OL.Reference(path)
+        elif os.path.exists(OL.REF_RELEASE_SO):
             self.lib = OL.Reference(OL.REF_RELEASE_SO)
         else:
             self.kind = "port"
@@ -252,7 +255,7 @@ def run_reference(args):
         return None
     model, data, desc = workload(args.workload)
     r = RefTimer(model, data)
-    r.exact_curve()
+    cpu_calc = r.exact_curve()[0]
     for _ in range(args.warmup):
         r.curve()
     ts = [r.curve() for _ in range(args.steps)]
@@ -265,7 +268,65 @@ def run_reference(args):
             "cpu_baseline": {"value": v, "unit": METRIC, "cores": os.cpu_count(), "kind": r.kind,
                              "sample": r.describe(args.steps, mean_t)},
             "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if args.workload == "wd_dm_large" and r.kind == "reference":
+        rc = reference_cuda_rate(args, cpu_calc)
+        if rc is not None:
+            line["reference_cuda"] = rc
     return line
+
+
+REF_CUDA_SO = os.path.join(ROOT, "oracle", "_ref", "liblcurve_ref_cuda.so")
+
+
+def reference_cuda_child(args):
+    """Runs in a child process (the reference's GPU build and its CPU build
+    define the same symbols): times whole light curves of the workload
+    through the reference's own CUDA path (oracle/_ref/liblcurve_ref_cuda.so:
+    its CPU sources with HAVE_CUDA plus comp_light_cuda.cu and
+    set_star_grid_cuda.cu for sm_100a, switched on by LCURVE_CUDA=1 and
+    LCURVE_CUDA_GRID=1 as its users do), and writes the unperturbed curve
+    for the parent's check."""
+    model, data, _ = workload(args.workload)
+    r = RefTimer(model, data, path=REF_CUDA_SO)
+    calc, chisq, _ = r.exact_curve()
+    np.save(args.ref_cuda_child, calc)
+    for _ in range(2):
+        r.curve()
+    ts = []
+    while len(ts) < 3 or (sum(ts) < 15.0 and len(ts) < 50):
+        ts.append(r.curve())
+    print(json.dumps({"t_curve": float(np.mean(ts)), "calls": len(ts), "chisq": chisq}),
+          flush=True)
+
+
+def reference_cuda_rate(args, cpu_calc):
+    """The reference's own GPU path on the same workload, timed in a child
+    process on whole light curves (an informative secondary baseline: the
+    reference arm's value stays its CPU path); None when that build is
+    absent."""
+    if not os.path.exists(REF_CUDA_SO):
+        return None
+    import subprocess
+    import tempfile
+    env = dict(os.environ, LCURVE_CUDA="1", LCURVE_CUDA_GRID="1")
+    with tempfile.TemporaryDirectory() as d:
+        out = os.path.join(d, "calc.npy")
+        r = subprocess.run([sys.executable, os.path.abspath(__file__), "--workload", args.workload,
+                            "--ref-cuda-child", out], env=env, capture_output=True, text=True,
+                           timeout=600)
+        lines = [x for x in r.stdout.splitlines() if x.startswith("{")]
+        if r.returncode != 0 or not lines:
+            return {"unavailable": "reference CUDA build failed: %s" % r.stderr.strip()[-300:]}
+        res = json.loads(lines[-1])
+        calc = np.load(out)
+    v = 1.0 / res["t_curve"]
+    return {"value": v, "unit": METRIC, "kind": "reference GPU path (comp_light_cuda.cu, "
+                                                "set_star_grid_cuda.cu, sm_100a)",
+            "precision": "the reference's CUDA default (FP32 sweep and grid)",
+            "sample": "whole light curves, grids rebuilt every call, %d timed calls; one light "
+                      "curve = %.3f s" % (res["calls"], res["t_curve"]),
+            "max_rel_flux_error_vs_its_cpu_path": float(np.max(np.abs(calc - cpu_calc) /
+                                                                np.abs(cpu_calc)))}
 
 
 # ---- our arm -------------------------------------------------------------------------
@@ -1197,6 +1258,8 @@ MCMC_NAMED = dict(mcmc_steps=20000)
 
 def main():
     args = parse()
+    if args.ref_cuda_child:
+        return reference_cuda_child(args) or 0
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
         return launch_ranks(args.gpus)
     rank, local, world = rank_info()
