@@ -943,7 +943,7 @@ def run_surrogate(args):
     chd, _, _, accd, wall_d, st = delayed_acceptance(exact2, sur_loc_chi, theta0, None,
                                                       args.mcmc_steps, seed=21, compact=comp2,
                                                       propose=walk_da)
-    launches_da = int(lib.lcg_kernel_launches(1))
+    launches_da = int(lib.lcg_kernel_launches(1)) + getattr(sur_loc_chi, "graph_launches", 0)
     clk = clocks.stop()
     sum_p, sum_d, sum_g = summary(chp, wall_p), summary(chd, wall_d), summary(chg, wall_g)
     shift, mcse = mean_shift(chd, chp)

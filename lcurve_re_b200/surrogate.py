@@ -427,6 +427,9 @@ class SurrogateChi2:
             self._pca(self.g_sx, self.g_sy, self.g_F, self.g_chr)
         self.gr_screen = self._capture(screen)
         self.gr_reverse = self._capture(reverse)
+        # this library's kernels per replay (the host launch counter does not
+        # see graph replays): the network and the chi**2 head, the chi**2 head
+        self.graph_launches = 0
 
     def _capture(self, fn):
         torch = self.torch
@@ -445,11 +448,13 @@ class SurrogateChi2:
         self.h_x.numpy()[:] = to_unit(theta)
         self.g_x.copy_(self.h_x, non_blocking=True)
         self.gr_screen.replay()
+        self.graph_launches += 2
         return self.g_chi.cpu().numpy()
 
     def reverse(self):
         """The bound reverse pass (g_F holds the proposals' exact curves)."""
         self.gr_reverse.replay()
+        self.graph_launches += 1
         return self.g_chr.cpu().numpy()
 
     def merge(self, accepted):
