@@ -77,7 +77,9 @@ def parse():
     ap.add_argument("--ncoef", type=int, default=64)
     ap.add_argument("--local-curves", type=int, default=131072)
     ap.add_argument("--refine-epochs", type=int, default=600)
-    ap.add_argument("--da-scales", type=float, nargs="+", default=[1.0, 1.5, 2.0, 3.0],
+    ap.add_argument("--da-min-accept", type=float, default=0.025,
+                    help="surrogate_da: least pilot acceptance of a delayed-acceptance scale")
+    ap.add_argument("--da-scales", type=float, nargs="+", default=[1.0, 1.5, 2.0, 2.5],
                     help="surrogate_da: multiples of the plain step scale tried by the "
                          "delayed-acceptance pilot runs")
     ap.add_argument("--adapt-rounds", type=int, default=2,
@@ -920,7 +922,9 @@ def run_surrogate(args):
     # delayed acceptance can afford bolder steps, since the surrogate screens
     # them: short pilot runs pick the multiple of the plain step scale with
     # the largest expected squared jump (in the walk's whitened coordinates)
-    # per second of sampling
+    # per second of sampling, among those whose acceptance stays at or above
+    # da_min_accept (rarer, larger jumps score well on the squared jump while
+    # the chains stick between them)
     da_pilots = []
     for k in args.da_scales:
         walk = tw.with_scale(tw.scale * k)
@@ -932,7 +936,8 @@ def run_surrogate(args):
         u = tw.forward(cpl.reshape(-1, 9)).reshape(cpl.shape) @ np.linalg.inv(tw.chol.T)
         esjd = float(np.mean(np.sum(np.diff(u, axis=0) ** 2, axis=2)))
         da_pilots.append((k, acc_k, esjd / wall_k))
-    da_scale = max(da_pilots, key=lambda t: t[2])[0]
+    ok = [t for t in da_pilots if t[1] >= args.da_min_accept] or da_pilots[:1]
+    da_scale = max(ok, key=lambda t: t[2])[0]
     walk_da = tw.with_scale(tw.scale * da_scale)
     chg, _, _, accg, wall_g, stg = delayed_acceptance(exact_g, sur_chi, theta0, None,
                                                        args.mcmc_steps, seed=21, compact=comp_g,

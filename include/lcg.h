@@ -227,8 +227,12 @@ const double *lcg_device_calc(lcg_ctx *ctx);
  * once for the whole batch (one CUDA graph, replayed while the batch keeps
  * its size and grid resolutions), and a model's grids are rebuilt only when
  * its geometry parameters changed since the previous batch call on ctx (its
- * continuum only when its brightness parameters did). Other models are
- * evaluated one by one. LCG_FLAG_DIAGNOSTICS is ignored. */
+ * continuum only when its brightness parameters did). Other models (every
+ * model on an FP64 context) take the single-model path, concurrently on up
+ * to eight worker contexts of ctx's device and precision (one host thread
+ * and stream each, created on first use, holding a copy of the resident
+ * points): their results are those of single calls. LCG_FLAG_DIAGNOSTICS is
+ * ignored. */
 lcg_status lcg_light_curve_batch(lcg_ctx *ctx, const lcg_model *models,
                                  int32_t nmodels, const lcg_datum *data,
                                  int32_t n, int32_t flags, double *sfac,

@@ -763,23 +763,75 @@ extern "C" lcg_status lcg_light_curve_batch_resident(lcg_ctx *c, const lcg_model
             if (md[m].live)
                 c->flux_elements += (B.face0[2 * m + 2] - B.face0[2 * m]) * B.nent;
     }
-    // the rest, one at a time
-    for (int32_t m = 0; m < nmodels; m++) {
-        if (inb[m] || status[m]) continue;
+    // the rest through the single-model path: on this context when there is
+    // one, else concurrently on up to kWorkers worker contexts (same device,
+    // precision and points; each model's arithmetic is that of the
+    // single-model path, so the results are those of evaluating them one at
+    // a time)
+    std::vector<int32_t> rest;
+    for (int32_t m = 0; m < nmodels; m++)
+        if (!inb[m] && !status[m]) rest.push_back(m);
+    auto one = [&](lcg_ctx *x, int32_t m) -> lcg_status {
         double sc[LCG_NOUT] = {0};
         if (chisq) sc[LCG_OUT_CHISQ] = chisq[m];
         if (wnok) sc[LCG_OUT_WNOK] = wnok[m];
-        lcg_status rc = lcg_light_curve_resident(c, models + m, flags, sfac + 5 * (size_t)m,
+        lcg_status rc = lcg_light_curve_resident(x, models + m, flags, sfac + 5 * (size_t)m,
                                                  calc ? calc + (size_t)m * n : nullptr, sc);
         status[m] = rc;
         if (rc) {
             if (calc) memset(calc + (size_t)m * n, 0, (size_t)n * sizeof(double));
-            if (rc == LCG_E_CUDA || rc == LCG_E_NOMEM) return rc;
-            continue;
+            return rc;
         }
         if (chisq) chisq[m] = sc[LCG_OUT_CHISQ];
         if (wnok) wnok[m] = sc[LCG_OUT_WNOK];
+        return LCG_OK;
+    };
+    constexpr int kWorkers = 8;
+    const int nw = (int)std::min<size_t>(rest.size(), kWorkers);
+    if (nw <= 1) {
+        for (int32_t m : rest) {
+            lcg_status rc = one(c, m);
+            if (rc == LCG_E_CUDA || rc == LCG_E_NOMEM) return rc;
+        }
+        c->err.clear();
+        return LCG_OK;
     }
+    lcg_options o;
+    lcg_default_options(&o);
+    o.device = c->device;
+    o.precision = c->precision;
+    o.eclipse_warp = c->eclipse_warp;
+    while ((int)c->workers.size() < nw) {
+        lcg_ctx *w = nullptr;
+        lcg_status rc = lcg_create(&w, &o);
+        if (rc) return c->fail(rc, "creating a batch worker context");
+        c->workers.push_back(w);
+        c->worker_data_version.push_back(-1);
+    }
+    for (int k = 0; k < nw; k++)
+        if (c->worker_data_version[k] != c->data_version) {
+            lcg_status rc = lcg_set_data(c->workers[k],
+                                         reinterpret_cast<const lcg_datum *>(c->h_data.data()),
+                                         (int32_t)c->h_data.size());
+            if (rc) return c->fail(rc, "resident points of a batch worker");
+            c->worker_data_version[k] = c->data_version;
+        }
+    std::vector<lcg_status> fatal((size_t)nw, LCG_OK);
+    std::vector<std::thread> threads;
+    for (int k = 0; k < nw; k++)
+        threads.emplace_back([&, k] {
+            cudaSetDevice(c->device);
+            for (size_t j = (size_t)k; j < rest.size(); j += (size_t)nw) {
+                lcg_status rc = one(c->workers[k], rest[j]);
+                if (rc == LCG_E_CUDA || rc == LCG_E_NOMEM) {
+                    fatal[(size_t)k] = rc;
+                    return;
+                }
+            }
+        });
+    for (auto &t : threads) t.join();
+    for (lcg_status rc : fatal)
+        if (rc) return rc;
     c->err.clear();
     return LCG_OK;
 }

@@ -165,6 +165,14 @@ struct lcg_ctx {
     Grid g1f, g2f, g1c, g2c;
     // batched evaluation (batch.cu); NULL until the first batch
     lcg::eng::BatchState *batch = nullptr;
+    // the models a batch call evaluates through the single-model path (every
+    // model of an FP64 context; those outside the batched stages otherwise)
+    // run on worker contexts, one host thread and one stream each, so that
+    // their latency-bound pipelines overlap on the GPU; each worker holds a
+    // copy of the resident points (h_data, from lcg_set_data)
+    std::vector<lcg_ctx *> workers;
+    std::vector<int64_t> worker_data_version;
+    std::vector<DatumRec> h_data;
     // work buffers
     DBuf<DevStatus> status;
     DBuf<int32_t> queue, counters, blockcnt;

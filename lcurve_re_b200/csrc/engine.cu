@@ -723,6 +723,8 @@ lcg_status lcg_create(lcg_ctx **out, const lcg_options *opt) {
 
 void lcg_destroy(lcg_ctx *c) {
     if (!c) return;
+    for (lcg_ctx *w : c->workers) lcg_destroy(w);
+    c->workers.clear();
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     c->collect_timers();
@@ -815,6 +817,8 @@ lcg_status lcg_set_data(lcg_ctx *c, const lcg_datum *data, int32_t n) {
         return c->cuda_fail(e, "data buffers");
     cudaMemcpyAsync(c->data.p, data, (size_t)n * sizeof(DatumRec), cudaMemcpyHostToDevice,
                     c->stream);
+    c->h_data.assign(reinterpret_cast<const DatumRec *>(data),
+                     reinterpret_cast<const DatumRec *>(data) + n);
     cudaMemcpyAsync(c->off.p, off.data(), (size_t)(n + 1) * sizeof(int64_t),
                     cudaMemcpyHostToDevice, c->stream);
     c->data_n = n;

@@ -17,8 +17,9 @@ covariance of its Jacobian, on a model that runs every branch
 
 Precision: on a mixed-precision engine context a round of perturbed models is
 one graph-captured batch. On an FP64 context lcg_light_curve_batch evaluates
-the models of the round one after another on the GPU (the batched flux sweep
-is the mixed-precision one), with the same results as single calls.
+the models of the round through the bit-identical FP64 single-model path,
+concurrently on up to eight worker contexts (their latency-bound pipelines
+overlap on the GPU), with the same results as single calls.
 """
 import numpy as np
 

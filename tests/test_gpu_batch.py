@@ -157,15 +157,32 @@ def test_batch_profiled_run_equals_graph_run(data):
         e.close()
 
 
-def test_batch_on_fp64_context_runs_one_by_one(data, oracle):
-    ms = _models(k=3, seed=41)
+def test_batch_on_fp64_context_runs_on_concurrent_workers(data, oracle):
+    """An FP64 batch takes the single-model path on up to eight concurrent
+    worker contexts: 12 models (the workers take several each) give exactly
+    the curves and chi**2 of single calls on the same points, within 1e-6 of
+    the oracle; a model outside its lobe keeps its own status; after new
+    points the workers evaluate on those."""
+    ms = _models(k=12, seed=41)
+    bad = ms[5].copy()
+    bad["r2"] = 0.9  # past the Roche lobe
+    ms[5] = bad
     e = Engine(precision="fp64")
     try:
-        calc, chisq, wnok, sf, st = e.light_curve_batch(ms, data)
-        assert np.all(st == 0)
-        for i, m in enumerate(ms):
-            o_st, err, o_calc, _, _ = oracle.light_curve(m, data, scale=True, rdata=True)
-            assert _rel(calc[i], o_calc) < 1e-6
+        for pts in (data, data[: len(data) // 2].copy()):
+            calc, chisq, wnok, sf, st = e.light_curve_batch(ms, pts)
+            assert st[5] != 0 and calc[5].max() == 0
+            for i, m in enumerate(ms):
+                if i == 5:
+                    continue
+                assert st[i] == 0
+                one = e.light_curve_comp(m, pts, scale=True, rdata=True, sfac=np.ones(5),
+                                         diagnostics=False)
+                assert np.array_equal(calc[i], one[0]), i
+                assert chisq[i] == one[2], i
+                if pts is data and i < 3:
+                    o_st, err, o_calc, _, _ = oracle.light_curve(m, pts, scale=True, rdata=True)
+                    assert _rel(calc[i], o_calc) < 1e-6
     finally:
         e.close()
 
