@@ -75,7 +75,7 @@ def parse():
                          "with its final proposal kept (no further adaptation), before the "
                          "local draws")
     ap.add_argument("--ncoef", type=int, default=64)
-    ap.add_argument("--local-curves", type=int, default=131072)
+    ap.add_argument("--local-curves", type=int, default=262144)
     ap.add_argument("--refine-epochs", type=int, default=600)
     ap.add_argument("--da-min-accept", type=float, default=0.025,
                     help="surrogate_da: least pilot acceptance of a delayed-acceptance scale")
