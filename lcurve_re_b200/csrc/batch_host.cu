@@ -23,6 +23,9 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
+#include <condition_variable>
+#include <functional>
 #include <map>
 #include <mutex>
 #include <thread>
@@ -44,22 +47,87 @@ struct RingSet {
 
 inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
-// Runs f(i) for i in [0, n) on up to 16 host threads.
+// Host threads kept for the per-model setup of batch calls (started on first
+// use): spawning them per call cost more than the setup of a few dozen
+// models. One job at a time (calls from several host threads queue on
+// call_mu); the caller works on the job too, so it finishes even before the
+// workers wake.
+class SetupPool {
+public:
+    static SetupPool &get() {
+        static SetupPool p;
+        return p;
+    }
+    int threads() const { return (int)th_.size() + 1; }
+
+    void run(int n, const std::function<void(int)> &f) {
+        std::lock_guard<std::mutex> call(call_mu_);
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            job_ = &f;
+            n_ = n;
+            next_.store(0);
+            busy_ = (int)th_.size();
+            gen_++;
+        }
+        cv_.notify_all();
+        work();
+        std::unique_lock<std::mutex> lk(mu_);
+        done_.wait(lk, [&] { return busy_ == 0; });
+        job_ = nullptr;
+    }
+
+private:
+    SetupPool() {
+        const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+        const int nt = (int)std::min<unsigned>(15u, hw > 1 ? hw - 1 : 0u);
+        for (int t = 0; t < nt; t++) th_.emplace_back([this] { loop(); });
+    }
+    ~SetupPool() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+            gen_++;
+        }
+        cv_.notify_all();
+        for (auto &t : th_) t.join();
+    }
+    void work() {
+        for (int i = next_.fetch_add(1); i < n_; i = next_.fetch_add(1)) (*job_)(i);
+    }
+    void loop() {
+        uint64_t seen = 0;
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+                if (stop_) return;
+                seen = gen_;
+            }
+            work();
+            std::lock_guard<std::mutex> lk(mu_);
+            if (--busy_ == 0) done_.notify_one();
+        }
+    }
+    std::vector<std::thread> th_;
+    std::mutex mu_, call_mu_;
+    std::condition_variable cv_, done_;
+    const std::function<void(int)> *job_ = nullptr;
+    int n_ = 0, busy_ = 0;
+    uint64_t gen_ = 0;
+    bool stop_ = false;
+    std::atomic<int> next_{0};
+};
+
+// Runs f(i) for i in [0, n): inline for a few items, else on SetupPool.
 template <class F>
 void parallel_for(int n, F f) {
-    int nt = (int)std::min<unsigned>(16u, std::max(1u, std::thread::hardware_concurrency()));
-    if (n < 32 || nt < 2) {
+    if (n < 8) {
         for (int i = 0; i < n; i++) f(i);
         return;
     }
-    nt = std::min(nt, n / 8);
-    std::vector<std::thread> th;
-    th.reserve(nt);
-    for (int t = 0; t < nt; t++)
-        th.emplace_back([&, t] {
-            for (int i = t; i < n; i += nt) f(i);
-        });
-    for (auto &x : th) x.join();
+    const std::function<void(int)> g = f;
+    SetupPool::get().run(n, g);
 }
 
 }  // namespace
