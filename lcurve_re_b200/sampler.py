@@ -396,12 +396,16 @@ class TriangularWalk:
         rng = np.random.default_rng(seed)
         L = np.linalg.cholesky(self.cov_u) * widen
         out = np.empty((0, self.d))
-        while len(out) < n:
+        for _ in range(1000):
+            if len(out) >= n:
+                return out[:n]
             x = self.inverse(self.mean_u + rng.standard_normal((2 * n, self.d)) @ L.T)
             if box_check is not None:
                 x = x[box_check(x)]
             out = np.r_[out, x]
-        return out[:n]
+        if len(out) >= n:
+            return out[:n]
+        raise ValueError("the box holds too few of the draws (%d of %d)" % (len(out), n))
 
     def __call__(self, rng, theta):
         # the samplers move few chains per step: map only the rows that
