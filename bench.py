@@ -77,7 +77,7 @@ def parse():
     ap.add_argument("--ncoef", type=int, default=64)
     ap.add_argument("--local-curves", type=int, default=262144)
     ap.add_argument("--refine-epochs", type=int, default=600)
-    ap.add_argument("--da-min-accept", type=float, default=0.025,
+    ap.add_argument("--da-min-accept", type=float, default=0.02,
                     help="surrogate_da: least pilot acceptance of a delayed-acceptance scale")
     ap.add_argument("--da-scales", type=float, nargs="+", default=[1.0, 1.5, 2.0, 2.5],
                     help="surrogate_da: multiples of the plain step scale tried by the "

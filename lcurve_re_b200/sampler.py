@@ -24,6 +24,7 @@ so the batched engine skips them entirely.
 """
 import copy
 import time
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 
@@ -302,13 +303,23 @@ class CompactExact:
 
 
 class GaussianWalk:
-    """The random-walk proposal y = x + N(0, cov)."""
+    """The random-walk proposal y = x + N(0, cov). delta draws every row's
+    step at once; apply forms the proposals of all chains from their steps,
+    apply_rows those of some of them (row by row: the rows of the whole)."""
 
     def __init__(self, cov):
         self.chol = np.linalg.cholesky(cov)
 
+    def delta(self, rng, shape):
+        return rng.standard_normal(shape) @ self.chol.T
+
+    def apply(self, theta, delta):
+        return theta + delta
+
+    apply_rows = apply
+
     def __call__(self, rng, theta):
-        return theta + rng.standard_normal(theta.shape) @ self.chol.T
+        return self.apply(theta, self.delta(rng, theta.shape))
 
 
 def _quadratic_features(z):
@@ -407,9 +418,14 @@ class TriangularWalk:
             return out[:n]
         raise ValueError("the box holds too few of the draws (%d of %d)" % (len(out), n))
 
-    def __call__(self, rng, theta):
-        # the samplers move few chains per step: map only the rows that
-        # changed since the last call (the cached u of the others is exact)
+    def delta(self, rng, shape):
+        """Every row's step in the straightened coordinates."""
+        return rng.standard_normal(shape) @ self.chol.T
+
+    def apply(self, theta, delta):
+        """Proposals T^-1(T(theta) + delta) of every chain. It maps only the
+        rows that changed since the last call (the samplers move few chains
+        per step)."""
         th, u = getattr(self, "_cache", (None, None))
         if th is None or th.shape != theta.shape:
             u = self.forward(theta)
@@ -419,7 +435,21 @@ class TriangularWalk:
                 u = u.copy()
                 u[moved] = self.forward(theta[moved])
         self._cache = (theta.copy(), u)
-        return self.inverse(u + rng.standard_normal(u.shape) @ self.chol.T)
+        return self.inverse(u + delta)
+
+    def apply_rows(self, theta, delta):
+        """The same map for some of the chains, row by row, leaving apply's
+        record of the last states alone."""
+        return self.inverse(self.forward(theta) + delta)
+
+    def __call__(self, rng, theta):
+        return self.apply(theta, self.delta(rng, theta.shape))
+
+
+def _splits(propose):
+    """Whether a proposal forms its steps as delta(rng, shape) then
+    apply(theta, delta) for every chain or apply_rows for some."""
+    return all(hasattr(propose, a) for a in ("delta", "apply", "apply_rows"))
 
 
 def _take(x, idx):
@@ -499,7 +529,14 @@ def _delayed_acceptance_graphs(exact, sur, theta0, propose, steps, seed, box_che
     CUDA graphs on static buffers (sur.bind): one launch each instead of the
     network's layer-by-layer launches and allocations. Same draws and
     decisions as the other loops; with compact (a CompactExact), the
-    stage-1 chains' exact evaluations go through its small batch."""
+    stage-1 chains' exact evaluations go through its small batch.
+
+    With a proposal that splits into delta and apply (both walks), the next
+    step's proposals are formed on the host while a worker thread runs this
+    step's exact evaluations: the next step's noise is drawn right after
+    this step's two uniforms (the order of the draws of the plain loop),
+    every chain's proposal is formed from its current state, and the rows of
+    the chains that then move are formed again from their new states."""
     import torch
     rng = np.random.default_rng(seed)
     theta = np.array(theta0, np.float64)
@@ -511,25 +548,45 @@ def _delayed_acceptance_graphs(exact, sur, theta0, propose, steps, seed, box_che
     last = theta.copy()
     chain = np.empty((steps,) + theta.shape) if record else None
     acc = stage1 = 0
+    split = _splits(propose)
+    pool = ThreadPoolExecutor(max_workers=1) if split else None
     t0 = time.perf_counter()
+    if split:
+        prop = propose.apply(theta, propose.delta(rng, theta.shape))
     for s in range(steps):
-        prop = propose(rng, theta)
+        if not split:
+            prop = propose(rng, theta)
         ok = box_check(prop)
         chi_a = sur.screen(prop)  # chi**2 of exact(x) s(y) / s(x)
         chi_a[~ok] = np.inf
         log_g = np.minimum(0.0, -(chi_a - chi) / 2)
         a1 = ok & (np.log(rng.random(nc)) < log_g)
         u2 = np.log(rng.random(nc))
+        ahead = split and s + 1 < steps
+        if ahead:
+            d = propose.delta(rng, theta.shape)
         if a1.any():
             if compact is not None:
-                chi_p = np.full(nc, np.inf)
                 idx = np.flatnonzero(a1)
-                chi_p[idx] = compact(idx, prop, sur.g_F)  # rows of a1 chains: exact(y)
+
+                def run(idx=idx, prop=prop):
+                    chi_p = np.full(nc, np.inf)
+                    chi_p[idx] = compact(idx, prop, sur.g_F)  # rows of a1 chains: exact(y)
+                    return chi_p
             else:
                 ev = np.where(a1[:, None], prop, last)
-                chi_p = exact(ev)
                 last = ev
-                exact.curves_all_device(sur.g_F)  # rows of a1 chains: exact(y)
+
+                def run(ev=ev):
+                    chi_p = exact(ev)
+                    exact.curves_all_device(sur.g_F)  # rows of a1 chains: exact(y)
+                    return chi_p
+            if ahead:
+                job = pool.submit(run)
+                nxt = propose.apply(theta, d)
+                chi_p = job.result()
+            else:
+                chi_p = run()
             chi_rev = sur.reverse()
             log_g_rev = np.where(a1, np.minimum(0.0, -(chi_rev - chi_p) / 2), 0.0)
             with np.errstate(invalid="ignore"):
@@ -539,11 +596,19 @@ def _delayed_acceptance_graphs(exact, sur, theta0, propose, steps, seed, box_che
             chi[a2] = chi_p[a2]
             if a2.any():
                 sur.merge(a2)
+                if ahead:
+                    nxt[a2] = propose.apply_rows(theta[a2], d[a2])
             acc += int(a2.sum())
             stage1 += int(a1.sum())
+        elif ahead:
+            nxt = propose.apply(theta, d)
         if record:
             chain[s] = theta
+        if ahead:
+            prop = nxt
     wall = time.perf_counter() - t0
+    if pool is not None:
+        pool.shutdown()
     n = steps * nc
     return chain, theta, chi, acc / n, wall, {"stage1_rate": stage1 / n,
                                               "stage2_rate": acc / max(stage1, 1)}
@@ -554,7 +619,15 @@ def metropolis(exact, theta0, cov, steps, seed=0, box_check=in_box, record=True,
     """Plain Metropolis on every chain at once, with the Gaussian random walk
     of covariance cov or another symmetric proposal (propose(rng, theta) ->
     proposals, e.g. TriangularWalk). Returns (chain [steps x chains x params]
-    or None, final theta, final chi**2, acceptance rate, wall seconds)."""
+    or None, final theta, final chi**2, acceptance rate, wall seconds).
+
+    With a proposal that splits into delta and apply (both walks), the next
+    step's proposals are formed on the host while a worker thread runs this
+    step's exact evaluations, as in the delayed-acceptance loop: the
+    acceptance uniforms are drawn before the evaluation and the next step's
+    noise after them (the same order of draws as drawing them in turn), and
+    the rows of the chains that move are formed again from their new
+    states. Same chains either way."""
     rng = np.random.default_rng(seed)
     propose = propose or GaussianWalk(cov)
     theta = np.array(theta0, np.float64)
@@ -562,21 +635,42 @@ def metropolis(exact, theta0, cov, steps, seed=0, box_check=in_box, record=True,
     last = theta.copy()
     chain = np.empty((steps,) + theta.shape) if record else None
     acc = 0
+    nc = theta.shape[0]
+    split = _splits(propose)
+    pool = ThreadPoolExecutor(max_workers=1) if split else None
     t0 = time.perf_counter()
+    if split:
+        prop = propose.apply(theta, propose.delta(rng, theta.shape))
     for s in range(steps):
-        prop = propose(rng, theta)
+        if not split:
+            prop = propose(rng, theta)
         ok = box_check(prop)
         ev = np.where(ok[:, None], prop, last)
-        chi_p = exact(ev)
+        ahead = split and s + 1 < steps
+        if ahead:
+            u = rng.random(nc)
+            d = propose.delta(rng, theta.shape)
+            job = pool.submit(exact, ev)
+            nxt = propose.apply(theta, d)
+            chi_p = job.result()
+        else:
+            chi_p = exact(ev)
+            u = rng.random(nc)
         chi_p[~ok] = np.inf
-        a = np.log(rng.random(theta.shape[0])) < -(chi_p - chi) / 2
+        a = np.log(u) < -(chi_p - chi) / 2
         theta[a] = prop[a]
         chi[a] = chi_p[a]
         last = ev
         acc += int(a.sum())
         if record:
             chain[s] = theta
+        if ahead:
+            if a.any():
+                nxt[a] = propose.apply_rows(theta[a], d[a])
+            prop = nxt
     wall = time.perf_counter() - t0
+    if pool is not None:
+        pool.shutdown()
     return chain, theta, chi, acc / (steps * theta.shape[0]), wall
 
 

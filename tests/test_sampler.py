@@ -316,3 +316,22 @@ def test_triangular_walk_mixes_a_curved_ridge_where_the_gaussian_walk_does_not()
         s = c.reshape(-1, 3)
         mcse = s.std(0) / np.sqrt(ess_bulk(c))
         assert np.all(np.abs(s.mean(0) - exact_mean) < 4 * mcse), (s.mean(0), mcse)
+
+
+def test_forming_proposals_ahead_keeps_the_chains():
+    """metropolis forms the next step's proposals while the exact model runs
+    (from the current states, then again for the chains that moved); the
+    chains equal those of proposing in turn, with the same draws, for the
+    Gaussian walk exactly and for the triangular walk to rounding (a row's
+    map formed alone or among all rows)."""
+    from lcurve_re_b200.sampler import GaussianWalk, TriangularWalk
+    theta0 = _banana_draws(64, 8)
+    tw = TriangularWalk(_banana_draws(20000, 9))
+    for walk, tol in ((GaussianWalk(np.cov(_banana_draws(5000, 10).T)), 0.0), (tw, 1e-12)):
+        in_turn = lambda rng, theta, w=walk: w(rng, theta)  # no delta/apply: one at a time
+        a = metropolis(_banana_chi, theta0, None, 300, seed=11, box_check=_everywhere,
+                       propose=walk)
+        b = metropolis(_banana_chi, theta0, None, 300, seed=11, box_check=_everywhere,
+                       propose=in_turn)
+        np.testing.assert_allclose(a[0], b[0], rtol=0, atol=tol)
+        assert a[3] == b[3]
