@@ -74,6 +74,12 @@ def parse():
                     help="surrogate_da: plain Metropolis steps after the adaptive burn-in, "
                          "with its final proposal kept (no further adaptation), before the "
                          "local draws")
+    ap.add_argument("--stm-inner", type=int, nargs="*", default=[20, 50],
+                    help="surrogate_da: inner steps per exact decision of each surrogate-"
+                         "transition run (none: skip them)")
+    ap.add_argument("--stm-steps", type=int, default=0,
+                    help="surrogate_da: exact decisions per chain of a surrogate-transition "
+                         "run (0: a tenth of --mcmc-steps)")
     ap.add_argument("--ncoef", type=int, default=64)
     ap.add_argument("--local-curves", type=int, default=262144)
     ap.add_argument("--refine-epochs", type=int, default=600)
@@ -787,9 +793,10 @@ def run_surrogate(args):
     from lcurve_re_b200 import surrogate as S
     from lcurve_re_b200 import workloads as W
     from lcurve_re_b200.engine import Engine
-    from lcurve_re_b200.sampler import (CompactExact, ExactChi2, TriangularWalk,
-                                        delayed_acceptance, mean_shift, metropolis,
-                                        shift_verdict, summary)
+    from lcurve_re_b200.sampler import (CompactExact, DeviceTransitions, ExactChi2,
+                                        TriangularWalk, delayed_acceptance, mean_shift,
+                                        metropolis, shift_verdict, summary,
+                                        surrogate_transitions)
 
     eng = Engine(device=local, precision="mixed")
     clocks = Clocks(local)
@@ -949,6 +956,24 @@ def run_surrogate(args):
                                                       args.mcmc_steps, seed=21, compact=comp2,
                                                       propose=walk_da)
     launches_da = int(lib.lcg_kernel_launches(1)) + getattr(sur_loc_chi, "graph_launches", 0)
+    # surrogate transitions: per exact decision, a run of inner Metropolis
+    # steps on the refined network's own posterior, on the device (one CUDA
+    # graph per run), with the plain step scale; the chains in two halves,
+    # one half's exact evaluations overlapping the other's inner steps
+    stm_runs = []
+    stm_steps = args.stm_steps or max(1, args.mcmc_steps // 10)
+    half = args.chains // 2
+    for L in args.stm_inner:
+        pair = [DeviceTransitions(sur_loc_chi, tw, S.BOX, n, L, seed=41 + 2 * rank + k)
+                for k, n in enumerate((half, args.chains - half))]
+        ex_t = ExactChi2(eng, data)
+        lib.lcg_kernel_launches(1)
+        cht, _, _, acct, wall_t, stt = surrogate_transitions(ex_t, sur_loc_chi, theta0, None,
+                                                             stm_steps, L, seed=21,
+                                                             device=pair)
+        stm_runs.append((L, cht, acct, wall_t, stt, ex_t.evals,
+                         int(lib.lcg_kernel_launches(1)) + sum(d.launches for d in pair)))
+        del pair
     clk = clocks.stop()
     sum_p, sum_d, sum_g = summary(chp, wall_p), summary(chd, wall_d), summary(chg, wall_g)
     shift, mcse = mean_shift(chd, chp)
@@ -958,6 +983,20 @@ def run_surrogate(args):
     shift_is = {k: (np.abs(c.reshape(-1, 9).mean(0) - mu_is) / sd_p).max()
                 for k, c in (("plain", chp), ("delayed_acceptance", chd))}
     del chg
+    stm = []
+    for L, cht, acct, wall_t, stt, evals_t, launches_t in stm_runs:
+        sum_t = summary(cht, wall_t)
+        shift_t, mcse_t = mean_shift(cht, chp)
+        stm.append(dict(sum_t, inner_steps=L, steps=cht.shape[0],
+                        ms_per_step=wall_t / cht.shape[0] * 1e3, acceptance=acct,
+                        exact_evals=evals_t, gpu_launches=launches_t,
+                        ess_per_s_ratio=sum_t["ess_bulk_per_s"] / sum_p["ess_bulk_per_s"],
+                        ess_per_s_ratio_geyer=sum_t["ess_geyer_per_s"] /
+                        sum_p["ess_geyer_per_s"],
+                        posterior_mean_shift_sigma_max=float(shift_t.max()),
+                        mcse_max=float(mcse_t.max()),
+                        verdict_0_1_sigma=shift_verdict(shift_t, mcse_t), **stt))
+    del stm_runs
     peak, peak_src = _bf16_peak()
     train_tflops = train_flop / sur.train_s / 1e12
     value = sum_d["ess_bulk_per_s"]
@@ -1044,6 +1083,7 @@ def run_surrogate(args):
         "da_scale_pilots": [{"scale": k, "acceptance": a, "sq_jump_per_s": e}
                             for k, a, e in da_pilots],
         "da_proposal_scale": da_scale,
+        "surrogate_transitions": stm,
         "clocks": clk,
     }
     if eng_c is not None:

@@ -467,6 +467,32 @@ lcg_status lcg_mlp_pca_chisq(void *stream, const float *coef, int32_t m, int32_t
                              const float *coef_x, const double *anchor, double *chisq,
                              double *scale);
 
+/* The inner steps of the sampler's surrogate transitions (no counterpart
+ * in the reference, whose mcmc_solver runs plain Metropolis): a random walk
+ * through a triangular quadratic map that straightens a curved posterior,
+ * screened by the surrogate's chi**2, one thread per chain, every argument
+ * a device pointer. par holds the walk, 7d + 2d^2 + d^3 doubles for
+ * dimension d (d <= 16): m[d] s[d] (z = (y - m) / s), c0[d] B[d*d] (B[i*d+k]
+ * multiplies z_i in P_k, i < k), A[d*d*d] (A[(k*d+i)*d+j] multiplies z_i z_j
+ * in P_k, i <= j < k), chol[d*d] (row-major lower-triangular step factor),
+ * mid[d] half[d] (the network's input (y - mid) / half), lo[d] hi[d] (the
+ * box). With u = T(z), u_k = z_k - P_k(z_<k), the proposal of chain i is
+ * T^-1(T(y_i) + chol n_i), n_i standard normal: from noise [nc x d] when
+ * non-NULL, else Philox4x32-10 (subsequence i, offset from *ctr + step).
+ * lcg_walk_propose writes prop [nc x d], xunit [nc x d] (FP32) and ok [nc]
+ * (inside the box). lcg_walk_accept moves chain i to prop_i when
+ * ok_i and log(u_i) < -(chi_i - chis_i) / 2 (u_i from unif when non-NULL),
+ * updating y, chis and moves (may be NULL). lcg_walk_advance adds inc to
+ * *ctr (the step counter a captured graph of steps reads). */
+lcg_status lcg_walk_propose(void *stream, int32_t nc, int32_t d, const double *par,
+                            const double *y, uint64_t seed, const int64_t *ctr, int32_t step,
+                            const double *noise, double *prop, float *xunit, uint8_t *ok);
+lcg_status lcg_walk_accept(void *stream, int32_t nc, int32_t d, const double *prop,
+                           const uint8_t *ok, const double *chi, double *y, double *chis,
+                           int32_t *moves, uint64_t seed, const int64_t *ctr, int32_t step,
+                           const double *unif);
+lcg_status lcg_walk_advance(void *stream, int64_t *ctr, int64_t inc);
+
 #ifdef __cplusplus
 }
 #endif

@@ -142,6 +142,11 @@ PROTOTYPES = {
     "lcg_light_curve_resident": (C.c_int, [P, C.POINTER(LcgModel), C.c_int32, D, D, D]),
     "lcg_device_calc": (P, [P]),
     "lcg_kernel_launches": (C.c_int64, [C.c_int32]),
+    "lcg_walk_propose": (C.c_int, [P, C.c_int32, C.c_int32, P, P, C.c_uint64, P, C.c_int32,
+                                   P, P, P, P]),
+    "lcg_walk_accept": (C.c_int, [P, C.c_int32, C.c_int32, P, P, P, P, P, P, C.c_uint64, P,
+                                  C.c_int32, P]),
+    "lcg_walk_advance": (C.c_int, [P, P, C.c_int64]),
     "lcg_sum_star_multi_noalloc": (C.c_int, [P, C.c_int32, C.c_int64, C.c_int64, P, P, P, P, P,
                                              P, C.c_int32, P, P, P, P, D, C.c_int32, C.c_double,
                                              P]),

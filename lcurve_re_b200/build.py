@@ -34,6 +34,7 @@ SOURCES = {
     "mlp.cu": ["--fmad=true"],
     "mlp_chain.cu": ["--fmad=true"],
     "components.cu": ["--fmad=false"],
+    "walk.cu": ["--fmad=false"],
 }
 HEADERS = ["roche.cuh", "eclipse.cuh", "disc.cuh", "ecl_screen.cuh", "engine.h", "tma.cuh",
            "context.h", "fixed_phase.cuh", "mlp_tc.cuh"]

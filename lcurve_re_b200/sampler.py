@@ -21,8 +21,15 @@ curve at the current state and, for g(y, x), at the proposal (ExactChi2.curves_o
 fetches just the rows it needs from the engine). Chains whose proposal the
 approximation rejects pass the engine the model it evaluated for them last,
 so the batched engine skips them entirely.
+
+Surrogate transitions (surrogate_transitions): per exact decision, a run of
+inner Metropolis steps on the surrogate's own posterior, then one exact
+test of the run's end point with the ratio of the two posteriors' weights;
+the inner steps run on the GPU as a CUDA graph (DeviceTransitions: the walk
+and decision kernels of walk.cu around the network and its chi**2 head).
 """
 import copy
+import ctypes as C
 import time
 from concurrent.futures import ThreadPoolExecutor
 
@@ -756,3 +763,205 @@ def delayed_acceptance(exact, sur, theta0, cov, steps, seed=0, box_check=in_box,
     n = steps * nc
     return chain, theta, chi, acc / n, wall, {"stage1_rate": stage1 / n,
                                               "stage2_rate": acc / max(stage1, 1)}
+
+
+def walk_parameters(walk, box):
+    """The device layout of a walk (lcg_walk_propose's par): m, s, c0, B, A,
+    chol, mid, half, lo, hi for a TriangularWalk, or the same with the
+    identity map (m 0, s 1, no polynomial) for a GaussianWalk. box: [d x 2]
+    bounds; mid and half are the network's unit coordinates as
+    surrogate.to_unit forms them."""
+    box = np.asarray(box, np.float64)
+    lo, hi = box[:, 0], box[:, 1]
+    d = box.shape[0]
+    m, s, c0 = np.zeros(d), np.ones(d), np.zeros(d)
+    B, A = np.zeros((d, d)), np.zeros((d, d, d))
+    if isinstance(walk, TriangularWalk):
+        m, s, c0, B = walk.m, walk.s, walk.c0, walk.B
+        for k in range(1, d):
+            A[k, :k, :k] = walk.A[k]
+    elif not isinstance(walk, GaussianWalk):
+        raise TypeError("the device walk takes a GaussianWalk or a TriangularWalk")
+    parts = (m, s, c0, B, A, walk.chol, (lo + hi) / 2, (hi - lo) / 2, lo, hi)
+    return np.ascontiguousarray(np.concatenate([np.ravel(p) for p in parts]), np.float64)
+
+
+class DeviceTransitions:
+    """The inner steps of surrogate_transitions on the GPU, for every chain
+    at once: inner x (lcg_walk_propose, the network's forward pass, the
+    chi**2 head, lcg_walk_accept), captured once as a CUDA graph and
+    replayed per outer step. The chains' states and surrogate chi**2 go to
+    the device and come back once per outer step. The random numbers come
+    from Philox on the device; with host_draws the caller's generator fills
+    them instead, in the order of the host loop (tests)."""
+
+    def __init__(self, sur_chi, walk, box, nc, inner, seed=0, host_draws=False):
+        torch = sur_chi.torch
+        self.torch, self.sur_chi, self.lib = torch, sur_chi, sur_chi.lib
+        dev = sur_chi.sur.dev
+        d = np.asarray(box).shape[0]
+        self.nc, self.d, self.inner, self.seed = nc, d, inner, int(seed) & (2 ** 63 - 1)
+        self.par = torch.as_tensor(walk_parameters(walk, box), device=dev)
+        f64 = dict(dtype=torch.float64, device=dev)
+        mid = np.asarray(box, np.float64).mean(axis=1)
+        self.y = torch.as_tensor(np.tile(mid, (nc, 1)), **f64)  # until the first run
+        self.prop = torch.zeros((nc, d), **f64)
+        self.chis, self.chi = torch.zeros(nc, **f64), torch.zeros(nc, **f64)
+        self.xu = torch.zeros((nc, d), dtype=torch.float32, device=dev)
+        self.ok = torch.zeros(nc, dtype=torch.uint8, device=dev)
+        self.moves = torch.zeros(nc, dtype=torch.int32, device=dev)
+        self.ctr = torch.zeros(1, dtype=torch.int64, device=dev)
+        self.h_y = torch.zeros((nc, d), dtype=torch.float64, pin_memory=True)
+        self.h_c = torch.zeros(nc, dtype=torch.float64, pin_memory=True)
+        self.host_draws = host_draws
+        if host_draws:
+            self.noise = torch.zeros((inner, nc, d), **f64)
+            self.unif = torch.zeros((inner, nc), **f64)
+        self.graph = sur_chi._capture(self._steps)
+        # this library's kernels per replay: propose, network, chi**2 and
+        # accept per inner step, and the counter
+        self.launches_per_run = 4 * inner + 1
+        self.launches = 0
+
+    def _ok(self, st, what):
+        if st != 0:
+            raise RuntimeError("%s failed (status %d)" % (what, st))
+
+    def _steps(self):
+        torch, lib = self.torch, self.lib
+        p = lambda t: C.c_void_p(t.data_ptr())
+        stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        net = self.sur_chi.sur.net
+        for l in range(self.inner):
+            noise = p(self.noise[l]) if self.host_draws else None
+            unif = p(self.unif[l]) if self.host_draws else None
+            self._ok(lib.lcg_walk_propose(stream, self.nc, self.d, p(self.par), p(self.y),
+                                          self.seed, p(self.ctr), l, noise, p(self.prop),
+                                          p(self.xu), p(self.ok)), "lcg_walk_propose")
+            coef = net.forward(self.xu)
+            self.sur_chi._pca(coef, None, None, self.chi)
+            self._ok(lib.lcg_walk_accept(stream, self.nc, self.d, p(self.prop), p(self.ok),
+                                         p(self.chi), p(self.y), p(self.chis), p(self.moves),
+                                         self.seed, p(self.ctr), l, unif), "lcg_walk_accept")
+        self._ok(lib.lcg_walk_advance(stream, p(self.ctr), self.inner), "lcg_walk_advance")
+
+    def run(self, theta, chis, rng=None):
+        """inner steps from the states theta (surrogate chi**2 chis): the end
+        states, their surrogate chi**2 and the number of inner moves."""
+        self.h_y.numpy()[:] = theta
+        self.h_c.numpy()[:] = chis
+        self.y.copy_(self.h_y, non_blocking=True)
+        self.chis.copy_(self.h_c, non_blocking=True)
+        self.moves.zero_()
+        if self.host_draws:
+            for l in range(self.inner):
+                self.noise[l].copy_(self.torch.as_tensor(rng.standard_normal((self.nc, self.d))))
+                self.unif[l].copy_(self.torch.as_tensor(rng.random(self.nc)))
+        self.graph.replay()
+        self.launches += self.launches_per_run
+        return self.y.cpu().numpy(), self.chis.cpu().numpy(), int(self.moves.sum())
+
+
+def surrogate_transitions(exact, sur, theta0, cov, steps, inner, seed=0, box_check=in_box,
+                          record=True, propose=None, device=None):
+    """Delayed acceptance with surrogate transitions (Liu's surrogate
+    transition method, Monte Carlo Strategies in Scientific Computing, 2001,
+    sec. 9.4.3): each step runs `inner` Metropolis steps of the random walk
+    on the surrogate's posterior exp(-chi_s / 2) from the chain's state x to
+    y, then the exact model judges y once, accepting it with probability
+    min(1, w(y) / w(x)), w = exp(-(chi - chi_s) / 2). The inner chain is
+    reversible for the surrogate's posterior, so the two stages together
+    are reversible for the exact one whatever the surrogate's error; a
+    rejected run leaves the chain at x. sur: a chi**2 callable, a fixed
+    function of the parameters (the anchored approximation of
+    delayed_acceptance moves with x and does not serve).
+
+    device: None (the inner steps on the host, with propose), a runner of
+    the inner steps for every chain (DeviceTransitions: its own walk and
+    inner count), or a pair of runners for the two halves of the chains:
+    then a worker thread evaluates one half's run ends on the exact model
+    while the GPU runs the other half's inner steps, so the two overlap.
+    Chains whose run ended where it started pass the engine the model it
+    evaluated for them last, so the batched engine skips them.
+
+    Returns (chain [steps x chains x params] or None, final theta, final
+    chi**2, acceptance rate of the runs, wall seconds, stats)."""
+    rng = np.random.default_rng(seed)
+    if device is None:
+        propose = propose or GaussianWalk(cov)
+    theta = np.array(theta0, np.float64)
+    nc = theta.shape[0]
+    pair = isinstance(device, (list, tuple))
+    parts = [slice(0, nc // 2), slice(nc // 2, nc)] if pair else [slice(0, nc)]
+    runners = list(device) if pair else [device]
+    chi = np.empty(nc)
+    for part in parts:  # the halves as the loop's calls will pass them
+        chi[part] = exact(theta[part])
+    chis = np.asarray(sur(theta), np.float64).copy()
+    last = theta.copy()
+    chain = np.empty((steps,) + theta.shape) if record else None
+    count = {"acc": 0, "moved": 0, "inner": 0}
+    inner_n = runners[0].inner if device is not None else inner
+
+    def run(k):
+        """inner steps of part k: end states, their surrogate chi**2."""
+        part, dev = parts[k], runners[k]
+        if dev is not None:
+            y, chy, mv = dev.run(theta[part], chis[part], rng)
+        else:
+            y, chy, mv = theta[part].copy(), chis[part].copy(), 0
+            n = y.shape[0]
+            for _ in range(inner):
+                prop = propose(rng, y)
+                ok = box_check(prop)
+                c = np.asarray(sur(prop), np.float64).copy()
+                with np.errstate(invalid="ignore"):
+                    a = ok & (np.log(rng.random(n)) < -(c - chy) / 2)
+                y[a] = prop[a]
+                chy[a] = c[a]
+                mv += int(a.sum())
+        count["inner"] += mv
+        moved = np.any(y != theta[part], axis=1)
+        ev = np.where(moved[:, None], y, last[part])
+        last[part] = ev
+        return y, chy, moved, ev
+
+    def judge(k, y, chy, moved, chi_y):
+        """the exact decision on part k's run ends."""
+        part = parts[k]
+        with np.errstate(invalid="ignore"):
+            log_r = -(chi_y - chi[part]) / 2 + (chy - chis[part]) / 2
+            a = moved & (np.log(rng.random(len(moved))) < log_r)
+        th, c, cs = theta[part], chi[part], chis[part]
+        th[a], c[a], cs[a] = y[a], chi_y[a], chy[a]
+        theta[part], chi[part], chis[part] = th, c, cs
+        count["acc"] += int(a.sum())
+        count["moved"] += int(moved.sum())
+
+    t0 = time.perf_counter()
+    if not pair:
+        for s in range(steps):
+            y, chy, moved, ev = run(0)
+            judge(0, y, chy, moved, exact(ev))
+            if record:
+                chain[s] = theta
+    else:
+        pool = ThreadPoolExecutor(max_workers=1)
+        ra = run(0)
+        for s in range(steps):
+            job = pool.submit(exact, ra[3])
+            rb = run(1)  # overlaps half 0's exact evaluation
+            judge(0, *ra[:3], job.result())
+            job = pool.submit(exact, rb[3])
+            if s + 1 < steps:
+                ra = run(0)  # overlaps half 1's exact evaluation
+            judge(1, *rb[:3], job.result())
+            if record:
+                chain[s] = theta
+        pool.shutdown()
+    wall = time.perf_counter() - t0
+    n = steps * nc
+    return chain, theta, chi, count["acc"] / n, wall, {
+        "inner_steps": inner_n, "inner_acceptance": count["inner"] / (n * inner_n),
+        "runs_moved": count["moved"] / n,
+        "exact_acceptance": count["acc"] / max(count["moved"], 1)}

@@ -335,3 +335,80 @@ def test_forming_proposals_ahead_keeps_the_chains():
                        propose=in_turn)
         np.testing.assert_allclose(a[0], b[0], rtol=0, atol=tol)
         assert a[3] == b[3]
+
+
+def test_surrogate_transitions_keep_the_exact_posterior():
+    """Surrogate transitions (inner Metropolis runs on the surrogate's
+    posterior, one exact decision per run): with a shifted, too-wide
+    surrogate the chains still hold the exact banana's first and second
+    moments (within 4 Monte Carlo errors); with the exact chi**2 as its own
+    surrogate every run that moved is accepted."""
+    from lcurve_re_b200.sampler import TriangularWalk, surrogate_transitions
+    chains, steps, inner = 128, 400, 10
+    sample = _banana_draws(20000, 12)
+    theta0 = _banana_draws(chains, 13)
+    tw = TriangularWalk(sample)
+    sur = lambda t: _banana_chi(t - 0.05) * 0.8
+    n_exact = [0]
+
+    def exact(t):
+        n_exact[0] += 1
+        return _banana_chi(t)
+    c, _, _, acc, _, st = surrogate_transitions(exact, sur, theta0, None, steps, inner, seed=14,
+                                                box_check=_everywhere, propose=tw)
+    assert n_exact[0] == steps + 1
+    assert 0.05 < st["exact_acceptance"] < 1.0 and 0.1 < st["inner_acceptance"] < 0.5, st
+    s = c.reshape(-1, 3)
+    ess = ess_bulk(c)
+    for stat, truth in ((s, np.array([0.0, 0.8, 0.0])),
+                        (s ** 2, np.array([1.0, 0.64 * 3 + 0.05 ** 2, 0.09]))):
+        mcse = stat.std(0) / np.sqrt(ess)
+        assert np.all(np.abs(stat.mean(0) - truth) < 4 * mcse), (stat.mean(0), truth, mcse)
+    _, _, _, _, _, st1 = surrogate_transitions(_banana_chi, _banana_chi, theta0, None, 20, inner,
+                                               seed=15, box_check=_everywhere, propose=tw)
+    assert st1["exact_acceptance"] == 1.0 and st1["runs_moved"] > 0.5, st1
+
+
+class _HostRunner:
+    """The inner steps of surrogate_transitions for some chains, on the host
+    (what DeviceTransitions does on the GPU)."""
+
+    def __init__(self, walk, sur, inner):
+        self.walk, self.sur, self.inner = walk, sur, inner
+
+    def run(self, theta, chis, rng):
+        y, chy, mv = np.array(theta), np.array(chis), 0
+        for _ in range(self.inner):
+            prop = self.walk.apply_rows(y, self.walk.delta(rng, y.shape))
+            c = self.sur(prop)
+            a = np.log(rng.random(len(y))) < -(c - chy) / 2
+            y[a], chy[a] = prop[a], c[a]
+            mv += int(a.sum())
+        return y, chy, mv
+
+
+def test_surrogate_transitions_in_two_overlapped_halves_keep_the_posterior():
+    """With a pair of runners, one half's exact evaluations overlap the
+    other half's inner steps; the chains keep the exact banana's moments and
+    every exact call is for one half."""
+    from lcurve_re_b200.sampler import TriangularWalk, surrogate_transitions
+    chains, steps, inner = 128, 400, 10
+    tw = TriangularWalk(_banana_draws(20000, 21))
+    theta0 = _banana_draws(chains, 22)
+    sur = lambda t: _banana_chi(t - 0.05) * 0.8
+    sizes = []
+
+    def exact(t):
+        sizes.append(len(t))
+        return _banana_chi(t)
+    pair = [_HostRunner(tw, sur, inner), _HostRunner(tw.with_scale(1.0), sur, inner)]
+    c, _, _, acc, _, st = surrogate_transitions(exact, sur, theta0, None, steps, inner, seed=23,
+                                                box_check=_everywhere, device=pair)
+    assert sizes == [chains // 2] * (2 * steps + 2)
+    assert 0.05 < st["exact_acceptance"] < 1.0, st
+    s = c.reshape(-1, 3)
+    ess = ess_bulk(c)
+    for stat, truth in ((s, np.array([0.0, 0.8, 0.0])),
+                        (s ** 2, np.array([1.0, 0.64 * 3 + 0.05 ** 2, 0.09]))):
+        mcse = stat.std(0) / np.sqrt(ess)
+        assert np.all(np.abs(stat.mean(0) - truth) < 4 * mcse), (stat.mean(0), truth, mcse)
