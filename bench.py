@@ -987,7 +987,7 @@ def run_surrogate(args):
     for L, cht, acct, wall_t, stt, evals_t, launches_t in stm_runs:
         sum_t = summary(cht, wall_t)
         shift_t, mcse_t = mean_shift(cht, chp)
-        stm.append(dict(sum_t, inner_steps=L, steps=cht.shape[0],
+        stm.append(dict(sum_t, steps=cht.shape[0],
                         ms_per_step=wall_t / cht.shape[0] * 1e3, acceptance=acct,
                         exact_evals=evals_t, gpu_launches=launches_t,
                         ess_per_s_ratio=sum_t["ess_bulk_per_s"] / sum_p["ess_bulk_per_s"],
