@@ -77,6 +77,11 @@ def parse():
     ap.add_argument("--stm-inner", type=int, nargs="*", default=[20, 50],
                     help="surrogate_da: inner steps per exact decision of each surrogate-"
                          "transition run (none: skip them)")
+    ap.add_argument("--stm-layouts", nargs="*", choices=("whole", "halves"),
+                    default=["whole", "halves"],
+                    help="surrogate_da: surrogate-transition runs over all chains at once, "
+                         "or in two halves whose exact evaluations overlap the other half's "
+                         "inner steps")
     ap.add_argument("--stm-steps", type=int, default=0,
                     help="surrogate_da: exact decisions per chain of a surrogate-transition "
                          "run (0: a tenth of --mcmc-steps)")
@@ -958,22 +963,26 @@ def run_surrogate(args):
     launches_da = int(lib.lcg_kernel_launches(1)) + getattr(sur_loc_chi, "graph_launches", 0)
     # surrogate transitions: per exact decision, a run of inner Metropolis
     # steps on the refined network's own posterior, on the device (one CUDA
-    # graph per run), with the plain step scale; the chains in two halves,
-    # one half's exact evaluations overlapping the other's inner steps
+    # graph per run), with the plain step scale; all chains at once, or in
+    # two halves, one half's exact evaluations overlapping the other's inner
+    # steps
     stm_runs = []
     stm_steps = args.stm_steps or max(1, args.mcmc_steps // 10)
     half = args.chains // 2
-    for L in args.stm_inner:
-        pair = [DeviceTransitions(sur_loc_chi, tw, S.BOX, n, L, seed=41 + 2 * rank + k)
-                for k, n in enumerate((half, args.chains - half))]
-        ex_t = ExactChi2(eng, data)
-        lib.lcg_kernel_launches(1)
-        cht, _, _, acct, wall_t, stt = surrogate_transitions(ex_t, sur_loc_chi, theta0, None,
-                                                             stm_steps, L, seed=21,
-                                                             device=pair)
-        stm_runs.append((L, cht, acct, wall_t, stt, ex_t.evals,
-                         int(lib.lcg_kernel_launches(1)) + sum(d.launches for d in pair)))
-        del pair
+    for layout in args.stm_layouts:
+        for L in args.stm_inner:
+            sizes = (args.chains,) if layout == "whole" else (half, args.chains - half)
+            runners = [DeviceTransitions(sur_loc_chi, tw, S.BOX, n, L, seed=41 + 2 * rank + k)
+                       for k, n in enumerate(sizes)]
+            ex_t = ExactChi2(eng, data)
+            lib.lcg_kernel_launches(1)
+            cht, _, _, acct, wall_t, stt = surrogate_transitions(
+                ex_t, sur_loc_chi, theta0, None, stm_steps, L, seed=21,
+                device=runners[0] if layout == "whole" else runners)
+            stt["layout"] = layout
+            stm_runs.append((L, cht, acct, wall_t, stt, ex_t.evals,
+                             int(lib.lcg_kernel_launches(1)) + sum(d.launches for d in runners)))
+            del runners
     clk = clocks.stop()
     sum_p, sum_d, sum_g = summary(chp, wall_p), summary(chd, wall_d), summary(chg, wall_g)
     shift, mcse = mean_shift(chd, chp)
