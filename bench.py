@@ -78,7 +78,7 @@ def parse():
                     help="surrogate_da: inner steps per exact decision of each surrogate-"
                          "transition run (none: skip them)")
     ap.add_argument("--stm-layouts", nargs="*", choices=("whole", "halves"),
-                    default=["whole", "halves"],
+                    default=["whole"],
                     help="surrogate_da: surrogate-transition runs over all chains at once, "
                          "or in two halves whose exact evaluations overlap the other half's "
                          "inner steps")
@@ -966,23 +966,28 @@ def run_surrogate(args):
     # graph per run), with the plain step scale; all chains at once, or in
     # two halves, one half's exact evaluations overlapping the other's inner
     # steps
-    stm_runs = []
+    stm_runs, stm_error = [], None
     stm_steps = args.stm_steps or max(1, args.mcmc_steps // 10)
     half = args.chains // 2
-    for layout in args.stm_layouts:
-        for L in args.stm_inner:
-            sizes = (args.chains,) if layout == "whole" else (half, args.chains - half)
-            runners = [DeviceTransitions(sur_loc_chi, tw, S.BOX, n, L, seed=41 + 2 * rank + k)
-                       for k, n in enumerate(sizes)]
-            ex_t = ExactChi2(eng, data)
-            lib.lcg_kernel_launches(1)
-            cht, _, _, acct, wall_t, stt = surrogate_transitions(
-                ex_t, sur_loc_chi, theta0, None, stm_steps, L, seed=21,
-                device=runners[0] if layout == "whole" else runners)
-            stt["layout"] = layout
-            stm_runs.append((L, cht, acct, wall_t, stt, ex_t.evals,
-                             int(lib.lcg_kernel_launches(1)) + sum(d.launches for d in runners)))
-            del runners
+    try:
+        for layout in args.stm_layouts:
+            for L in args.stm_inner:
+                sizes = (args.chains,) if layout == "whole" else (half, args.chains - half)
+                runners = [DeviceTransitions(sur_loc_chi, tw, S.BOX, n, L,
+                                             seed=41 + 2 * rank + k)
+                           for k, n in enumerate(sizes)]
+                ex_t = ExactChi2(eng, data)
+                lib.lcg_kernel_launches(1)
+                cht, _, _, acct, wall_t, stt = surrogate_transitions(
+                    ex_t, sur_loc_chi, theta0, None, stm_steps, L, seed=21,
+                    device=runners[0] if layout == "whole" else runners)
+                stt["layout"] = layout
+                stm_runs.append((L, cht, acct, wall_t, stt, ex_t.evals,
+                                 int(lib.lcg_kernel_launches(1)) +
+                                 sum(d.launches for d in runners)))
+                del runners
+    except Exception as exc:  # a comparison beside the metric: the line keeps the rest
+        stm_error = "%s: %s" % (type(exc).__name__, exc)
     clk = clocks.stop()
     sum_p, sum_d, sum_g = summary(chp, wall_p), summary(chd, wall_d), summary(chg, wall_g)
     shift, mcse = mean_shift(chd, chp)
@@ -1092,7 +1097,8 @@ def run_surrogate(args):
         "da_scale_pilots": [{"scale": k, "acceptance": a, "sq_jump_per_s": e}
                             for k, a, e in da_pilots],
         "da_proposal_scale": da_scale,
-        "surrogate_transitions": stm,
+        "surrogate_transitions": stm if stm_error is None else {"runs": stm,
+                                                                 "error": stm_error},
         "clocks": clk,
     }
     if eng_c is not None:
