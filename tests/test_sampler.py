@@ -412,3 +412,45 @@ def test_surrogate_transitions_in_two_overlapped_halves_keep_the_posterior():
                         (s ** 2, np.array([1.0, 0.64 * 3 + 0.05 ** 2, 0.09]))):
         mcse = stat.std(0) / np.sqrt(ess)
         assert np.all(np.abs(stat.mean(0) - truth) < 4 * mcse), (stat.mean(0), truth, mcse)
+
+
+def _walk_from_par(par, d, y, n):
+    """The proposal of lcg_walk_propose (walk.cu), restated in numpy from the
+    packed layout: m, s, c0, B, A, chol, mid, half, lo, hi."""
+    sizes = [d, d, d, d * d, d * d * d, d * d, d, d, d, d]
+    parts, o = [], 0
+    for k in sizes:
+        parts.append(par[o:o + k])
+        o += k
+    assert o == len(par) == 7 * d + 2 * d * d + d ** 3
+    m, s, c0, B, A, chol, mid, half, lo, hi = parts
+    B, A, chol = B.reshape(d, d), A.reshape(d, d, d), chol.reshape(d, d)
+
+    def poly(k, z):
+        return c0[k] + sum(z[i] * (B[i, k] + sum(A[k, i, j] * z[j] for j in range(i, k)))
+                           for i in range(k))
+    out = np.empty_like(y)
+    for r in range(len(y)):
+        z = (y[r] - m) / s
+        v = np.array([z[k] - poly(k, z) + chol[k, :k + 1] @ n[r, :k + 1] for k in range(d)])
+        for k in range(d):
+            v[k] = v[k] + poly(k, v)
+        out[r] = m + v * s
+    return out, (out - mid) / half, np.all((out >= lo) & (out <= hi), axis=1)
+
+
+def test_walk_parameters_pack_the_maps_for_the_device_walk():
+    """walk_parameters packs a TriangularWalk (and a GaussianWalk as the
+    identity map) in lcg_walk_propose's layout: the kernel's arithmetic,
+    restated from that layout, gives the walks' own proposals."""
+    from lcurve_re_b200.sampler import GaussianWalk, TriangularWalk, walk_parameters
+    box = np.array([[-3.0, 3.0], [-1.0, 9.0], [-2.0, 2.0]])
+    tw = TriangularWalk(_banana_draws(5000, 31), scale=0.7)
+    gw = GaussianWalk(np.diag([0.1, 0.2, 0.05]))
+    y = _banana_draws(40, 32)
+    n = np.random.default_rng(33).standard_normal((40, 3))
+    for walk, ref in ((tw, tw.apply_rows(y, n @ tw.chol.T)), (gw, y + n @ gw.chol.T)):
+        got, unit, ok = _walk_from_par(walk_parameters(walk, box), 3, y, n)
+        np.testing.assert_allclose(got, ref, rtol=0, atol=1e-12)
+        np.testing.assert_allclose(unit, (got - box.mean(1)) / ((box[:, 1] - box[:, 0]) / 2))
+        assert np.array_equal(ok, np.all((got >= box[:, 0]) & (got <= box[:, 1]), axis=1))
