@@ -177,11 +177,13 @@ def summary(chain, wall):
         bulk.append(_ess_chains(z))
         rh.append(_rhat_split(s, z))
     geyer, _ = ess_total(chain)
+    per = [round(float(b)) for b in bulk]
     bulk = float(np.min(bulk))
     return {"ess_bulk": bulk, "ess_bulk_per_s": bulk / wall, "ess_geyer": geyer,
             "ess_geyer_per_s": geyer / wall,
             "ess_between_chains": ess_between_chains(chain)[0], "rhat_max": float(np.max(rh)),
-            "wall_s": wall}
+            "wall_s": wall, "ess_bulk_per_parameter": per,
+            "rhat_per_parameter": [round(float(r), 4) for r in rh]}
 
 
 def mean_shift(chain_a, chain_b):
