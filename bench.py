@@ -947,7 +947,10 @@ def run_surrogate(args):
                                                          compact=comp_p, propose=walk)
         u = tw.forward(cpl.reshape(-1, 9)).reshape(cpl.shape) @ np.linalg.inv(tw.chol.T)
         esjd = float(np.mean(np.sum(np.diff(u, axis=0) ** 2, axis=2)))
-        da_pilots.append((k, acc_k, esjd / wall_k))
+        # the slowest parameter's squared jump over its variance (1 - its lag-1
+        # autocorrelation, x2): reported beside the choice
+        per = np.mean(np.diff(cpl, axis=0) ** 2, axis=(0, 1)) / cpl.reshape(-1, 9).var(0)
+        da_pilots.append((k, acc_k, esjd / wall_k, float(per.min()) / wall_k))
     ok = [t for t in da_pilots if t[1] >= args.da_min_accept] or da_pilots[:1]
     da_scale = max(ok, key=lambda t: t[2])[0]
     walk_da = tw.with_scale(tw.scale * da_scale)
@@ -1094,8 +1097,9 @@ def run_surrogate(args):
                     % (args.adapt_rounds, args.burn_tuned),
         "proposal_tuning": {"scale_acceptance": tuning, "chosen": f_best,
                             "burn_in_steps": args.adapt_rounds * args.burn_tuned},
-        "da_scale_pilots": [{"scale": k, "acceptance": a, "sq_jump_per_s": e}
-                            for k, a, e in da_pilots],
+        "da_scale_pilots": [{"scale": k, "acceptance": a, "sq_jump_per_s": e,
+                             "min_param_jump_per_s": mp}
+                            for k, a, e, mp in da_pilots],
         "da_proposal_scale": da_scale,
         "surrogate_transitions": stm if stm_error is None else {"runs": stm,
                                                                  "error": stm_error},
