@@ -928,7 +928,7 @@ def surrogate_transitions(exact, sur, theta0, cov, steps, inner, seed=0, box_che
         last[part] = ev
         return y, chy, moved, ev
 
-    def judge(k, y, chy, moved, chi_y):
+    def decide(k, y, chy, moved, chi_y):
         """the exact decision on part k's run ends."""
         part = parts[k]
         with np.errstate(invalid="ignore"):
@@ -944,7 +944,7 @@ def surrogate_transitions(exact, sur, theta0, cov, steps, inner, seed=0, box_che
     if not pair:
         for s in range(steps):
             y, chy, moved, ev = run(0)
-            judge(0, y, chy, moved, exact(ev))
+            decide(0, y, chy, moved, exact(ev))
             if record:
                 chain[s] = theta
     else:
@@ -953,11 +953,11 @@ def surrogate_transitions(exact, sur, theta0, cov, steps, inner, seed=0, box_che
         for s in range(steps):
             job = pool.submit(exact, ra[3])
             rb = run(1)  # overlaps half 0's exact evaluation
-            judge(0, *ra[:3], job.result())
+            decide(0, *ra[:3], job.result())
             job = pool.submit(exact, rb[3])
             if s + 1 < steps:
                 ra = run(0)  # overlaps half 1's exact evaluation
-            judge(1, *rb[:3], job.result())
+            decide(1, *rb[:3], job.result())
             if record:
                 chain[s] = theta
         pool.shutdown()
