@@ -77,3 +77,27 @@ def test_struct_layouts_match_header():
         for f in cls._fields_:
             assert lay[(name, f[0])] == getattr(cls, f[0]).offset, (name, f[0])
     assert abi.datum_dtype().itemsize == C.sizeof(abi.LcgDatum) == 48
+
+
+def test_walk_entry_points_reject_bad_arguments_before_any_launch(lib):
+    """lcg_walk_propose / lcg_walk_accept / lcg_walk_advance check their
+    sizes and pointers on the host and return LCG_E_INVALID without touching
+    the device (the dummy addresses below are never dereferenced)."""
+    P = C.c_void_p(4096)  # non-NULL, never used: every call fails its checks first
+    N = None
+    propose = [  # (nc, d, par, y, ctr, step, noise, prop, xunit, ok)
+        (0, 9, P, P, P, 0, N, P, P, P), (8, 0, P, P, P, 0, N, P, P, P),
+        (8, 17, P, P, P, 0, N, P, P, P), (8, 9, N, P, P, 0, N, P, P, P),
+        (8, 9, P, P, N, 0, N, P, P, P), (8, 9, P, P, P, -1, N, P, P, P),
+        (8, 9, P, P, P, 0, N, P, N, P)]
+    for nc, d, par, y, ctr, step, noise, prop, xu, ok in propose:
+        assert lib.lcg_walk_propose(N, nc, d, par, y, 0, ctr, step, noise, prop, xu,
+                                    ok) == abi.E_INVALID
+    accept = [  # (nc, d, prop, ok, chi, y, chis, ctr, step, unif)
+        (0, 9, P, P, P, P, P, P, 0, N), (8, 17, P, P, P, P, P, P, 0, N),
+        (8, 9, P, P, N, P, P, P, 0, N), (8, 9, P, P, P, P, P, N, 0, N),
+        (8, 9, P, P, P, P, P, P, -2, N)]
+    for nc, d, prop, ok, chi, y, chis, ctr, step, unif in accept:
+        assert lib.lcg_walk_accept(N, nc, d, prop, ok, chi, y, chis, N, 0, ctr, step,
+                                   unif) == abi.E_INVALID
+    assert lib.lcg_walk_advance(N, N, 1) == abi.E_INVALID
