@@ -82,6 +82,11 @@ def parse():
                     help="surrogate_da: surrogate-transition runs over all chains at once, "
                          "or in two halves whose exact evaluations overlap the other half's "
                          "inner steps")
+    ap.add_argument("--stm-anchor", nargs="*", choices=("none", "start"),
+                    default=["none", "start"],
+                    help="surrogate_da: the surrogate-transition runs' approximation: the "
+                         "network's own chi**2, or anchored at each chain's exact curve at its "
+                         "starting state (fixed for the run)")
     ap.add_argument("--stm-steps", type=int, default=0,
                     help="surrogate_da: exact decisions per chain of a surrogate-transition "
                          "run (0: a tenth of --mcmc-steps)")
@@ -973,22 +978,36 @@ def run_surrogate(args):
     stm_steps = args.stm_steps or max(1, args.mcmc_steps // 10)
     half = args.chains // 2
     try:
-        for layout in args.stm_layouts:
-            for L in args.stm_inner:
-                sizes = (args.chains,) if layout == "whole" else (half, args.chains - half)
-                runners = [DeviceTransitions(sur_loc_chi, tw, S.BOX, n, L,
-                                             seed=41 + 2 * rank + k)
-                           for k, n in enumerate(sizes)]
-                ex_t = ExactChi2(eng, data)
-                lib.lcg_kernel_launches(1)
-                cht, _, _, acct, wall_t, stt = surrogate_transitions(
-                    ex_t, sur_loc_chi, theta0, None, stm_steps, L, seed=21,
-                    device=runners[0] if layout == "whole" else runners)
-                stt["layout"] = layout
-                stm_runs.append((L, cht, acct, wall_t, stt, ex_t.evals,
-                                 int(lib.lcg_kernel_launches(1)) +
-                                 sum(d.launches for d in runners)))
-                del runners
+        fixed = None
+        if "start" in args.stm_anchor:
+            # every chain's exact curve at its starting state, the anchor of
+            # its approximation for the whole run
+            ex_a = ExactChi2(eng, data, curves=True)
+            ex_a(theta0)
+            f0 = torch.empty((args.chains, eng._n), dtype=torch.float64, device="cuda")
+            ex_a.curves_all_device(f0)
+            fixed = sur_loc_chi.fixed_anchor(theta0, f0)
+        for mode in args.stm_anchor:
+            sur_t = fixed if mode == "start" else sur_loc_chi
+            for layout in args.stm_layouts:
+                parts = ([slice(0, args.chains)] if layout == "whole" else
+                         [slice(0, half), slice(half, args.chains)])
+                for L in args.stm_inner:
+                    runners = [DeviceTransitions(
+                        sur_loc_chi, tw, S.BOX, part.stop - part.start, L,
+                        seed=41 + 2 * rank + k,
+                        anchor=fixed.rows(part) if mode == "start" else None)
+                        for k, part in enumerate(parts)]
+                    ex_t = ExactChi2(eng, data)
+                    lib.lcg_kernel_launches(1)
+                    cht, _, _, acct, wall_t, stt = surrogate_transitions(
+                        ex_t, sur_t, theta0, None, stm_steps, L, seed=21,
+                        device=runners[0] if layout == "whole" else runners)
+                    stt["layout"], stt["anchor"] = layout, mode
+                    stm_runs.append((L, cht, acct, wall_t, stt, ex_t.evals,
+                                     int(lib.lcg_kernel_launches(1)) +
+                                     sum(d.launches for d in runners)))
+                    del runners
     except Exception as exc:  # a comparison beside the metric: the line keeps the rest
         stm_error = "%s: %s" % (type(exc).__name__, exc)
     clk = clocks.stop()

@@ -795,9 +795,12 @@ class DeviceTransitions:
     replayed per outer step. The chains' states and surrogate chi**2 go to
     the device and come back once per outer step. The random numbers come
     from Philox on the device; with host_draws the caller's generator fills
-    them instead, in the order of the host loop (tests)."""
+    them instead, in the order of the host loop (tests). anchor: None (the
+    network's own chi**2) or (coefficients [nc x ncoef] FP32, exact curves
+    [nc x points] FP64) of each chain's fixed anchor (FixedAnchorChi2.rows).
+    """
 
-    def __init__(self, sur_chi, walk, box, nc, inner, seed=0, host_draws=False):
+    def __init__(self, sur_chi, walk, box, nc, inner, seed=0, host_draws=False, anchor=None):
         torch = sur_chi.torch
         self.torch, self.sur_chi, self.lib = torch, sur_chi, sur_chi.lib
         dev = sur_chi.sur.dev
@@ -816,6 +819,14 @@ class DeviceTransitions:
         self.h_y = torch.zeros((nc, d), dtype=torch.float64, pin_memory=True)
         self.h_c = torch.zeros(nc, dtype=torch.float64, pin_memory=True)
         self.host_draws = host_draws
+        self.a_coef = self.a_f = None
+        if anchor is not None:
+            self.a_coef, self.a_f = (t.contiguous() for t in anchor)
+            if (self.a_coef.dtype != torch.float32 or self.a_f.dtype != torch.float64 or
+                    self.a_coef.shape[0] != nc or self.a_f.shape != (nc, sur_chi.npts) or
+                    self.a_coef.shape[1] != sur_chi.sur.net.nout):
+                raise ValueError("anchor: [nc x ncoef] FP32 coefficients and [nc x points] "
+                                 "FP64 curves")
         if host_draws:
             self.noise = torch.zeros((inner, nc, d), **f64)
             self.unif = torch.zeros((inner, nc), **f64)
@@ -841,7 +852,7 @@ class DeviceTransitions:
                                           self.seed, p(self.ctr), l, noise, p(self.prop),
                                           p(self.xu), p(self.ok)), "lcg_walk_propose")
             coef = net.forward(self.xu)
-            self.sur_chi._pca(coef, None, None, self.chi)
+            self.sur_chi._pca(coef, self.a_coef, self.a_f, self.chi)
             self._ok(lib.lcg_walk_accept(stream, self.nc, self.d, p(self.prop), p(self.ok),
                                          p(self.chi), p(self.y), p(self.chis), p(self.moves),
                                          self.seed, p(self.ctr), l, unif), "lcg_walk_accept")

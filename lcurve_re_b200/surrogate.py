@@ -402,6 +402,12 @@ class SurrogateChi2:
         self._pca(coef, coef_x.contiguous() if coef_x is not None else None, an, chi)
         return chi.cpu().numpy()
 
+    def fixed_anchor(self, theta_ref, curves_ref):
+        """The anchored approximation with every chain's anchor fixed:
+        FixedAnchorChi2 over the chains of theta_ref [chains x 9] with their
+        exact curves curves_ref [chains x points] (float64 device tensor)."""
+        return FixedAnchorChi2(self, theta_ref, curves_ref)
+
     # -- fixed-shape passes of the device delayed-acceptance loop -------------
     def bind(self, sx0, f0):
         """Static buffers for the chains of sx0 (their states) and f0 (their
@@ -463,3 +469,31 @@ class SurrogateChi2:
         m = torch.as_tensor(accepted, device=self.sur.dev)[:, None]
         self.g_sx.copy_(torch.where(m, self.g_sy, self.g_sx))
         self.g_f.copy_(torch.where(m, self.g_F, self.g_f))
+
+
+class FixedAnchorChi2:
+    """chi**2 of exact(r_i) * s(theta_i) / s(r_i) for chain i: the anchored
+    approximation of SurrogateChi2 with each chain's anchor r_i fixed before
+    sampling (its exact curve at r_i), so that it is one fixed function of the
+    parameters per chain, which surrogate transitions need; the network's
+    error then enters only through its change between r_i and theta_i. Called
+    with one row per chain, in the chains' order."""
+
+    def __init__(self, sur_chi, theta_ref, curves_ref):
+        torch = sur_chi.torch
+        self.sur_chi = sur_chi
+        self.coef_ref = sur_chi.state(theta_ref)  # [chains x ncoef] FP32
+        f = torch.as_tensor(curves_ref, dtype=torch.float64, device=sur_chi.sur.dev)
+        self.f_ref = f.contiguous()
+        if self.f_ref.shape != (self.coef_ref.shape[0], sur_chi.npts):
+            raise ValueError("one exact curve at the data points per chain expected")
+
+    def __call__(self, theta):
+        if len(theta) != self.coef_ref.shape[0]:
+            raise ValueError("one row per chain expected")
+        return self.sur_chi.chi2(self.sur_chi.state(theta), self.coef_ref, self.f_ref)
+
+    def rows(self, part):
+        """The anchors (coefficients, curves) of the chains in slice part."""
+        return self.coef_ref[part].contiguous(), self.f_ref[part].contiguous()
+

@@ -454,3 +454,27 @@ def test_walk_parameters_pack_the_maps_for_the_device_walk():
         np.testing.assert_allclose(got, ref, rtol=0, atol=1e-12)
         np.testing.assert_allclose(unit, (got - box.mean(1)) / ((box[:, 1] - box[:, 0]) / 2))
         assert np.array_equal(ok, np.all((got >= box[:, 0]) & (got <= box[:, 1]), axis=1))
+
+
+def test_surrogate_transitions_with_a_fixed_approximation_per_chain():
+    """Each chain may have its own approximation, fixed for the run (an
+    anchor at its starting state, as FixedAnchorChi2 gives): the chains
+    still hold the exact banana's moments."""
+    from lcurve_re_b200.sampler import TriangularWalk, surrogate_transitions
+    chains, steps, inner = 128, 400, 10
+    tw = TriangularWalk(_banana_draws(20000, 41))
+    theta0 = _banana_draws(chains, 42)
+    ref = theta0.copy()
+    tilt = np.random.default_rng(43).standard_normal((chains, 3))
+
+    def sur(t):  # exact at the anchor, wrong elsewhere by a chain-specific tilt
+        return _banana_chi(t) * 0.8 + 2.0 * np.sum(tilt * (t - ref), axis=1)
+    c, _, _, acc, _, st = surrogate_transitions(_banana_chi, sur, theta0, None, steps, inner,
+                                                seed=44, box_check=_everywhere, propose=tw)
+    assert 0.05 < st["exact_acceptance"] < 1.0, st
+    s = c.reshape(-1, 3)
+    ess = ess_bulk(c)
+    for stat, truth in ((s, np.array([0.0, 0.8, 0.0])),
+                        (s ** 2, np.array([1.0, 0.64 * 3 + 0.05 ** 2, 0.09]))):
+        mcse = stat.std(0) / np.sqrt(ess)
+        assert np.all(np.abs(stat.mean(0) - truth) < 4 * mcse), (stat.mean(0), truth, mcse)
