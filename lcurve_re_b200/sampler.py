@@ -899,6 +899,8 @@ def surrogate_transitions(exact, sur, theta0, cov, steps, inner, seed=0, box_che
 
     Returns (chain [steps x chains x params] or None, final theta, final
     chi**2, acceptance rate of the runs, wall seconds, stats)."""
+    if steps < 1 or (device is None and inner < 1):
+        raise ValueError("surrogate_transitions needs at least one step and one inner step")
     rng = np.random.default_rng(seed)
     if device is None:
         propose = propose or GaussianWalk(cov)

@@ -7,6 +7,7 @@ screened by a deliberately wrong surrogate (shifted and too wide), must
 still sample the exact posterior while calling the exact model less often.
 """
 import numpy as np
+import pytest
 
 from lcurve_re_b200.sampler import (delayed_acceptance, ess_bulk, ess_geyer, ess_mean,
                                     ess_total, mean_shift, metropolis, rhat, shift_verdict,
@@ -478,3 +479,30 @@ def test_surrogate_transitions_with_a_fixed_approximation_per_chain():
                         (s ** 2, np.array([1.0, 0.64 * 3 + 0.05 ** 2, 0.09]))):
         mcse = stat.std(0) / np.sqrt(ess)
         assert np.all(np.abs(stat.mean(0) - truth) < 4 * mcse), (stat.mean(0), truth, mcse)
+
+
+def test_surrogate_transitions_edge_cases():
+    """An odd number of chains splits into unequal halves; without a record
+    no chain is kept; the box rejects proposals outside it; zero steps are
+    refused."""
+    from lcurve_re_b200.sampler import TriangularWalk, surrogate_transitions
+    tw = TriangularWalk(_banana_draws(5000, 61))
+    theta0 = _banana_draws(7, 62)
+    sizes = []
+
+    def exact(t):
+        sizes.append(len(t))
+        return _banana_chi(t)
+    pair = [_HostRunner(tw, _banana_chi, 3), _HostRunner(tw, _banana_chi, 3)]
+    ch, th, chi, acc, _, st = surrogate_transitions(exact, _banana_chi, theta0, None, 5, 3,
+                                                    seed=63, box_check=_everywhere,
+                                                    device=pair, record=False)
+    assert ch is None and sizes == [3, 4] * 6 and st["exact_acceptance"] == 1.0
+    np.testing.assert_array_equal(chi, _banana_chi(th))
+    inside = lambda t: np.all(np.abs(t) < 0.5, axis=1)  # a box the walk leaves often
+    start = np.zeros((16, 3)) + [0.0, 0.1, 0.0]
+    c, *_ = surrogate_transitions(_banana_chi, _banana_chi, start, None, 50, 4, seed=64,
+                                  box_check=inside, propose=tw)
+    assert np.all(inside(c.reshape(-1, 3)))
+    with pytest.raises(ValueError):
+        surrogate_transitions(_banana_chi, _banana_chi, start, None, 0, 4, propose=tw)
